@@ -1,0 +1,305 @@
+"""Benchmark of the SAMoS hot path on B200: particle-steps/s of the FP64
+active-Brownian step at 4,194,304 particles.
+
+Workload (the single-GPU headline shape): 4,194,304 soft disks in a 2D
+periodic box at packing fraction 0.8, radii 1.0 / 1.4 (50:50), positions
+uniform from a seed, soft repulsion k=10 on particle radii, nematic aligner
+J=0.5, brownian v0=0.3 nu=0.1, dt=5e-4, neighbour list rcut 2.8 + pad 0.3.
+A step is one full integration step (forces, torques, integration, skin test,
+rebuilds when triggered) of that system.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs one independent replica per rank (weak scaling, no data-path
+collective; the path has no exchange step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s @4M ABPs; batched vs serial; FIRE s to Fmax<1e-10 ML vs plain"
+UNIT = "particle-steps/s"
+N_PART = 4_194_304
+PHI = 0.8
+RADII = (1.0, 1.4)
+BYTES_PER_PARTICLE_STEP = 88  # 2-D: read x,y,nx,ny,r (40 B) + write x,y,nx,ny,vx,vy (48 B)
+WORKLOAD = ("4,194,304 active soft disks, 2D periodic box, phi=0.8, radii 1.0/1.4 50:50, soft k=10 "
+            "(particle radii) + nematic J=0.5, brownian v0=0.3 nu=0.1 dt=5e-4, nlist rcut 2.8 pad 0.3, FP64")
+
+
+def make_particles(n, seed):
+    rng = np.random.default_rng(seed)
+    r = np.where(np.arange(n) % 2 == 0, RADII[0], RADII[1]).astype(np.float64)
+    rng.shuffle(r)
+    L = float(np.sqrt(np.sum(np.pi * r * r) / PHI))
+    th = rng.uniform(0.0, 2.0 * np.pi, n)
+    parts = dict(x=rng.uniform(-L / 2, L / 2, n), y=rng.uniform(-L / 2, L / 2, n), z=np.zeros(n),
+                 vx=np.zeros(n), vy=np.zeros(n), vz=np.zeros(n),
+                 nx=np.cos(th), ny=np.sin(th), nz=np.zeros(n), radius=r)
+    return parts, L
+
+
+def configure(sim, parts, L):
+    sim.box(L, L, 10.0, True)
+    sim.input(**parts)
+    sim.nlist(2.8, 0.3)
+    sim.constraint("plane", {})
+    sim.pair_potential("soft", {"k": "10", "use_particle_radii": ""})
+    sim.pair_align("nematic", {"J": "0.5"})
+    sim.timestep(5e-4)
+    sim.integrator("brownian", {"v0": "0.3", "nu": "0.1", "mu": "1", "mur": "1", "seed": "1"})
+    sim.commit()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if not self.path or not os.path.exists(self.path):
+            return out
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        if sm:
+            out.update(sm_mhz=float(np.median(sm)), sm_max_mhz=float(max(smax)), reasons=sorted(reasons),
+                       samples=len(sm))
+        return out
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle on a bounded sample of the same workload
+# ---------------------------------------------------------------------------
+def _cpu_sample(args):
+    n, warm, steps, seed = args
+    from oracle.oracle import OracleSystem
+    from samos_b200.plugins import Simulation
+    parts, L = make_particles(n, seed)
+    o = OracleSystem(n)
+    sim = Simulation(o)
+    configure(sim, parts, L)
+    sim.run(warm - 1)
+    t0 = time.perf_counter()
+    o.run(steps - 1)
+    dt = time.perf_counter() - t0
+    return n * steps / dt
+
+
+def cpu_baseline(n=131_072, warm=100, steps=60, procs=1):
+    import multiprocessing as mp
+    if procs == 1:
+        v = _cpu_sample((n, warm, steps, 11))
+    else:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(procs) as pool:
+            v = sum(pool.map(_cpu_sample, [(n, warm, steps, 11 + i) for i in range(procs)]))
+    return dict(value=v, unit=UNIT, cores=procs, kind="port",
+                sample=f"{n} particles of the same density/composition (box scaled), {warm} untimed + "
+                       f"{steps} timed steps per process, {procs} single-threaded process(es)")
+
+
+# ---------------------------------------------------------------------------
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference_arm(args, ws, rank):
+    if rank != 0:
+        return 0
+    procs = os.cpu_count() or 1
+    per = max(4096, min(262_144, int(4e7 / max(1, args.steps + args.warmup))))
+    per = (per // 2) * 2
+    base = cpu_baseline(per, args.warmup, args.steps, procs)
+    line = dict(metric=METRIC, value=base["value"], unit=UNIT, n_gpus=args.gpus, steps=args.steps,
+                warmup=args.warmup, ms_per_step=None, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f64", data="synthetic", impl="reference",
+                config=dict(workload=WORKLOAD + " (CPU: bounded sample, see cpu_baseline)", parallelism="processes"),
+                cpu_baseline=base, e2e=dict(value=base["value"], unit=UNIT, h2d_bytes_per_step=0,
+                                            d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    if args.impl == "reference":
+        rc = run_reference_arm(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return rc
+    args.warmup = max(args.warmup, 3)
+
+    from samos_b200 import Engine
+    from samos_b200.plugins import Simulation
+
+    parts, L = make_particles(N_PART, seed=1 + rank)
+    eng = Engine(N_PART, device=local)
+    sim = Simulation(eng)
+    configure(sim, parts, L)
+
+    # warm-up (untimed)
+    sim.run(args.warmup - 1)
+
+    # timed region: K steps with inputs resident in HBM (state 1.4 GB >> 126 MB L2)
+    barrier(ws)
+    launches0 = eng.kernel_launches()
+    with ClockSampler(local) as clocks:
+        st = eng.run(args.steps - 1)
+    launches = eng.kernel_launches() - launches0
+    t_ms = max_over_ranks(st.device_ms, ws)
+    value = ws * N_PART * args.steps / (t_ms * 1e-3)
+
+    # dominant kernel: per-launch CUDA-event time of the fused step kernel
+    eng.set_profiling(True)
+    pst = eng.run(min(args.steps, 200) - 1)
+    eng.set_profiling(False)
+    k_ms = pst.step_kernel_ms / max(1, pst.step_kernels)
+    achieved = N_PART * BYTES_PER_PARTICLE_STEP / (k_ms * 1e-3) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get("bytes_per_launch_4M")
+
+    # end to end through the C ABI with host buffers
+    barrier(ws)
+    e2e_steps = args.steps
+    fields_in = ("x", "y", "z", "vx", "vy", "vz", "nx", "ny", "nz", "radius")
+    fields_out = ("x", "y", "nx", "ny", "vx", "vy")
+    t0 = time.perf_counter()
+    for f in fields_in:
+        eng.upload(f, parts[f])
+    eng.build_nlist()
+    est = eng.run(e2e_steps - 1)
+    outs = {f: eng.download(f) for f in fields_out}
+    e2e_s = max_over_ranks(time.perf_counter() - t0, ws)
+    h2d = len(fields_in) * 8 * N_PART / e2e_steps
+    d2h = len(fields_out) * 8 * N_PART / e2e_steps
+    e2e_value = ws * N_PART * e2e_steps / e2e_s
+    finite = all(np.isfinite(v).all() for v in outs.values())
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline()
+
+    if rank == 0:
+        line = dict(
+            metric=METRIC, value=value, unit=UNIT, n_gpus=ws, steps=args.steps, warmup=args.warmup,
+            ms_per_step=t_ms / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
+            dtype="f64", data="synthetic",
+            config=dict(workload=WORKLOAD, n_particles=N_PART, box=L, parallelism=f"replicas x{ws}",
+                        l2="state resident in HBM, 1.4 GB per buffer set >> 126 MB L2 (no flush needed)",
+                        nlist_builds_timed=st.nlist_builds),
+            roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
+                          traffic=traffic, kernel="k_step_brownian", kernel_ms=k_ms,
+                          algorithmic_bytes_per_particle_step=BYTES_PER_PARTICLE_STEP,
+                          peak_source="MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"),
+            e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
+                     steps=e2e_steps, finite=bool(finite)),
+            gpu_launches=int(launches),
+            clocks=clocks.summary(),
+            cpu_baseline=cpu,
+        )
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

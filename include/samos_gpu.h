@@ -1,0 +1,167 @@
+/*
+ * samos_gpu.h -- C ABI of the B200 (sm_100a) SAMoS particle-dynamics engine.
+ *
+ * One handle owns a packed ensemble of R independent replicas (R = 1 for an
+ * ordinary `samos` run) resident in HBM as structure-of-arrays FP64 buffers.
+ * Components are configured with the same kinds, parameter meanings and
+ * ordering rules as SAMoS's class factories; every entry point below names
+ * the reference interface it replaces (paths relative to the SAMoS tree).
+ *
+ * Conventions: every call returns SG_OK (0) or a negative SG_ERR_* code; no
+ * exception crosses the ABI; sg_last_error() gives a one-line reason.  All
+ * pointers are host pointers unless the name says _device.  A handle is not
+ * thread-safe (the reference is single-threaded, src/samos.cpp:878-970).
+ */
+#ifndef SAMOS_GPU_H
+#define SAMOS_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SG_OK               0
+#define SG_ERR_ARG         -1   /* bad argument / unknown field or kind      */
+#define SG_ERR_CUDA        -2   /* CUDA runtime error                        */
+#define SG_ERR_NOMEM       -3   /* device allocation failed                  */
+#define SG_ERR_STATE       -4   /* call out of order (e.g. run before nlist) */
+#define SG_ERR_OVERFLOW    -5   /* neighbour capacity exceeded after regrow  */
+#define SG_ERR_NONFINITE   -6   /* NaN/Inf detected in the particle state    */
+#define SG_ERR_UNSUPPORTED -7   /* configuration outside the GPU path        */
+#define SG_ERR_TIMEOUT     -8   /* a bounded device wait gave up             */
+
+/* ---- component kinds (factory names of src/utils/register_*.cpp) -------- */
+enum { SG_PAIR_SOFT = 0, SG_PAIR_LJ = 1, SG_PAIR_MORSE = 2, SG_PAIR_GAUSSIAN = 3 };
+enum { SG_ALIGN_POLAR = 0, SG_ALIGN_NEMATIC = 1, SG_ALIGN_VICSEK = 2 };
+enum { SG_EXT_SELF_PROPULSION = 0 };
+enum { SG_CONS_NONE = 0, SG_CONS_PLANE = 1, SG_CONS_SPHERE = 2 };
+enum { SG_INT_BROWNIAN = 0, SG_INT_BROWNIAN_POS = 1, SG_INT_BROWNIAN_ALIGN = 2,
+       SG_INT_LANGEVIN = 3, SG_INT_FIRE = 4 };
+enum { SG_VALUE_CONSTANT = 0, SG_VALUE_LINEAR = 1 };
+enum { SG_LANGEVIN_BAOAB = 0, SG_LANGEVIN_SPV = 1, SG_LANGEVIN_BBK = 2 };
+
+#define SG_PAIR_NPARAM 8
+#define SG_INT_NPARAM 16
+#define SG_MAX_TYPES 16
+
+typedef struct sg_system sg_system;
+
+typedef struct {
+  int64_t steps_done;      /* integration steps executed by the last sg_run  */
+  int64_t nlist_builds;    /* neighbour-list builds during the last sg_run   */
+  int64_t kernel_launches; /* engine kernels launched during the last sg_run */
+  int32_t max_neighbours;  /* largest full-list neighbour count seen         */
+  int32_t status;          /* device status word (0 = clean)                 */
+  double  device_ms;       /* CUDA-event time of the whole call on its stream */
+  double  step_kernel_ms;  /* summed event time of the dominant step kernel   */
+  int64_t step_kernels;    /* launches timed in step_kernel_ms (profiling on) */
+} sg_run_stats;
+
+/* ---- lifetime ------------------------------------------------------------
+ * Replaces System::System (src/system/system.cpp:64-452) as the owner of the
+ * particle store: n_particles[r] particles of ntypes types per replica.     */
+int  sg_create(int n_replicas, const int32_t* n_particles, int ntypes, sg_system** out);
+/* Select the CUDA device that the next sg_create binds (per calling thread);
+ * a handle keeps its device for all later calls.                           */
+int  sg_set_device(int device);
+int  sg_destroy(sg_system* s);
+const char* sg_error_string(int code);
+const char* sg_last_error(const sg_system* s);
+
+/* Box(lx,ly,lz) centred at the origin, src/system/box.hpp:56-62; periodic
+ * flag of `box periodic|fixed` (src/samos.cpp:205-230).                      */
+int  sg_set_box(sg_system* s, int replica, double lx, double ly, double lz, int periodic);
+/* `timestep dt` -> System::set_integrator_step (src/samos.cpp:1348)          */
+int  sg_set_timestep(sg_system* s, double dt);
+
+/* ---- particle data -------------------------------------------------------
+ * Field names follow Particle (src/system/particle.hpp:257-306): doubles
+ * "x","y","z","vx","vy","vz","fx","fy","fz","tau_x","tau_y","tau_z","nx",
+ * "ny","nz","Nx","Ny","Nz","omega","age","radius","mass"; int32 "type",
+ * "ix","iy","iz".  Arrays are in particle-id order (length n_particles[r]). */
+int  sg_upload(sg_system* s, int replica, const char* field, const void* host);
+int  sg_download(sg_system* s, int replica, const char* field, void* host);
+
+/* ---- neighbour list ------------------------------------------------------
+ * NeighbourList(sys, msg, rcut, pad) (src/system/neighbour_list.hpp:124-217)
+ * including the immediate build; build() / build_cell() / build_nsq()
+ * (src/system/neighbour_list.cpp:117-273).                                  */
+int  sg_set_nlist(sg_system* s, double rcut, double pad);
+int  sg_build_nlist(sg_system* s);
+/* Half list of replica r as (i<j) id pairs in the reference's list order
+ * (NeighbourList::get_neighbours, neighbour_list.hpp:237).                  */
+int  sg_get_pairs(sg_system* s, int replica, int32_t* out_i, int32_t* out_j,
+                  int64_t cap, int64_t* n_pairs);
+
+/* ---- components ----------------------------------------------------------
+ * Pair potential (factory pair_potentials[name], register_pair_potentials.cpp
+ * :35-69; parameters pair_soft/lj/morse/gaussian_potential.hpp).  `global`
+ * holds the conf-level parameters, `table` (ntypes*ntypes*SG_PAIR_NPARAM,
+ * may be NULL) the per-type-pair values of set_pair_parameters (pair_param
+ * command).  phase_value = {kind, min_val, max_val, steps} of the phase-in
+ * Value object.  Parameter slots: soft {k,a}; lj {epsilon,sigma,rcut};
+ * morse {D,a,re,rcut}; gaussian {A,B,alpha,beta,rA,rB,rcut}.               */
+int  sg_add_pair(sg_system* s, int kind, const double* global, const double* table,
+                 int use_particle_radii, int phase_in, int shifted, int has_pair_params,
+                 const double* phase_value);
+/* Pair aligner (register_pair_aligners.cpp:35-41): polar / nematic / vicsek
+ * with global J and rcut; table = ntypes*ntypes*{J, rcut} of align_param.   */
+int  sg_add_align(sg_system* s, int kind, double J, double rcut, const double* table,
+                  int has_pair_params);
+/* External potential self_propulsion {alpha} with optional per-type alpha
+ * (external_self_propulsion.cpp:33-50).                                     */
+int  sg_add_external(sg_system* s, int kind, double alpha, const double* type_alpha,
+                     int has_params);
+/* Constraint (register_constraints.cpp:35-61): params =
+ * {plane: zpos | sphere: r, plane: unlimited, maxiter, tol, rescale,
+ *  rescale_steps, rescale_freq}; enforced on every particle at once like
+ * src/samos.cpp:518-522.                                                     */
+int  sg_add_constraint(sg_system* s, int kind, const double* params);
+/* Integrator (register_integrators.cpp:35-55).  params[SG_INT_NPARAM]:
+ *  brownian       : 0 dt, 1 v0, 2 nu, 3 mu, 4 mur, 5 seed, 6 nematic, 7 tau, 8 velocity_align
+ *  brownian_pos   : 0 dt, 3 mu, 5 seed
+ *  brownian_align : 0 dt, 2 nu, 4 mur, 5 seed, 6 nematic, 7 tau
+ *  langevin       : 0 dt, 5 seed, 9 gamma, 10 method
+ *  fire           : 0 dt, 1 alpha, 2 alpha_scale, 3 f_tolerance, 4 e_tolerance,
+ *                   6 dt_inc, 7 dt_dec, 8 dt_max, 9 min_neg_steps, 11 fmax_tolerance
+ * temperature_value = {kind, min_val, max_val, steps} (Value, value.hpp).
+ * Integrators must be added in std::map key order (type + "_" + group).     */
+int  sg_add_integrator(sg_system* s, int kind, const double* params,
+                       const double* temperature_value);
+/* Per-replica override of one numeric parameter (batched ensembles):
+ * cls 0 pair global, 1 aligner {0:J,1:rcut}, 2 external alpha,
+ * 3 constraint {0: zpos|r}, 4 integrator params[] (slot 5 = seed).          */
+int  sg_set_replica_param(sg_system* s, int replica, int cls, int comp, int slot, double value);
+
+/* ---- execution -----------------------------------------------------------
+ * sg_compute: reset_forces/reset_torques + Potential::compute(dt) +
+ * Aligner::compute() (potential.cpp:36-52, aligner.cpp:35-45) on the current
+ * state, no integration.                                                    */
+int  sg_compute(sg_system* s, double dt);
+/* Constrainer::enforce on every particle (constrainer.hpp:73-77).           */
+int  sg_enforce(sg_system* s);
+/* `run steps` (src/samos.cpp:864-972): steps+1 integration steps with the
+ * skin-triggered neighbour-list rebuilds of samos.cpp:944-966.              */
+int  sg_run(sg_system* s, int64_t steps, sg_run_stats* stats);
+/* FIRE minimisation driver: run until every replica's FIRE integrator has
+ * converged or max_steps integration steps; converged[r] (may be NULL) gets
+ * the step count per replica or -1.                                         */
+int  sg_minimize(sg_system* s, int64_t max_steps, int64_t* converged, sg_run_stats* stats);
+/* Energy of component `comp` of class cls (0 pair, 1 aligner) for replica r
+ * from the last force evaluation (PairPotential::get_potential_energy).     */
+int  sg_energy(sg_system* s, int replica, int cls, int comp, double* out);
+/* FIRE scalars of replica r: {dt, alpha, last_neg, converged, old_energy}.  */
+int  sg_fire_state(sg_system* s, int replica, double* out5);
+/* Cumulative kernel launches of this handle (for launch accounting).       */
+int64_t sg_kernel_launches(const sg_system* s);
+/* Time every launch of the dominant per-step kernel with CUDA events on the
+ * handle's stream (reported in sg_run_stats.step_kernel_ms).  No reference
+ * counterpart (instrumentation).                                            */
+int  sg_set_profiling(sg_system* s, int on);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

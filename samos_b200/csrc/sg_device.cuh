@@ -1,0 +1,450 @@
+// sg_device.cuh -- device-side data model and per-particle physics of the
+// SAMoS hot path on sm_100a.
+//
+// Every routine restates one reference routine (paths relative to the SAMoS
+// source tree).  The translation unit is compiled with -fmad=false so that no
+// a*b+c is contracted into an FMA: together with IEEE-rounded division and
+// square root this reproduces the reference's arithmetic term by term (CUDA
+// exp/sin/cos aside, which differ from glibc by at most a few ulp).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+#include <math.h>
+
+namespace sg {
+
+constexpr int MAX_PAIR = 4;
+constexpr int MAX_ALIGN = 3;
+constexpr int MAX_EXT = 2;
+constexpr int MAX_CONS = 4;
+constexpr int MAX_INTEG = 5;
+constexpr int PAIR_NPARAM = 8;
+constexpr int INT_NPARAM = 16;
+constexpr int BLOCK = 128;          // particle slots per block; replicas are padded to it
+
+enum { PAIR_SOFT = 0, PAIR_LJ = 1, PAIR_MORSE = 2, PAIR_GAUSSIAN = 3 };
+enum { ALIGN_POLAR = 0, ALIGN_NEMATIC = 1, ALIGN_VICSEK = 2 };
+enum { CONS_NONE = 0, CONS_PLANE = 1, CONS_SPHERE = 2 };
+enum { INT_BROWNIAN = 0, INT_BROWNIAN_POS = 1, INT_BROWNIAN_ALIGN = 2, INT_LANGEVIN = 3, INT_FIRE = 4 };
+enum { LANGEVIN_BAOAB = 0, LANGEVIN_SPV = 1, LANGEVIN_BBK = 2 };
+
+// device status word bits
+enum { ST_OVERFLOW = 1, ST_NONFINITE = 2, ST_TIMEOUT = 4 };
+
+// Value objects, system/value.hpp:115-178
+struct Value { int kind; int steps; double min_val, max_val, dv; };
+
+__host__ __device__ inline double value_get(const Value& v, int step) {
+  if (v.kind == 0) return v.min_val;
+  if (step > v.steps) return v.max_val;
+  return v.min_val + (double)step * v.dv;
+}
+
+struct PairComp { int kind, use_radii, phase_in, shifted, has_pp; Value phase; const double* table; };
+struct AlignComp { int kind, has_pp; const double* table; };
+struct ExtComp { int kind, has_params; const double* type_alpha; };
+struct ConsComp { int kind, unlimited; };
+struct IntegComp { int kind, method, nematic, velocity; Value temp; };
+
+// The configured component program, passed by value to every kernel.
+struct Program {
+  int ntypes;
+  int npair, nalign, next, ncons, ninteg;
+  PairComp pair[MAX_PAIR];
+  AlignComp align[MAX_ALIGN];
+  ExtComp ext[MAX_EXT];
+  ConsComp cons[MAX_CONS];
+  IntegComp integ[MAX_INTEG];
+};
+
+// Per-replica numeric parameters and geometry (device array).
+struct Replica {
+  int off, n;                  // first slot, particle count
+  int cell_off, ncell;         // cell range in the packed cell arrays
+  int cnx, cny, cnz, use_cell; // grid; use_cell = reference cell path, else N^2 order
+  int periodic, pad_i;
+  double Lx, Ly, Lz, xlo, xhi, ylo, yhi, zlo, zhi;
+  double cwx, cwy, cwz;
+  double cut2, pad;
+  double pair_g[MAX_PAIR][PAIR_NPARAM];
+  double align_J[MAX_ALIGN], align_rcut[MAX_ALIGN];
+  double ext_alpha[MAX_EXT];
+  double cons_p[MAX_CONS];     // plane: zpos; sphere: r
+  double integ_p[MAX_INTEG][INT_NPARAM];
+  uint32_t seed[MAX_INTEG];
+};
+
+// Per-replica evolving scalars (device array, updated by the tail kernels).
+struct Clock {
+  int run_step, time_step;
+  uint64_t ctr[MAX_INTEG];     // noise counter base per integrator
+  double fire_dt, fire_alpha, fire_old_e;
+  int fire_last_neg, fire_converged, fire_conv_step, pad;
+  double fire_P, fire_F, fire_V, fire_E, fire_Fmax2;
+};
+
+// Particle arrays of one buffer set.
+struct Dyn {
+  double *x, *y, *z, *vx, *vy, *vz, *nx, *ny, *nz;
+  double *fx, *fy, *fz, *tx, *ty, *tz, *omega, *age;
+  int *ix, *iy, *iz;
+};
+struct Stat { double *r, *mass; int *type, *id; };
+struct NbList { int *nb, *cnt, *lo; int cap; int stride; double *ox, *oy, *oz; };
+
+struct Part {
+  double x, y, z, vx, vy, vz, nx, ny, nz, fx, fy, fz, tx, ty, tz, omega, age, r, mass;
+  int ix, iy, iz, type, id;
+};
+
+__device__ __forceinline__ void load_dyn(const Dyn& d, int k, Part& p) {
+  p.x = d.x[k]; p.y = d.y[k]; p.z = d.z[k];
+  p.vx = d.vx[k]; p.vy = d.vy[k]; p.vz = d.vz[k];
+  p.nx = d.nx[k]; p.ny = d.ny[k]; p.nz = d.nz[k];
+  p.fx = d.fx[k]; p.fy = d.fy[k]; p.fz = d.fz[k];
+  p.tx = d.tx[k]; p.ty = d.ty[k]; p.tz = d.tz[k];
+  p.omega = d.omega[k]; p.age = d.age[k];
+  p.ix = d.ix[k]; p.iy = d.iy[k]; p.iz = d.iz[k];
+}
+__device__ __forceinline__ void store_dyn(const Dyn& d, int k, const Part& p) {
+  d.x[k] = p.x; d.y[k] = p.y; d.z[k] = p.z;
+  d.vx[k] = p.vx; d.vy[k] = p.vy; d.vz[k] = p.vz;
+  d.nx[k] = p.nx; d.ny[k] = p.ny; d.nz[k] = p.nz;
+  d.fx[k] = p.fx; d.fy[k] = p.fy; d.fz[k] = p.fz;
+  d.tx[k] = p.tx; d.ty[k] = p.ty; d.tz[k] = p.tz;
+  d.omega[k] = p.omega; d.age[k] = p.age;
+  d.ix[k] = p.ix; d.iy[k] = p.iy; d.iz[k] = p.iz;
+}
+
+// ---------------------------------------------------------------------------
+// noise stream: Philox-4x32-10 (Salmon et al., SC'11) + polar method of
+// Marsaglia & Bray (1964); one counter value per draw.  The same stream is
+// restated independently by the CPU oracle.
+// ---------------------------------------------------------------------------
+constexpr uint32_t NOISE_KEY1 = 0x53414D4Fu;
+
+__host__ __device__ __forceinline__ uint32_t mulhi32(uint32_t a, uint32_t b) {
+  return (uint32_t)(((uint64_t)a * (uint64_t)b) >> 32);
+}
+
+__host__ __device__ __forceinline__ void philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                                uint32_t k0, uint32_t k1, uint32_t out[4]) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    uint32_t lo0 = 0xD2511F53u * c0, hi0 = mulhi32(0xD2511F53u, c0);
+    uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = mulhi32(0xCD9E8D57u, c2);
+    uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+__host__ __device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
+  return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+__host__ __device__ __forceinline__ uint64_t dbits(double x) {
+#ifdef __CUDA_ARCH__
+  return (uint64_t)__double_as_longlong(x);
+#else
+  uint64_t u; memcpy(&u, &x, sizeof(u)); return u;
+#endif
+}
+__host__ __device__ __forceinline__ double bitsd(uint64_t u) {
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double((long long)u);
+#else
+  double x; memcpy(&x, &u, sizeof(x)); return x;
+#endif
+}
+
+// log(x) from log(m) = 2 atanh((m-1)/(m+1)), x = m 2^e, m in [sqrt(1/2), sqrt(2));
+// fixed operation order, no FMA (see the oracle's or_noise_log).
+__host__ __device__ __forceinline__ double noise_log(double x) {
+  uint64_t u = dbits(x);
+  int e = (int)((u >> 52) & 0x7ff) - 1023;
+  u = (u & 0x000fffffffffffffull) | 0x3ff0000000000000ull;
+  double m = bitsd(u);
+  if (m > 1.4142135623730951) { m = m * 0.5; e = e + 1; }
+  double z = (m - 1.0) / (m + 1.0);
+  double z2 = z * z;
+  double p = 1.0 / 23.0;
+  p = p * z2 + 1.0 / 21.0;
+  p = p * z2 + 1.0 / 19.0;
+  p = p * z2 + 1.0 / 17.0;
+  p = p * z2 + 1.0 / 15.0;
+  p = p * z2 + 1.0 / 13.0;
+  p = p * z2 + 1.0 / 11.0;
+  p = p * z2 + 1.0 / 9.0;
+  p = p * z2 + 1.0 / 7.0;
+  p = p * z2 + 1.0 / 5.0;
+  p = p * z2 + 1.0 / 3.0;
+  double lm = 2.0 * z + 2.0 * z * (z2 * p);
+  double de = (double)e;
+  const double LN2_HI = 6.93147180369123816490e-01;
+  const double LN2_LO = 1.90821492927058770002e-10;
+  return (de * LN2_HI + lm) + de * LN2_LO;
+}
+
+__host__ __device__ __forceinline__ double noise_gauss(uint32_t seed, uint64_t counter) {
+  for (uint32_t attempt = 0; attempt < 64; attempt++) {
+    uint32_t r[4];
+    philox((uint32_t)counter, (uint32_t)(counter >> 32), attempt, 0u, seed, NOISE_KEY1, r);
+    double v1 = 2.0 * u53(r[0], r[1]) - 1.0;
+    double v2 = 2.0 * u53(r[2], r[3]) - 1.0;
+    double s = v1 * v1 + v2 * v2;
+    if (s < 1.0 && s > 0.0) return v2 * sqrt(-2.0 * noise_log(s) / s);
+  }
+  return 0.0;
+}
+
+__host__ __device__ __forceinline__ double noise_uniform(uint32_t seed, uint64_t counter) {
+  uint32_t r[4];
+  philox((uint32_t)counter, (uint32_t)(counter >> 32), 0u, 1u, seed, NOISE_KEY1, r);
+  return u53(r[0], r[1]);
+}
+
+// ---------------------------------------------------------------------------
+// periodic box, system/system.cpp:1083-1154
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void apply_periodic(const Replica& R, double& dx, double& dy, double& dz) {
+  if (R.periodic) {
+    if (dx > R.xhi) dx -= R.Lx; else if (dx < R.xlo) dx += R.Lx;
+    if (dy > R.yhi) dy -= R.Ly; else if (dy < R.ylo) dy += R.Ly;
+    if (dz > R.zhi) dz -= R.Lz; else if (dz < R.zlo) dz += R.Lz;
+  }
+}
+
+__device__ __forceinline__ void enforce_periodic(const Replica& R, Part& p) {
+  if (R.periodic) {
+    if (p.x <= R.xlo) { p.x += R.Lx; p.ix--; } else if (p.x > R.xhi) { p.x -= R.Lx; p.ix++; }
+    if (p.y <= R.ylo) { p.y += R.Ly; p.iy--; } else if (p.y > R.yhi) { p.y -= R.Ly; p.iy++; }
+    if (p.z <= R.zlo) { p.z += R.Lz; p.iz--; } else if (p.z > R.zhi) { p.z -= R.Lz; p.iz++; }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// constraints
+// ---------------------------------------------------------------------------
+// ConstraintPlane::enforce, constraints/constraint_plane.cpp:36-89
+__device__ __forceinline__ void plane_enforce(const Replica& R, double zpos, int unlimited, Part& p) {
+  double xlo = -0.5 * R.Lx, xhi = 0.5 * R.Lx;
+  double ylo = -0.5 * R.Ly, yhi = 0.5 * R.Ly;
+  p.z = zpos; p.vz = 0.0; p.fz = 0.0;
+  if (R.periodic) enforce_periodic(R, p);
+  else if (!unlimited) {
+    if (p.x < xlo) { p.x = xlo; p.vx = -p.vx; } else if (p.x > xhi) { p.x = xhi; p.vx = -p.vx; }
+    if (p.y < ylo) { p.y = ylo; p.vy = -p.vy; } else if (p.y > yhi) { p.y = yhi; p.vy = -p.vy; }
+  }
+  p.nz = 0.0;
+  double len_n = sqrt(p.nx * p.nx + p.ny * p.ny);
+  double inv_len = 1.0;
+  if (len_n != 0.0) inv_len = 1.0 / len_n;  // the reference recomputes the same sqrt
+  p.nx *= inv_len; p.ny *= inv_len;
+}
+
+// ConstraintSphere::enforce, constraints/constraint_sphere.cpp:38-81
+__device__ __forceinline__ void sphere_enforce(double Rs, Part& p) {
+  double R = sqrt(p.x * p.x + p.y * p.y + p.z * p.z);
+  double s = Rs / R;
+  p.x *= s; p.y *= s; p.z *= s;
+  double Nx = p.x / Rs, Ny = p.y / Rs, Nz = p.z / Rs;
+  double v_dot_N = p.vx * Nx + p.vy * Ny + p.vz * Nz;
+  double n_dot_N = p.nx * Nx + p.ny * Ny + p.nz * Nz;
+  p.vx -= v_dot_N * Nx; p.vy -= v_dot_N * Ny; p.vz -= v_dot_N * Nz;
+  p.nx -= n_dot_N * Nx; p.ny -= n_dot_N * Ny; p.nz -= n_dot_N * Nz;
+  double inv_len = 1.0 / sqrt(p.nx * p.nx + p.ny * p.ny + p.nz * p.nz);
+  p.nx *= inv_len; p.ny *= inv_len; p.nz *= inv_len;
+}
+
+// Constrainer::enforce (constrainer.hpp:73-77); ConstraintNone::enforce
+// (constraint_none.hpp:58-62)
+__device__ __forceinline__ void enforce_all(const Program& P, const Replica& R, Part& p) {
+  for (int c = 0; c < P.ncons; c++) {
+    int kind = P.cons[c].kind;
+    if (kind == CONS_PLANE) plane_enforce(R, R.cons_p[c], P.cons[c].unlimited, p);
+    else if (kind == CONS_SPHERE) sphere_enforce(R.cons_p[c], p);
+    else enforce_periodic(R, p);
+  }
+}
+
+// Constrainer::project_torque (constrainer.hpp:93-99) over
+// Constraint::project_torque (constraint.cpp:158-173, sphere normal
+// constraint_sphere.hpp:76) and ConstraintPlane::project_torque
+// (constraint_plane.cpp:150-162)
+__device__ __forceinline__ double project_torque(const Program& P, const Replica& R, const Part& p) {
+  double val = 0.0;
+  for (int c = 0; c < P.ncons; c++) {
+    int kind = P.cons[c].kind;
+    if (kind == CONS_PLANE) val += p.tz;
+    else if (kind == CONS_SPHERE) {
+      double Rs = R.cons_p[c];
+      double Nx = p.x / Rs, Ny = p.y / Rs, Nz = p.z / Rs;
+      val += p.tx * Nx + p.ty * Ny + p.tz * Nz;
+    } else val += 0.0;
+  }
+  return val;
+}
+
+// Constraint::rotate_director (Rodrigues, constraint.cpp:96-119) and
+// ConstraintPlane::rotate_director (constraint_plane.cpp:97-114)
+__device__ __forceinline__ void rotate_director(const Program& P, const Replica& R, Part& p, double phi) {
+  for (int c = 0; c < P.ncons; c++) {
+    int kind = P.cons[c].kind;
+    if (kind == CONS_PLANE) {
+      double cs = cos(phi), sn = sin(phi);
+      double Rxx = cs, Rxy = -sn, Ryx = sn, Ryy = cs;
+      double nx = Rxx * p.nx + Rxy * p.ny;
+      double ny = Ryx * p.nx + Ryy * p.ny;
+      double len = sqrt(nx * nx + ny * ny);
+      p.nx = nx / len; p.ny = ny / len;
+    } else if (kind == CONS_SPHERE) {
+      double Rs = R.cons_p[c];
+      double U = p.x / Rs, V = p.y / Rs, W = p.z / Rs;
+      double cs = cos(phi), sn = sin(phi);
+      double dot = U * p.nx + V * p.ny + W * p.nz;
+      double nx = U * dot * (1.0 - cs) + p.nx * cs + (-W * p.ny + V * p.nz) * sn;
+      double ny = V * dot * (1.0 - cs) + p.ny * cs + (W * p.nx - U * p.nz) * sn;
+      double nz = W * dot * (1.0 - cs) + p.nz * cs + (-V * p.nx + U * p.ny) * sn;
+      double len = sqrt(nx * nx + ny * ny + nz * nz);
+      p.nx = nx / len; p.ny = ny / len; p.nz = nz / len;
+    }
+  }
+}
+
+// Constraint::rotate_velocity (constraint.cpp:128-150) and the plane
+// variant (constraint_plane.cpp:122-143)
+__device__ __forceinline__ void rotate_velocity(const Program& P, const Replica& R, Part& p, double phi) {
+  for (int c = 0; c < P.ncons; c++) {
+    int kind = P.cons[c].kind;
+    if (kind == CONS_PLANE) {
+      double cs = cos(phi), sn = sin(phi);
+      double Rxx = cs, Rxy = -sn, Ryx = sn, Ryy = cs;
+      double vx = Rxx * p.vx + Rxy * p.vy;
+      double vy = Ryx * p.vx + Ryy * p.vy;
+      p.vx = vx; p.vy = vy;
+    } else if (kind == CONS_SPHERE) {
+      double Rs = R.cons_p[c];
+      double U = p.x / Rs, V = p.y / Rs, W = p.z / Rs;
+      double cs = cos(phi), sn = sin(phi);
+      double dot = U * p.vx + V * p.vy + W * p.vz;
+      double vx = U * dot * (1.0 - cs) + p.vx * cs + (-W * p.vy + V * p.vz) * sn;
+      double vy = V * dot * (1.0 - cs) + p.vy * cs + (W * p.vx - U * p.vz) * sn;
+      double vz = W * dot * (1.0 - cs) + p.vz * cs + (-V * p.vx + U * p.vy) * sn;
+      p.vx = vx; p.vy = vy; p.vz = vz;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pair terms.  With d = x_other - x_self (minimum image), every reference pair
+// potential gives the force on the particle at hand as  -ff * d  and every
+// polar/nematic aligner its torque as  +J' (n_self x n_other), bit for bit in
+// either role of the pair (IEEE negation is exact and the box is centred).
+// ---------------------------------------------------------------------------
+struct Nb { double x, y, z, r, nx, ny, nz, vx, vy, vz, age; int type; };
+
+__device__ __forceinline__ double phase_factor(const PairComp& C, double age, double dt) {
+  return 0.5 * (1.0 + value_get(C.phase, (int)(age / dt)));
+}
+__device__ __forceinline__ double phase_pair(double ai, double aj) {
+  if (ai < 1.0 && aj < 1.0) return ai + aj - 1.0;
+  return ai * aj;
+}
+
+// Returns ff (force factor) and adds the pair energy to *pe if in range.
+// soft: pair_soft_potential.cpp:57-117; lj: pair_lj_potential.cpp:54-122;
+// morse: pair_morse_potential.cpp:52-120; gaussian:
+// pair_gaussian_potential.cpp:55-126.
+__device__ __forceinline__ bool pair_term(const PairComp& C, const double* g, int ntypes,
+                                          const Part& me, const Nb& o, double r_sq,
+                                          double alpha, double& ff, double& pe) {
+  const double* t = C.table + ((size_t)(me.type - 1) * ntypes + (size_t)(o.type - 1)) * PAIR_NPARAM;
+  switch (C.kind) {
+    case PAIR_SOFT: {
+      double k = t[0];
+      double r = sqrt(r_sq);
+      double ai_p_aj = C.use_radii ? me.r + o.r : t[1];
+      if (r < ai_p_aj) {
+        double diff = ai_p_aj - r;
+        pe = 0.5 * k * alpha * diff * diff;
+        if (r > 0.0) ff = k * alpha * diff / r; else ff = k * diff;
+        return true;
+      }
+      return false;
+    }
+    case PAIR_LJ: {
+      double rcut = C.has_pp ? t[2] : g[2];
+      double rcut_sq = rcut * rcut;
+      if (r_sq <= rcut_sq) {
+        double sigma = C.has_pp ? t[1] : g[1];
+        double eps = C.has_pp ? t[0] : g[0];
+        if (C.use_radii) sigma = me.r + o.r;
+        double sigma_sq = sigma * sigma;
+        double inv_r_sq = sigma_sq / r_sq;
+        double inv_r_6 = inv_r_sq * inv_r_sq * inv_r_sq;
+        double e = 4.0 * eps * alpha * inv_r_6 * (inv_r_6 - 1.0);
+        if (C.shifted) {
+          double ic = sigma_sq / rcut_sq;
+          double ic6 = ic * ic * ic;
+          e -= 4.0 * eps * alpha * ic6 * (ic6 - 1.0);
+        }
+        pe = e;
+        ff = 48.0 * eps * alpha * inv_r_6 * (inv_r_6 - 0.5) * inv_r_sq;
+        return true;
+      }
+      return false;
+    }
+    case PAIR_MORSE: {
+      double rcut = C.has_pp ? t[3] : g[3];
+      double rcut_sq = rcut * rcut;
+      if (r_sq <= rcut_sq) {
+        double D = C.has_pp ? t[0] : g[0];
+        double a = C.has_pp ? t[1] : g[1];
+        double re = C.has_pp ? t[2] : g[2];
+        if (C.use_radii) re = me.r + o.r;
+        double r = sqrt(r_sq);
+        double exp_fact = exp(-a * (r - re));
+        double pot_fact = exp_fact - 1.0;
+        double e = D * alpha * (pot_fact * pot_fact - 1.0);
+        if (C.shifted) {
+          double sf = exp(-a * (rcut - re)) - 1.0;
+          e -= D * alpha * (sf * sf - 1.0);
+        }
+        pe = e;
+        ff = 2.0 * D * a * alpha * exp_fact * pot_fact / r;
+        return true;
+      }
+      return false;
+    }
+    default: {  // PAIR_GAUSSIAN
+      double rcut = C.has_pp ? t[6] : g[6];
+      double rcut_sq = rcut * rcut;
+      if (r_sq <= rcut_sq) {
+        double A = C.has_pp ? t[0] : g[0];
+        double B = C.has_pp ? t[1] : g[1];
+        double al = C.has_pp ? t[2] : g[2];
+        double be = C.has_pp ? t[3] : g[3];
+        double rA = C.has_pp ? t[4] : g[4];
+        double rB = C.has_pp ? t[5] : g[5];
+        if (C.use_radii) rB = me.r + o.r;
+        double r = sqrt(r_sq);
+        double r_m_rA = r - rA, r_m_rB = r - rB;
+        double e = A * alpha * exp(-al * r_m_rA * r_m_rA) + B * exp(-be * r_m_rB * r_m_rB);
+        if (C.shifted) {
+          double ca = rcut - rA, cb = rcut - rB;
+          e -= A * alpha * exp(-al * ca * ca) + B * exp(-be * cb * cb);
+        }
+        pe = e;
+        ff = (2.0 / r) * alpha * (A * al * r_m_rA * exp(-al * r_m_rA * r_m_rA) +
+                                  B * be * r_m_rB * exp(-be * r_m_rB * r_m_rB));
+        return true;
+      }
+      return false;
+    }
+  }
+}
+
+}  // namespace sg

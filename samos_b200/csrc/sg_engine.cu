@@ -1,0 +1,903 @@
+// sg_engine.cu -- host side of the B200 SAMoS engine: the C ABI declared in
+// include/samos_gpu.h.  One stream per handle; device buffers are allocated
+// once per configuration and reused by every step.
+#include "samos_gpu.h"
+#include "sg_kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace sg;
+
+namespace {
+
+struct DevBuf {
+  std::vector<void*> ptrs;
+  cudaError_t err = cudaSuccess;
+  template <class T> T* alloc(size_t n) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, (n ? n : 1) * sizeof(T));
+    if (e != cudaSuccess) { err = e; return nullptr; }
+    cudaMemset(p, 0, (n ? n : 1) * sizeof(T));
+    cudaDeviceSynchronize();
+    ptrs.push_back(p);
+    return (T*)p;
+  }
+  void release(void* p) {
+    if (!p) return;
+    auto it = std::find(ptrs.begin(), ptrs.end(), p);
+    if (it != ptrs.end()) { cudaFree(p); ptrs.erase(it); }
+  }
+  void free_all() { for (void* p : ptrs) cudaFree(p); ptrs.clear(); }
+};
+
+const char* kDoubleFields[] = {"x", "y", "z", "vx", "vy", "vz", "nx", "ny", "nz",
+                               "fx", "fy", "fz", "tau_x", "tau_y", "tau_z", "omega", "age"};
+const int kNumDynDouble = 17;
+
+}  // namespace
+
+struct sg_system {
+  int device = 0;
+  int nrep = 0, ntypes = 1;
+  std::vector<int> n, off;
+  int slots = 0, nblocks = 0;
+  int* blk_rep = nullptr;
+  std::vector<int> blk_rep_h, rep_blk0_h, rep_nblk_h;
+  int *rep_blk0 = nullptr, *rep_nblk = nullptr;
+  std::vector<Replica> reps_h;
+  Replica* reps = nullptr;
+  std::vector<Clock> clk_h;
+  Clock* clk = nullptr;
+  Program prog{};
+  std::vector<double*> tables;
+  Dyn cur{}, alt{};
+  Stat st{}, st_alt{};
+  NbList nl{};
+  bool has_nlist = false;
+  double rcut = 0.0, pad = 0.0;
+  int ncell_total = 0;
+  int *pcell = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
+  int *tmp = nullptr, *perm = nullptr, *scan_bsum = nullptr;
+  int *rebuild = nullptr, *status = nullptr, *maxnb = nullptr;
+  int* rebuild_h = nullptr;  // pinned
+  double *epart = nullptr, *fire_part = nullptr, *alpha_mix = nullptr, *Rn = nullptr;
+  double dt_global = 0.0;
+  bool e1_applied = false;
+  bool configured_nlist_once = false;
+  int64_t launches = 0;
+  int64_t builds_run = 0;
+  int profile = 0;
+  int maxnb_seen = 0;
+  cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr, ev_k0 = nullptr, ev_k1 = nullptr;
+  cudaStream_t stream = nullptr;
+  DevBuf mem;
+  std::string last_error;
+  std::vector<double> uploaded_N[3];
+};
+
+static int fail(sg_system* s, int code, const std::string& msg) {
+  if (s) s->last_error = msg;
+  return code;
+}
+
+#define CU(s, call)                                                                  \
+  do {                                                                               \
+    cudaError_t e__ = (call);                                                        \
+    if (e__ != cudaSuccess)                                                          \
+      return fail((s), SG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)); \
+  } while (0)
+
+#define LAUNCH_CHECK(s)                                                              \
+  do {                                                                               \
+    (s)->launches++;                                                                 \
+    cudaError_t e__ = cudaGetLastError();                                            \
+    if (e__ != cudaSuccess)                                                          \
+      return fail((s), SG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e__)); \
+  } while (0)
+
+static double* dyn_field(Dyn& d, int i) {
+  double* f[kNumDynDouble] = {d.x, d.y, d.z, d.vx, d.vy, d.vz, d.nx, d.ny, d.nz,
+                              d.fx, d.fy, d.fz, d.tx, d.ty, d.tz, d.omega, d.age};
+  return f[i];
+}
+
+static bool alloc_dyn(DevBuf& m, Dyn& d, size_t n) {
+  d.x = m.alloc<double>(n); d.y = m.alloc<double>(n); d.z = m.alloc<double>(n);
+  d.vx = m.alloc<double>(n); d.vy = m.alloc<double>(n); d.vz = m.alloc<double>(n);
+  d.nx = m.alloc<double>(n); d.ny = m.alloc<double>(n); d.nz = m.alloc<double>(n);
+  d.fx = m.alloc<double>(n); d.fy = m.alloc<double>(n); d.fz = m.alloc<double>(n);
+  d.tx = m.alloc<double>(n); d.ty = m.alloc<double>(n); d.tz = m.alloc<double>(n);
+  d.omega = m.alloc<double>(n); d.age = m.alloc<double>(n);
+  d.ix = m.alloc<int>(n); d.iy = m.alloc<int>(n); d.iz = m.alloc<int>(n);
+  return m.err == cudaSuccess;
+}
+
+static bool alloc_stat(DevBuf& m, Stat& s, size_t n) {
+  s.r = m.alloc<double>(n); s.mass = m.alloc<double>(n);
+  s.type = m.alloc<int>(n); s.id = m.alloc<int>(n);
+  return m.err == cudaSuccess;
+}
+
+static int push_reps(sg_system* s) {
+  CU(s, cudaMemcpyAsync(s->reps, s->reps_h.data(), sizeof(Replica) * s->nrep, cudaMemcpyHostToDevice, s->stream));
+  return SG_OK;
+}
+static int push_clk(sg_system* s) {
+  CU(s, cudaMemcpyAsync(s->clk, s->clk_h.data(), sizeof(Clock) * s->nrep, cudaMemcpyHostToDevice, s->stream));
+  return SG_OK;
+}
+static int pull_clk(sg_system* s) {
+  CU(s, cudaMemcpyAsync(s->clk_h.data(), s->clk, sizeof(Clock) * s->nrep, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  return SG_OK;
+}
+
+extern "C" {
+
+const char* sg_error_string(int code) {
+  switch (code) {
+    case SG_OK: return "ok";
+    case SG_ERR_ARG: return "invalid argument";
+    case SG_ERR_CUDA: return "CUDA error";
+    case SG_ERR_NOMEM: return "device out of memory";
+    case SG_ERR_STATE: return "call out of order";
+    case SG_ERR_OVERFLOW: return "neighbour capacity exceeded";
+    case SG_ERR_NONFINITE: return "non-finite particle state";
+    case SG_ERR_UNSUPPORTED: return "configuration not supported by the GPU path";
+    case SG_ERR_TIMEOUT: return "bounded device wait gave up";
+    default: return "unknown error";
+  }
+}
+
+const char* sg_last_error(const sg_system* s) { return s ? s->last_error.c_str() : "null handle"; }
+
+int sg_set_device(int device) {
+  return cudaSetDevice(device) == cudaSuccess ? SG_OK : SG_ERR_CUDA;
+}
+int64_t sg_kernel_launches(const sg_system* s) { return s ? s->launches : 0; }
+
+int sg_create(int n_replicas, const int32_t* n_particles, int ntypes, sg_system** out) {
+  if (!out || n_replicas <= 0 || !n_particles || ntypes <= 0 || ntypes > SG_MAX_TYPES) return SG_ERR_ARG;
+  for (int r = 0; r < n_replicas; r++)
+    if (n_particles[r] < 0) return SG_ERR_ARG;
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return SG_ERR_CUDA;
+  sg_system* s = new sg_system();
+  cudaGetDevice(&s->device);
+  s->nrep = n_replicas;
+  s->ntypes = ntypes;
+  s->n.assign(n_particles, n_particles + n_replicas);
+  s->off.resize(n_replicas);
+  int slot = 0;
+  for (int r = 0; r < n_replicas; r++) {
+    s->off[r] = slot;
+    int padded = ((s->n[r] + BLOCK - 1) / BLOCK) * BLOCK;
+    if (padded == 0) padded = BLOCK;
+    s->rep_blk0_h.push_back(slot / BLOCK);
+    s->rep_nblk_h.push_back(padded / BLOCK);
+    for (int b = 0; b < padded / BLOCK; b++) s->blk_rep_h.push_back(r);
+    slot += padded;
+  }
+  s->slots = slot;
+  s->nblocks = slot / BLOCK;
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) { delete s; return SG_ERR_CUDA; }
+  DevBuf& m = s->mem;
+  s->blk_rep = m.alloc<int>(s->nblocks);
+  s->rep_blk0 = m.alloc<int>(n_replicas);
+  s->rep_nblk = m.alloc<int>(n_replicas);
+  s->reps = m.alloc<Replica>(n_replicas);
+  s->clk = m.alloc<Clock>(n_replicas);
+  bool ok = alloc_dyn(m, s->cur, s->slots) && alloc_dyn(m, s->alt, s->slots) &&
+            alloc_stat(m, s->st, s->slots) && alloc_stat(m, s->st_alt, s->slots);
+  s->rebuild = m.alloc<int>(n_replicas);
+  s->status = m.alloc<int>(1);
+  s->maxnb = m.alloc<int>(1);
+  s->epart = m.alloc<double>((size_t)(MAX_PAIR + MAX_ALIGN) * s->nblocks);
+  s->fire_part = m.alloc<double>((size_t)4 * s->nblocks);
+  s->alpha_mix = m.alloc<double>(n_replicas);
+  s->pcell = m.alloc<int>(s->slots);
+  s->tmp = m.alloc<int>(s->slots);
+  s->perm = m.alloc<int>(s->slots);
+  if (!ok || m.err != cudaSuccess) { m.free_all(); cudaStreamDestroy(s->stream); delete s; return SG_ERR_NOMEM; }
+  cudaMallocHost((void**)&s->rebuild_h, sizeof(int) * n_replicas);
+  cudaEventCreate(&s->ev_run0); cudaEventCreate(&s->ev_run1);
+  cudaEventCreate(&s->ev_k0); cudaEventCreate(&s->ev_k1);
+  cudaMemcpy(s->blk_rep, s->blk_rep_h.data(), sizeof(int) * s->nblocks, cudaMemcpyHostToDevice);
+  cudaMemcpy(s->rep_blk0, s->rep_blk0_h.data(), sizeof(int) * n_replicas, cudaMemcpyHostToDevice);
+  cudaMemcpy(s->rep_nblk, s->rep_nblk_h.data(), sizeof(int) * n_replicas, cudaMemcpyHostToDevice);
+  // defaults of Particle's ctor (particle.hpp:68-90) and of the input reader
+  std::vector<double> ones(s->slots, 1.0);
+  std::vector<int> ids(s->slots, 0), types(s->slots, 1);
+  for (int r = 0; r < n_replicas; r++)
+    for (int i = 0; i < s->n[r]; i++) ids[s->off[r] + i] = i;
+  cudaMemcpy(s->st.r, ones.data(), sizeof(double) * s->slots, cudaMemcpyHostToDevice);
+  cudaMemcpy(s->st.mass, ones.data(), sizeof(double) * s->slots, cudaMemcpyHostToDevice);
+  cudaMemcpy(s->st.id, ids.data(), sizeof(int) * s->slots, cudaMemcpyHostToDevice);
+  cudaMemcpy(s->st.type, types.data(), sizeof(int) * s->slots, cudaMemcpyHostToDevice);
+  s->reps_h.assign(n_replicas, Replica{});
+  s->clk_h.assign(n_replicas, Clock{});
+  for (int r = 0; r < n_replicas; r++) {
+    Replica& R = s->reps_h[r];
+    std::memset(&R, 0, sizeof(R));
+    R.off = s->off[r]; R.n = s->n[r];
+    R.Lx = R.Ly = R.Lz = 10.0;
+    R.xlo = R.ylo = R.zlo = -5.0; R.xhi = R.yhi = R.zhi = 5.0;
+    R.cnx = R.cny = R.cnz = 1; R.cwx = R.cwy = R.cwz = 10.0;
+    Clock& C = s->clk_h[r];
+    std::memset(&C, 0, sizeof(C));
+    C.fire_conv_step = -1;
+  }
+  s->prog.ntypes = ntypes;
+  for (int k = 0; k < 3; k++) s->uploaded_N[k].assign((size_t)s->slots, 0.0);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) { m.free_all(); cudaStreamDestroy(s->stream); delete s; return SG_ERR_CUDA; }
+  if (push_reps(s) != SG_OK || push_clk(s) != SG_OK) { m.free_all(); delete s; return SG_ERR_CUDA; }
+  *out = s;
+  return SG_OK;
+}
+
+int sg_destroy(sg_system* s) {
+  if (!s) return SG_ERR_ARG;
+  cudaStreamSynchronize(s->stream);
+  s->mem.free_all();
+  for (double* t : s->tables) cudaFree(t);
+  if (s->rebuild_h) cudaFreeHost(s->rebuild_h);
+  for (cudaEvent_t ev : {s->ev_run0, s->ev_run1, s->ev_k0, s->ev_k1})
+    if (ev) cudaEventDestroy(ev);
+  cudaStreamDestroy(s->stream);
+  delete s;
+  return SG_OK;
+}
+
+int sg_set_box(sg_system* s, int replica, double lx, double ly, double lz, int periodic) {
+  if (!s || replica < 0 || replica >= s->nrep || !(lx > 0.0) || !(ly > 0.0) || !(lz > 0.0))
+    return fail(s, SG_ERR_ARG, "sg_set_box: bad replica or box size");
+  if (s->has_nlist) return fail(s, SG_ERR_STATE, "sg_set_box: box must be set before the neighbour list");
+  Replica& R = s->reps_h[replica];
+  R.Lx = lx; R.Ly = ly; R.Lz = lz;
+  R.xlo = -0.5 * lx; R.xhi = 0.5 * lx;
+  R.ylo = -0.5 * ly; R.yhi = 0.5 * ly;
+  R.zlo = -0.5 * lz; R.zhi = 0.5 * lz;
+  R.periodic = periodic ? 1 : 0;
+  return push_reps(s);
+}
+
+int sg_set_timestep(sg_system* s, double dt) {
+  if (!s || !(dt > 0.0)) return fail(s, SG_ERR_ARG, "sg_set_timestep: dt must be > 0");
+  s->dt_global = dt;
+  return SG_OK;
+}
+
+// host-side id -> slot map of one replica (slots are permuted by rebuilds)
+static int slot_map(sg_system* s, int replica, std::vector<int>& slot_of_id) {
+  const int n = s->n[replica], off = s->off[replica];
+  std::vector<int> ids(n);
+  CU(s, cudaMemcpyAsync(ids.data(), s->st.id + off, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  slot_of_id.assign(n, -1);
+  for (int k = 0; k < n; k++) {
+    if (ids[k] < 0 || ids[k] >= n) return fail(s, SG_ERR_STATE, "corrupt id map");
+    slot_of_id[ids[k]] = k;
+  }
+  return SG_OK;
+}
+
+static int field_ptr(sg_system* s, const char* field, void** p, bool* is_int, int* nfield) {
+  *nfield = -1;
+  for (int i = 0; i < kNumDynDouble; i++)
+    if (std::strcmp(field, kDoubleFields[i]) == 0) { *p = dyn_field(s->cur, i); *is_int = false; *nfield = i; return SG_OK; }
+  if (!std::strcmp(field, "radius")) { *p = s->st.r; *is_int = false; return SG_OK; }
+  if (!std::strcmp(field, "mass")) { *p = s->st.mass; *is_int = false; return SG_OK; }
+  if (!std::strcmp(field, "type")) { *p = s->st.type; *is_int = true; return SG_OK; }
+  if (!std::strcmp(field, "ix")) { *p = s->cur.ix; *is_int = true; return SG_OK; }
+  if (!std::strcmp(field, "iy")) { *p = s->cur.iy; *is_int = true; return SG_OK; }
+  if (!std::strcmp(field, "iz")) { *p = s->cur.iz; *is_int = true; return SG_OK; }
+  if (!std::strcmp(field, "Nx") || !std::strcmp(field, "Ny") || !std::strcmp(field, "Nz")) {
+    *p = nullptr; *is_int = false; return SG_OK;
+  }
+  return fail(s, SG_ERR_ARG, std::string("unknown particle field '") + field + "'");
+}
+
+int sg_upload(sg_system* s, int replica, const char* field, const void* host) {
+  if (!s || !field || !host || replica < 0 || replica >= s->nrep) return fail(s, SG_ERR_ARG, "sg_upload: bad argument");
+  void* dp; bool is_int; int nf;
+  int rc = field_ptr(s, field, &dp, &is_int, &nf);
+  if (rc) return rc;
+  const int n = s->n[replica], off = s->off[replica];
+  std::vector<int> slot_of_id;
+  if ((rc = slot_map(s, replica, slot_of_id))) return rc;
+  if (!dp) {  // surface normal: kept on the host, used where no constraint sets it
+    int c = field[1] - 'x';
+    const double* h = (const double*)host;
+    for (int i = 0; i < n; i++) s->uploaded_N[c][off + i] = h[i];
+    return SG_OK;
+  }
+  if (is_int) {
+    std::vector<int> buf(n);
+    const int* h = (const int*)host;
+    for (int i = 0; i < n; i++) buf[slot_of_id[i]] = h[i];
+    if (!std::strcmp(field, "type"))
+      for (int i = 0; i < n; i++)
+        if (h[i] < 1 || h[i] > s->ntypes) return fail(s, SG_ERR_ARG, "particle type outside 1..ntypes");
+    CU(s, cudaMemcpyAsync((int*)dp + off, buf.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s->stream));
+  } else {
+    std::vector<double> buf(n);
+    const double* h = (const double*)host;
+    for (int i = 0; i < n; i++) buf[slot_of_id[i]] = h[i];
+    CU(s, cudaMemcpyAsync((double*)dp + off, buf.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+  }
+  CU(s, cudaStreamSynchronize(s->stream));
+  s->e1_applied = false;
+  return SG_OK;
+}
+
+int sg_download(sg_system* s, int replica, const char* field, void* host) {
+  if (!s || !field || !host || replica < 0 || replica >= s->nrep) return fail(s, SG_ERR_ARG, "sg_download: bad argument");
+  void* dp; bool is_int; int nf;
+  int rc = field_ptr(s, field, &dp, &is_int, &nf);
+  if (rc) return rc;
+  const int n = s->n[replica], off = s->off[replica];
+  std::vector<int> ids(n);
+  CU(s, cudaMemcpyAsync(ids.data(), s->st.id + off, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+  if (!dp) {
+    // surface normal of the last constraint that sets one (plane: (0,0,1),
+    // sphere: x/R as in constraint_sphere.hpp:76)
+    const int comp = field[1] - 'x';
+    std::vector<double> X(n), Y(n), Z(n);
+    CU(s, cudaMemcpyAsync(X.data(), s->cur.x + off, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+    CU(s, cudaMemcpyAsync(Y.data(), s->cur.y + off, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+    CU(s, cudaMemcpyAsync(Z.data(), s->cur.z + off, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+    CU(s, cudaStreamSynchronize(s->stream));
+    double* h = (double*)host;
+    for (int i = 0; i < n; i++) h[i] = s->uploaded_N[comp][off + i];
+    for (int c = 0; c < s->prog.ncons; c++) {
+      if (s->prog.cons[c].kind == CONS_PLANE)
+        for (int i = 0; i < n; i++) h[i] = comp == 2 ? 1.0 : 0.0;
+      else if (s->prog.cons[c].kind == CONS_SPHERE) {
+        double Rs = s->reps_h[replica].cons_p[c];
+        for (int k = 0; k < n; k++) h[ids[k]] = (comp == 0 ? X[k] : comp == 1 ? Y[k] : Z[k]) / Rs;
+      }
+    }
+    return SG_OK;
+  }
+  if (is_int) {
+    std::vector<int> buf(n);
+    CU(s, cudaMemcpyAsync(buf.data(), (int*)dp + off, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+    CU(s, cudaStreamSynchronize(s->stream));
+    int* h = (int*)host;
+    for (int k = 0; k < n; k++) h[ids[k]] = buf[k];
+  } else {
+    std::vector<double> buf(n);
+    CU(s, cudaMemcpyAsync(buf.data(), (double*)dp + off, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+    CU(s, cudaStreamSynchronize(s->stream));
+    double* h = (double*)host;
+    for (int k = 0; k < n; k++) h[ids[k]] = buf[k];
+  }
+  return SG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// neighbour list
+// ---------------------------------------------------------------------------
+static int nlist_alloc(sg_system* s, int cap) {
+  DevBuf& m = s->mem;
+  m.release(s->nl.nb); m.release(s->nl.cnt); m.release(s->nl.lo);
+  s->nl.cap = cap;
+  s->nl.stride = s->slots;
+  s->nl.nb = m.alloc<int>((size_t)cap * s->slots);
+  s->nl.cnt = m.alloc<int>(s->slots);
+  s->nl.lo = m.alloc<int>(s->slots);
+  if (!s->nl.ox) { s->nl.ox = m.alloc<double>(s->slots); s->nl.oy = m.alloc<double>(s->slots); s->nl.oz = m.alloc<double>(s->slots); }
+  if (m.err != cudaSuccess) { m.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "neighbour list allocation failed"); }
+  return SG_OK;
+}
+
+// builds the lists of the replicas flagged in s->rebuild (device)
+static int rebuild_flagged(sg_system* s) {
+  const int nb = s->nblocks;
+  for (int attempt = 0; attempt < 4; attempt++) {
+    CU(s, cudaMemsetAsync(s->cell_cnt, 0, sizeof(int) * (size_t)s->ncell_total, s->stream));
+    CU(s, cudaMemsetAsync(s->cell_fill, 0, sizeof(int) * (size_t)s->ncell_total, s->stream));
+    CU(s, cudaMemsetAsync(s->status, 0, sizeof(int), s->stream));
+    CU(s, cudaMemsetAsync(s->maxnb, 0, sizeof(int), s->stream));
+    k_rb_bin<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->pcell, s->cell_cnt);
+    LAUNCH_CHECK(s);
+    const int nscan = (s->ncell_total + SCAN_TILE - 1) / SCAN_TILE;
+    k_scan_a<<<nscan, SCAN_T, 0, s->stream>>>(s->cell_cnt, s->ncell_total, s->scan_bsum);
+    LAUNCH_CHECK(s);
+    k_scan_b<<<1, SCAN_T, 0, s->stream>>>(s->scan_bsum, nscan);
+    LAUNCH_CHECK(s);
+    k_scan_c<<<nscan, SCAN_T, 0, s->stream>>>(s->cell_cnt, s->ncell_total, s->scan_bsum, s->cell_start);
+    LAUNCH_CHECK(s);
+    k_rb_scatter<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->pcell, s->cell_start, s->cell_fill, s->tmp);
+    LAUNCH_CHECK(s);
+    k_rb_rank<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->pcell, s->cell_start, s->cell_cnt,
+                                          s->tmp, s->st.id, s->perm);
+    LAUNCH_CHECK(s);
+    k_rb_gather<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->perm, s->cur, s->alt, s->st, s->st_alt);
+    LAUNCH_CHECK(s);
+    k_rb_copyback<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->alt, s->cur, s->st_alt, s->st);
+    LAUNCH_CHECK(s);
+    k_rb_build<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->st, s->nl, s->pcell,
+                                           s->cell_start, s->cell_cnt, s->status, s->maxnb);
+    LAUNCH_CHECK(s);
+    int st = 0, mx = 0;
+    CU(s, cudaMemcpyAsync(&st, s->status, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CU(s, cudaMemcpyAsync(&mx, s->maxnb, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CU(s, cudaStreamSynchronize(s->stream));
+    if (!(st & ST_OVERFLOW)) {
+      s->builds_run++;
+      s->maxnb_seen = std::max(s->maxnb_seen, mx);
+      return SG_OK;
+    }
+    if (mx > NB_LOCAL) return fail(s, SG_ERR_OVERFLOW, "more than " + std::to_string(NB_LOCAL) + " neighbours within rcut+pad");
+    int cap = std::max(mx + 8, s->nl.cap * 2);
+    int rc = nlist_alloc(s, cap);
+    if (rc) return rc;
+  }
+  return fail(s, SG_ERR_OVERFLOW, "neighbour list did not fit after regrowth");
+}
+
+int sg_set_nlist(sg_system* s, double rcut, double pad) {
+  if (!s || !(rcut > 0.0) || !(pad >= 0.0)) return fail(s, SG_ERR_ARG, "sg_set_nlist: rcut must be > 0, pad >= 0");
+  const double cut = rcut + pad;
+  s->rcut = rcut; s->pad = pad;
+  int cell_off = 0;
+  for (int r = 0; r < s->nrep; r++) {
+    Replica& R = s->reps_h[r];
+    // NeighbourList ctor, neighbour_list.hpp:138-150
+    R.use_cell = (R.Lx > 2.0 * cut && R.Ly > 2.0 * cut && R.Lz > 2.0 * cut) ? 1 : 0;
+    R.cnx = std::max(1, (int)(R.Lx / cut));
+    R.cny = std::max(1, (int)(R.Ly / cut));
+    R.cnz = std::max(1, (int)(R.Lz / cut));
+    R.cwx = R.Lx / (double)R.cnx; R.cwy = R.Ly / (double)R.cny; R.cwz = R.Lz / (double)R.cnz;
+    R.ncell = R.cnx * R.cny * R.cnz;
+    R.cell_off = cell_off;
+    cell_off += R.ncell;
+    R.cut2 = cut * cut;
+    R.pad = pad;
+  }
+  s->ncell_total = cell_off;
+  DevBuf& m = s->mem;
+  m.release(s->cell_cnt); m.release(s->cell_start); m.release(s->cell_fill); m.release(s->scan_bsum);
+  s->cell_cnt = m.alloc<int>(cell_off);
+  s->cell_start = m.alloc<int>(cell_off);
+  s->cell_fill = m.alloc<int>(cell_off);
+  s->scan_bsum = m.alloc<int>((cell_off + SCAN_TILE - 1) / SCAN_TILE + 1);
+  if (m.err != cudaSuccess) { m.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "cell list allocation failed"); }
+  int rc = push_reps(s);
+  if (rc) return rc;
+  if (!s->nl.nb && (rc = nlist_alloc(s, 32))) return rc;
+  s->has_nlist = true;
+  return sg_build_nlist(s);
+}
+
+int sg_build_nlist(sg_system* s) {
+  if (!s) return SG_ERR_ARG;
+  if (!s->has_nlist) return fail(s, SG_ERR_STATE, "no neighbour list configured");
+  for (int r = 0; r < s->nrep; r++) s->rebuild_h[r] = 1;
+  CU(s, cudaMemcpyAsync(s->rebuild, s->rebuild_h, sizeof(int) * s->nrep, cudaMemcpyHostToDevice, s->stream));
+  int rc = rebuild_flagged(s);
+  if (rc) return rc;
+  CU(s, cudaMemsetAsync(s->rebuild, 0, sizeof(int) * s->nrep, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  return SG_OK;
+}
+
+int sg_get_pairs(sg_system* s, int replica, int32_t* out_i, int32_t* out_j, int64_t cap, int64_t* n_pairs) {
+  if (!s || replica < 0 || replica >= s->nrep || !n_pairs) return fail(s, SG_ERR_ARG, "sg_get_pairs: bad argument");
+  if (!s->has_nlist) return fail(s, SG_ERR_STATE, "no neighbour list");
+  const int n = s->n[replica], off = s->off[replica], C = s->nl.cap;
+  std::vector<int> cnt(n), lo(n), ids(n), nb((size_t)C * n);
+  CU(s, cudaMemcpyAsync(cnt.data(), s->nl.cnt + off, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaMemcpyAsync(lo.data(), s->nl.lo + off, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaMemcpyAsync(ids.data(), s->st.id + off, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+  for (int q = 0; q < C; q++)
+    CU(s, cudaMemcpyAsync(nb.data() + (size_t)q * n, s->nl.nb + (size_t)q * s->nl.stride + off, sizeof(int) * n,
+                          cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  // emit list[i] for i ascending: the upper part of particle i's list
+  std::vector<int> slot_of_id(n);
+  for (int k = 0; k < n; k++) slot_of_id[ids[k]] = k;
+  int64_t total = 0;
+  for (int i = 0; i < n; i++) {
+    int k = slot_of_id[i];
+    for (int q = lo[k]; q < cnt[k]; q++) {
+      if (total < cap && out_i && out_j) { out_i[total] = i; out_j[total] = ids[nb[(size_t)q * n + k] - off]; }
+      total++;
+    }
+  }
+  *n_pairs = total;
+  return total > cap ? fail(s, SG_ERR_ARG, "sg_get_pairs: capacity too small") : SG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// components
+// ---------------------------------------------------------------------------
+static Value make_value(const double* v) {
+  Value r{};
+  if (!v) { r.kind = 0; r.min_val = 0.0; r.max_val = 1.0; r.steps = 1000; r.dv = 0.0; return r; }
+  r.kind = (int)v[0]; r.min_val = v[1]; r.max_val = v[2]; r.steps = (int)v[3];
+  r.dv = (r.max_val - r.min_val) / (double)r.steps;
+  return r;
+}
+
+static double* upload_table(sg_system* s, const std::vector<double>& t) {
+  double* d = nullptr;
+  if (cudaMalloc(&d, sizeof(double) * std::max<size_t>(1, t.size())) != cudaSuccess) return nullptr;
+  cudaMemcpy(d, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice);
+  s->tables.push_back(d);
+  return d;
+}
+
+int sg_add_pair(sg_system* s, int kind, const double* global, const double* table, int use_radii,
+                int phase_in, int shifted, int has_pp, const double* phase_value) {
+  if (!s || kind < SG_PAIR_SOFT || kind > SG_PAIR_GAUSSIAN || !global) return fail(s, SG_ERR_ARG, "sg_add_pair: bad kind");
+  Program& P = s->prog;
+  if (P.npair >= MAX_PAIR) return fail(s, SG_ERR_ARG, "too many pair potentials");
+  for (int c = 0; c < P.npair; c++)
+    if (P.pair[c].kind == kind) return fail(s, SG_ERR_ARG, "pair potential already defined");
+  const size_t nt = (size_t)s->ntypes * s->ntypes * PAIR_NPARAM;
+  std::vector<double> t(nt);
+  for (size_t i = 0; i < nt; i++) t[i] = table ? table[i] : global[i % PAIR_NPARAM];
+  PairComp& C = P.pair[P.npair];
+  C.kind = kind; C.use_radii = use_radii; C.phase_in = phase_in; C.shifted = shifted; C.has_pp = has_pp;
+  C.phase = make_value(phase_value);
+  C.table = upload_table(s, t);
+  if (!C.table) return fail(s, SG_ERR_NOMEM, "table allocation failed");
+  for (int r = 0; r < s->nrep; r++)
+    for (int i = 0; i < PAIR_NPARAM; i++) s->reps_h[r].pair_g[P.npair][i] = global[i];
+  P.npair++;
+  return push_reps(s);
+}
+
+int sg_add_align(sg_system* s, int kind, double J, double rcut, const double* table, int has_pp) {
+  if (!s || kind < SG_ALIGN_POLAR || kind > SG_ALIGN_VICSEK) return fail(s, SG_ERR_ARG, "sg_add_align: bad kind");
+  Program& P = s->prog;
+  if (P.nalign >= MAX_ALIGN) return fail(s, SG_ERR_ARG, "too many aligners");
+  const size_t nt = (size_t)s->ntypes * s->ntypes * 2;
+  std::vector<double> t(nt);
+  for (size_t i = 0; i < nt; i++) t[i] = table ? table[i] : ((i & 1) ? rcut : J);
+  AlignComp& C = P.align[P.nalign];
+  C.kind = kind; C.has_pp = has_pp;
+  C.table = upload_table(s, t);
+  if (!C.table) return fail(s, SG_ERR_NOMEM, "table allocation failed");
+  for (int r = 0; r < s->nrep; r++) { s->reps_h[r].align_J[P.nalign] = J; s->reps_h[r].align_rcut[P.nalign] = rcut; }
+  P.nalign++;
+  return push_reps(s);
+}
+
+int sg_add_external(sg_system* s, int kind, double alpha, const double* type_alpha, int has_params) {
+  if (!s || kind != SG_EXT_SELF_PROPULSION) return fail(s, SG_ERR_ARG, "sg_add_external: bad kind");
+  Program& P = s->prog;
+  if (P.next >= MAX_EXT) return fail(s, SG_ERR_ARG, "too many external potentials");
+  std::vector<double> t(s->ntypes);
+  for (int i = 0; i < s->ntypes; i++) t[i] = type_alpha ? type_alpha[i] : alpha;
+  ExtComp& C = P.ext[P.next];
+  C.kind = kind; C.has_params = has_params;
+  C.type_alpha = upload_table(s, t);
+  for (int r = 0; r < s->nrep; r++) s->reps_h[r].ext_alpha[P.next] = alpha;
+  P.next++;
+  return push_reps(s);
+}
+
+int sg_add_constraint(sg_system* s, int kind, const double* params) {
+  if (!s || kind < SG_CONS_NONE || kind > SG_CONS_SPHERE) return fail(s, SG_ERR_ARG, "sg_add_constraint: bad kind");
+  Program& P = s->prog;
+  if (P.ncons >= MAX_CONS) return fail(s, SG_ERR_ARG, "too many constraints");
+  if (params && params[4] != 0.0 && params[4] != 1.0)
+    return fail(s, SG_ERR_UNSUPPORTED, "constraint rescale is not supported by the GPU path");
+  ConsComp& C = P.cons[P.ncons];
+  C.kind = kind;
+  C.unlimited = (kind == CONS_PLANE && params) ? (int)params[1] : 0;
+  for (int r = 0; r < s->nrep; r++)
+    s->reps_h[r].cons_p[P.ncons] = params ? params[0] : (kind == CONS_SPHERE ? 1.0 : 0.0);
+  P.ncons++;
+  int rc = push_reps(s);
+  if (rc) return rc;
+  return sg_enforce(s);  // samos.cpp:518-522
+}
+
+int sg_add_integrator(sg_system* s, int kind, const double* params, const double* temp) {
+  if (!s || !params || kind < SG_INT_BROWNIAN || kind > SG_INT_FIRE) return fail(s, SG_ERR_ARG, "sg_add_integrator: bad kind");
+  Program& P = s->prog;
+  if (P.ninteg >= MAX_INTEG) return fail(s, SG_ERR_ARG, "too many integrators");
+  if (!(params[0] > 0.0)) return fail(s, SG_ERR_ARG, "integrator step size has to be larger than 0");
+  IntegComp& C = P.integ[P.ninteg];
+  C.kind = kind;
+  C.method = kind == INT_LANGEVIN ? (int)params[10] : 0;
+  C.nematic = (kind == INT_BROWNIAN || kind == INT_BROWNIAN_ALIGN) ? (params[6] != 0.0) : 0;
+  C.velocity = kind == INT_BROWNIAN ? (params[8] != 0.0) : 0;
+  C.temp = make_value(temp);
+  const int c = P.ninteg;
+  for (int r = 0; r < s->nrep; r++) {
+    for (int i = 0; i < INT_NPARAM; i++) s->reps_h[r].integ_p[c][i] = params[i];
+    s->reps_h[r].seed[c] = (uint32_t)(int32_t)params[5];
+    s->clk_h[r].ctr[c] = 0;
+  }
+  P.ninteg++;
+  int rc = push_reps(s);
+  if (rc) return rc;
+  if (kind == INT_FIRE) {
+    for (int r = 0; r < s->nrep; r++) {
+      Clock& K = s->clk_h[r];
+      K.fire_dt = params[0]; K.fire_alpha = params[1]; K.fire_old_e = 1e15;
+      K.fire_last_neg = 0; K.fire_converged = 0; K.fire_conv_step = -1;
+    }
+  }
+  if (kind == INT_LANGEVIN && C.method == LANGEVIN_BBK) {
+    // integrator_langevin.hpp:103-111: 3 draws per particle at construction
+    if (!s->Rn) s->Rn = s->mem.alloc<double>((size_t)3 * s->slots);
+    std::vector<double> h((size_t)3 * s->slots, 0.0);
+    for (int r = 0; r < s->nrep; r++) {
+      uint32_t seed = s->reps_h[r].seed[c];
+      for (int i = 0; i < s->n[r]; i++)
+        for (int d = 0; d < 3; d++) {
+          // same stream as the device: counter = 3 i + d
+          h[(size_t)3 * (s->off[r] + i) + d] = noise_gauss(seed, (uint64_t)3 * i + d);
+        }
+      s->clk_h[r].ctr[c] = (uint64_t)3 * s->n[r];
+    }
+    CU(s, cudaMemcpy(s->Rn, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  }
+  return push_clk(s);
+}
+
+int sg_set_replica_param(sg_system* s, int replica, int cls, int comp, int slot, double value) {
+  if (!s || replica < 0 || replica >= s->nrep) return fail(s, SG_ERR_ARG, "sg_set_replica_param: bad replica");
+  Replica& R = s->reps_h[replica];
+  switch (cls) {
+    case 0: if (comp >= s->prog.npair || slot < 0 || slot >= PAIR_NPARAM) return SG_ERR_ARG; R.pair_g[comp][slot] = value; break;
+    case 1:
+      if (comp >= s->prog.nalign || slot < 0 || slot > 1) return SG_ERR_ARG;
+      if (slot == 0) R.align_J[comp] = value; else R.align_rcut[comp] = value;
+      break;
+    case 2: if (comp >= s->prog.next) return SG_ERR_ARG; R.ext_alpha[comp] = value; break;
+    case 3: if (comp >= s->prog.ncons) return SG_ERR_ARG; R.cons_p[comp] = value; break;
+    case 4:
+      if (comp >= s->prog.ninteg || slot < 0 || slot >= INT_NPARAM) return SG_ERR_ARG;
+      R.integ_p[comp][slot] = value;
+      if (slot == 5) R.seed[comp] = (uint32_t)(int32_t)value;
+      if (slot == 0 && s->prog.integ[comp].kind == INT_FIRE) { s->clk_h[replica].fire_dt = value; push_clk(s); }
+      if (slot == 1 && s->prog.integ[comp].kind == INT_FIRE) { s->clk_h[replica].fire_alpha = value; push_clk(s); }
+      break;
+    default: return fail(s, SG_ERR_ARG, "sg_set_replica_param: bad class");
+  }
+  return push_reps(s);
+}
+
+// ---------------------------------------------------------------------------
+// execution
+// ---------------------------------------------------------------------------
+int sg_enforce(sg_system* s) {
+  if (!s) return SG_ERR_ARG;
+  k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st);
+  LAUNCH_CHECK(s);
+  CU(s, cudaStreamSynchronize(s->stream));
+  return SG_OK;
+}
+
+static int launch_force(sg_system* s, double dt, bool fire_dt, bool with_pair, bool with_align, bool energy) {
+  if (energy)
+    k_force<true><<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, s->nl, dt,
+                                                       fire_dt, with_pair, with_align, s->epart, s->nblocks);
+  else
+    k_force<false><<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, s->nl, dt,
+                                                        fire_dt, with_pair, with_align, s->epart, s->nblocks);
+  LAUNCH_CHECK(s);
+  return SG_OK;
+}
+
+int sg_compute(sg_system* s, double dt) {
+  if (!s) return SG_ERR_ARG;
+  if (!s->has_nlist && (s->prog.npair + s->prog.nalign) > 0) return fail(s, SG_ERR_STATE, "pair terms need a neighbour list");
+  if (!s->nl.nb) { int rc = nlist_alloc(s, 1); if (rc) return rc; }
+  int rc = launch_force(s, dt, false, true, true, true);
+  if (rc) return rc;
+  CU(s, cudaStreamSynchronize(s->stream));
+  return SG_OK;
+}
+
+static bool fused_program(const Program& P) {
+  for (int c = 0; c < P.ninteg; c++)
+    if (P.integ[c].kind != INT_BROWNIAN && P.integ[c].kind != INT_BROWNIAN_POS && P.integ[c].kind != INT_BROWNIAN_ALIGN)
+      return false;
+  return true;
+}
+
+// one unfused integration step (reference phase order, in place)
+static int step_unfused(sg_system* s, bool energy, bool driver) {
+  const int nb = s->nblocks;
+  k_enforce<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st);
+  LAUNCH_CHECK(s);
+  int rc = launch_force(s, s->dt_global, false, true, true, energy);
+  if (rc) return rc;
+  for (int c = 0; c < s->prog.ninteg; c++) {
+    const IntegComp& ic = s->prog.integ[c];
+    if (ic.kind == INT_LANGEVIN) {
+      k_langevin_a<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, c, s->Rn);
+      LAUNCH_CHECK(s);
+      if ((rc = launch_force(s, s->reps_h[0].integ_p[c][0], false, true, false, true))) return rc;
+      k_langevin_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, c, s->Rn);
+      LAUNCH_CHECK(s);
+    } else if (ic.kind == INT_FIRE) {
+      k_fire_a<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st);
+      LAUNCH_CHECK(s);
+      if ((rc = launch_force(s, 0.0, true, true, true, true))) return rc;
+      k_fire_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, s->fire_part, nb);
+      LAUNCH_CHECK(s);
+      k_fire_c<<<(s->nrep + 127) / 128, 128, 0, s->stream>>>(s->prog, s->reps, s->clk, s->rep_blk0, s->rep_nblk,
+                                                             s->fire_part, s->epart, nb, s->nrep, c, driver ? 1 : 0,
+                                                             s->alpha_mix);
+      LAUNCH_CHECK(s);
+      k_fire_d<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alpha_mix);
+      LAUNCH_CHECK(s);
+    } else {
+      return fail(s, SG_ERR_UNSUPPORTED, "mixing Brownian-family integrators with Langevin/FIRE is not supported");
+    }
+  }
+  if (s->has_nlist) {
+    k_skin<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->nl, s->rebuild, s->status);
+    LAUNCH_CHECK(s);
+  }
+  return SG_OK;
+}
+
+static int step_fused(sg_system* s, bool apply_e1, bool energy) {
+  const int nb = s->nblocks;
+  if (s->profile) CU(s, cudaEventRecord(s->ev_k0, s->stream));
+  if (energy)
+    k_step_brownian<true><<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alt, s->st, s->nl,
+                                                       s->rebuild, s->status, s->dt_global, apply_e1 ? 1 : 0,
+                                                       s->epart, nb);
+  else
+    k_step_brownian<false><<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alt, s->st, s->nl,
+                                                        s->rebuild, s->status, s->dt_global, apply_e1 ? 1 : 0,
+                                                        s->epart, nb);
+  LAUNCH_CHECK(s);
+  if (s->profile) CU(s, cudaEventRecord(s->ev_k1, s->stream));
+  std::swap(s->cur, s->alt);
+  return SG_OK;
+}
+
+static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool driver, int64_t* conv_out) {
+  if (!s || steps < 0) return SG_ERR_ARG;
+  if (s->prog.ninteg == 0) return fail(s, SG_ERR_STATE, "Integrator has not been defined");
+  if (s->prog.ncons == 0) return fail(s, SG_ERR_STATE, "Constraint has not been defined");
+  if (!(s->dt_global > 0.0)) return fail(s, SG_ERR_STATE, "timestep has not been set");
+  const bool needs_nl = (s->prog.npair + s->prog.nalign) > 0;
+  if (needs_nl && !s->has_nlist) return fail(s, SG_ERR_STATE, "pair terms need a neighbour list");
+  if (!s->nl.nb) { int rc = nlist_alloc(s, 1); if (rc) return rc; }
+  const bool fused = fused_program(s->prog);
+  const int64_t launches0 = s->launches, builds0 = s->builds_run;
+  double kernel_ms = 0.0;
+  int64_t kernels_timed = 0;
+  CU(s, cudaEventRecord(s->ev_run0, s->stream));
+  CU(s, cudaMemsetAsync(s->status, 0, sizeof(int), s->stream));
+  // run-step counters restart with every `run` (samos.cpp:881)
+  {
+    int rc = pull_clk(s);
+    if (rc) return rc;
+    for (int r = 0; r < s->nrep; r++) s->clk_h[r].run_step = 0;
+    if ((rc = push_clk(s))) return rc;
+  }
+  int64_t done = 0;
+  for (int64_t t = 0; t <= steps; t++) {
+    const bool last = (t == steps);
+    int rc;
+    if (fused) {
+      if (!s->e1_applied) {
+        k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st);
+        LAUNCH_CHECK(s);
+      }
+      rc = step_fused(s, !last, last);
+      s->e1_applied = !last;
+    } else {
+      rc = step_unfused(s, last, driver);
+      s->e1_applied = false;
+    }
+    if (rc) return rc;
+    k_tail<<<(s->nrep + 127) / 128, 128, 0, s->stream>>>(s->prog, s->reps, s->clk, s->nrep);
+    LAUNCH_CHECK(s);
+    done++;
+    if (s->profile && fused) {
+      CU(s, cudaEventSynchronize(s->ev_k1));
+      float ms = 0.f;
+      CU(s, cudaEventElapsedTime(&ms, s->ev_k0, s->ev_k1));
+      kernel_ms += ms;
+      kernels_timed++;
+    }
+    if (needs_nl) {
+      CU(s, cudaMemcpyAsync(s->rebuild_h, s->rebuild, sizeof(int) * s->nrep, cudaMemcpyDeviceToHost, s->stream));
+      CU(s, cudaStreamSynchronize(s->stream));
+      bool any = false;
+      for (int r = 0; r < s->nrep; r++) any = any || s->rebuild_h[r];
+      if (any) {
+        if ((rc = rebuild_flagged(s))) return rc;
+        CU(s, cudaMemsetAsync(s->rebuild, 0, sizeof(int) * s->nrep, s->stream));
+      }
+    }
+    if (driver) {
+      if ((rc = pull_clk(s))) return rc;
+      bool all = true;
+      for (int r = 0; r < s->nrep; r++) all = all && s->clk_h[r].fire_conv_step >= 0;
+      if (all) break;
+    }
+  }
+  CU(s, cudaEventRecord(s->ev_run1, s->stream));
+  int st = 0;
+  CU(s, cudaMemcpyAsync(&st, s->status, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  float run_ms = 0.f;
+  CU(s, cudaEventElapsedTime(&run_ms, s->ev_run0, s->ev_run1));
+  int rc = pull_clk(s);
+  if (rc) return rc;
+  if (conv_out)
+    for (int r = 0; r < s->nrep; r++) conv_out[r] = s->clk_h[r].fire_conv_step >= 0 ? s->clk_h[r].fire_conv_step + 1 : -1;
+  if (stats) {
+    stats->steps_done = done;
+    stats->nlist_builds = s->builds_run - builds0;
+    stats->kernel_launches = s->launches - launches0;
+    stats->max_neighbours = s->maxnb_seen;
+    stats->status = st;
+    stats->device_ms = run_ms;
+    stats->step_kernel_ms = kernel_ms;
+    stats->step_kernels = kernels_timed;
+  }
+  if (st & ST_NONFINITE) return fail(s, SG_ERR_NONFINITE, "non-finite particle position detected");
+  return SG_OK;
+}
+
+int sg_run(sg_system* s, int64_t steps, sg_run_stats* stats) { return run_impl(s, steps, stats, false, nullptr); }
+
+int sg_minimize(sg_system* s, int64_t max_steps, int64_t* converged, sg_run_stats* stats) {
+  if (!s) return SG_ERR_ARG;
+  bool has_fire = false;
+  for (int c = 0; c < s->prog.ninteg; c++) has_fire = has_fire || s->prog.integ[c].kind == INT_FIRE;
+  if (!has_fire) return fail(s, SG_ERR_STATE, "sg_minimize needs a FIRE integrator");
+  int rc = pull_clk(s);
+  if (rc) return rc;
+  for (int r = 0; r < s->nrep; r++) s->clk_h[r].fire_conv_step = -1;
+  rc = push_clk(s);
+  if (rc) return rc;
+  return run_impl(s, max_steps, stats, true, converged);
+}
+
+int sg_set_profiling(sg_system* s, int on) {
+  if (!s) return SG_ERR_ARG;
+  s->profile = on ? 1 : 0;
+  return SG_OK;
+}
+
+int sg_energy(sg_system* s, int replica, int cls, int comp, double* out) {
+  if (!s || !out || replica < 0 || replica >= s->nrep || cls < 0 || cls > 1) return fail(s, SG_ERR_ARG, "sg_energy: bad argument");
+  if ((cls == 0 && comp >= s->prog.npair) || (cls == 1 && comp >= s->prog.nalign) || comp < 0)
+    return fail(s, SG_ERR_ARG, "sg_energy: no such component");
+  const int row = cls == 0 ? comp : MAX_PAIR + comp;
+  const int b0 = s->rep_blk0_h[replica], nb = s->rep_nblk_h[replica];
+  std::vector<double> h(nb);
+  CU(s, cudaMemcpyAsync(h.data(), s->epart + (size_t)row * s->nblocks + b0, sizeof(double) * nb, cudaMemcpyDeviceToHost,
+                        s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  double e = 0.0;
+  for (int b = 0; b < nb; b++) e += h[b];
+  *out = e;
+  return SG_OK;
+}
+
+int sg_fire_state(sg_system* s, int replica, double* out5) {
+  if (!s || !out5 || replica < 0 || replica >= s->nrep) return SG_ERR_ARG;
+  int rc = pull_clk(s);
+  if (rc) return rc;
+  const Clock& C = s->clk_h[replica];
+  out5[0] = C.fire_dt; out5[1] = C.fire_alpha; out5[2] = C.fire_last_neg;
+  out5[3] = C.fire_converged; out5[4] = C.fire_old_e;
+  return SG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,922 @@
+// sg_kernels.cuh -- sm_100a kernels of the SAMoS hot path.
+//
+// Layout: particles of all replicas live in one packed slot range; replica r
+// owns slots [off_r, off_r + n_r) padded to BLOCK, so a thread block never
+// straddles two replicas and finds its replica through blk_rep[].  Inside a
+// replica the slots are kept in cell order (rebuilt with the neighbour list)
+// and Stat::id maps a slot back to the particle id of the reference.
+//
+// Neighbour lists are full lists stored slot-major (nb[q * stride + k]) so a
+// warp reads 32 consecutive ints per neighbour rank.  For particle k the list
+// holds first its lower-id neighbours in ascending id, then its higher-id
+// neighbours in the reference's list[k] order (27-cell stencil order, or
+// ascending id on the N^2 path).  Gathering in that order reproduces the
+// summation order of the reference's half-list scatter loops exactly.
+#pragma once
+#include "sg_device.cuh"
+
+namespace sg {
+
+__device__ __forceinline__ int my_replica(const int* blk_rep) { return blk_rep[blockIdx.x]; }
+
+// ---------------------------------------------------------------------------
+// neighbour data fetch (only the fields the program needs)
+// ---------------------------------------------------------------------------
+struct Need { bool r, type, n, v, age; };
+
+__device__ __forceinline__ void fetch_nb(const Dyn& d, const Stat& st, int j, const Need& nd, Nb& o) {
+  o.x = d.x[j]; o.y = d.y[j]; o.z = d.z[j];
+  if (nd.r) o.r = st.r[j];
+  o.type = nd.type ? st.type[j] : 1;
+  if (nd.n) { o.nx = d.nx[j]; o.ny = d.ny[j]; o.nz = d.nz[j]; }
+  if (nd.v) { o.vx = d.vx[j]; o.vy = d.vy[j]; o.vz = d.vz[j]; }
+  if (nd.age) o.age = d.age[j];
+}
+
+__device__ __forceinline__ Need program_needs(const Program& P) {
+  Need nd{false, P.ntypes > 1, false, false, false};
+  for (int c = 0; c < P.npair; c++) {
+    if (P.pair[c].use_radii) nd.r = true;
+    if (P.pair[c].phase_in) nd.age = true;
+  }
+  for (int c = 0; c < P.nalign; c++) {
+    if (P.align[c].kind == ALIGN_VICSEK) nd.v = true; else nd.n = true;
+    if (P.align[c].has_pp) nd.type = true;
+  }
+  return nd;
+}
+
+// ---------------------------------------------------------------------------
+// force + torque gather for one particle.  Component loop c handles pair
+// potential c and aligner c (std::map order each); forces and torques are
+// separate accumulators, so sharing the neighbour sweep keeps each one's
+// summation order.  Pair energies are counted once, on the lower id.
+// ---------------------------------------------------------------------------
+template <bool ENERGY>
+__device__ void compute_ft(const Program& P, const Replica& R, const Dyn& d, const Stat& st,
+                           const NbList& nl, int k, Part& me, double dt, bool with_pair,
+                           bool with_align, double* epair, double* ealign) {
+  me.fx = 0.0; me.fy = 0.0; me.fz = 0.0;
+  me.tx = 0.0; me.ty = 0.0; me.tz = 0.0;
+  const Need nd = program_needs(P);
+  const int cnt = nl.cnt[k], lo = nl.lo[k];
+  const int npair = with_pair ? P.npair : 0;
+  const int nalign = with_align ? P.nalign : 0;
+  const int nloops = npair > nalign ? npair : nalign;
+  for (int c = 0; c < nloops; c++) {
+    const bool hp = c < npair, ha = c < nalign;
+    PairComp pc; AlignComp ac;
+    double a_i = 1.0, Jg = 0.0, rcg = 0.0;
+    int akind = -1;
+    if (hp) { pc = P.pair[c]; if (pc.phase_in) a_i = phase_factor(pc, me.age, dt); }
+    if (ha) {
+      ac = P.align[c]; akind = ac.kind;
+      Jg = R.align_J[c]; rcg = R.align_rcut[c];
+      if (akind == ALIGN_NEMATIC) Jg = 2.0 * Jg;  // pair_nematic_aligner.cpp:37
+    }
+    const double* g = R.pair_g[hp ? c : 0];
+    for (int q = 0; q < cnt; q++) {
+      const int j = nl.nb[(size_t)q * nl.stride + k];
+      Nb o;
+      fetch_nb(d, st, j, nd, o);
+      double dx = o.x - me.x, dy = o.y - me.y, dz = o.z - me.z;
+      apply_periodic(R, dx, dy, dz);
+      const double r_sq = dx * dx + dy * dy + dz * dz;
+      const bool upper = q >= lo;
+      if (hp) {
+        double alpha = 1.0;
+        if (pc.phase_in) alpha = phase_pair(a_i, phase_factor(pc, o.age, dt));
+        double ff, pe;
+        if (pair_term(pc, g, P.ntypes, me, o, r_sq, alpha, ff, pe)) {
+          me.fx -= ff * dx; me.fy -= ff * dy; me.fz -= ff * dz;
+          if (ENERGY && upper) epair[c] += pe;
+        }
+      }
+      if (ha) {
+        double J = Jg, rcut = rcg;
+        if (ac.has_pp) {
+          const double* t = ac.table + ((size_t)(me.type - 1) * P.ntypes + (size_t)(o.type - 1)) * 2;
+          J = t[0]; rcut = t[1];
+        }
+        if (r_sq <= rcut * rcut) {
+          if (akind == ALIGN_VICSEK) {
+            me.tx += o.vx; me.ty += o.vy; me.tz += o.vz;
+          } else {
+            double tau_x = me.ny * o.nz - me.nz * o.ny;
+            double tau_y = me.nz * o.nx - me.nx * o.nz;
+            double tau_z = me.nx * o.ny - me.ny * o.nx;
+            if (akind == ALIGN_POLAR) {
+              me.tx += J * tau_x; me.ty += J * tau_y; me.tz += J * tau_z;
+              if (ENERGY && upper) ealign[c] += -2.0 * J * (me.nx * o.nx + me.ny * o.ny + me.nz * o.nz);
+            } else {
+              double cdot = me.nx * o.nx + me.ny * o.ny + me.nz * o.nz;
+              me.tx += J * cdot * tau_x; me.ty += J * cdot * tau_y; me.tz += J * cdot * tau_z;
+              if (ENERGY && upper) ealign[c] += -2.0 * J * (2.0 * cdot * cdot - 1.0);
+            }
+          }
+        }
+      }
+    }
+    if (ha && akind == ALIGN_VICSEK) {  // pair_vicsek_aligner.cpp:72-82
+      me.tx += me.vx; me.ty += me.vy; me.tz += me.vz;
+      double v = sqrt(me.tx * me.tx + me.ty * me.ty + me.tz * me.tz);
+      if (v == 0.0) v = 1.0;
+      double inv_v = 1.0 / v;
+      me.tx *= inv_v; me.ty *= inv_v; me.tz *= inv_v;
+    }
+  }
+  if (with_pair) {
+    for (int c = 0; c < P.next; c++) {  // external_self_propulsion.cpp:33-50
+      double alpha = R.ext_alpha[c];
+      if (P.ext[c].has_params) alpha = P.ext[c].type_alpha[me.type - 1];
+      me.fx += alpha * me.nx; me.fy += alpha * me.ny; me.fz += alpha * me.nz;
+    }
+  }
+}
+
+// block reduction of up to NV doubles into out[v * nblocks + blockIdx.x]
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out, int nblocks) {
+  __shared__ double sh[NV][BLOCK / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    double x = v[i];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[i][w] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double s = 0.0;
+    for (int i = 0; i < BLOCK / 32; i++) s += sh[threadIdx.x][i];
+    out[(size_t)threadIdx.x * nblocks + blockIdx.x] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// integrators (per particle).  `g` is the particle's position in its group
+// (the particle id for group "all"); noise counters follow the reference's
+// draw order: optional nematic flip draws for every particle first, then per
+// particle the translational draws followed by the rotational one.
+// ---------------------------------------------------------------------------
+
+// IntegratorBrownian::integrate, integrators/integrator_brownian.cpp:42-124
+__device__ __forceinline__ void integ_brownian(const Program& P, const Replica& R, const IntegComp& ic,
+                                               const double* ip, uint32_t seed, uint64_t base,
+                                               int run_step, int n, Part& p) {
+  const double dt = ip[0], v0 = ip[1], nu = ip[2], mu = ip[3], mur = ip[4];
+  const uint64_t g = (uint64_t)p.id;
+  if (ic.nematic) {
+    double flip = dt / ip[7];
+    if (noise_uniform(seed, base + g) < flip) {
+      p.nx = -p.nx; p.ny = -p.ny; p.nz = -p.nz;
+      if (ic.velocity) { p.vx = -p.vx; p.vy = -p.vy; p.vz = -p.vz; }
+    }
+    base += (uint64_t)n;
+  }
+  const double T = value_get(ic.temp, run_step);
+  const int D = T > 0.0 ? 4 : 1;
+  const uint64_t c0 = base + g * (uint64_t)D;
+  double fd_x = v0 * p.nx + mu * p.fx;
+  double fd_y = v0 * p.ny + mu * p.fy;
+  double fd_z = v0 * p.nz + mu * p.fz;
+  p.vx = fd_x; p.vy = fd_y; p.vz = fd_z;
+  p.x += dt * fd_x; p.y += dt * fd_y; p.z += dt * fd_z;
+  if (T > 0.0) {
+    const double B = sqrt(2.0 * mu * T);
+    const double sqrt_dt = sqrt(dt);
+    double fr_x = B * noise_gauss(seed, c0 + 0);
+    double fr_y = B * noise_gauss(seed, c0 + 1);
+    double fr_z = B * noise_gauss(seed, c0 + 2);
+    p.vx += fr_x; p.vy += fr_y; p.vz += fr_z;
+    p.x += sqrt_dt * fr_x; p.y += sqrt_dt * fr_y; p.z += sqrt_dt * fr_z;
+  }
+  enforce_all(P, R, p);
+  p.omega = mur * project_torque(P, R, p);
+  const double stoch = sqrt(nu * dt);
+  double dtheta = dt * p.omega + stoch * noise_gauss(seed, c0 + (uint64_t)(D - 1));
+  rotate_director(P, R, p, dtheta);
+  if (ic.velocity) rotate_velocity(P, R, p, dtheta);
+  p.age += dt;
+}
+
+// IntegratorBrownianPos::integrate, integrators/integrator_brownian_pos.cpp:37-84
+__device__ __forceinline__ void integ_brownian_pos(const Program& P, const Replica& R, const IntegComp& ic,
+                                                   const double* ip, uint32_t seed, uint64_t base,
+                                                   int run_step, Part& p) {
+  const double dt = ip[0], mu = ip[3];
+  const double T = value_get(ic.temp, run_step);
+  p.vx = mu * p.fx; p.vy = mu * p.fy; p.vz = mu * p.fz;
+  p.x += dt * p.vx; p.y += dt * p.vy; p.z += dt * p.vz;
+  if (T > 0.0) {
+    const uint64_t c0 = base + (uint64_t)p.id * 3u;
+    const double B = sqrt(2.0 * mu * T);
+    const double sqrt_dt = sqrt(dt);
+    double fr_x = B * noise_gauss(seed, c0 + 0);
+    double fr_y = B * noise_gauss(seed, c0 + 1);
+    double fr_z = B * noise_gauss(seed, c0 + 2);
+    p.vx += fr_x; p.vy += fr_y; p.vz += fr_z;
+    p.x += sqrt_dt * fr_x; p.y += sqrt_dt * fr_y; p.z += sqrt_dt * fr_z;
+  }
+  enforce_all(P, R, p);
+  p.age += dt;
+}
+
+// IntegratorBrownianAlign::integrate, integrators/integrator_brownian_align.cpp:41-76
+__device__ __forceinline__ void integ_brownian_align(const Program& P, const Replica& R, const IntegComp& ic,
+                                                     const double* ip, uint32_t seed, uint64_t base,
+                                                     int n, Part& p) {
+  const double dt = ip[0], nu = ip[2], mur = ip[4];
+  const uint64_t g = (uint64_t)p.id;
+  if (ic.nematic) {
+    double flip = dt / ip[7];
+    if (noise_uniform(seed, base + g) < flip) { p.nx = -p.nx; p.ny = -p.ny; p.nz = -p.nz; }
+    base += (uint64_t)n;
+  }
+  p.omega = mur * project_torque(P, R, p);
+  const double stoch = sqrt(nu * dt);
+  double dtheta = dt * p.omega + stoch * noise_gauss(seed, base + g);
+  rotate_director(P, R, p, dtheta);
+}
+
+// noise draws consumed per call by integrator c of a replica of n particles
+__host__ __device__ inline uint64_t draws_per_call(const IntegComp& ic, int run_step, int n) {
+  double T = value_get(ic.temp, run_step);
+  switch (ic.kind) {
+    case INT_BROWNIAN: return (uint64_t)n * ((ic.nematic ? 1u : 0u) + (T > 0.0 ? 4u : 1u));
+    case INT_BROWNIAN_POS: return T > 0.0 ? (uint64_t)n * 3u : 0u;
+    case INT_BROWNIAN_ALIGN: return (uint64_t)n * ((ic.nematic ? 1u : 0u) + 1u);
+    default: return 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// skin test, NeighbourList::need_update (neighbour_list.cpp:278-302)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool need_update(const Replica& R, const NbList& nl, int k, const Part& p) {
+  double dx = nl.ox[k] - p.x, dy = nl.oy[k] - p.y, dz = nl.oz[k] - p.z;
+  if (R.periodic) {
+    if (dx > R.xhi) dx -= R.Lx; else if (dx < R.xlo) dx += R.Lx;
+    if (dy > R.yhi) dy -= R.Ly; else if (dy < R.ylo) dy += R.Ly;
+    if (dz > R.zhi) dz -= R.Lz; else if (dz < R.zlo) dz += R.Lz;
+  }
+  return !(dx * dx + dy * dy + dz * dz < 0.25 * R.pad * R.pad);
+}
+
+__device__ __forceinline__ bool finite3(double a, double b, double c) {
+  return isfinite(a) && isfinite(b) && isfinite(c);
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+// Constrainer::enforce on every particle (samos.cpp:887-888)
+__global__ void k_enforce(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                          Dyn d, Stat st) {
+  const Replica& R = reps[my_replica(blk_rep)];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  Part p;
+  load_dyn(d, k, p);
+  p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
+  enforce_all(P, R, p);
+  store_dyn(d, k, p);
+}
+
+// reset + Potential::compute + Aligner::compute, storing F, tau and the
+// per-block energy partials (pair c at row c, aligner c at row MAX_PAIR + c)
+template <bool ENERGY>
+__global__ void k_force(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                        const Clock* __restrict__ clk, Dyn d, Stat st, NbList nl, double dt,
+                        int use_fire_dt, int with_pair, int with_align, double* epart, int nblocks) {
+  const int r = my_replica(blk_rep);
+  const Replica& R = reps[r];
+  if (use_fire_dt) dt = clk[r].fire_dt;
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  double e[MAX_PAIR + MAX_ALIGN];
+#pragma unroll
+  for (int i = 0; i < MAX_PAIR + MAX_ALIGN; i++) e[i] = 0.0;
+  if (k - R.off < R.n) {
+    Part me;
+    me.x = d.x[k]; me.y = d.y[k]; me.z = d.z[k];
+    me.nx = d.nx[k]; me.ny = d.ny[k]; me.nz = d.nz[k];
+    me.vx = d.vx[k]; me.vy = d.vy[k]; me.vz = d.vz[k];
+    me.age = d.age[k]; me.r = st.r[k]; me.type = st.type[k];
+    compute_ft<ENERGY>(P, R, d, st, nl, k, me, dt, with_pair != 0, with_align != 0, e, e + MAX_PAIR);
+    if (with_pair) { d.fx[k] = me.fx; d.fy[k] = me.fy; d.fz[k] = me.fz; }
+    if (with_align) { d.tx[k] = me.tx; d.ty[k] = me.ty; d.tz[k] = me.tz; }
+  }
+  if (ENERGY) block_reduce_store<MAX_PAIR + MAX_ALIGN>(e, epart, nblocks);
+}
+
+// Fused Brownian-family step: F, tau from the current buffer, integrators in
+// map order, skin test, then (apply_e1) the next step's start-of-step
+// Constrainer::enforce; result into the next buffer.
+template <bool ENERGY>
+__global__ void __launch_bounds__(BLOCK)
+k_step_brownian(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                const Clock* __restrict__ clk, Dyn cur, Dyn nxt, Stat st, NbList nl,
+                int* __restrict__ rebuild, int* __restrict__ status, double dt_global, int apply_e1,
+                double* epart, int nblocks) {
+  const int r = my_replica(blk_rep);
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  double e[MAX_PAIR + MAX_ALIGN];
+#pragma unroll
+  for (int i = 0; i < MAX_PAIR + MAX_ALIGN; i++) e[i] = 0.0;
+  if (k - R.off < R.n) {
+    Part p;
+    load_dyn(cur, k, p);
+    p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
+    compute_ft<ENERGY>(P, R, cur, st, nl, k, p, dt_global, true, true, e, e + MAX_PAIR);
+    const int run_step = clk[r].run_step;
+    for (int c = 0; c < P.ninteg; c++) {
+      const IntegComp ic = P.integ[c];
+      const uint64_t base = clk[r].ctr[c];
+      if (ic.kind == INT_BROWNIAN)
+        integ_brownian(P, R, ic, R.integ_p[c], R.seed[c], base, run_step, R.n, p);
+      else if (ic.kind == INT_BROWNIAN_POS)
+        integ_brownian_pos(P, R, ic, R.integ_p[c], R.seed[c], base, run_step, p);
+      else if (ic.kind == INT_BROWNIAN_ALIGN)
+        integ_brownian_align(P, R, ic, R.integ_p[c], R.seed[c], base, R.n, p);
+    }
+    if (need_update(R, nl, k, p)) {
+      if (rebuild[r] == 0) atomicOr(&rebuild[r], 1);
+    }
+    if (!finite3(p.x, p.y, p.z)) atomicOr(status, ST_NONFINITE);
+    if (apply_e1) enforce_all(P, R, p);
+    store_dyn(nxt, k, p);
+  }
+  if (ENERGY) block_reduce_store<MAX_PAIR + MAX_ALIGN>(e, epart, nblocks);
+}
+
+// Skin test over all particles of the current buffer (unfused path)
+__global__ void k_skin(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                       Dyn d, NbList nl, int* __restrict__ rebuild, int* __restrict__ status) {
+  const int r = my_replica(blk_rep);
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  Part p;
+  p.x = d.x[k]; p.y = d.y[k]; p.z = d.z[k];
+  if (need_update(R, nl, k, p)) {
+    if (rebuild[r] == 0) atomicOr(&rebuild[r], 1);
+  }
+  if (!finite3(p.x, p.y, p.z)) atomicOr(status, ST_NONFINITE);
+}
+
+// noise draws consumed per call by a Langevin integrator
+__host__ __device__ inline uint64_t langevin_draws(const IntegComp& ic, const double* ip, int run_step, int n) {
+  const double T = value_get(ic.temp, run_step);
+  const double dt = ip[0], gamma = ip[9];
+  if (ic.method == LANGEVIN_SPV) return sqrt(T * (1.0 - exp(-2.0 * gamma * dt))) != 0.0 ? (uint64_t)n * 3u : 0u;
+  if (ic.method == LANGEVIN_BBK) return sqrt(2.0 * T * dt * gamma) != 0.0 ? (uint64_t)n * 3u : 0u;
+  return sqrt(T * (1.0 - exp(-2.0 * gamma * dt))) != 0.0 ? (uint64_t)n * 3u : 0u;
+}
+
+// per-replica clock advance after one integration step
+__global__ void k_tail(Program P, const Replica* __restrict__ reps, Clock* clk, int nrep) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrep) return;
+  Clock& C = clk[r];
+  for (int c = 0; c < P.ninteg; c++) {
+    const IntegComp& ic = P.integ[c];
+    if (ic.kind == INT_LANGEVIN) C.ctr[c] += langevin_draws(ic, reps[r].integ_p[c], C.run_step, reps[r].n);
+    else C.ctr[c] += draws_per_call(ic, C.run_step, reps[r].n);
+  }
+  C.run_step++;
+  C.time_step++;
+}
+
+// ---------------------------------------------------------------------------
+// Langevin (integrators/integrator_langevin.cpp): phase A before and phase B
+// after the integrator's own force evaluation.
+// ---------------------------------------------------------------------------
+__global__ void k_langevin_a(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                             const Clock* __restrict__ clk, Dyn d, Stat st, int c, const double* Rn) {
+  const int r = my_replica(blk_rep);
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  Part p;
+  load_dyn(d, k, p);
+  p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
+  const IntegComp ic = P.integ[c];
+  const double* ip = R.integ_p[c];
+  const double dt = ip[0], gamma = ip[9];
+  const double T = value_get(ic.temp, clk[r].run_step);
+  const double dt2 = 0.5 * dt;
+  const uint32_t seed = R.seed[c];
+  const uint64_t base = clk[r].ctr[c];
+  if (ic.method == LANGEVIN_SPV) {  // integrator_langevin.cpp:136-146
+    p.x += dt2 * p.vx; p.y += dt2 * p.vy; p.z += dt2 * p.vz;
+    enforce_all(P, R, p);
+  } else if (ic.method == LANGEVIN_BBK) {  // integrator_langevin.cpp:203-223
+    const double B = sqrt(2.0 * T * dt * gamma);
+    const double one_m_dt2 = 1.0 - gamma * dt2;
+    const double dt2_over_mass = dt2 / p.mass;
+    p.vx = one_m_dt2 * p.vx + dt2_over_mass * p.fx;
+    p.vy = one_m_dt2 * p.vy + dt2_over_mass * p.fy;
+    p.vz = one_m_dt2 * p.vz + dt2_over_mass * p.fz;
+    if (B != 0.0) {
+      const double stoch_fact = 0.5 * B / sqrt(p.mass);
+      const size_t gi = (size_t)R.off + (size_t)p.id;
+      p.vx += stoch_fact * Rn[3 * gi + 0];
+      p.vy += stoch_fact * Rn[3 * gi + 1];
+      p.vz += stoch_fact * Rn[3 * gi + 2];
+    }
+    p.x += dt * p.vx; p.y += dt * p.vy; p.z += dt * p.vz;
+    enforce_all(P, R, p);
+  } else {  // BAOAB, integrator_langevin.cpp:63-95
+    const double B = sqrt(T * (1.0 - exp(-2.0 * gamma * dt)));
+    const double exp_dt = exp(-gamma * dt);
+    const double fact = dt2 / p.mass;
+    p.vx += fact * p.fx; p.vy += fact * p.fy; p.vz += fact * p.fz;
+    p.x += dt2 * p.vx; p.y += dt2 * p.vy; p.z += dt2 * p.vz;
+    enforce_all(P, R, p);
+    p.vx *= exp_dt; p.vy *= exp_dt; p.vz *= exp_dt;
+    if (B != 0.0) {
+      const double stoch_fact = B / sqrt(p.mass);
+      const uint64_t c0 = base + (uint64_t)p.id * 3u;
+      p.vx += stoch_fact * noise_gauss(seed, c0 + 0);
+      p.vy += stoch_fact * noise_gauss(seed, c0 + 1);
+      p.vz += stoch_fact * noise_gauss(seed, c0 + 2);
+    }
+    p.x += dt2 * p.vx; p.y += dt2 * p.vy; p.z += dt2 * p.vz;
+    enforce_all(P, R, p);
+  }
+  store_dyn(d, k, p);
+}
+
+__global__ void k_langevin_b(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                             const Clock* __restrict__ clk, Dyn d, Stat st, int c, double* Rn) {
+  const int r = my_replica(blk_rep);
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  Part p;
+  load_dyn(d, k, p);
+  p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
+  const IntegComp ic = P.integ[c];
+  const double* ip = R.integ_p[c];
+  const double dt = ip[0], gamma = ip[9];
+  const double T = value_get(ic.temp, clk[r].run_step);
+  const double dt2 = 0.5 * dt;
+  const uint32_t seed = R.seed[c];
+  const uint64_t base = clk[r].ctr[c];
+  if (ic.method == LANGEVIN_SPV) {  // integrator_langevin.cpp:158-183
+    const double zeta = sqrt(T * (1.0 - exp(-2.0 * gamma * dt)));
+    const double eta = (gamma == 0.0) ? 0.0 : (1.0 - exp(-dt * gamma)) / gamma;
+    const double exp_dt = exp(-dt * gamma);
+    const double fact = eta / p.mass;
+    p.vx = exp_dt * p.vx + fact * p.fx;
+    p.vy = exp_dt * p.vy + fact * p.fy;
+    p.vz = exp_dt * p.vz + fact * p.fz;
+    if (zeta != 0.0) {
+      const double stoch_fact = zeta / sqrt(p.mass);
+      const uint64_t c0 = base + (uint64_t)p.id * 3u;
+      p.vx += stoch_fact * noise_gauss(seed, c0 + 0);
+      p.vy += stoch_fact * noise_gauss(seed, c0 + 1);
+      p.vz += stoch_fact * noise_gauss(seed, c0 + 2);
+    }
+    p.x += dt2 * p.vx; p.y += dt2 * p.vy; p.z += dt2 * p.vz;
+    enforce_all(P, R, p);
+    p.age += dt;
+  } else if (ic.method == LANGEVIN_BBK) {  // integrator_langevin.cpp:232-252
+    const double B = sqrt(2.0 * T * dt * gamma);
+    const double one_div_one_p_dt2 = 1.0 / (1.0 + gamma * dt2);
+    const double dt2_over_mass = dt2 / p.mass;
+    p.vx = one_div_one_p_dt2 * (p.vx + dt2_over_mass * p.fx);
+    p.vy = one_div_one_p_dt2 * (p.vy + dt2_over_mass * p.fy);
+    p.vz = one_div_one_p_dt2 * (p.vz + dt2_over_mass * p.fz);
+    if (B != 0.0) {
+      const double stoch_fact = 0.5 * B * one_div_one_p_dt2 / sqrt(p.mass);
+      const uint64_t c0 = base + (uint64_t)p.id * 3u;
+      const size_t gi = (size_t)R.off + (size_t)p.id;
+      double rx = noise_gauss(seed, c0 + 0), ry = noise_gauss(seed, c0 + 1), rz = noise_gauss(seed, c0 + 2);
+      Rn[3 * gi + 0] = rx; Rn[3 * gi + 1] = ry; Rn[3 * gi + 2] = rz;
+      p.vx += stoch_fact * rx; p.vy += stoch_fact * ry; p.vz += stoch_fact * rz;
+      p.age += dt;
+    }
+  } else {  // BAOAB final B step, integrator_langevin.cpp:104-111
+    const double fact = dt2 / p.mass;
+    p.vx += fact * p.fx; p.vy += fact * p.fy; p.vz += fact * p.fz;
+    p.age += dt;
+  }
+  store_dyn(d, k, p);
+}
+
+// ---------------------------------------------------------------------------
+// FIRE (integrators/integrator_fire.cpp:34-148)
+// ---------------------------------------------------------------------------
+// first half: half kick, drift, enforce, omega, director rotation (49-66)
+__global__ void k_fire_a(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                         const Clock* __restrict__ clk, Dyn d, Stat st) {
+  const int r = my_replica(blk_rep);
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  if (clk[r].fire_conv_step >= 0) return;  // frozen after convergence (driver mode)
+  Part p;
+  load_dyn(d, k, p);
+  p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
+  const double dt = clk[r].fire_dt;
+  const double dt_2 = 0.5 * dt;
+  p.vx += dt_2 * p.fx; p.vy += dt_2 * p.fy; p.vz += dt_2 * p.fz;
+  p.x += dt * p.vx; p.y += dt * p.vy; p.z += dt * p.vz;
+  enforce_all(P, R, p);
+  p.omega += dt_2 * project_torque(P, R, p);
+  double dtheta = dt * p.omega;
+  rotate_director(P, R, p, dtheta);
+  store_dyn(d, k, p);
+}
+
+// second half kick + P, |F|^2, |v|^2, max|F|^2 partials (79-94)
+__global__ void k_fire_b(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                         const Clock* __restrict__ clk, Dyn d, Stat st, double* part, int nblocks) {
+  const int r = my_replica(blk_rep);
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  double v[3] = {0.0, 0.0, 0.0};
+  double fmax2 = 0.0;
+  const bool frozen = clk[r].fire_conv_step >= 0;
+  if (k - R.off < R.n && !frozen) {
+    Part p;
+    load_dyn(d, k, p);
+    p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
+    const double dt_2 = 0.5 * clk[r].fire_dt;
+    p.vx += dt_2 * p.fx; p.vy += dt_2 * p.fy; p.vz += dt_2 * p.fz;
+    v[0] = p.vx * p.fx + p.vy * p.fy + p.vz * p.fz;
+    double f2 = p.fx * p.fx + p.fy * p.fy + p.fz * p.fz;
+    v[1] = f2;
+    fmax2 = f2;
+    v[2] = p.vx * p.vx + p.vy * p.vy + p.vz * p.vz;
+    enforce_all(P, R, p);
+    p.omega += dt_2 * project_torque(P, R, p);
+    store_dyn(d, k, p);
+  }
+  block_reduce_store<3>(v, part, nblocks);
+  // max reduction (exact in any order)
+  for (int o = 16; o > 0; o >>= 1) fmax2 = fmax(fmax2, __shfl_down_sync(0xffffffffu, fmax2, o));
+  __shared__ double shm[BLOCK / 32];
+  if ((threadIdx.x & 31) == 0) shm[threadIdx.x >> 5] = fmax2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int i = 0; i < BLOCK / 32; i++) m = fmax(m, shm[i]);
+    part[(size_t)3 * nblocks + blockIdx.x] = m;
+  }
+}
+
+// per replica: fixed-order sums over its blocks, convergence test and the
+// dt / alpha control (96-147).  One thread per replica.  alpha_mix[r] keeps
+// the alpha the mixing step must use (the value before this update).
+__global__ void k_fire_c(Program P, const Replica* __restrict__ reps, Clock* clk, const int* __restrict__ rep_blk0,
+                         const int* __restrict__ rep_nblk, const double* part, const double* epart,
+                         int nblocks, int nrep, int c, int driver, double* alpha_mix) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrep) return;
+  Clock& C = clk[r];
+  if (C.fire_conv_step >= 0) return;
+  const Replica& R = reps[r];
+  const double* ip = R.integ_p[c];
+  double Ps = 0.0, Fn = 0.0, Vn = 0.0, Fm = 0.0, E = 0.0;
+  const int b0 = rep_blk0[r], nb = rep_nblk[r];
+  for (int b = b0; b < b0 + nb; b++) {
+    Ps += part[b]; Fn += part[(size_t)nblocks + b]; Vn += part[(size_t)2 * nblocks + b];
+    Fm = fmax(Fm, part[(size_t)3 * nblocks + b]);
+  }
+  for (int pc = 0; pc < P.npair; pc++) {
+    double s = 0.0;
+    for (int b = b0; b < b0 + nb; b++) s += epart[(size_t)pc * nblocks + b];
+    E += s;
+  }
+  Fn = sqrt(Fn);
+  Vn = sqrt(Vn);
+  C.fire_P = Ps; C.fire_F = Fn; C.fire_V = Vn; C.fire_E = E; C.fire_Fmax2 = Fm;
+  const double sqrt_ndof = sqrt((double)(3 * R.n));
+  const double fmax_tol = ip[11];
+  const bool conv = (fmax_tol > 0.0) ? (sqrt(Fm) < fmax_tol)
+                                     : (Fn / sqrt_ndof < ip[3] && fabs(E - C.fire_old_e) < ip[4]);
+  if (conv) {
+    C.fire_converged = 1;
+    if (driver) C.fire_conv_step = C.run_step;
+    return;
+  }
+  alpha_mix[r] = C.fire_alpha;
+  if (Ps > 0.0) {
+    C.fire_last_neg++;
+    if (C.fire_last_neg > (int)ip[9]) {
+      double ndt = C.fire_dt * ip[6];
+      C.fire_dt = ndt < ip[8] ? ndt : ip[8];
+      C.fire_alpha *= ip[2];
+    }
+  } else {
+    C.fire_dt *= ip[7];
+    C.fire_alpha = ip[1];
+    C.fire_last_neg = 0;
+  }
+  C.fire_converged = 0;
+  C.fire_old_e = E;
+}
+
+// FIRE velocity mixing (110-121) with the pre-update alpha, then the
+// P <= 0 restart that zeroes the velocities (131-142).
+__global__ void k_fire_d(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                         const Clock* __restrict__ clk, Dyn d, const double* alpha_mix) {
+  const int r = my_replica(blk_rep);
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  const Clock& C = clk[r];
+  if (C.fire_converged || C.fire_conv_step >= 0) return;
+  const double a = alpha_mix[r];
+  const double inv_Fnorm = 1.0 / C.fire_F;
+  const double fact_1 = 1.0 - a;
+  const double fact_2 = a * inv_Fnorm * C.fire_V;
+  double vx = fact_1 * d.vx[k] + fact_2 * d.fx[k];
+  double vy = fact_1 * d.vy[k] + fact_2 * d.fy[k];
+  double vz = fact_1 * d.vz[k] + fact_2 * d.fz[k];
+  if (!(C.fire_P > 0.0)) { vx = 0.0; vy = 0.0; vz = 0.0; }
+  d.vx[k] = vx; d.vy[k] = vy; d.vz[k] = vz;
+}
+
+// ---------------------------------------------------------------------------
+// neighbour-list rebuild: counting-sort cell binning + ordered list build
+// (CellList::populate, cell_list.cpp:82-104; NeighbourList::build_cell /
+// build_nsq, neighbour_list.cpp:178-273)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int cell_of(const Replica& R, double x, double y, double z, int& a, int& b, int& c) {
+  a = (int)((x - R.xlo) / R.cwx);
+  b = (int)((y - R.ylo) / R.cwy);
+  c = (int)((z - R.zlo) / R.cwz);
+  a = a < 0 ? 0 : (a >= R.cnx ? R.cnx - 1 : a);
+  b = b < 0 ? 0 : (b >= R.cny ? R.cny - 1 : b);
+  c = c < 0 ? 0 : (c >= R.cnz ? R.cnz - 1 : c);
+  return R.cny * R.cnz * a + R.cnz * b + c;
+}
+
+// populate wrap (no image update) + cell index + count
+__global__ void k_rb_bin(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                         const int* __restrict__ rebuild, Dyn d, int* __restrict__ pcell,
+                         int* __restrict__ cell_cnt) {
+  const int r = my_replica(blk_rep);
+  if (!rebuild[r]) return;
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  double x = d.x[k], y = d.y[k], z = d.z[k];
+  if (R.periodic) {
+    bool ch = false;
+    if (x < R.xlo) { x += R.Lx; ch = true; } else if (x > R.xhi) { x -= R.Lx; ch = true; }
+    if (y < R.ylo) { y += R.Ly; ch = true; } else if (y > R.yhi) { y -= R.Ly; ch = true; }
+    if (z < R.zlo) { z += R.Lz; ch = true; } else if (z > R.zhi) { z -= R.Lz; ch = true; }
+    if (ch) { d.x[k] = x; d.y[k] = y; d.z[k] = z; }
+  }
+  int a, b, c;
+  const int cl = cell_of(R, x, y, z, a, b, c);
+  pcell[k] = cl;
+  atomicAdd(&cell_cnt[R.cell_off + cl], 1);
+}
+
+// exclusive scan of the packed cell counts: A) block sums, B) scan of block
+// sums (one block), C) block-local scan plus block prefix
+constexpr int SCAN_T = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_T * SCAN_ITEMS;
+
+__global__ void k_scan_a(const int* __restrict__ in, int n, int* __restrict__ bsum) {
+  __shared__ int sh[SCAN_T / 32];
+  const int base = blockIdx.x * SCAN_TILE;
+  int s = 0;
+#pragma unroll
+  for (int i = 0; i < SCAN_ITEMS; i++) {
+    int idx = base + threadIdx.x * SCAN_ITEMS + i;
+    if (idx < n) s += in[idx];
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int v = sh[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = v;
+  }
+}
+
+__device__ __forceinline__ int block_excl_scan(int v, int* sh_warp, int& total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh_warp[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int s = lane < (blockDim.x >> 5) ? sh_warp[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    sh_warp[lane] = s;
+  }
+  __syncthreads();
+  total = sh_warp[(blockDim.x >> 5) - 1];
+  const int wp = w > 0 ? sh_warp[w - 1] : 0;
+  __syncthreads();
+  return wp + x - v;
+}
+
+__global__ void k_scan_b(int* bsum, int nb) {
+  __shared__ int shw[32];
+  int carry = 0;
+  for (int base = 0; base < nb; base += SCAN_T) {
+    int idx = base + threadIdx.x;
+    int v = idx < nb ? bsum[idx] : 0;
+    int tot;
+    int ex = block_excl_scan(v, shw, tot);
+    if (idx < nb) bsum[idx] = carry + ex;
+    carry += tot;
+    __syncthreads();
+  }
+}
+
+__global__ void k_scan_c(const int* __restrict__ in, int n, const int* __restrict__ bsum, int* __restrict__ out) {
+  __shared__ int shw[32];
+  const int base = blockIdx.x * SCAN_TILE;
+  int v[SCAN_ITEMS];
+  int s = 0;
+#pragma unroll
+  for (int i = 0; i < SCAN_ITEMS; i++) {
+    int idx = base + threadIdx.x * SCAN_ITEMS + i;
+    v[i] = idx < n ? in[idx] : 0;
+    s += v[i];
+  }
+  int tot;
+  int ex = block_excl_scan(s, shw, tot) + bsum[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < SCAN_ITEMS; i++) {
+    int idx = base + threadIdx.x * SCAN_ITEMS + i;
+    if (idx < n) out[idx] = ex;
+    ex += v[i];
+  }
+}
+
+// unordered placement into the cell segments
+__global__ void k_rb_scatter(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                             const int* __restrict__ rebuild, const int* __restrict__ pcell,
+                             const int* __restrict__ cstart, int* __restrict__ cfill, int* __restrict__ tmp) {
+  const int r = my_replica(blk_rep);
+  if (!rebuild[r]) return;
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  const int cg = R.cell_off + pcell[k];
+  const int pos = cstart[cg] - cstart[R.cell_off] + atomicAdd(&cfill[cg], 1);
+  tmp[R.off + pos] = k;
+}
+
+// rank inside the cell by particle id -> deterministic ascending-id order
+__global__ void k_rb_rank(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                          const int* __restrict__ rebuild, const int* __restrict__ pcell,
+                          const int* __restrict__ cstart, const int* __restrict__ ccnt,
+                          const int* __restrict__ tmp, const int* __restrict__ id, int* __restrict__ perm) {
+  const int r = my_replica(blk_rep);
+  if (!rebuild[r]) return;
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  const int cg = R.cell_off + pcell[k];
+  const int s0 = R.off + cstart[cg] - cstart[R.cell_off];
+  const int n = ccnt[cg];
+  const int myid = id[k];
+  int rank = 0;
+  for (int q = 0; q < n; q++) rank += id[tmp[s0 + q]] < myid ? 1 : 0;
+  perm[s0 + rank] = k;
+}
+
+// gather all particle arrays into the permuted order (dst = src[perm])
+__global__ void k_rb_gather(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                            const int* __restrict__ rebuild, const int* __restrict__ perm,
+                            Dyn src, Dyn dst, Stat ssrc, Stat sdst) {
+  const int r = my_replica(blk_rep);
+  if (!rebuild[r]) return;
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  const int o = perm[k];
+  Part p;
+  load_dyn(src, o, p);
+  store_dyn(dst, k, p);
+  sdst.r[k] = ssrc.r[o]; sdst.mass[k] = ssrc.mass[o];
+  sdst.type[k] = ssrc.type[o]; sdst.id[k] = ssrc.id[o];
+}
+
+// copy back (dst -> src) for the rebuilt replicas
+__global__ void k_rb_copyback(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                              const int* __restrict__ rebuild, Dyn tmpd, Dyn d, Stat tmps, Stat st) {
+  const int r = my_replica(blk_rep);
+  if (!rebuild[r]) return;
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  Part p;
+  load_dyn(tmpd, k, p);
+  store_dyn(d, k, p);
+  st.r[k] = tmps.r[k]; st.mass[k] = tmps.mass[k]; st.type[k] = tmps.type[k]; st.id[k] = tmps.id[k];
+}
+
+constexpr int NB_LOCAL = 96;  // per-thread staging for the ordered list build
+
+// ordered full-list build.  Cell path: the reference's 27-cell stencil with
+// periodic index wrap (duplicates kept when a dimension has 2 cells, as in
+// cell_list.cpp:52-63); higher-id neighbours stay in visiting order.  N^2
+// path: each distinct neighbour cell once, higher ids sorted ascending
+// (build_nsq appends in ascending i).  Lower-id neighbours ascending in both.
+__global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                           const int* __restrict__ rebuild, Dyn d, Stat st, NbList nl,
+                           const int* __restrict__ pcell, const int* __restrict__ cstart,
+                           const int* __restrict__ ccnt, int* __restrict__ status, int* __restrict__ maxnb) {
+  const int r = my_replica(blk_rep);
+  if (!rebuild[r]) return;
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  // cell of this particle (positions are already in cell-sorted slots; the
+  // cell index is recomputed from the wrapped position)
+  const double x = d.x[k], y = d.y[k], z = d.z[k];
+  const int myid = st.id[k];
+  int a, b, c;
+  cell_of(R, x, y, z, a, b, c);
+  int lo_id[NB_LOCAL], lo_slot[NB_LOCAL];
+  int up_id[NB_LOCAL], up_slot[NB_LOCAL];
+  int nlo = 0, nup = 0;
+  bool overflow = false;
+  const int base0 = cstart[R.cell_off];
+  // stencil offsets: reference order; on the N^2 path skip repeated cells
+  int seen[27];
+  int nseen = 0;
+  for (int ox = -1; ox <= 1; ox++)
+    for (int oy = -1; oy <= 1; oy++)
+      for (int oz = -1; oz <= 1; oz++) {
+        int ia = a + ox, ib = b + oy, ic = c + oz;
+        if (ia < 0) ia = R.cnx - 1; else if (ia == R.cnx) ia = 0;
+        if (ib < 0) ib = R.cny - 1; else if (ib == R.cny) ib = 0;
+        if (ic < 0) ic = R.cnz - 1; else if (ic == R.cnz) ic = 0;
+        const int cl = R.cny * R.cnz * ia + R.cnz * ib + ic;
+        if (!R.use_cell) {
+          bool dup = false;
+          for (int q = 0; q < nseen; q++) dup = dup || (seen[q] == cl);
+          if (dup) continue;
+          seen[nseen++] = cl;
+        }
+        const int cg = R.cell_off + cl;
+        const int s0 = R.off + cstart[cg] - base0;
+        const int n = ccnt[cg];
+        for (int q = 0; q < n; q++) {
+          const int j = s0 + q;
+          const int jid = st.id[j];
+          if (jid == myid) continue;
+          double dx, dy, dz;
+          if (myid < jid) { dx = x - d.x[j]; dy = y - d.y[j]; dz = z - d.z[j]; }
+          else { dx = d.x[j] - x; dy = d.y[j] - y; dz = d.z[j] - z; }
+          apply_periodic(R, dx, dy, dz);
+          const double d2 = dx * dx + dy * dy + dz * dz;
+          if (d2 < R.cut2) {
+            if (jid < myid) {
+              if (nlo < NB_LOCAL) { lo_id[nlo] = jid; lo_slot[nlo] = j; nlo++; } else overflow = true;
+            } else {
+              if (nup < NB_LOCAL) { up_id[nup] = jid; up_slot[nup] = j; nup++; } else overflow = true;
+            }
+          }
+        }
+      }
+  // stable insertion sorts by id
+  for (int i = 1; i < nlo; i++) {
+    int ki = lo_id[i], ks = lo_slot[i], m = i - 1;
+    while (m >= 0 && lo_id[m] > ki) { lo_id[m + 1] = lo_id[m]; lo_slot[m + 1] = lo_slot[m]; m--; }
+    lo_id[m + 1] = ki; lo_slot[m + 1] = ks;
+  }
+  if (!R.use_cell) {
+    for (int i = 1; i < nup; i++) {
+      int ki = up_id[i], ks = up_slot[i], m = i - 1;
+      while (m >= 0 && up_id[m] > ki) { up_id[m + 1] = up_id[m]; up_slot[m + 1] = up_slot[m]; m--; }
+      up_id[m + 1] = ki; up_slot[m + 1] = ks;
+    }
+  }
+  const int total = nlo + nup;
+  atomicMax(maxnb, total);
+  if (total > nl.cap || overflow) {
+    atomicOr(status, ST_OVERFLOW);
+    nl.cnt[k] = 0; nl.lo[k] = 0;
+  } else {
+    for (int q = 0; q < nlo; q++) nl.nb[(size_t)q * nl.stride + k] = lo_slot[q];
+    for (int q = 0; q < nup; q++) nl.nb[(size_t)(nlo + q) * nl.stride + k] = up_slot[q];
+    nl.cnt[k] = total; nl.lo[k] = nlo;
+  }
+  nl.ox[k] = x; nl.oy[k] = y; nl.oz[k] = z;
+}
+
+}  // namespace sg

@@ -1,0 +1,238 @@
+"""ctypes binding of the C ABI in include/samos_gpu.h.
+
+The binding is deliberately thin: every method forwards to one ``sg_*``
+entry point and turns a negative status into :class:`EngineError` carrying
+``sg_last_error``.  Loading fails loudly when the CUDA library has not been
+built -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsamos_gpu.so")
+_lib = None
+
+PAIR = {"soft": 0, "lj": 1, "morse": 2, "gaussian": 3}
+ALIGN = {"polar": 0, "nematic": 1, "vicsek": 2}
+EXTERNAL = {"self_propulsion": 0}
+CONSTRAINT = {"none": 0, "plane": 1, "sphere": 2}
+INTEGRATOR = {"brownian": 0, "brownian_pos": 1, "brownian_align": 2, "langevin": 3, "fire": 4}
+PAIR_NPARAM = 8
+INT_NPARAM = 16
+
+DOUBLE_FIELDS = ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "tau_x", "tau_y", "tau_z",
+                 "nx", "ny", "nz", "Nx", "Ny", "Nz", "omega", "age", "radius", "mass")
+INT_FIELDS = ("type", "ix", "iy", "iz")
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"samos_gpu error {code}: {msg}")
+        self.code = code
+
+
+class RunStats(C.Structure):
+    _fields_ = [("steps_done", C.c_int64), ("nlist_builds", C.c_int64),
+                ("kernel_launches", C.c_int64), ("max_neighbours", C.c_int32),
+                ("status", C.c_int32), ("device_ms", C.c_double), ("step_kernel_ms", C.c_double),
+                ("step_kernels", C.c_int64)]
+
+
+def library_path() -> str:
+    return _LIB_PATH
+
+
+def load() -> C.CDLL:
+    """Load libsamos_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(f"{_LIB_PATH} is missing: build it with "
+                          "`python -m samos_b200.build` (nvcc, sm_100a)")
+    lib = C.CDLL(_LIB_PATH)
+    P, I, D, I64 = C.c_void_p, C.c_int, C.c_double, C.c_int64
+    dp = C.POINTER(C.c_double)
+    sig = {
+        "sg_create": (I, [I, C.POINTER(C.c_int32), I, C.POINTER(P)]),
+        "sg_destroy": (I, [P]),
+        "sg_error_string": (C.c_char_p, [I]),
+        "sg_last_error": (C.c_char_p, [P]),
+        "sg_set_box": (I, [P, I, D, D, D, I]),
+        "sg_set_timestep": (I, [P, D]),
+        "sg_upload": (I, [P, I, C.c_char_p, P]),
+        "sg_download": (I, [P, I, C.c_char_p, P]),
+        "sg_set_nlist": (I, [P, D, D]),
+        "sg_build_nlist": (I, [P]),
+        "sg_get_pairs": (I, [P, I, C.POINTER(C.c_int32), C.POINTER(C.c_int32), I64, C.POINTER(I64)]),
+        "sg_add_pair": (I, [P, I, dp, dp, I, I, I, I, dp]),
+        "sg_add_align": (I, [P, I, D, D, dp, I]),
+        "sg_add_external": (I, [P, I, D, dp, I]),
+        "sg_add_constraint": (I, [P, I, dp]),
+        "sg_add_integrator": (I, [P, I, dp, dp]),
+        "sg_set_replica_param": (I, [P, I, I, I, I, D]),
+        "sg_compute": (I, [P, D]),
+        "sg_enforce": (I, [P]),
+        "sg_run": (I, [P, I64, C.POINTER(RunStats)]),
+        "sg_minimize": (I, [P, I64, C.POINTER(I64), C.POINTER(RunStats)]),
+        "sg_energy": (I, [P, I, I, I, dp]),
+        "sg_fire_state": (I, [P, I, dp]),
+        "sg_kernel_launches": (I64, [P]),
+        "sg_set_profiling": (I, [P, I]),
+        "sg_set_device": (I, [I]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _arr(a):
+    """float64 contiguous copy (or None); the caller keeps it alive across the call."""
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _dptr(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Engine:
+    """One device ensemble of ``len(n_particles)`` replicas."""
+
+    def __init__(self, n_particles, ntypes: int = 1, device: int | None = None):
+        self.lib = load()
+        if device is not None and self.lib.sg_set_device(int(device)) != 0:
+            raise EngineError(-2, f"cannot select CUDA device {device}")
+        if np.isscalar(n_particles):
+            n_particles = [int(n_particles)]
+        self.n = [int(v) for v in n_particles]
+        self.ntypes = int(ntypes)
+        arr = (C.c_int32 * len(self.n))(*self.n)
+        h = C.c_void_p()
+        rc = self.lib.sg_create(len(self.n), arr, self.ntypes, C.byref(h))
+        if rc != 0:
+            raise EngineError(rc, self.lib.sg_error_string(rc).decode())
+        self.h = h
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            raise EngineError(rc, self.lib.sg_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.sg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- configuration -----------------------------------------------------
+    def set_box(self, lx, ly, lz, periodic=True, replica=None):
+        for r in (range(len(self.n)) if replica is None else [replica]):
+            self._check(self.lib.sg_set_box(self.h, r, lx, ly, lz, int(bool(periodic))))
+
+    def set_timestep(self, dt):
+        self._check(self.lib.sg_set_timestep(self.h, float(dt)))
+
+    def upload(self, field: str, values, replica: int = 0):
+        dtype = np.int32 if field in INT_FIELDS else np.float64
+        a = np.ascontiguousarray(values, dtype=dtype)
+        if a.shape != (self.n[replica],):
+            raise ValueError(f"{field}: expected {self.n[replica]} values, got {a.shape}")
+        self._check(self.lib.sg_upload(self.h, replica, field.encode(), a.ctypes.data_as(C.c_void_p)))
+
+    def download(self, field: str, replica: int = 0) -> np.ndarray:
+        dtype = np.int32 if field in INT_FIELDS else np.float64
+        a = np.empty(self.n[replica], dtype=dtype)
+        self._check(self.lib.sg_download(self.h, replica, field.encode(), a.ctypes.data_as(C.c_void_p)))
+        return a
+
+    def set_nlist(self, rcut, pad):
+        self._check(self.lib.sg_set_nlist(self.h, float(rcut), float(pad)))
+
+    def build_nlist(self):
+        self._check(self.lib.sg_build_nlist(self.h))
+
+    def pairs(self, replica: int = 0):
+        n = C.c_int64()
+        self.lib.sg_get_pairs(self.h, replica, None, None, 0, C.byref(n))
+        cap = max(1, n.value)
+        i = np.empty(cap, np.int32)
+        j = np.empty(cap, np.int32)
+        self._check(self.lib.sg_get_pairs(self.h, replica, i.ctypes.data_as(C.POINTER(C.c_int32)),
+                                          j.ctypes.data_as(C.POINTER(C.c_int32)), cap, C.byref(n)))
+        return i[:n.value], j[:n.value]
+
+    def add_pair(self, kind, global_params, table=None, use_radii=False, phase_in=False,
+                 shifted=False, has_pair_params=False, phase_value=None):
+        g = np.zeros(PAIR_NPARAM)
+        g[:len(global_params)] = global_params
+        t, pv = _arr(table), _arr(phase_value)
+        self._check(self.lib.sg_add_pair(self.h, int(kind), _dptr(g), _dptr(t), int(use_radii),
+                                         int(phase_in), int(shifted), int(has_pair_params), _dptr(pv)))
+
+    def add_align(self, kind, J, rcut, table=None, has_pair_params=False):
+        t = _arr(table)
+        self._check(self.lib.sg_add_align(self.h, int(kind), float(J), float(rcut), _dptr(t),
+                                          int(has_pair_params)))
+
+    def add_external(self, kind, alpha, type_alpha=None, has_params=False):
+        t = _arr(type_alpha)
+        self._check(self.lib.sg_add_external(self.h, int(kind), float(alpha), _dptr(t), int(has_params)))
+
+    def add_constraint(self, kind, params):
+        p = np.zeros(8)
+        p[:len(params)] = params
+        self._check(self.lib.sg_add_constraint(self.h, int(kind), _dptr(p)))
+
+    def add_integrator(self, kind, params, temperature=None):
+        p = np.zeros(INT_NPARAM)
+        p[:len(params)] = params
+        t = _arr(temperature)
+        self._check(self.lib.sg_add_integrator(self.h, int(kind), _dptr(p), _dptr(t)))
+
+    def set_replica_param(self, replica, cls, comp, slot, value):
+        self._check(self.lib.sg_set_replica_param(self.h, replica, cls, comp, slot, float(value)))
+
+    # -- execution ---------------------------------------------------------
+    def compute(self, dt):
+        self._check(self.lib.sg_compute(self.h, float(dt)))
+
+    def enforce(self):
+        self._check(self.lib.sg_enforce(self.h))
+
+    def run(self, steps: int) -> RunStats:
+        st = RunStats()
+        self._check(self.lib.sg_run(self.h, int(steps), C.byref(st)))
+        return st
+
+    def minimize(self, max_steps: int):
+        st = RunStats()
+        conv = np.full(len(self.n), -1, np.int64)
+        self._check(self.lib.sg_minimize(self.h, int(max_steps),
+                                         conv.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(st)))
+        return conv, st
+
+    def energy(self, cls: int, comp: int, replica: int = 0) -> float:
+        out = C.c_double()
+        self._check(self.lib.sg_energy(self.h, replica, cls, comp, C.byref(out)))
+        return out.value
+
+    def fire_state(self, replica: int = 0):
+        out = np.zeros(5)
+        self._check(self.lib.sg_fire_state(self.h, replica, _dptr(out)))
+        return out
+
+    def set_profiling(self, on: bool) -> None:
+        self._check(self.lib.sg_set_profiling(self.h, int(bool(on))))
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.sg_kernel_launches(self.h))

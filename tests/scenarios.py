@@ -1,0 +1,71 @@
+"""Seeded synthetic inputs shaped like the benchmark configurations, and a
+helper that drives the same conf-level command sequence through any backend
+(the GPU engine or the CPU oracle)."""
+from __future__ import annotations
+
+import numpy as np
+
+from samos_b200.plugins import Simulation
+
+
+def plane_disks(n, phi, rmin=0.9, rmax=1.1, seed=1, bidisperse=None):
+    """n disks uniform in a square periodic box at packing fraction phi
+    (overlaps allowed), uniform random polar directions in the plane."""
+    rng = np.random.default_rng(seed)
+    if bidisperse is None:
+        r = rng.uniform(rmin, rmax, n)
+    else:
+        r = np.where(np.arange(n) % 2 == 0, bidisperse[0], bidisperse[1]).astype(float)
+        rng.shuffle(r)
+    L = float(np.sqrt(np.sum(np.pi * r * r) / phi))
+    th = rng.uniform(0.0, 2.0 * np.pi, n)
+    parts = dict(x=rng.uniform(-L / 2, L / 2, n), y=rng.uniform(-L / 2, L / 2, n), z=np.zeros(n),
+                 vx=np.zeros(n), vy=np.zeros(n), vz=np.zeros(n),
+                 nx=np.cos(th), ny=np.sin(th), nz=np.zeros(n), radius=r)
+    return parts, L
+
+
+def sphere_disks(n, R=None, seed=1, radius=1.0):
+    """n particles uniform on a sphere (z ~ U[-R,R], phi ~ U[0,2pi)) with
+    random tangent directors; R from n*pi*r^2 = 4 pi R^2 by default."""
+    rng = np.random.default_rng(seed)
+    if R is None:
+        R = float(np.sqrt(n * radius * radius / 4.0))
+    z = rng.uniform(-R, R, n)
+    ph = rng.uniform(0.0, 2.0 * np.pi, n)
+    s = np.sqrt(np.maximum(R * R - z * z, 0.0))
+    x, y = s * np.cos(ph), s * np.sin(ph)
+    pos = np.stack([x, y, z], 1)
+    Nn = pos / R
+    a = rng.normal(size=(n, 3))
+    t = a - np.sum(a * Nn, 1)[:, None] * Nn
+    t /= np.linalg.norm(t, axis=1)[:, None]
+    parts = dict(x=x, y=y, z=z, vx=np.zeros(n), vy=np.zeros(n), vz=np.zeros(n),
+                 nx=t[:, 0], ny=t[:, 1], nz=t[:, 2], radius=np.full(n, radius))
+    return parts, R
+
+
+def drive(backend, parts, box, periodic=True, nlist=(2.4, 0.3), constraint=("plane", {}),
+          pairs=(), aligns=(), externals=(), dt=1e-3, integrators=(), ntypes=1,
+          pair_params=(), align_params=()):
+    sim = Simulation(backend, ntypes=ntypes)
+    sim.box(*box, periodic)
+    sim.input(**parts)
+    if nlist is not None:
+        sim.nlist(*nlist)
+    if constraint is not None:
+        sim.constraint(*constraint)
+    for name, p in pairs:
+        sim.pair_potential(name, dict(p))
+    for name, p in pair_params:
+        sim.pair_param(name, dict(p))
+    for name, p in aligns:
+        sim.pair_align(name, dict(p))
+    for name, p in align_params:
+        sim.align_param(name, dict(p))
+    for name, p in externals:
+        sim.external(name, dict(p))
+    sim.timestep(dt)
+    for name, p in integrators:
+        sim.integrator(name, dict(p))
+    return sim

@@ -1,0 +1,172 @@
+"""CPU checks of the oracle against hand-derived known answers (the
+reference ships no test vectors): two-particle forces/energies of each pair
+potential, aligner torques, constraint projections, integrator steps, the
+neighbour-list build invariants and the noise stream."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle.oracle import OracleSystem, noise_gauss, noise_log, noise_uniform
+from samos_b200 import engine as E
+from scenarios import drive, plane_disks, sphere_disks
+
+
+def two(x2, y2=0.0, r=(1.0, 1.0), box=20.0, n1=(1.0, 0.0, 0.0), n2=(0.0, 1.0, 0.0)):
+    parts = dict(x=np.array([0.0, x2]), y=np.array([0.0, y2]), z=np.zeros(2),
+                 nx=np.array([n1[0], n2[0]]), ny=np.array([n1[1], n2[1]]), nz=np.array([n1[2], n2[2]]),
+                 radius=np.array(r, float))
+    return parts, (box, box, box)
+
+
+def run_compute(parts, box, pairs=(), aligns=(), externals=(), nlist=(3.0, 0.5)):
+    o = OracleSystem(len(parts["x"]))
+    sim = drive(o, parts, box, nlist=nlist, constraint=None, pairs=pairs, aligns=aligns, externals=externals)
+    sim.commit()
+    o.compute(1e-3)
+    return o
+
+
+def test_soft_two_particles():
+    parts, box = two(1.5, r=(1.0, 0.8))
+    o = run_compute(parts, box, pairs=[("soft", {"k": "10", "use_particle_radii": ""})])
+    # U = k/2 (a_i + a_j - r)^2, F_i = -k (a_i+a_j-r) * (x_j - x_i)/r
+    d = 1.8 - 1.5
+    assert o.energy(0, 0) == pytest.approx(0.5 * 10 * d * d, rel=1e-15)
+    fx = o.download("fx")
+    assert fx[0] == pytest.approx(-10 * d, rel=1e-14)
+    assert fx[1] == -fx[0]
+
+
+def test_soft_out_of_contact_is_zero():
+    parts, box = two(2.5, r=(1.0, 1.0))
+    o = run_compute(parts, box, pairs=[("soft", {"k": "10", "use_particle_radii": ""})])
+    assert o.energy(0, 0) == 0.0
+    assert np.all(o.download("fx") == 0.0)
+
+
+def test_lj_two_particles_reference_force_factor():
+    parts, box = two(1.2)
+    o = run_compute(parts, box, pairs=[("lj", {"epsilon": "1.5", "sigma": "1.1", "rcut": "2.5"})])
+    s2 = 1.1 ** 2 / 1.2 ** 2
+    s6 = s2 ** 3
+    assert o.energy(0, 0) == pytest.approx(4 * 1.5 * s6 * (s6 - 1), rel=1e-13)
+    # the reference multiplies by sigma^2/r^2 (pair_lj_potential.cpp:107)
+    ff = 48 * 1.5 * s6 * (s6 - 0.5) * s2
+    assert o.download("fx")[0] == pytest.approx(ff * (0.0 - 1.2), rel=1e-13)
+
+
+def test_morse_two_particles():
+    parts, box = two(1.3)
+    o = run_compute(parts, box, pairs=[("morse", {"D": "2", "a": "1.5", "re": "1.1", "rcut": "3"})])
+    e = math.exp(-1.5 * (1.3 - 1.1))
+    assert o.energy(0, 0) == pytest.approx(2 * (e - 1) ** 2 - 2, rel=1e-13)
+    ff = 2 * 2 * 1.5 * e * (e - 1) / 1.3
+    assert o.download("fx")[0] == pytest.approx(ff * (0.0 - 1.3), rel=1e-13)
+
+
+def test_gaussian_shift_and_table_quirk():
+    parts, box = two(1.0)
+    o = run_compute(parts, box, pairs=[("gaussian", {"A": "2", "B": "-1", "alpha": "1", "beta": "3",
+                                                     "rA": "0", "rB": "1.5", "rcut": "2.5", "shifted": ""})])
+    u = 2 * math.exp(-1.0) - math.exp(-3 * 0.25)
+    shift = 2 * math.exp(-6.25) - math.exp(-3 * 1.0)
+    assert o.energy(0, 0) == pytest.approx(u - shift, rel=1e-13)
+
+
+def test_polar_and_nematic_torques():
+    parts, box = two(1.0, n1=(1.0, 0.0, 0.0), n2=(math.cos(0.3), math.sin(0.3), 0.0))
+    o = run_compute(parts, box, aligns=[("polar", {"J": "0.7", "rcut": "2"})])
+    tz = o.download("tau_z")
+    assert tz[0] == pytest.approx(0.7 * math.sin(0.3), rel=1e-14)
+    assert tz[1] == -tz[0]
+    assert o.energy(1, 0) == pytest.approx(-2 * 0.7 * math.cos(0.3), rel=1e-14)
+    o = run_compute(parts, box, aligns=[("nematic", {"J": "0.7", "rcut": "2"})])
+    # J doubled by default (pair_nematic_aligner.cpp:37)
+    assert o.download("tau_z")[0] == pytest.approx(1.4 * math.cos(0.3) * math.sin(0.3), rel=1e-14)
+
+
+def test_vicsek_normalises():
+    parts, box = two(1.0)
+    parts["vx"] = np.array([1.0, 0.0])
+    parts["vy"] = np.array([0.0, 2.0])
+    o = run_compute(parts, box, aligns=[("vicsek", {"rcut": "2"})])
+    t = np.stack([o.download("tau_x"), o.download("tau_y")], 1)
+    assert np.allclose(np.linalg.norm(t, axis=1), 1.0)
+    assert np.allclose(t[0], np.array([1.0, 2.0]) / math.sqrt(5))
+
+
+def test_self_propulsion_adds_alpha_n():
+    parts, box = two(5.0)
+    o = run_compute(parts, box, externals=[("self_propulsion", {"alpha": "0.5"})])
+    assert np.allclose(o.download("fx"), [0.5, 0.0])
+    assert np.allclose(o.download("fy"), [0.0, 0.5])
+
+
+def test_brownian_step_without_force_or_noise():
+    # one step, zero force, nu = 0: x advances exactly by dt*v0*n
+    parts, box = two(8.0)
+    o = OracleSystem(2)
+    sim = drive(o, parts, box, constraint=("plane", {}), pairs=[("soft", {"k": "1", "use_particle_radii": ""})],
+                dt=0.01, integrators=[("brownian", {"v0": "0.5", "nu": "0", "seed": "1"})])
+    sim.run(0)  # run 0 = one integration step
+    assert o.download("x")[0] == 0.0 + 0.01 * 0.5
+    assert o.download("y")[1] == 0.0 + 0.01 * 0.5
+
+
+def test_sphere_projection_keeps_radius():
+    parts, R = sphere_disks(300, seed=3)
+    o = OracleSystem(300)
+    drive(o, parts, (2 * R + 10, 2 * R + 10, 2 * R + 10), periodic=False, constraint=("sphere", {"r": str(R)}))
+    r = np.sqrt(o.download("x") ** 2 + o.download("y") ** 2 + o.download("z") ** 2)
+    assert np.allclose(r, R, rtol=1e-15, atol=0)
+    n = np.stack([o.download("nx"), o.download("ny"), o.download("nz")], 1)
+    pos = np.stack([o.download("x"), o.download("y"), o.download("z")], 1)
+    assert np.allclose(np.sum(n * pos, 1) / R, 0.0, atol=1e-14)
+
+
+def test_cell_and_nsq_builds_give_same_pair_set():
+    parts, L = plane_disks(600, 0.6, seed=4)
+    a = OracleSystem(600)
+    drive(a, parts, (L, L, 10.0), nlist=(2.4, 0.3), constraint=None)
+    assert a.uses_cells()
+    b = OracleSystem(600)
+    drive(b, parts, (L, L, 4.0), nlist=(2.4, 0.3), constraint=None)  # lz <= 2 cut -> N^2 path
+    assert not b.uses_cells()
+    sa = set(zip(*[x.tolist() for x in a.pairs()]))
+    sb = set(zip(*[x.tolist() for x in b.pairs()]))
+    assert sa == sb and len(sa) > 0
+    assert all(i < j for i, j in sa)
+
+
+def test_fire_relaxes_two_overlapping_disks_to_contact():
+    parts, box = two(1.2, r=(1.0, 1.0))
+    o = OracleSystem(2)
+    sim = drive(o, parts, box, constraint=("plane", {}), pairs=[("soft", {"k": "1", "use_particle_radii": ""})],
+                dt=0.01, integrators=[("fire", {"fmax_tolerance": "1e-10"})])
+    sim.commit()
+    steps, _ = o.minimize(100000)
+    assert steps[0] > 0
+    x = o.download("x")
+    # soft repulsion is flat beyond contact: the minimum is any separation >= 2
+    assert abs(x[1] - x[0]) > 2.0 - 1e-10
+    assert np.max(np.abs(o.download("fx"))) < 1e-10
+
+
+def test_noise_stream_statistics():
+    g = np.array([noise_gauss(5, c) for c in range(20000)])
+    assert abs(g.mean()) < 0.03 and abs(g.std() - 1.0) < 0.02
+    u = np.array([noise_uniform(5, c) for c in range(20000)])
+    assert u.min() >= 0.0 and u.max() < 1.0 and abs(u.mean() - 0.5) < 0.01
+    for x in (1e-300, 1e-5, 0.3, 0.7071, 0.99999999):
+        assert noise_log(x) == pytest.approx(math.log(x), rel=4e-16, abs=1e-300)
+
+
+def test_run_executes_steps_plus_one():
+    parts, box = two(8.0)
+    o = OracleSystem(2)
+    sim = drive(o, parts, box, constraint=("plane", {}), pairs=[("soft", {})], dt=0.01,
+                integrators=[("brownian", {"v0": "1", "nu": "0"})])
+    sim.run(9)  # samos.cpp:878 runs t = 0..9
+    assert o.download("x")[0] == pytest.approx(10 * 0.01, rel=1e-14)
+    assert o.download("age")[0] == pytest.approx(10 * 0.01, rel=1e-14)
