@@ -201,6 +201,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--particles", type=int, default=N_PART,
+                    help="system size (profiling runs use a smaller system of the same density)")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if ws > 1:
@@ -220,8 +222,9 @@ def main():
     from samos_b200 import Engine
     from samos_b200.plugins import Simulation
 
-    parts, L = make_particles(N_PART, seed=1 + rank)
-    eng = Engine(N_PART, device=local)
+    n_part = args.particles
+    parts, L = make_particles(n_part, seed=1 + rank)
+    eng = Engine(n_part, device=local)
     sim = Simulation(eng)
     configure(sim, parts, L)
 
@@ -235,14 +238,14 @@ def main():
         st = eng.run(args.steps - 1)
     launches = eng.kernel_launches() - launches0
     t_ms = max_over_ranks(st.device_ms, ws)
-    value = ws * N_PART * args.steps / (t_ms * 1e-3)
+    value = ws * n_part * args.steps / (t_ms * 1e-3)
 
     # dominant kernel: per-launch CUDA-event time of the fused step kernel
     eng.set_profiling(True)
     pst = eng.run(min(args.steps, 200) - 1)
     eng.set_profiling(False)
     k_ms = pst.step_kernel_ms / max(1, pst.step_kernels)
-    achieved = N_PART * BYTES_PER_PARTICLE_STEP / (k_ms * 1e-3) / 1e9
+    achieved = n_part * BYTES_PER_PARTICLE_STEP / (k_ms * 1e-3) / 1e9
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -266,9 +269,9 @@ def main():
     est = eng.run(e2e_steps - 1)
     outs = {f: eng.download(f) for f in fields_out}
     e2e_s = max_over_ranks(time.perf_counter() - t0, ws)
-    h2d = len(fields_in) * 8 * N_PART / e2e_steps
-    d2h = len(fields_out) * 8 * N_PART / e2e_steps
-    e2e_value = ws * N_PART * e2e_steps / e2e_s
+    h2d = len(fields_in) * 8 * n_part / e2e_steps
+    d2h = len(fields_out) * 8 * n_part / e2e_steps
+    e2e_value = ws * n_part * e2e_steps / e2e_s
     finite = all(np.isfinite(v).all() for v in outs.values())
 
     cpu = None
@@ -280,7 +283,8 @@ def main():
             metric=METRIC, value=value, unit=UNIT, n_gpus=ws, steps=args.steps, warmup=args.warmup,
             ms_per_step=t_ms / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
             dtype="f64", data="synthetic",
-            config=dict(workload=WORKLOAD, n_particles=N_PART, box=L, parallelism=f"replicas x{ws}",
+            config=dict(workload=WORKLOAD if n_part == N_PART else WORKLOAD.replace("4,194,304", f"{n_part:,}"),
+                        n_particles=n_part, box=L, parallelism=f"replicas x{ws}",
                         l2="state resident in HBM, 1.4 GB per buffer set >> 126 MB L2 (no flush needed)",
                         nlist_builds_timed=st.nlist_builds),
             roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,

@@ -160,6 +160,11 @@ int64_t sg_kernel_launches(const sg_system* s);
  * handle's stream (reported in sg_run_stats.step_kernel_ms).  No reference
  * counterpart (instrumentation).                                            */
 int  sg_set_profiling(sg_system* s, int on);
+/* Execution path: 0 = automatic (packed hot kernels for a periodic plane or
+ * a sphere), 1 = always the generic structure-of-arrays kernels.  Both give
+ * the same results; the switch exists so tests can compare them.  No
+ * reference counterpart.                                                    */
+int  sg_set_path(sg_system* s, int path);
 
 #ifdef __cplusplus
 }

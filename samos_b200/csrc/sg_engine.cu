@@ -2,7 +2,7 @@
 // include/samos_gpu.h.  One stream per handle; device buffers are allocated
 // once per configuration and reused by every step.
 #include "samos_gpu.h"
-#include "sg_kernels.cuh"
+#include "sg_hot.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -78,6 +78,9 @@ struct sg_system {
   DevBuf mem;
   std::string last_error;
   std::vector<double> uploaded_N[3];
+  D4 *G[2] = {nullptr, nullptr}, *H[2] = {nullptr, nullptr};
+  int hot_buf = 0;
+  int force_generic = 0;  // testing aid: keep the generic SoA kernels
 };
 
 static int fail(sg_system* s, int code, const std::string& msg) {
@@ -765,6 +768,82 @@ static int step_fused(sg_system* s, bool apply_e1, bool energy) {
   return SG_OK;
 }
 
+// The two packed shapes: one plane constraint on a periodic box with zpos
+// inside it, or one sphere constraint; Brownian-family integrators; no
+// vicsek aligner (needs neighbour velocities) and no phase-in (needs ages).
+static int hot_shape(const sg_system* s) {
+  const Program& P = s->prog;
+  if (s->force_generic || !fused_program(P) || P.ncons != 1) return HOT_NONE;
+  for (int c = 0; c < P.nalign; c++)
+    if (P.align[c].kind == ALIGN_VICSEK) return HOT_NONE;
+  for (int c = 0; c < P.npair; c++)
+    if (P.pair[c].phase_in) return HOT_NONE;
+  if (P.cons[0].kind == CONS_PLANE) {
+    for (const Replica& R : s->reps_h)
+      if (!R.periodic || !(R.cons_p[0] > R.zlo && R.cons_p[0] <= R.zhi)) return HOT_NONE;
+    return HOT_PLANE;
+  }
+  if (P.cons[0].kind == CONS_SPHERE) return HOT_SPHERE;
+  return HOT_NONE;
+}
+
+static int hot_alloc(sg_system* s, int shape) {
+  for (int b = 0; b < 2; b++) {
+    if (!s->G[b]) s->G[b] = s->mem.alloc<D4>(s->slots);
+    if (shape == HOT_SPHERE && !s->H[b]) s->H[b] = s->mem.alloc<D4>(s->slots);
+  }
+  if (s->mem.err != cudaSuccess) { s->mem.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "hot buffers"); }
+  return SG_OK;
+}
+
+static int hot_pack(sg_system* s, int shape) {
+  if (shape == HOT_PLANE)
+    k_hot_pack<HOT_PLANE><<<s->nblocks, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->st, s->G[s->hot_buf], nullptr);
+  else
+    k_hot_pack<HOT_SPHERE><<<s->nblocks, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->st, s->G[s->hot_buf],
+                                                                s->H[s->hot_buf]);
+  LAUNCH_CHECK(s);
+  return SG_OK;
+}
+
+static int hot_unpack(sg_system* s, int shape) {
+  if (shape == HOT_PLANE)
+    k_hot_unpack<HOT_PLANE><<<s->nblocks, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->G[s->hot_buf], nullptr);
+  else
+    k_hot_unpack<HOT_SPHERE><<<s->nblocks, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->G[s->hot_buf],
+                                                                  s->H[s->hot_buf]);
+  LAUNCH_CHECK(s);
+  return SG_OK;
+}
+
+}  // extern "C"
+
+template <int SHAPE>
+static void launch_hot(sg_system* s, bool apply_e1, bool last, bool energy) {
+  const int b = s->hot_buf;
+  D4 *Gi = s->G[b], *Go = s->G[1 - b], *Hi = s->H[b], *Ho = s->H[1 - b];
+  if (energy)
+    k_hot_step<SHAPE, true><<<s->nblocks, BLOCK, 0, s->stream>>>(
+        s->prog, s->reps, s->blk_rep, s->clk, Gi, Go, Hi, Ho, s->cur, s->st, s->nl, s->rebuild, s->status,
+        s->dt_global, apply_e1 ? 1 : 0, last ? 1 : 0, s->epart, s->nblocks);
+  else
+    k_hot_step<SHAPE, false><<<s->nblocks, BLOCK, 0, s->stream>>>(
+        s->prog, s->reps, s->blk_rep, s->clk, Gi, Go, Hi, Ho, s->cur, s->st, s->nl, s->rebuild, s->status,
+        s->dt_global, apply_e1 ? 1 : 0, last ? 1 : 0, s->epart, s->nblocks);
+}
+
+extern "C" {
+
+static int step_hot(sg_system* s, int shape, bool apply_e1, bool last, bool energy) {
+  if (s->profile) CU(s, cudaEventRecord(s->ev_k0, s->stream));
+  if (shape == HOT_PLANE) launch_hot<HOT_PLANE>(s, apply_e1, last, energy);
+  else launch_hot<HOT_SPHERE>(s, apply_e1, last, energy);
+  LAUNCH_CHECK(s);
+  if (s->profile) CU(s, cudaEventRecord(s->ev_k1, s->stream));
+  s->hot_buf = 1 - s->hot_buf;
+  return SG_OK;
+}
+
 static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool driver, int64_t* conv_out) {
   if (!s || steps < 0) return SG_ERR_ARG;
   if (s->prog.ninteg == 0) return fail(s, SG_ERR_STATE, "Integrator has not been defined");
@@ -774,6 +853,8 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
   if (needs_nl && !s->has_nlist) return fail(s, SG_ERR_STATE, "pair terms need a neighbour list");
   if (!s->nl.nb) { int rc = nlist_alloc(s, 1); if (rc) return rc; }
   const bool fused = fused_program(s->prog);
+  const int shape = fused ? hot_shape(s) : HOT_NONE;
+  if (shape != HOT_NONE) { int rc = hot_alloc(s, shape); if (rc) return rc; }
   const int64_t launches0 = s->launches, builds0 = s->builds_run;
   double kernel_ms = 0.0;
   int64_t kernels_timed = 0;
@@ -790,7 +871,17 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
   for (int64_t t = 0; t <= steps; t++) {
     const bool last = (t == steps);
     int rc;
-    if (fused) {
+    if (shape != HOT_NONE) {
+      if (t == 0) {
+        if (!s->e1_applied) {
+          k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st);
+          LAUNCH_CHECK(s);
+        }
+        if ((rc = hot_pack(s, shape))) return rc;
+      }
+      rc = step_hot(s, shape, !last, last, last);
+      s->e1_applied = !last;
+    } else if (fused) {
       if (!s->e1_applied) {
         k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st);
         LAUNCH_CHECK(s);
@@ -805,6 +896,7 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
     k_tail<<<(s->nrep + 127) / 128, 128, 0, s->stream>>>(s->prog, s->reps, s->clk, s->nrep);
     LAUNCH_CHECK(s);
     done++;
+    if (shape != HOT_NONE && last && (rc = hot_unpack(s, shape))) return rc;
     if (s->profile && fused) {
       CU(s, cudaEventSynchronize(s->ev_k1));
       float ms = 0.f;
@@ -818,7 +910,9 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
       bool any = false;
       for (int r = 0; r < s->nrep; r++) any = any || s->rebuild_h[r];
       if (any) {
+        if (shape != HOT_NONE && !last && (rc = hot_unpack(s, shape))) return rc;
         if ((rc = rebuild_flagged(s))) return rc;
+        if (shape != HOT_NONE && !last && (rc = hot_pack(s, shape))) return rc;
         CU(s, cudaMemsetAsync(s->rebuild, 0, sizeof(int) * s->nrep, s->stream));
       }
     }
@@ -866,6 +960,12 @@ int sg_minimize(sg_system* s, int64_t max_steps, int64_t* converged, sg_run_stat
   rc = push_clk(s);
   if (rc) return rc;
   return run_impl(s, max_steps, stats, true, converged);
+}
+
+int sg_set_path(sg_system* s, int path) {
+  if (!s || path < 0 || path > 1) return SG_ERR_ARG;
+  s->force_generic = path;
+  return SG_OK;
 }
 
 int sg_set_profiling(sg_system* s, int on) {

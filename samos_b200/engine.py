@@ -83,6 +83,7 @@ def load() -> C.CDLL:
         "sg_kernel_launches": (I64, [P]),
         "sg_set_profiling": (I, [P, I]),
         "sg_set_device": (I, [I]),
+        "sg_set_path": (I, [P, I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -233,6 +234,10 @@ class Engine:
 
     def set_profiling(self, on: bool) -> None:
         self._check(self.lib.sg_set_profiling(self.h, int(bool(on))))
+
+    def set_generic_path(self, on: bool) -> None:
+        """Force the generic structure-of-arrays kernels (for comparisons)."""
+        self._check(self.lib.sg_set_path(self.h, int(bool(on))))
 
     def kernel_launches(self) -> int:
         return int(self.lib.sg_kernel_launches(self.h))

@@ -214,3 +214,39 @@ def test_fire_matches_oracle():
         assert f.max() < 1e-10
     assert abs(se - so) <= max(5, so // 20)
     assert_traj(e, o, ("x", "y"), tol=1e-7)
+
+
+@pytest.mark.parametrize("shape", ["plane", "sphere"])
+def test_hot_kernels_match_generic_kernels_bitwise(shape):
+    n = 2500
+    if shape == "plane":
+        parts, L = plane_disks(n, 0.7, seed=21)
+        kw = dict(box=(L, L, 10.0), periodic=True, constraint=("plane", {}))
+    else:
+        parts, R = sphere_disks(n, seed=21)
+        b = 2 * R + 6.0
+        kw = dict(box=(b, b, b), periodic=False, constraint=("sphere", {"r": repr(R)}))
+    out = []
+    for generic in (False, True):
+        e = Engine(n)
+        if generic:
+            e.set_generic_path(True)
+        sim = drive(e, parts, kw["box"], periodic=kw["periodic"], nlist=(2.4, 0.3), constraint=kw["constraint"],
+                    pairs=[("soft", {"k": "10", "use_particle_radii": ""})], aligns=[("polar", {"J": "0.3"})],
+                    externals=[("self_propulsion", {"alpha": "0.2"})], dt=1e-3,
+                    integrators=[("brownian", {"v0": "0.5", "nu": "0.2", "seed": "9", "min_val": "0.05"})])
+        sim.run(300)
+        out.append(e)
+    for f in ("x", "y", "z", "nx", "ny", "nz", "vx", "vy", "vz", "fx", "fy", "tau_z", "omega", "age", "ix", "iy"):
+        np.testing.assert_array_equal(out[0].download(f), out[1].download(f), err_msg=f)
+
+
+def test_trajectory_vicsek_generic_fused_path():
+    n = 1200
+    parts, L = plane_disks(n, 0.5, seed=12)
+    rng = np.random.default_rng(12)
+    parts["vx"], parts["vy"] = rng.normal(size=n), rng.normal(size=n)
+    e, o = run_both(n, parts, (L, L, 10.0), 299, nlist=(2.4, 0.3),
+                    pairs=[("soft", {"k": "10", "use_particle_radii": ""})], aligns=[("vicsek", {"rcut": "2.0"})],
+                    dt=1e-3, integrators=[("brownian", {"v0": "0.5", "nu": "0.1", "seed": "3"})])
+    assert_traj(e, o)
