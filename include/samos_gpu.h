@@ -161,10 +161,20 @@ int64_t sg_kernel_launches(const sg_system* s);
  * counterpart (instrumentation).                                            */
 int  sg_set_profiling(sg_system* s, int on);
 /* Execution path: 0 = automatic (packed hot kernels for a periodic plane or
- * a sphere), 1 = always the generic structure-of-arrays kernels.  Both give
- * the same results; the switch exists so tests can compare them.  No
- * reference counterpart.                                                    */
+ * a sphere, specialised when the program is the active-Brownian one),
+ * 1 = always the generic structure-of-arrays kernels, 2 = packed kernels
+ * without the specialisation.  All give the same results; the switch exists
+ * so tests can compare them.  No reference counterpart.                     */
 int  sg_set_path(sg_system* s, int path);
+/* Kernel variant of the specialised active-Brownian step (0..4: per-particle
+ * neighbour sweep, neighbour records fetched ahead x resident blocks per SM;
+ * 5: flattened warp-wide pair sweep); all variants compute the
+ * same bits.  By default the engine's autotuner times every variant on the
+ * first steps of a run and keeps the fastest; sg_set_variant pins one
+ * (-1 re-enables tuning), sg_get_variant reports the choice (-1 = not yet
+ * tuned).  No reference counterpart.                                        */
+int  sg_set_variant(sg_system* s, int variant);
+int  sg_get_variant(const sg_system* s);
 
 #ifdef __cplusplus
 }

@@ -55,6 +55,7 @@ def load() -> C.CDLL:
         "or_noise_gauss": (D, [C.c_uint32, C.c_uint64]),
         "or_noise_uniform": (D, [C.c_uint32, C.c_uint64]),
         "or_noise_log": (D, [D]),
+        "or_noise_cos2pi": (D, [D]),
         "or_philox4x32_10": (None, [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     }
     for name, (res, args) in sig.items():
@@ -197,6 +198,10 @@ def noise_uniform(seed: int, counter: int) -> float:
 
 def noise_log(x: float) -> float:
     return float(load().or_noise_log(x))
+
+
+def noise_cos2pi(u: float) -> float:
+    return float(load().or_noise_cos2pi(u))
 
 
 def philox(ctr, key):

@@ -91,23 +91,60 @@ double or_noise_log(double x)
   return (de * LN2_HI + lm) + de * LN2_LO;
 }
 
-/* Standard normal draw number `counter` of stream `seed`: polar method of
-   Marsaglia and Bray (1964) on Philox blocks (counter, attempt). */
+/* cos(2 pi u) for u in [0,1) given to 53 bits.  4u splits exactly into a
+   quadrant q and a fraction f, and the reflection f -> 1-f is exact, so the
+   polynomial only sees theta = g pi/2 with g in [0, 1/2]: Taylor series of
+   sin to x^15 and cos to x^16 (truncation < 5e-17 on [0, pi/4]). */
+static double cos2pi(double u)
+{
+  double t = u * 4.0;
+  int q = (int)t;
+  double f = t - (double)q;
+  int use_sin = q & 1;            /* q=1,3 need sin(pi f/2) */
+  double g = f;
+  if (f > 0.5) { g = 1.0 - f; use_sin = !use_sin; }
+  double x = g * 1.5707963267948966;
+  double x2 = x * x;
+  double v;
+  if (use_sin) {
+    double p = -1.0 / 1307674368000.0;
+    p = p * x2 + 1.0 / 6227020800.0;
+    p = p * x2 - 1.0 / 39916800.0;
+    p = p * x2 + 1.0 / 362880.0;
+    p = p * x2 - 1.0 / 5040.0;
+    p = p * x2 + 1.0 / 120.0;
+    p = p * x2 - 1.0 / 6.0;
+    v = x + x * (x2 * p);
+  } else {
+    double p = 1.0 / 20922789888000.0;
+    p = p * x2 - 1.0 / 87178291200.0;
+    p = p * x2 + 1.0 / 479001600.0;
+    p = p * x2 - 1.0 / 3628800.0;
+    p = p * x2 + 1.0 / 40320.0;
+    p = p * x2 - 1.0 / 720.0;
+    p = p * x2 + 1.0 / 24.0;
+    p = p * x2 - 0.5;
+    v = 1.0 + x2 * p;
+  }
+  /* cos(pi/2 (q + f)): q=0 +cos, q=1 -sin, q=2 -cos, q=3 +sin */
+  return (q == 1 || q == 2) ? -v : v;
+}
+
+/* Standard normal draw number `counter` of stream `seed`: Box-Muller
+   (Box & Muller 1958) on one Philox block, u1 in (0,1] from words 0-1 and
+   u2 in [0,1) from words 2-3: g = sqrt(-2 ln u1) cos(2 pi u2). */
 double or_noise_gauss(uint32_t seed, uint64_t counter)
 {
   uint32_t key[2] = { seed, OR_NOISE_KEY1 };
-  for (uint32_t attempt = 0; attempt < 64; attempt++) {
-    uint32_t ctr[4] = { (uint32_t)counter, (uint32_t)(counter >> 32), attempt, 0u };
-    uint32_t r[4];
-    or_philox4x32_10(ctr, key, r);
-    double v1 = 2.0 * u53(r[0], r[1]) - 1.0;
-    double v2 = 2.0 * u53(r[2], r[3]) - 1.0;
-    double s = v1 * v1 + v2 * v2;
-    if (s < 1.0 && s > 0.0)
-      return v2 * sqrt(-2.0 * or_noise_log(s) / s);
-  }
-  return 0.0;
+  uint32_t ctr[4] = { (uint32_t)counter, (uint32_t)(counter >> 32), 0u, 0u };
+  uint32_t r[4];
+  or_philox4x32_10(ctr, key, r);
+  double u1 = u53(r[0], r[1]) + (1.0 / 9007199254740992.0);
+  double u2 = u53(r[2], r[3]);
+  return sqrt(-2.0 * or_noise_log(u1)) * cos2pi(u2);
 }
+
+double or_noise_cos2pi(double u) { return cos2pi(u); }
 
 /* Uniform [0,1) draw number `counter` of stream `seed` */
 double or_noise_uniform(uint32_t seed, uint64_t counter)

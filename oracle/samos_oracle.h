@@ -15,8 +15,8 @@
  *
  * Noise: the reference draws from GSL's default generator, which is not
  * available.  Both this oracle and the CUDA path read one project-defined
- * counter-based Gaussian stream (Philox-4x32-10, Salmon et al. SC'11, fed to
- * the Marsaglia-Bray polar method, the method GSL's gsl_ran_gaussian uses),
+ * counter-based Gaussian stream (Philox-4x32-10, Salmon et al. SC'11, one
+ * block per draw, Box-Muller transform with project-written log and cos),
  * consumed in the reference's draw order: RNG object = (seed, counter),
  * one counter value per draw.
  *
@@ -53,6 +53,7 @@ double or_noise_gauss(uint32_t seed, uint64_t counter);
 double or_noise_uniform(uint32_t seed, uint64_t counter);
 void   or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 double or_noise_log(double x);
+double or_noise_cos2pi(double u);
 
 or_system* or_create(int n, int ntypes);
 void       or_destroy(or_system* s);

@@ -1,0 +1,512 @@
+// sg_abp.cuh -- specialised step kernel for the active-Brownian programs the
+// benchmarks run: one `soft` pair potential (single particle type), at most
+// one polar or nematic aligner, optional self_propulsion, one `brownian`
+// integrator, on a periodic plane or a sphere.
+//
+// Compared with k_hot_step the component kinds are template parameters, the
+// replica's parameters are staged once per block in shared memory, and the
+// neighbour sweep fetches four neighbour records before using any of them.
+// The arithmetic per term is the reference's (see sg_kernels.cuh), so results
+// are bit-identical to the generic kernels.
+#pragma once
+#include "sg_hot.cuh"
+
+namespace sg {
+
+enum { ABP_ALIGN_NONE = -1 };
+
+// per-replica constants of the specialised program (host-built)
+struct AbpParams {
+  double xlo, xhi, ylo, yhi, zlo, zhi, Lx, Ly, Lz;
+  double pad2q;           // 0.25*pad*pad  (neighbour_list.cpp:298)
+  double k, a;            // soft: table [1][1] (pair_soft_potential.cpp:77,85)
+  double J, rc2;          // aligner: effective J (nematic: 2J unless align_param), rcut*rcut
+  double alpha;           // self_propulsion alpha
+  double dt, v0, nu, mu, mur, stoch, flip;  // brownian; stoch = sqrt(nu*dt), flip = dt/tau
+  double Rs;              // sphere radius
+  Value temp;
+  int off, n, periodic, use_radii, nematic, velocity;
+  uint32_t seed, pad0;
+};
+
+// Tuning variants (chunk of neighbour records fetched ahead, min blocks/SM):
+// the engine's autotuner times them on the live system and keeps the fastest.
+constexpr int ABP_NVARIANT = 6;  // 0-4 per-particle sweep, 5 flattened sweep
+__host__ __device__ constexpr int abp_chunk(int v) { return v == 0 ? 4 : v == 1 ? 4 : v == 2 ? 2 : v == 3 ? 2 : 8; }
+__host__ __device__ constexpr int abp_minb(int v) { return v == 0 ? 5 : v == 1 ? 4 : v == 2 ? 6 : v == 3 ? 4 : 3; }
+
+template <int SHAPE, int ALIGN, bool SP, bool ENERGY, int VAR>
+__global__ void __launch_bounds__(BLOCK, abp_minb(VAR))
+k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, const Clock* __restrict__ clk,
+           const D4* __restrict__ Gin, D4* __restrict__ Gout, const D4* __restrict__ Hin, D4* __restrict__ Hout,
+           Dyn d, Stat st, NbList nl, int* __restrict__ rebuild, int* __restrict__ status, int apply_e1, int last,
+           double* epart, int nblocks) {
+  constexpr bool PLANE = SHAPE == HOT_PLANE;
+  __shared__ AbpParams S;
+  __shared__ uint64_t s_base;
+  __shared__ int s_step;
+  const int r = blk_rep[blockIdx.x];
+  {
+    constexpr int NW = (int)(sizeof(AbpParams) / 8);
+    static_assert(sizeof(AbpParams) % 8 == 0, "AbpParams must be 8-byte granular");
+    static_assert(NW <= BLOCK, "AbpParams too large for one-word-per-thread staging");
+    if (threadIdx.x < NW)
+      reinterpret_cast<unsigned long long*>(&S)[threadIdx.x] =
+          reinterpret_cast<const unsigned long long*>(prm + r)[threadIdx.x];
+    if (threadIdx.x == 0) { s_base = clk[r].ctr[0]; s_step = clk[r].run_step; }
+  }
+  __syncthreads();
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  double epair = 0.0, ealign = 0.0;
+  if (k - S.off < S.n) {
+    // ---- own state ----------------------------------------------------------
+    double x, y, z, nx, ny, nz, ri;
+    {
+      const D4 g = ldg4(Gin + k);
+      x = g.x; y = g.y;
+      if (PLANE) { z = 0.0; nx = g.z; ny = g.w; nz = 0.0; ri = st.r[k]; }
+      else { z = g.z; ri = g.w; const D4 h = ldg4(Hin + k); nx = h.x; ny = h.y; nz = h.z; }
+    }
+    const int cnt = nl.cnt[k], lo = nl.lo[k];
+    const uint64_t gid = (uint64_t)st.id[k];
+    const double ox = nl.ox[k], oy = nl.oy[k], oz = PLANE ? 0.0 : nl.oz[k];
+    const double age0 = d.age[k];
+
+    // ---- forces and torques ---------------------------------------------------
+    double fx = 0.0, fy = 0.0, fz = 0.0, tx = 0.0, ty = 0.0, tz = 0.0;
+    constexpr int CH = abp_chunk(VAR);
+    bool noise_done = false;
+    double g_rot = 0.0, g_x = 0.0, g_y = 0.0, g_z = 0.0;
+    const double T = value_get(S.temp, s_step);
+    uint64_t base = s_base;
+    if (S.nematic) base += (uint64_t)S.n;
+    const int D = T > 0.0 ? 4 : 1;
+    const uint64_t c0 = base + gid * (uint64_t)D;
+    for (int q0 = 0; q0 < cnt || !noise_done; q0 += CH) {
+      int jj[CH];
+      D4 gg[CH], hh[CH];
+      double rr[CH];
+#pragma unroll
+      for (int u = 0; u < CH; u++) {
+        const int q = q0 + u;
+        jj[u] = q < cnt ? __ldg(nl.nb + (size_t)q * nl.stride + k) : k;
+      }
+#pragma unroll
+      for (int u = 0; u < CH; u++) {
+        gg[u] = ldg4(Gin + jj[u]);
+        if (PLANE) rr[u] = S.use_radii ? __ldg(st.r + jj[u]) : 1.0;
+        if (!PLANE && ALIGN != ABP_ALIGN_NONE) hh[u] = ldg4(Hin + jj[u]);
+      }
+      if (!noise_done) {  // independent of the loads above: overlaps their latency
+        g_rot = noise_gauss(S.seed, c0 + (uint64_t)(D - 1));
+        if (T > 0.0) {
+          g_x = noise_gauss(S.seed, c0 + 0);
+          g_y = noise_gauss(S.seed, c0 + 1);
+          if (!PLANE) g_z = noise_gauss(S.seed, c0 + 2);
+        }
+        noise_done = true;
+      }
+#pragma unroll
+      for (int u = 0; u < CH; u++) {
+        const int q = q0 + u;
+        if (q < cnt) {
+          double dx = gg[u].x - x, dy = gg[u].y - y, dz = 0.0;
+          if (!PLANE) dz = gg[u].z - z;
+          if (S.periodic) {
+            if (dx > S.xhi) dx -= S.Lx; else if (dx < S.xlo) dx += S.Lx;
+            if (dy > S.yhi) dy -= S.Ly; else if (dy < S.ylo) dy += S.Ly;
+            if (!PLANE) { if (dz > S.zhi) dz -= S.Lz; else if (dz < S.zlo) dz += S.Lz; }
+          }
+          const double r_sq = PLANE ? dx * dx + dy * dy : dx * dx + dy * dy + dz * dz;
+          // PairSoftPotential::compute, pair_soft_potential.cpp:79-104
+          const double rj = PLANE ? rr[u] : gg[u].w;
+          const double rd = sqrt(r_sq);
+          const double sig = S.use_radii ? ri + rj : S.a;
+          if (rd < sig) {
+            const double diff = sig - rd;
+            double ff;
+            if (rd > 0.0) ff = S.k * diff / rd; else ff = S.k * diff;
+            fx -= ff * dx; fy -= ff * dy;
+            if (!PLANE) fz -= ff * dz;
+            if (ENERGY && q >= lo) epair += 0.5 * S.k * diff * diff;
+          }
+          if (ALIGN != ABP_ALIGN_NONE && r_sq <= S.rc2) {
+            double onx, ony, onz;
+            if (PLANE) { onx = gg[u].z; ony = gg[u].w; onz = 0.0; }
+            else { onx = hh[u].x; ony = hh[u].y; onz = hh[u].z; }
+            if (PLANE) {
+              const double tau_z = nx * ony - ny * onx;
+              if (ALIGN == ALIGN_POLAR) {
+                tz += S.J * tau_z;
+                if (ENERGY && q >= lo) ealign += -2.0 * S.J * (nx * onx + ny * ony);
+              } else {
+                const double cd = nx * onx + ny * ony;
+                tz += S.J * cd * tau_z;
+                if (ENERGY && q >= lo) ealign += -2.0 * S.J * (2.0 * cd * cd - 1.0);
+              }
+            } else {
+              const double tau_x = ny * onz - nz * ony;
+              const double tau_y = nz * onx - nx * onz;
+              const double tau_z = nx * ony - ny * onx;
+              if (ALIGN == ALIGN_POLAR) {
+                tx += S.J * tau_x; ty += S.J * tau_y; tz += S.J * tau_z;
+                if (ENERGY && q >= lo) ealign += -2.0 * S.J * (nx * onx + ny * ony + nz * onz);
+              } else {
+                const double cd = nx * onx + ny * ony + nz * onz;
+                tx += S.J * cd * tau_x; ty += S.J * cd * tau_y; tz += S.J * cd * tau_z;
+                if (ENERGY && q >= lo) ealign += -2.0 * S.J * (2.0 * cd * cd - 1.0);
+              }
+            }
+          }
+        }
+      }
+    }
+    if (SP) { fx += S.alpha * nx; fy += S.alpha * ny; if (!PLANE) fz += S.alpha * nz; }
+
+    // ---- IntegratorBrownian::integrate (integrator_brownian.cpp:57-121) ----
+    Hp p;
+    p.x = x; p.y = y; p.z = z; p.nx = nx; p.ny = ny; p.nz = nz;
+    p.vx = 0.0; p.vy = 0.0; p.vz = 0.0;
+    if (S.nematic) {
+      // the velocity flip of velocity_align is overwritten below (v = fd)
+      if (noise_uniform(S.seed, s_base + gid) < S.flip) { p.nx = -p.nx; p.ny = -p.ny; p.nz = -p.nz; }
+    }
+    double fd_x = S.v0 * p.nx + S.mu * fx;
+    double fd_y = S.v0 * p.ny + S.mu * fy;
+    double fd_z = S.v0 * p.nz + S.mu * fz;
+    p.vx = fd_x; p.vy = fd_y; p.vz = fd_z;
+    p.x += S.dt * fd_x; p.y += S.dt * fd_y;
+    if (!PLANE) p.z += S.dt * fd_z;
+    if (T > 0.0) {
+      const double B = sqrt(2.0 * S.mu * T), sqrt_dt = sqrt(S.dt);
+      const double fr_x = B * g_x, fr_y = B * g_y;
+      p.vx += fr_x; p.vy += fr_y;
+      p.x += sqrt_dt * fr_x; p.y += sqrt_dt * fr_y;
+      if (!PLANE) { const double fr_z = B * g_z; p.vz += fr_z; p.z += sqrt_dt * fr_z; }
+    }
+    int dix = 0, diy = 0;
+    const ShapeGeom Rb{S.xlo, S.xhi, S.Lx, S.ylo, S.yhi, S.Ly, S.Rs};
+    hot_enforce<SHAPE>(Rb, p, dix, diy);
+    if (PLANE) p.vz = 0.0;
+    p.tx = tx; p.ty = ty; p.tz = tz;
+    p.omega = S.mur * hot_project_torque<SHAPE>(Rb, p);
+    const double dtheta = S.dt * p.omega + S.stoch * g_rot;
+    hot_rotate<SHAPE>(Rb, p, dtheta, S.velocity != 0);
+    const double age = age0 + S.dt;
+
+    // ---- skin test, NeighbourList::need_update (neighbour_list.cpp:278-302)
+    {
+      double ddx = ox - p.x, ddy = oy - p.y, ddz = PLANE ? 0.0 : oz - p.z;
+      if (S.periodic) {
+        if (ddx > S.xhi) ddx -= S.Lx; else if (ddx < S.xlo) ddx += S.Lx;
+        if (ddy > S.yhi) ddy -= S.Ly; else if (ddy < S.ylo) ddy += S.Ly;
+        if (!PLANE) { if (ddz > S.zhi) ddz -= S.Lz; else if (ddz < S.zlo) ddz += S.Lz; }
+      }
+      const double d2 = PLANE ? ddx * ddx + ddy * ddy : ddx * ddx + ddy * ddy + ddz * ddz;
+      if (!(d2 < S.pad2q)) {
+        if (rebuild[r] == 0) atomicOr(&rebuild[r], 1);
+      }
+    }
+    if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) atomicOr(status, ST_NONFINITE);
+    if (apply_e1) hot_enforce<SHAPE>(Rb, p, dix, diy);
+
+    // ---- stores ---------------------------------------------------------------
+    if (PLANE) {
+      stg4(Gout + k, D4{p.x, p.y, p.nx, p.ny});
+      d.vx[k] = p.vx; d.vy[k] = p.vy;
+    } else {
+      stg4(Gout + k, D4{p.x, p.y, p.z, ri});
+      stg4(Hout + k, D4{p.nx, p.ny, p.nz, 0.0});
+      d.vx[k] = p.vx; d.vy[k] = p.vy; d.vz[k] = p.vz;
+    }
+    d.age[k] = age;
+    if (dix) d.ix[k] += dix;
+    if (diy) d.iy[k] += diy;
+    if (last) {
+      d.omega[k] = p.omega;
+      d.fx[k] = fx; d.fy[k] = fy; d.fz[k] = PLANE ? 0.0 : fz;
+      d.tx[k] = tx; d.ty[k] = ty; d.tz[k] = tz;
+    }
+  }
+  if (ENERGY) {
+    double ev[MAX_PAIR + MAX_ALIGN];
+#pragma unroll
+    for (int i = 0; i < MAX_PAIR + MAX_ALIGN; i++) ev[i] = 0.0;
+    ev[0] = epair;
+    ev[MAX_PAIR] = ealign;
+    block_reduce_store<MAX_PAIR + MAX_ALIGN>(ev, epart, nblocks);
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Flattened variant: a warp's (particle, neighbour) items are laid out
+// contiguously in shared memory (exclusive scan of the list lengths) and the
+// expensive part of every pair term (sqrt, IEEE divide, cross products) is
+// evaluated with all 32 lanes busy, whatever the spread of list lengths.
+// Each lane then folds its own particle's terms in list order, so forces and
+// torques are summed exactly as in the per-particle kernels.
+// ---------------------------------------------------------------------------
+template <int SHAPE>
+struct FlatCfg {
+  static constexpr int ITEMS = SHAPE == HOT_PLANE ? 192 : 128;  // item slots per warp
+};
+
+template <int SHAPE, bool ENERGY>
+struct FlatWarp {
+  static constexpr int W = FlatCfg<SHAPE>::ITEMS;
+  static constexpr bool PL = SHAPE == HOT_PLANE;
+  double ox[32], oy[32], oz[PL ? 1 : 32], onx[32], ony[32], onz[PL ? 1 : 32], orr[32];
+  double tfx[W], tfy[W], tfz[PL ? 1 : W];
+  double ttx[PL ? 1 : W], tty[PL ? 1 : W], ttz[W];
+  double tep[ENERGY ? W : 1], tea[ENERGY ? W : 1];
+  int idx[W];
+  unsigned char own[W], valid[W];
+};
+
+template <int SHAPE, int ALIGN, bool SP, bool ENERGY>
+__global__ void __launch_bounds__(BLOCK, 4)
+k_abp_flat(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, const Clock* __restrict__ clk,
+           const D4* __restrict__ Gin, D4* __restrict__ Gout, const D4* __restrict__ Hin, D4* __restrict__ Hout,
+           Dyn d, Stat st, NbList nl, int* __restrict__ rebuild, int* __restrict__ status, int apply_e1, int last,
+           double* epart, int nblocks) {
+  constexpr bool PLANE = SHAPE == HOT_PLANE;
+  using FW = FlatWarp<SHAPE, ENERGY>;
+  constexpr int W = FW::W;
+  extern __shared__ __align__(16) unsigned char flat_smem[];
+  FW& F = reinterpret_cast<FW*>(flat_smem)[threadIdx.x >> 5];
+  __shared__ AbpParams S;
+  __shared__ uint64_t s_base;
+  __shared__ int s_step;
+  const int r = blk_rep[blockIdx.x];
+  {
+    constexpr int NW = (int)(sizeof(AbpParams) / 8);
+    if (threadIdx.x < NW)
+      reinterpret_cast<unsigned long long*>(&S)[threadIdx.x] =
+          reinterpret_cast<const unsigned long long*>(prm + r)[threadIdx.x];
+    if (threadIdx.x == 0) { s_base = clk[r].ctr[0]; s_step = clk[r].run_step; }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  const bool active = k - S.off < S.n;
+
+  // ---- own state into registers and the warp's shared table -------------------
+  double x = 0.0, y = 0.0, z = 0.0, nx = 0.0, ny = 0.0, nz = 0.0, ri = 1.0;
+  int cnt = 0, lo = 0;
+  uint64_t gid = 0;
+  double oxr = 0.0, oyr = 0.0, ozr = 0.0, age0 = 0.0;
+  if (active) {
+    const D4 g = ldg4(Gin + k);
+    x = g.x; y = g.y;
+    if (PLANE) { nx = g.z; ny = g.w; ri = st.r[k]; }
+    else { z = g.z; ri = g.w; const D4 h = ldg4(Hin + k); nx = h.x; ny = h.y; nz = h.z; }
+    cnt = nl.cnt[k]; lo = nl.lo[k];
+    gid = (uint64_t)st.id[k];
+    oxr = nl.ox[k]; oyr = nl.oy[k];
+    if (!PLANE) ozr = nl.oz[k];
+    age0 = d.age[k];
+  }
+  F.ox[lane] = x; F.oy[lane] = y; F.onx[lane] = nx; F.ony[lane] = ny; F.orr[lane] = ri;
+  if (!PLANE) { F.oz[lane] = z; F.onz[lane] = nz; }
+  // exclusive scan of list lengths over the warp
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int excl = incl - cnt;
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+
+  // rotational (and translational) noise: pure ALU, independent of the sweep
+  const double T = value_get(S.temp, s_step);
+  uint64_t base = s_base;
+  if (S.nematic) base += (uint64_t)S.n;
+  const int D = T > 0.0 ? 4 : 1;
+  const uint64_t c0 = base + gid * (uint64_t)D;
+  double g_rot = 0.0, g_x = 0.0, g_y = 0.0, g_z = 0.0;
+
+  double fx = 0.0, fy = 0.0, fz = 0.0, tx = 0.0, ty = 0.0, tz = 0.0;
+  double epair = 0.0, ealign = 0.0;
+  bool noise_done = false;
+  for (int b0 = 0; b0 < total || !noise_done; b0 += W) {
+    // stage this batch's neighbour slots (coalesced per list rank)
+    for (int q = 0; q < cnt; q++) {
+      const int it = excl + q - b0;
+      if (it >= 0 && it < W) { F.idx[it] = __ldg(nl.nb + (size_t)q * nl.stride + k); F.own[it] = (unsigned char)lane; }
+    }
+    if (!noise_done) {
+      if (active) {
+        g_rot = noise_gauss(S.seed, c0 + (uint64_t)(D - 1));
+        if (T > 0.0) {
+          g_x = noise_gauss(S.seed, c0 + 0);
+          g_y = noise_gauss(S.seed, c0 + 1);
+          if (!PLANE) g_z = noise_gauss(S.seed, c0 + 2);
+        }
+      }
+      noise_done = true;
+    }
+    __syncwarp();
+    const int nit = min(W, total - b0);
+    // evaluate the batch's items with every lane busy
+    for (int it = lane; it < nit; it += 32) {
+      const int p = F.own[it];
+      const int j = F.idx[it];
+      const D4 gj = ldg4(Gin + j);
+      double rj, onx, ony, onz = 0.0;
+      if (PLANE) { rj = S.use_radii ? __ldg(st.r + j) : 1.0; onx = gj.z; ony = gj.w; }
+      else {
+        rj = gj.w;
+        if (ALIGN != ABP_ALIGN_NONE) { const D4 hj = ldg4(Hin + j); onx = hj.x; ony = hj.y; onz = hj.z; }
+        else { onx = 0.0; ony = 0.0; }
+      }
+      const double px = F.ox[p], py = F.oy[p], pz = PLANE ? 0.0 : F.oz[p];
+      double dx = gj.x - px, dy = gj.y - py, dz = 0.0;
+      if (!PLANE) dz = gj.z - pz;
+      if (S.periodic) {
+        if (dx > S.xhi) dx -= S.Lx; else if (dx < S.xlo) dx += S.Lx;
+        if (dy > S.yhi) dy -= S.Ly; else if (dy < S.ylo) dy += S.Ly;
+        if (!PLANE) { if (dz > S.zhi) dz -= S.Lz; else if (dz < S.zlo) dz += S.Lz; }
+      }
+      const double r_sq = PLANE ? dx * dx + dy * dy : dx * dx + dy * dy + dz * dz;
+      unsigned char v = 0;
+      // PairSoftPotential::compute, pair_soft_potential.cpp:79-104
+      const double rd = sqrt(r_sq);
+      const double sig = S.use_radii ? F.orr[p] + rj : S.a;
+      if (rd < sig) {
+        const double diff = sig - rd;
+        double ff;
+        if (rd > 0.0) ff = S.k * diff / rd; else ff = S.k * diff;
+        F.tfx[it] = ff * dx; F.tfy[it] = ff * dy;
+        if (!PLANE) F.tfz[it] = ff * dz;
+        if (ENERGY) F.tep[it] = 0.5 * S.k * diff * diff;
+        v |= 1;
+      }
+      if (ALIGN != ABP_ALIGN_NONE && r_sq <= S.rc2) {
+        const double pnx = F.onx[p], pny = F.ony[p], pnz = PLANE ? 0.0 : F.onz[p];
+        if (PLANE) {
+          const double tau_z = pnx * ony - pny * onx;
+          if (ALIGN == ALIGN_POLAR) {
+            F.ttz[it] = S.J * tau_z;
+            if (ENERGY) F.tea[it] = -2.0 * S.J * (pnx * onx + pny * ony);
+          } else {
+            const double cd = pnx * onx + pny * ony;
+            F.ttz[it] = S.J * cd * tau_z;
+            if (ENERGY) F.tea[it] = -2.0 * S.J * (2.0 * cd * cd - 1.0);
+          }
+        } else {
+          const double tau_x = pny * onz - pnz * ony;
+          const double tau_y = pnz * onx - pnx * onz;
+          const double tau_z = pnx * ony - pny * onx;
+          if (ALIGN == ALIGN_POLAR) {
+            F.ttx[it] = S.J * tau_x; F.tty[it] = S.J * tau_y; F.ttz[it] = S.J * tau_z;
+            if (ENERGY) F.tea[it] = -2.0 * S.J * (pnx * onx + pny * ony + pnz * onz);
+          } else {
+            const double cd = pnx * onx + pny * ony + pnz * onz;
+            const double Jc = S.J * cd;
+            F.ttx[it] = Jc * tau_x; F.tty[it] = Jc * tau_y; F.ttz[it] = Jc * tau_z;
+            if (ENERGY) F.tea[it] = -2.0 * S.J * (2.0 * cd * cd - 1.0);
+          }
+        }
+        v |= 2;
+      }
+      F.valid[it] = v;
+    }
+    __syncwarp();
+    // ordered fold of this particle's terms (reference summation order)
+    for (int q = 0; q < cnt; q++) {
+      const int it = excl + q - b0;
+      if (it >= 0 && it < W) {
+        const unsigned char v = F.valid[it];
+        if (v & 1) {
+          fx -= F.tfx[it]; fy -= F.tfy[it];
+          if (!PLANE) fz -= F.tfz[it];
+          if (ENERGY && q >= lo) epair += F.tep[it];
+        }
+        if (v & 2) {
+          if (!PLANE) { tx += F.ttx[it]; ty += F.tty[it]; }
+          tz += F.ttz[it];
+          if (ENERGY && q >= lo) ealign += F.tea[it];
+        }
+      }
+    }
+    __syncwarp();
+  }
+
+  if (active) {
+    if (SP) { fx += S.alpha * nx; fy += S.alpha * ny; if (!PLANE) fz += S.alpha * nz; }
+    // ---- IntegratorBrownian::integrate (integrator_brownian.cpp:57-121) ----
+    Hp p;
+    p.x = x; p.y = y; p.z = z; p.nx = nx; p.ny = ny; p.nz = nz;
+    if (S.nematic) {
+      // the velocity flip of velocity_align is overwritten below (v = fd)
+      if (noise_uniform(S.seed, s_base + gid) < S.flip) { p.nx = -p.nx; p.ny = -p.ny; p.nz = -p.nz; }
+    }
+    double fd_x = S.v0 * p.nx + S.mu * fx;
+    double fd_y = S.v0 * p.ny + S.mu * fy;
+    double fd_z = S.v0 * p.nz + S.mu * fz;
+    p.vx = fd_x; p.vy = fd_y; p.vz = fd_z;
+    p.x += S.dt * fd_x; p.y += S.dt * fd_y;
+    if (!PLANE) p.z += S.dt * fd_z;
+    if (T > 0.0) {
+      const double B = sqrt(2.0 * S.mu * T), sqrt_dt = sqrt(S.dt);
+      const double fr_x = B * g_x, fr_y = B * g_y;
+      p.vx += fr_x; p.vy += fr_y;
+      p.x += sqrt_dt * fr_x; p.y += sqrt_dt * fr_y;
+      if (!PLANE) { const double fr_z = B * g_z; p.vz += fr_z; p.z += sqrt_dt * fr_z; }
+    }
+    int dix = 0, diy = 0;
+    const ShapeGeom Rb{S.xlo, S.xhi, S.Lx, S.ylo, S.yhi, S.Ly, S.Rs};
+    hot_enforce<SHAPE>(Rb, p, dix, diy);
+    if (PLANE) p.vz = 0.0;
+    p.tx = tx; p.ty = ty; p.tz = tz;
+    p.omega = S.mur * hot_project_torque<SHAPE>(Rb, p);
+    const double dtheta = S.dt * p.omega + S.stoch * g_rot;
+    hot_rotate<SHAPE>(Rb, p, dtheta, S.velocity != 0);
+    const double age = age0 + S.dt;
+    {
+      double ddx = oxr - p.x, ddy = oyr - p.y, ddz = PLANE ? 0.0 : ozr - p.z;
+      if (S.periodic) {
+        if (ddx > S.xhi) ddx -= S.Lx; else if (ddx < S.xlo) ddx += S.Lx;
+        if (ddy > S.yhi) ddy -= S.Ly; else if (ddy < S.ylo) ddy += S.Ly;
+        if (!PLANE) { if (ddz > S.zhi) ddz -= S.Lz; else if (ddz < S.zlo) ddz += S.Lz; }
+      }
+      const double d2 = PLANE ? ddx * ddx + ddy * ddy : ddx * ddx + ddy * ddy + ddz * ddz;
+      if (!(d2 < S.pad2q)) {
+        if (rebuild[r] == 0) atomicOr(&rebuild[r], 1);
+      }
+    }
+    if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) atomicOr(status, ST_NONFINITE);
+    if (apply_e1) hot_enforce<SHAPE>(Rb, p, dix, diy);
+    if (PLANE) {
+      stg4(Gout + k, D4{p.x, p.y, p.nx, p.ny});
+      d.vx[k] = p.vx; d.vy[k] = p.vy;
+    } else {
+      stg4(Gout + k, D4{p.x, p.y, p.z, ri});
+      stg4(Hout + k, D4{p.nx, p.ny, p.nz, 0.0});
+      d.vx[k] = p.vx; d.vy[k] = p.vy; d.vz[k] = p.vz;
+    }
+    d.age[k] = age;
+    if (dix) d.ix[k] += dix;
+    if (diy) d.iy[k] += diy;
+    if (last) {
+      d.omega[k] = p.omega;
+      d.fx[k] = fx; d.fy[k] = fy; d.fz[k] = PLANE ? 0.0 : fz;
+      d.tx[k] = tx; d.ty[k] = ty; d.tz[k] = tz;
+    }
+  }
+  if (ENERGY) {
+    double ev[MAX_PAIR + MAX_ALIGN];
+#pragma unroll
+    for (int i = 0; i < MAX_PAIR + MAX_ALIGN; i++) ev[i] = 0.0;
+    ev[0] = epair;
+    ev[MAX_PAIR] = ealign;
+    block_reduce_store<MAX_PAIR + MAX_ALIGN>(ev, epart, nblocks);
+  }
+}
+
+template <int SHAPE, bool ENERGY>
+constexpr size_t flat_smem_bytes() { return sizeof(FlatWarp<SHAPE, ENERGY>) * (BLOCK / 32); }
+
+}  // namespace sg

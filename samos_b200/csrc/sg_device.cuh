@@ -118,8 +118,8 @@ __device__ __forceinline__ void store_dyn(const Dyn& d, int k, const Part& p) {
 }
 
 // ---------------------------------------------------------------------------
-// noise stream: Philox-4x32-10 (Salmon et al., SC'11) + polar method of
-// Marsaglia & Bray (1964); one counter value per draw.  The same stream is
+// noise stream: Philox-4x32-10 (Salmon et al., SC'11), one block per draw,
+// Box-Muller transform; one counter value per draw.  The same stream is
 // restated independently by the CPU oracle.
 // ---------------------------------------------------------------------------
 constexpr uint32_t NOISE_KEY1 = 0x53414D4Fu;
@@ -188,16 +188,50 @@ __host__ __device__ __forceinline__ double noise_log(double x) {
   return (de * LN2_HI + lm) + de * LN2_LO;
 }
 
-__host__ __device__ __forceinline__ double noise_gauss(uint32_t seed, uint64_t counter) {
-  for (uint32_t attempt = 0; attempt < 64; attempt++) {
-    uint32_t r[4];
-    philox((uint32_t)counter, (uint32_t)(counter >> 32), attempt, 0u, seed, NOISE_KEY1, r);
-    double v1 = 2.0 * u53(r[0], r[1]) - 1.0;
-    double v2 = 2.0 * u53(r[2], r[3]) - 1.0;
-    double s = v1 * v1 + v2 * v2;
-    if (s < 1.0 && s > 0.0) return v2 * sqrt(-2.0 * noise_log(s) / s);
+// cos(2 pi u), u in [0,1) to 53 bits: exact quadrant split of 4u, exact
+// reflection to g in [0,1/2], Taylor polynomials of sin (to x^15) / cos (to
+// x^16) at x = g pi/2 (same sequence as the oracle's cos2pi).
+__host__ __device__ __forceinline__ double noise_cos2pi(double u) {
+  double t = u * 4.0;
+  int q = (int)t;
+  double f = t - (double)q;
+  int use_sin = q & 1;
+  double g = f;
+  if (f > 0.5) { g = 1.0 - f; use_sin = !use_sin; }
+  double x = g * 1.5707963267948966;
+  double x2 = x * x;
+  double v;
+  if (use_sin) {
+    double p = -1.0 / 1307674368000.0;
+    p = p * x2 + 1.0 / 6227020800.0;
+    p = p * x2 - 1.0 / 39916800.0;
+    p = p * x2 + 1.0 / 362880.0;
+    p = p * x2 - 1.0 / 5040.0;
+    p = p * x2 + 1.0 / 120.0;
+    p = p * x2 - 1.0 / 6.0;
+    v = x + x * (x2 * p);
+  } else {
+    double p = 1.0 / 20922789888000.0;
+    p = p * x2 - 1.0 / 87178291200.0;
+    p = p * x2 + 1.0 / 479001600.0;
+    p = p * x2 - 1.0 / 3628800.0;
+    p = p * x2 + 1.0 / 40320.0;
+    p = p * x2 - 1.0 / 720.0;
+    p = p * x2 + 1.0 / 24.0;
+    p = p * x2 - 0.5;
+    v = 1.0 + x2 * p;
   }
-  return 0.0;
+  return (q == 1 || q == 2) ? -v : v;
+}
+
+// standard normal draw `counter` of stream `seed`: Box-Muller on one Philox
+// block, g = sqrt(-2 ln u1) cos(2 pi u2), u1 in (0,1], u2 in [0,1)
+__host__ __device__ __forceinline__ double noise_gauss(uint32_t seed, uint64_t counter) {
+  uint32_t r[4];
+  philox((uint32_t)counter, (uint32_t)(counter >> 32), 0u, 0u, seed, NOISE_KEY1, r);
+  const double u1 = u53(r[0], r[1]) + (1.0 / 9007199254740992.0);
+  const double u2 = u53(r[2], r[3]);
+  return sqrt(-2.0 * noise_log(u1)) * noise_cos2pi(u2);
 }
 
 __host__ __device__ __forceinline__ double noise_uniform(uint32_t seed, uint64_t counter) {

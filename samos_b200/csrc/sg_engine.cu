@@ -2,7 +2,7 @@
 // include/samos_gpu.h.  One stream per handle; device buffers are allocated
 // once per configuration and reused by every step.
 #include "samos_gpu.h"
-#include "sg_hot.cuh"
+#include "sg_abp.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -79,6 +79,17 @@ struct sg_system {
   std::string last_error;
   std::vector<double> uploaded_N[3];
   D4 *G[2] = {nullptr, nullptr}, *H[2] = {nullptr, nullptr};
+  std::vector<std::vector<double>> pair_tab_h, align_tab_h, ext_tab_h;
+  AbpParams* abp = nullptr;
+  bool abp_on = false;
+  int abp_variant = 1;
+  // autotuner: every variant yields the same bits, so candidates are timed on
+  // the run's own first steps (CUDA events around the step kernel)
+  bool tuned = false;
+  int tune_trial = 0;
+  double tune_ms[8] = {0};
+  int tune_n[8] = {0};
+  cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
   int hot_buf = 0;
   int force_generic = 0;  // testing aid: keep the generic SoA kernels
 };
@@ -210,6 +221,7 @@ int sg_create(int n_replicas, const int32_t* n_particles, int ntypes, sg_system*
   cudaMallocHost((void**)&s->rebuild_h, sizeof(int) * n_replicas);
   cudaEventCreate(&s->ev_run0); cudaEventCreate(&s->ev_run1);
   cudaEventCreate(&s->ev_k0); cudaEventCreate(&s->ev_k1);
+  cudaEventCreate(&s->ev_t0); cudaEventCreate(&s->ev_t1);
   cudaMemcpy(s->blk_rep, s->blk_rep_h.data(), sizeof(int) * s->nblocks, cudaMemcpyHostToDevice);
   cudaMemcpy(s->rep_blk0, s->rep_blk0_h.data(), sizeof(int) * n_replicas, cudaMemcpyHostToDevice);
   cudaMemcpy(s->rep_nblk, s->rep_nblk_h.data(), sizeof(int) * n_replicas, cudaMemcpyHostToDevice);
@@ -250,7 +262,7 @@ int sg_destroy(sg_system* s) {
   s->mem.free_all();
   for (double* t : s->tables) cudaFree(t);
   if (s->rebuild_h) cudaFreeHost(s->rebuild_h);
-  for (cudaEvent_t ev : {s->ev_run0, s->ev_run1, s->ev_k0, s->ev_k1})
+  for (cudaEvent_t ev : {s->ev_run0, s->ev_run1, s->ev_k0, s->ev_k1, s->ev_t0, s->ev_t1})
     if (ev) cudaEventDestroy(ev);
   cudaStreamDestroy(s->stream);
   delete s;
@@ -553,6 +565,7 @@ int sg_add_pair(sg_system* s, int kind, const double* global, const double* tabl
   C.phase = make_value(phase_value);
   C.table = upload_table(s, t);
   if (!C.table) return fail(s, SG_ERR_NOMEM, "table allocation failed");
+  s->pair_tab_h.push_back(t);
   for (int r = 0; r < s->nrep; r++)
     for (int i = 0; i < PAIR_NPARAM; i++) s->reps_h[r].pair_g[P.npair][i] = global[i];
   P.npair++;
@@ -570,6 +583,7 @@ int sg_add_align(sg_system* s, int kind, double J, double rcut, const double* ta
   C.kind = kind; C.has_pp = has_pp;
   C.table = upload_table(s, t);
   if (!C.table) return fail(s, SG_ERR_NOMEM, "table allocation failed");
+  s->align_tab_h.push_back(t);
   for (int r = 0; r < s->nrep; r++) { s->reps_h[r].align_J[P.nalign] = J; s->reps_h[r].align_rcut[P.nalign] = rcut; }
   P.nalign++;
   return push_reps(s);
@@ -584,6 +598,7 @@ int sg_add_external(sg_system* s, int kind, double alpha, const double* type_alp
   ExtComp& C = P.ext[P.next];
   C.kind = kind; C.has_params = has_params;
   C.type_alpha = upload_table(s, t);
+  s->ext_tab_h.push_back(t);
   for (int r = 0; r < s->nrep; r++) s->reps_h[r].ext_alpha[P.next] = alpha;
   P.next++;
   return push_reps(s);
@@ -773,7 +788,7 @@ static int step_fused(sg_system* s, bool apply_e1, bool energy) {
 // vicsek aligner (needs neighbour velocities) and no phase-in (needs ages).
 static int hot_shape(const sg_system* s) {
   const Program& P = s->prog;
-  if (s->force_generic || !fused_program(P) || P.ncons != 1) return HOT_NONE;
+  if (s->force_generic == 1 || !fused_program(P) || P.ncons != 1) return HOT_NONE;
   for (int c = 0; c < P.nalign; c++)
     if (P.align[c].kind == ALIGN_VICSEK) return HOT_NONE;
   for (int c = 0; c < P.npair; c++)
@@ -834,13 +849,136 @@ static void launch_hot(sg_system* s, bool apply_e1, bool last, bool energy) {
 
 extern "C" {
 
+// The specialised active-Brownian program: single type, soft (+ polar or
+// nematic) (+ self_propulsion), one brownian integrator.
+static bool abp_program(const sg_system* s) {
+  const Program& P = s->prog;
+  if (P.ntypes != 1 || P.npair != 1 || P.pair[0].kind != PAIR_SOFT || P.pair[0].phase_in) return false;
+  if (P.nalign > 1 || (P.nalign == 1 && P.align[0].kind == ALIGN_VICSEK)) return false;
+  if (P.next > 1 || P.ninteg != 1 || P.integ[0].kind != INT_BROWNIAN) return false;
+  return true;
+}
+
+static int abp_upload(sg_system* s) {
+  const Program& P = s->prog;
+  std::vector<AbpParams> h(s->nrep);
+  for (int r = 0; r < s->nrep; r++) {
+    const Replica& R = s->reps_h[r];
+    AbpParams& A = h[r];
+    std::memset(&A, 0, sizeof(A));
+    A.xlo = R.xlo; A.xhi = R.xhi; A.ylo = R.ylo; A.yhi = R.yhi; A.zlo = R.zlo; A.zhi = R.zhi;
+    A.Lx = R.Lx; A.Ly = R.Ly; A.Lz = R.Lz;
+    A.pad2q = 0.25 * R.pad * R.pad;
+    A.k = s->pair_tab_h[0][0];
+    A.a = s->pair_tab_h[0][1];
+    if (P.nalign == 1) {
+      double J, rc;
+      if (P.align[0].has_pp) { J = s->align_tab_h[0][0]; rc = s->align_tab_h[0][1]; }
+      else { J = R.align_J[0]; rc = R.align_rcut[0]; if (P.align[0].kind == ALIGN_NEMATIC) J = 2.0 * J; }
+      A.J = J; A.rc2 = rc * rc;
+    }
+    if (P.next == 1) A.alpha = P.ext[0].has_params ? s->ext_tab_h[0][0] : R.ext_alpha[0];
+    const double* ip = R.integ_p[0];
+    A.dt = ip[0]; A.v0 = ip[1]; A.nu = ip[2]; A.mu = ip[3]; A.mur = ip[4];
+    A.stoch = std::sqrt(ip[2] * ip[0]);
+    A.flip = P.integ[0].nematic ? ip[0] / ip[7] : 0.0;
+    A.Rs = R.cons_p[0];
+    A.temp = P.integ[0].temp;
+    A.off = R.off; A.n = R.n; A.periodic = R.periodic; A.use_radii = P.pair[0].use_radii;
+    A.nematic = P.integ[0].nematic; A.velocity = P.integ[0].velocity;
+    A.seed = R.seed[0];
+  }
+  if (!s->abp) s->abp = s->mem.alloc<AbpParams>(s->nrep);
+  if (!s->abp) { s->mem.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "abp params"); }
+  CU(s, cudaMemcpyAsync(s->abp, h.data(), sizeof(AbpParams) * s->nrep, cudaMemcpyHostToDevice, s->stream));
+  return SG_OK;
+}
+
+}  // extern "C"
+
+template <int SHAPE, int ALIGN, bool SP, bool ENERGY, int VAR>
+static void launch_abp_v(sg_system* s, bool apply_e1, bool last) {
+  const int b = s->hot_buf;
+  k_abp_step<SHAPE, ALIGN, SP, ENERGY, VAR><<<s->nblocks, BLOCK, 0, s->stream>>>(
+      s->abp, s->blk_rep, s->clk, s->G[b], s->G[1 - b], s->H[b], s->H[1 - b], s->cur, s->st, s->nl, s->rebuild,
+      s->status, apply_e1 ? 1 : 0, last ? 1 : 0, s->epart, s->nblocks);
+}
+
+template <int SHAPE, int ALIGN, bool SP, bool ENERGY>
+static void launch_abp_flat(sg_system* s, bool apply_e1, bool last) {
+  const int b = s->hot_buf;
+  constexpr size_t smem = flat_smem_bytes<SHAPE, ENERGY>();
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_abp_flat<SHAPE, ALIGN, SP, ENERGY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  k_abp_flat<SHAPE, ALIGN, SP, ENERGY><<<s->nblocks, BLOCK, smem, s->stream>>>(
+      s->abp, s->blk_rep, s->clk, s->G[b], s->G[1 - b], s->H[b], s->H[1 - b], s->cur, s->st, s->nl, s->rebuild,
+      s->status, apply_e1 ? 1 : 0, last ? 1 : 0, s->epart, s->nblocks);
+}
+
+template <int SHAPE, int ALIGN, bool SP>
+static void launch_abp3(sg_system* s, bool apply_e1, bool last, bool energy) {
+  if (energy) { launch_abp_v<SHAPE, ALIGN, SP, true, 1>(s, apply_e1, last); return; }
+  switch (s->abp_variant) {
+    case 5: launch_abp_flat<SHAPE, ALIGN, SP, false>(s, apply_e1, last); break;
+    case 0: launch_abp_v<SHAPE, ALIGN, SP, false, 0>(s, apply_e1, last); break;
+    case 1: launch_abp_v<SHAPE, ALIGN, SP, false, 1>(s, apply_e1, last); break;
+    case 2: launch_abp_v<SHAPE, ALIGN, SP, false, 2>(s, apply_e1, last); break;
+    case 3: launch_abp_v<SHAPE, ALIGN, SP, false, 3>(s, apply_e1, last); break;
+    default: launch_abp_v<SHAPE, ALIGN, SP, false, 4>(s, apply_e1, last); break;
+  }
+}
+
+template <int SHAPE>
+static void launch_abp(sg_system* s, bool apply_e1, bool last, bool energy) {
+  const Program& P = s->prog;
+  const int al = P.nalign == 0 ? ABP_ALIGN_NONE : P.align[0].kind;
+  const bool sp = P.next == 1;
+  if (al == ABP_ALIGN_NONE) { if (sp) launch_abp3<SHAPE, ABP_ALIGN_NONE, true>(s, apply_e1, last, energy);
+                              else launch_abp3<SHAPE, ABP_ALIGN_NONE, false>(s, apply_e1, last, energy); }
+  else if (al == ALIGN_POLAR) { if (sp) launch_abp3<SHAPE, ALIGN_POLAR, true>(s, apply_e1, last, energy);
+                                else launch_abp3<SHAPE, ALIGN_POLAR, false>(s, apply_e1, last, energy); }
+  else { if (sp) launch_abp3<SHAPE, ALIGN_NEMATIC, true>(s, apply_e1, last, energy);
+         else launch_abp3<SHAPE, ALIGN_NEMATIC, false>(s, apply_e1, last, energy); }
+}
+
+extern "C" {
+
+static constexpr int TUNE_REPS = 3;  // timed steps per candidate (after one untimed)
+
 static int step_hot(sg_system* s, int shape, bool apply_e1, bool last, bool energy) {
+  const bool tuning = s->abp_on && !s->tuned && !energy;
+  if (tuning) {
+    s->abp_variant = (s->tune_trial / (TUNE_REPS + 1)) % ABP_NVARIANT;
+    CU(s, cudaEventRecord(s->ev_t0, s->stream));
+  }
   if (s->profile) CU(s, cudaEventRecord(s->ev_k0, s->stream));
-  if (shape == HOT_PLANE) launch_hot<HOT_PLANE>(s, apply_e1, last, energy);
+  if (s->abp_on) {
+    if (shape == HOT_PLANE) launch_abp<HOT_PLANE>(s, apply_e1, last, energy);
+    else launch_abp<HOT_SPHERE>(s, apply_e1, last, energy);
+  } else if (shape == HOT_PLANE) launch_hot<HOT_PLANE>(s, apply_e1, last, energy);
   else launch_hot<HOT_SPHERE>(s, apply_e1, last, energy);
   LAUNCH_CHECK(s);
   if (s->profile) CU(s, cudaEventRecord(s->ev_k1, s->stream));
   s->hot_buf = 1 - s->hot_buf;
+  if (tuning) {
+    CU(s, cudaEventRecord(s->ev_t1, s->stream));
+    CU(s, cudaEventSynchronize(s->ev_t1));
+    float ms = 0.f;
+    CU(s, cudaEventElapsedTime(&ms, s->ev_t0, s->ev_t1));
+    const int v = s->abp_variant;
+    if (s->tune_trial % (TUNE_REPS + 1) != 0) { s->tune_ms[v] += ms; s->tune_n[v]++; }
+    s->tune_trial++;
+    if (s->tune_trial >= ABP_NVARIANT * (TUNE_REPS + 1)) {
+      int best = 0;
+      for (int c = 1; c < ABP_NVARIANT; c++)
+        if (s->tune_ms[c] / s->tune_n[c] < s->tune_ms[best] / s->tune_n[best]) best = c;
+      s->abp_variant = best;
+      s->tuned = true;
+    }
+  }
   return SG_OK;
 }
 
@@ -855,6 +993,8 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
   const bool fused = fused_program(s->prog);
   const int shape = fused ? hot_shape(s) : HOT_NONE;
   if (shape != HOT_NONE) { int rc = hot_alloc(s, shape); if (rc) return rc; }
+  s->abp_on = shape != HOT_NONE && abp_program(s) && s->force_generic == 0;
+  if (s->abp_on) { int rc = abp_upload(s); if (rc) return rc; }
   const int64_t launches0 = s->launches, builds0 = s->builds_run;
   double kernel_ms = 0.0;
   int64_t kernels_timed = 0;
@@ -962,8 +1102,22 @@ int sg_minimize(sg_system* s, int64_t max_steps, int64_t* converged, sg_run_stat
   return run_impl(s, max_steps, stats, true, converged);
 }
 
+int sg_set_variant(sg_system* s, int variant) {
+  if (!s || variant < -1 || variant >= ABP_NVARIANT) return SG_ERR_ARG;
+  if (variant < 0) {  // re-tune on the next run
+    s->tuned = false; s->tune_trial = 0;
+    for (int v = 0; v < 8; v++) { s->tune_ms[v] = 0.0; s->tune_n[v] = 0; }
+    return SG_OK;
+  }
+  s->abp_variant = variant;
+  s->tuned = true;
+  return SG_OK;
+}
+
+int sg_get_variant(const sg_system* s) { return s ? (s->tuned ? s->abp_variant : -1) : SG_ERR_ARG; }
+
 int sg_set_path(sg_system* s, int path) {
-  if (!s || path < 0 || path > 1) return SG_ERR_ARG;
+  if (!s || path < 0 || path > 2) return SG_ERR_ARG;
   s->force_generic = path;
   return SG_OK;
 }

@@ -77,9 +77,10 @@ struct Hp {  // hot particle registers
 
 // ConstraintPlane::enforce on a periodic box (constraint_plane.cpp:36-89);
 // z = zpos, vz = fz = nz = 0 are implicit in the planar registers.
-__device__ __forceinline__ void hot_plane_enforce(const Replica& R, Hp& p, int& dix, int& diy) {
-  if (p.x <= R.xlo) { p.x += R.Lx; dix--; } else if (p.x > R.xhi) { p.x -= R.Lx; dix++; }
-  if (p.y <= R.ylo) { p.y += R.Ly; diy--; } else if (p.y > R.yhi) { p.y -= R.Ly; diy++; }
+__device__ __forceinline__ void hot_plane_enforce(double xlo, double xhi, double Lx, double ylo, double yhi,
+                                                  double Ly, Hp& p, int& dix, int& diy) {
+  if (p.x <= xlo) { p.x += Lx; dix--; } else if (p.x > xhi) { p.x -= Lx; dix++; }
+  if (p.y <= ylo) { p.y += Ly; diy--; } else if (p.y > yhi) { p.y -= Ly; diy++; }
   double len_n = sqrt(p.nx * p.nx + p.ny * p.ny);
   double inv_len = 1.0;
   if (len_n != 0.0) inv_len = 1.0 / len_n;
@@ -136,24 +137,31 @@ __device__ __forceinline__ void hot_sphere_rotate(double Rs, Hp& p, double phi, 
   }
 }
 
-template <int SHAPE>
-__device__ __forceinline__ void hot_enforce(const Replica& R, Hp& p, int& dix, int& diy) {
-  if (SHAPE == HOT_PLANE) hot_plane_enforce(R, p, dix, diy);
-  else hot_sphere_enforce(R.cons_p[0], p);
+// Box/constraint scalars the shape routines read (plane: box; sphere: Rs).
+struct ShapeGeom { double xlo, xhi, Lx, ylo, yhi, Ly, Rs; };
+
+__device__ __forceinline__ ShapeGeom geom_of(const Replica& R) {
+  return ShapeGeom{R.xlo, R.xhi, R.Lx, R.ylo, R.yhi, R.Ly, R.cons_p[0]};
 }
 
 template <int SHAPE>
-__device__ __forceinline__ double hot_project_torque(const Replica& R, const Hp& p) {
+__device__ __forceinline__ void hot_enforce(const ShapeGeom& G, Hp& p, int& dix, int& diy) {
+  if (SHAPE == HOT_PLANE) hot_plane_enforce(G.xlo, G.xhi, G.Lx, G.ylo, G.yhi, G.Ly, p, dix, diy);
+  else hot_sphere_enforce(G.Rs, p);
+}
+
+template <int SHAPE>
+__device__ __forceinline__ double hot_project_torque(const ShapeGeom& G, const Hp& p) {
   if (SHAPE == HOT_PLANE) return 0.0 + p.tz;
-  const double Rs = R.cons_p[0];
+  const double Rs = G.Rs;
   double Nx = p.x / Rs, Ny = p.y / Rs, Nz = p.z / Rs;
   return 0.0 + (p.tx * Nx + p.ty * Ny + p.tz * Nz);
 }
 
 template <int SHAPE>
-__device__ __forceinline__ void hot_rotate(const Replica& R, Hp& p, double phi, bool velocity) {
+__device__ __forceinline__ void hot_rotate(const ShapeGeom& G, Hp& p, double phi, bool velocity) {
   if (SHAPE == HOT_PLANE) hot_plane_rotate(p, phi, velocity);
-  else hot_sphere_rotate(R.cons_p[0], p, phi, velocity);
+  else hot_sphere_rotate(G.Rs, p, phi, velocity);
 }
 
 // ---------------------------------------------------------------------------
@@ -278,6 +286,7 @@ k_hot_step(Program P, const Replica* __restrict__ reps, const int* __restrict__ 
 
     // ---- integrators in map order -----------------------------------------
     const int run_step = clk[r].run_step;
+    const ShapeGeom Gm = geom_of(R);
     int dix = 0, diy = 0;
     bool aged = false, vset = false, wset = false;
     double age = 0.0;
@@ -320,11 +329,11 @@ k_hot_step(Program P, const Replica* __restrict__ reps, const int* __restrict__ 
             p.vz += fr_z; p.z += sqrt_dt * fr_z;
           }
         }
-        hot_enforce<SHAPE>(R, p, dix, diy);
+        hot_enforce<SHAPE>(Gm, p, dix, diy);
         if (SHAPE == HOT_PLANE) p.vz = 0.0;
-        p.omega = mur * hot_project_torque<SHAPE>(R, p);
+        p.omega = mur * hot_project_torque<SHAPE>(Gm, p);
         double dtheta = dt * p.omega + sqrt(nu * dt) * noise_gauss(seed, c0 + (uint64_t)(D - 1));
-        hot_rotate<SHAPE>(R, p, dtheta, ic.velocity != 0);
+        hot_rotate<SHAPE>(Gm, p, dtheta, ic.velocity != 0);
         if (!aged) { age = d.age[k]; aged = true; }
         age += dt;
       } else if (ic.kind == INT_BROWNIAN_POS) {  // integrator_brownian_pos.cpp:52-81
@@ -346,16 +355,16 @@ k_hot_step(Program P, const Replica* __restrict__ reps, const int* __restrict__ 
             p.vz += fr_z; p.z += sqrt_dt * fr_z;
           }
         }
-        hot_enforce<SHAPE>(R, p, dix, diy);
+        hot_enforce<SHAPE>(Gm, p, dix, diy);
         if (SHAPE == HOT_PLANE) p.vz = 0.0;
         if (!aged) { age = d.age[k]; aged = true; }
         age += dt;
       } else if (ic.kind == INT_BROWNIAN_ALIGN) {  // integrator_brownian_align.cpp:63-75
         const double nu = ip[2], mur = ip[4];
-        p.omega = mur * hot_project_torque<SHAPE>(R, p);
+        p.omega = mur * hot_project_torque<SHAPE>(Gm, p);
         wset = true;
         double dtheta = dt * p.omega + sqrt(nu * dt) * noise_gauss(seed, base + gid);
-        hot_rotate<SHAPE>(R, p, dtheta, false);
+        hot_rotate<SHAPE>(Gm, p, dtheta, false);
       }
     }
 
@@ -374,7 +383,7 @@ k_hot_step(Program P, const Replica* __restrict__ reps, const int* __restrict__ 
       }
     }
     if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) atomicOr(status, ST_NONFINITE);
-    if (apply_e1) hot_enforce<SHAPE>(R, p, dix, diy);  // next step's Constrainer::enforce
+    if (apply_e1) hot_enforce<SHAPE>(Gm, p, dix, diy);  // next step's Constrainer::enforce
 
     // ---- stores -------------------------------------------------------------
     if (SHAPE == HOT_PLANE) {

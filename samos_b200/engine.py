@@ -84,6 +84,8 @@ def load() -> C.CDLL:
         "sg_set_profiling": (I, [P, I]),
         "sg_set_device": (I, [I]),
         "sg_set_path": (I, [P, I]),
+        "sg_set_variant": (I, [P, I]),
+        "sg_get_variant": (I, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -238,6 +240,17 @@ class Engine:
     def set_generic_path(self, on: bool) -> None:
         """Force the generic structure-of-arrays kernels (for comparisons)."""
         self._check(self.lib.sg_set_path(self.h, int(bool(on))))
+
+    def set_path(self, path: int) -> None:
+        """0 automatic, 1 generic SoA kernels, 2 packed kernels unspecialised."""
+        self._check(self.lib.sg_set_path(self.h, int(path)))
+
+    def set_variant(self, v: int) -> None:
+        """Pin a step-kernel variant (0..4) or re-enable autotuning (-1)."""
+        self._check(self.lib.sg_set_variant(self.h, int(v)))
+
+    def variant(self) -> int:
+        return int(self.lib.sg_get_variant(self.h))
 
     def kernel_launches(self) -> int:
         return int(self.lib.sg_kernel_launches(self.h))

@@ -227,10 +227,9 @@ def test_hot_kernels_match_generic_kernels_bitwise(shape):
         b = 2 * R + 6.0
         kw = dict(box=(b, b, b), periodic=False, constraint=("sphere", {"r": repr(R)}))
     out = []
-    for generic in (False, True):
+    for path in (0, 1, 2):
         e = Engine(n)
-        if generic:
-            e.set_generic_path(True)
+        e.set_path(path)
         sim = drive(e, parts, kw["box"], periodic=kw["periodic"], nlist=(2.4, 0.3), constraint=kw["constraint"],
                     pairs=[("soft", {"k": "10", "use_particle_radii": ""})], aligns=[("polar", {"J": "0.3"})],
                     externals=[("self_propulsion", {"alpha": "0.2"})], dt=1e-3,
@@ -238,7 +237,29 @@ def test_hot_kernels_match_generic_kernels_bitwise(shape):
         sim.run(300)
         out.append(e)
     for f in ("x", "y", "z", "nx", "ny", "nz", "vx", "vy", "vz", "fx", "fy", "tau_z", "omega", "age", "ix", "iy"):
-        np.testing.assert_array_equal(out[0].download(f), out[1].download(f), err_msg=f)
+        ref = out[1].download(f)
+        np.testing.assert_array_equal(out[0].download(f), ref, err_msg=f + " (specialised vs generic)")
+        np.testing.assert_array_equal(out[2].download(f), ref, err_msg=f + " (packed vs generic)")
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+def test_every_tuning_variant_gives_identical_bits(variant):
+    n = 3000
+    parts, L = plane_disks(n, 0.8, seed=22, bidisperse=(1.0, 1.4))
+    outs = []
+    for v in (variant, -2):
+        e = Engine(n)
+        if v >= 0:
+            e.set_variant(v)
+        else:
+            e.set_path(1)
+        sim = drive(e, parts, (L, L, 10.0), nlist=(2.8, 0.3), pairs=[("soft", {"k": "10", "use_particle_radii": ""})],
+                    aligns=[("nematic", {"J": "0.5"})], dt=5e-4,
+                    integrators=[("brownian", {"v0": "0.3", "nu": "0.1", "seed": "1"})])
+        sim.run(120)
+        outs.append(e)
+    for f in ("x", "y", "nx", "ny", "vx", "vy", "fx", "fy", "tau_z", "omega", "age", "ix", "iy"):
+        np.testing.assert_array_equal(outs[0].download(f), outs[1].download(f), err_msg=f)
 
 
 def test_trajectory_vicsek_generic_fused_path():
