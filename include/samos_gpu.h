@@ -176,6 +176,39 @@ int  sg_set_path(sg_system* s, int path);
 int  sg_set_variant(sg_system* s, int variant);
 int  sg_get_variant(const sg_system* s);
 
+/* ---- evaluation without allocation -------------------------------------
+ * No counterpart in the reference: an addition of this library for callers
+ * that cannot call cudaMalloc -- code running inside another framework's
+ * memory pool or under a no-allocation policy, plugins that only receive
+ * device pointers from their host application.  Computes the same forces
+ * and torques as sg_compute for a single-type program made of one `soft`
+ * pair potential {k, a, use_particle_radii} and at most one aligner
+ * (align_kind SG_ALIGN_POLAR or SG_ALIGN_NEMATIC, or -1 for none; J and
+ * rcut as in pair_align), with neighbours within rcut+pad taken from a cell
+ * list in the reference's list order, bit for bit equal to sg_compute.
+ * All pointers are DEVICE pointers of n doubles; positions must lie inside
+ * the box.  Nothing is allocated: every intermediate array lives in one
+ * fixed file-scope device array of sg_compute_static_scratch_bytes() bytes
+ * (about 4 MB) that every GPU loading this library holds until exit.  Limits:
+ * n <= SG_STATIC_MAX_PARTICLES and int(lx/(rcut+pad))*int(ly/(rcut+pad))*
+ * int(lz/(rcut+pad)) <= SG_STATIC_MAX_CELLS, else SG_ERR_ARG.  A particle
+ * with more than 64 neighbours on one side of its id gets NaN outputs.  The
+ * call is asynchronous on `stream` (NULL = default stream).  The first call
+ * on a device looks up the scratch address for that device
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one scratch array: calls whose work overlaps on the
+ * GPU (different streams or host threads) race and must be serialised.     */
+#define SG_STATIC_MAX_PARTICLES 65536
+#define SG_STATIC_MAX_CELLS 262144
+int  sg_compute_static(int n, double lx, double ly, double lz, int periodic, double rcut, double pad,
+                       const double* x_device, const double* y_device, const double* z_device,
+                       const double* nx_device, const double* ny_device, const double* nz_device,
+                       const double* radius_device, double k_soft, double a_soft,
+                       int use_particle_radii, int align_kind, double J, double align_rcut,
+                       double* fx_device, double* fy_device, double* fz_device,
+                       double* tau_x_device, double* tau_y_device, double* tau_z_device, void* stream);
+int64_t sg_compute_static_scratch_bytes(void);
+
 #ifdef __cplusplus
 }
 #endif

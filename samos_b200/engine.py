@@ -86,6 +86,8 @@ def load() -> C.CDLL:
         "sg_set_path": (I, [P, I]),
         "sg_set_variant": (I, [P, I]),
         "sg_get_variant": (I, [P]),
+        "sg_compute_static": (I, [I, D, D, D, I, D, D] + [P] * 7 + [D, D, I, I, D, D] + [P] * 6 + [P]),
+        "sg_compute_static_scratch_bytes": (I64, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
