@@ -154,6 +154,60 @@ def cpu_baseline(n=131_072, warm=100, steps=60, procs=1):
 
 
 # ---------------------------------------------------------------------------
+# batched replicas vs the same replicas launched one at a time
+# ---------------------------------------------------------------------------
+def sphere_parts(n, seed):
+    rng = np.random.default_rng(seed)
+    R = float(np.sqrt(n / 4.0))  # packing fraction 1 at radius 1: n pi = 4 pi R^2
+    z = rng.uniform(-R, R, n)
+    ph = rng.uniform(0.0, 2.0 * np.pi, n)
+    s = np.sqrt(np.maximum(R * R - z * z, 0.0))
+    pos = np.stack([s * np.cos(ph), s * np.sin(ph), z], 1)
+    nrm = pos / R
+    a = rng.normal(size=(n, 3))
+    t = a - np.sum(a * nrm, 1)[:, None] * nrm
+    t /= np.linalg.norm(t, axis=1)[:, None]
+    return dict(x=pos[:, 0].copy(), y=pos[:, 1].copy(), z=z, nx=t[:, 0].copy(), ny=t[:, 1].copy(),
+                nz=t[:, 2].copy(), radius=np.ones(n)), R
+
+
+def batched_leg(n_rep=256, warm=30, steps=50, seed=7, device=0):
+    """256 sphere systems, N log-uniform in [1024, 65536], R = sqrt(N/4), v0 ~ U[0.01,1],
+    J ~ U[0,1], nu ~ logU[1e-3,1], own seeds; soft k=10 + polar, dt=1e-3."""
+    from samos_b200 import Engine
+    from samos_b200.ensemble import SphereReplica, sphere_ensemble
+    rng = np.random.default_rng(seed)
+    reps = []
+    for i in range(n_rep):
+        n = int(round(np.exp(rng.uniform(np.log(1024), np.log(65536)))))
+        parts, R = sphere_parts(n, seed * 1000 + i)
+        reps.append(SphereReplica(parts=parts, R=R, v0=float(rng.uniform(0.01, 1.0)), J=float(rng.uniform(0.0, 1.0)),
+                                  nu=float(np.exp(rng.uniform(np.log(1e-3), 0.0))), seed=int(rng.integers(1, 2**31 - 1))))
+    total = sum(len(r.parts["x"]) for r in reps)
+    eng = sphere_ensemble(reps, engine=Engine([len(r.parts["x"]) for r in reps], device=device))
+    eng.run(warm - 1)
+    st = eng.run(steps - 1)
+    batched_s = st.device_ms * 1e-3
+    final_b = [eng.download("x", replica=i) for i in range(n_rep)]
+    eng.close()
+    serial_s, identical = 0.0, True
+    t_wall = time.perf_counter()
+    for i, r in enumerate(reps):
+        e1 = sphere_ensemble([r], engine=Engine([len(r.parts["x"])], device=device))
+        e1.run(warm - 1)
+        s1 = e1.run(steps - 1)
+        serial_s += s1.device_ms * 1e-3
+        identical = identical and bool(np.array_equal(e1.download("x"), final_b[i]))
+        e1.close()
+    t_wall = time.perf_counter() - t_wall
+    return dict(replicas=n_rep, particles=total, steps=steps,
+                batched_particle_steps_per_s=total * steps / batched_s,
+                serial_particle_steps_per_s=total * steps / serial_s,
+                speedup=serial_s / batched_s, identical_results=identical,
+                timing="CUDA events on the engine stream around the timed steps (serial: summed over the "
+                       "256 one-at-a-time runs)", serial_wall_s=t_wall)
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -201,6 +255,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-serial replica leg")
     ap.add_argument("--particles", type=int, default=N_PART,
                     help="system size (profiling runs use a smaller system of the same density)")
     args = ap.parse_args()
@@ -277,6 +332,10 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline()
+    batched = None
+    if ws == 1 and not args.no_batched and args.particles == N_PART:
+        eng.close()
+        batched = batched_leg(device=local)
 
     if rank == 0:
         line = dict(
@@ -296,9 +355,11 @@ def main():
             gpu_launches=int(launches),
             clocks=clocks.summary(),
             cpu_baseline=cpu,
+            batched=batched,
         )
         print(json.dumps(line), flush=True)
-    eng.close()
+    if eng.h:
+        eng.close()
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -57,6 +57,7 @@ typedef struct {
   double  device_ms;       /* CUDA-event time of the whole call on its stream */
   double  step_kernel_ms;  /* summed event time of the dominant step kernel   */
   int64_t step_kernels;    /* launches timed in step_kernel_ms (profiling on) */
+  double  rebuild_ms;      /* CUDA-event time spent in neighbour-list rebuilds */
 } sg_run_stats;
 
 /* ---- lifetime ------------------------------------------------------------
@@ -119,6 +120,10 @@ int  sg_add_external(sg_system* s, int kind, double alpha, const double* type_al
  *  rescale_steps, rescale_freq}; enforced on every particle at once like
  * src/samos.cpp:518-522.                                                     */
 int  sg_add_constraint(sg_system* s, int kind, const double* params);
+/* As sg_add_constraint, with params[0] (plane zpos / sphere r) given per
+ * replica in value0[n_replicas] before the immediate enforce, so each
+ * replica is projected exactly as its own single-system run would be.      */
+int  sg_add_constraint_per_replica(sg_system* s, int kind, const double* params, const double* value0);
 /* Integrator (register_integrators.cpp:35-55).  params[SG_INT_NPARAM]:
  *  brownian       : 0 dt, 1 v0, 2 nu, 3 mu, 4 mur, 5 seed, 6 nematic, 7 tau, 8 velocity_align
  *  brownian_pos   : 0 dt, 3 mu, 5 seed

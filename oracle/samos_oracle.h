@@ -6,12 +6,11 @@
  * is the checker for the CUDA path: only tests/, __graft_entry__.smoke() and
  * bench.py's CPU-baseline leg may load it.  The product never calls it.
  *
- * Parity status: the reference cannot be compiled here as shipped (it needs
- * Boost, GSL and CGAL, none of which are installed), and it carries no test
- * vectors.  The oracle is pinned against the reference's own hot-path source
- * files compiled against project shim headers (oracle/ref_build.sh ->
- * oracle/_ref/), see tests/test_oracle_vs_ref.py.  Where that build is absent
- * the oracle is "parity unpinned" and the tests say so.
+ * Parity status: PARITY UNPINNED.  The reference cannot be compiled here (it
+ * needs Boost, GSL and CGAL, none of which are installed) and its tree holds
+ * no tests or golden vectors, so no reference output exists to pin against.
+ * The oracle is checked against hand-derived known answers instead
+ * (tests/test_oracle_cpu.py).
  *
  * Noise: the reference draws from GSL's default generator, which is not
  * available.  Both this oracle and the CUDA path read one project-defined

@@ -120,8 +120,10 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
           const double r_sq = PLANE ? dx * dx + dy * dy : dx * dx + dy * dy + dz * dz;
           // PairSoftPotential::compute, pair_soft_potential.cpp:79-104
           const double rj = PLANE ? rr[u] : gg[u].w;
-          const double rd = sqrt(r_sq);
           const double sig = S.use_radii ? ri + rj : S.a;
+          // r_sq >= sig^2 (1 + 2^-40) implies sqrt(r_sq) >= sig after rounding:
+          // no contact, so the square root can be skipped without changing a bit
+          const double rd = r_sq < sig * sig * (1.0 + 0x1p-40) ? sqrt(r_sq) : sig;
           if (rd < sig) {
             const double diff = sig - rd;
             double ff;
@@ -372,8 +374,8 @@ k_abp_flat(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
       const double r_sq = PLANE ? dx * dx + dy * dy : dx * dx + dy * dy + dz * dz;
       unsigned char v = 0;
       // PairSoftPotential::compute, pair_soft_potential.cpp:79-104
-      const double rd = sqrt(r_sq);
       const double sig = S.use_radii ? F.orr[p] + rj : S.a;
+      const double rd = r_sq < sig * sig * (1.0 + 0x1p-40) ? sqrt(r_sq) : sig;  // see k_abp_step
       if (rd < sig) {
         const double diff = sig - rd;
         double ff;

@@ -48,6 +48,7 @@ struct sg_system {
   int slots = 0, nblocks = 0;
   int* blk_rep = nullptr;
   std::vector<int> blk_rep_h, rep_blk0_h, rep_nblk_h;
+  std::vector<int64_t> rep_builds;  // neighbour-list builds per replica
   int *rep_blk0 = nullptr, *rep_nblk = nullptr;
   std::vector<Replica> reps_h;
   Replica* reps = nullptr;
@@ -74,6 +75,7 @@ struct sg_system {
   int profile = 0;
   int maxnb_seen = 0;
   cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr, ev_k0 = nullptr, ev_k1 = nullptr;
+  cudaEvent_t ev_b0 = nullptr, ev_b1 = nullptr;
   cudaStream_t stream = nullptr;
   DevBuf mem;
   std::string last_error;
@@ -222,6 +224,7 @@ int sg_create(int n_replicas, const int32_t* n_particles, int ntypes, sg_system*
   cudaEventCreate(&s->ev_run0); cudaEventCreate(&s->ev_run1);
   cudaEventCreate(&s->ev_k0); cudaEventCreate(&s->ev_k1);
   cudaEventCreate(&s->ev_t0); cudaEventCreate(&s->ev_t1);
+  cudaEventCreate(&s->ev_b0); cudaEventCreate(&s->ev_b1);
   cudaMemcpy(s->blk_rep, s->blk_rep_h.data(), sizeof(int) * s->nblocks, cudaMemcpyHostToDevice);
   cudaMemcpy(s->rep_blk0, s->rep_blk0_h.data(), sizeof(int) * n_replicas, cudaMemcpyHostToDevice);
   cudaMemcpy(s->rep_nblk, s->rep_nblk_h.data(), sizeof(int) * n_replicas, cudaMemcpyHostToDevice);
@@ -235,6 +238,7 @@ int sg_create(int n_replicas, const int32_t* n_particles, int ntypes, sg_system*
   cudaMemcpy(s->st.id, ids.data(), sizeof(int) * s->slots, cudaMemcpyHostToDevice);
   cudaMemcpy(s->st.type, types.data(), sizeof(int) * s->slots, cudaMemcpyHostToDevice);
   s->reps_h.assign(n_replicas, Replica{});
+  s->rep_builds.assign(n_replicas, 0);
   s->clk_h.assign(n_replicas, Clock{});
   for (int r = 0; r < n_replicas; r++) {
     Replica& R = s->reps_h[r];
@@ -262,7 +266,7 @@ int sg_destroy(sg_system* s) {
   s->mem.free_all();
   for (double* t : s->tables) cudaFree(t);
   if (s->rebuild_h) cudaFreeHost(s->rebuild_h);
-  for (cudaEvent_t ev : {s->ev_run0, s->ev_run1, s->ev_k0, s->ev_k1, s->ev_t0, s->ev_t1})
+  for (cudaEvent_t ev : {s->ev_run0, s->ev_run1, s->ev_k0, s->ev_k1, s->ev_t0, s->ev_t1, s->ev_b0, s->ev_b1})
     if (ev) cudaEventDestroy(ev);
   cudaStreamDestroy(s->stream);
   delete s;
@@ -412,9 +416,26 @@ static int nlist_alloc(sg_system* s, int cap) {
   return SG_OK;
 }
 
-// builds the lists of the replicas flagged in s->rebuild (device)
-static int rebuild_flagged(sg_system* s) {
+// Rebuilds the lists of the replicas flagged in s->rebuild_h (host copy of
+// the device flags).  A replica's particle arrays are also re-sorted into
+// cell order on its first build and every kSortEvery-th one after (flag 2);
+// otherwise only the lists are rebuilt through the cell-ordered slot index
+// (flag 1).  Lists, and so results, are identical either way; the schedule
+// depends only on the replica's own history.  Sets *sorted if any replica
+// was re-sorted.
+static constexpr int kSortEvery = 8;
+
+static int rebuild_flagged(sg_system* s, bool* sorted) {
   const int nb = s->nblocks;
+  bool any_sort = false;
+  for (int r = 0; r < s->nrep; r++) {
+    if (!s->rebuild_h[r]) continue;
+    const bool srt = (s->rep_builds[r] % kSortEvery) == 0;
+    s->rebuild_h[r] = srt ? 2 : 1;
+    any_sort = any_sort || srt;
+  }
+  if (sorted) *sorted = any_sort;
+  CU(s, cudaMemcpyAsync(s->rebuild, s->rebuild_h, sizeof(int) * s->nrep, cudaMemcpyHostToDevice, s->stream));
   for (int attempt = 0; attempt < 4; attempt++) {
     CU(s, cudaMemsetAsync(s->cell_cnt, 0, sizeof(int) * (size_t)s->ncell_total, s->stream));
     CU(s, cudaMemsetAsync(s->cell_fill, 0, sizeof(int) * (size_t)s->ncell_total, s->stream));
@@ -434,11 +455,14 @@ static int rebuild_flagged(sg_system* s) {
     k_rb_rank<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->pcell, s->cell_start, s->cell_cnt,
                                           s->tmp, s->st.id, s->perm);
     LAUNCH_CHECK(s);
-    k_rb_gather<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->perm, s->cur, s->alt, s->st, s->st_alt);
-    LAUNCH_CHECK(s);
-    k_rb_copyback<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->alt, s->cur, s->st_alt, s->st);
-    LAUNCH_CHECK(s);
-    k_rb_build<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->st, s->nl, s->pcell,
+    if (any_sort) {
+      k_rb_gather<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->perm, s->cur, s->alt, s->st,
+                                               s->st_alt);
+      LAUNCH_CHECK(s);
+      k_rb_copyback<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->alt, s->cur, s->st_alt, s->st);
+      LAUNCH_CHECK(s);
+    }
+    k_rb_build<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->st, s->nl, s->perm,
                                            s->cell_start, s->cell_cnt, s->status, s->maxnb);
     LAUNCH_CHECK(s);
     int st = 0, mx = 0;
@@ -448,9 +472,18 @@ static int rebuild_flagged(sg_system* s) {
     if (!(st & ST_OVERFLOW)) {
       s->builds_run++;
       s->maxnb_seen = std::max(s->maxnb_seen, mx);
+      for (int r = 0; r < s->nrep; r++)
+        if (s->rebuild_h[r]) s->rep_builds[r]++;
       return SG_OK;
     }
-    if (mx > NB_LOCAL) return fail(s, SG_ERR_OVERFLOW, "more than " + std::to_string(NB_LOCAL) + " neighbours within rcut+pad");
+    if (any_sort) {  // arrays are now sorted: retry as list-only rebuilds of the same replicas
+      for (int r = 0; r < s->nrep; r++)
+        if (s->rebuild_h[r] == 2) s->rebuild_h[r] = 1;
+      any_sort = false;
+      CU(s, cudaMemcpyAsync(s->rebuild, s->rebuild_h, sizeof(int) * s->nrep, cudaMemcpyHostToDevice, s->stream));
+    }
+    if (mx > 2 * NB_LOCAL)
+      return fail(s, SG_ERR_OVERFLOW, "more than " + std::to_string(NB_LOCAL) + " neighbours on one side within rcut+pad");
     int cap = std::max(mx + 8, s->nl.cap * 2);
     int rc = nlist_alloc(s, cap);
     if (rc) return rc;
@@ -496,8 +529,7 @@ int sg_build_nlist(sg_system* s) {
   if (!s) return SG_ERR_ARG;
   if (!s->has_nlist) return fail(s, SG_ERR_STATE, "no neighbour list configured");
   for (int r = 0; r < s->nrep; r++) s->rebuild_h[r] = 1;
-  CU(s, cudaMemcpyAsync(s->rebuild, s->rebuild_h, sizeof(int) * s->nrep, cudaMemcpyHostToDevice, s->stream));
-  int rc = rebuild_flagged(s);
+  int rc = rebuild_flagged(s, nullptr);
   if (rc) return rc;
   CU(s, cudaMemsetAsync(s->rebuild, 0, sizeof(int) * s->nrep, s->stream));
   CU(s, cudaStreamSynchronize(s->stream));
@@ -602,6 +634,22 @@ int sg_add_external(sg_system* s, int kind, double alpha, const double* type_alp
   for (int r = 0; r < s->nrep; r++) s->reps_h[r].ext_alpha[P.next] = alpha;
   P.next++;
   return push_reps(s);
+}
+
+int sg_add_constraint_per_replica(sg_system* s, int kind, const double* params, const double* value0) {
+  if (!s || !value0 || kind < SG_CONS_NONE || kind > SG_CONS_SPHERE) return fail(s, SG_ERR_ARG, "bad constraint");
+  Program& P = s->prog;
+  if (P.ncons >= MAX_CONS) return fail(s, SG_ERR_ARG, "too many constraints");
+  if (params && params[4] != 0.0 && params[4] != 1.0)
+    return fail(s, SG_ERR_UNSUPPORTED, "constraint rescale is not supported by the GPU path");
+  ConsComp& C = P.cons[P.ncons];
+  C.kind = kind;
+  C.unlimited = (kind == CONS_PLANE && params) ? (int)params[1] : 0;
+  for (int r = 0; r < s->nrep; r++) s->reps_h[r].cons_p[P.ncons] = value0[r];
+  P.ncons++;
+  int rc = push_reps(s);
+  if (rc) return rc;
+  return sg_enforce(s);
 }
 
 int sg_add_constraint(sg_system* s, int kind, const double* params) {
@@ -996,7 +1044,7 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
   s->abp_on = shape != HOT_NONE && abp_program(s) && s->force_generic == 0;
   if (s->abp_on) { int rc = abp_upload(s); if (rc) return rc; }
   const int64_t launches0 = s->launches, builds0 = s->builds_run;
-  double kernel_ms = 0.0;
+  double kernel_ms = 0.0, rebuild_ms = 0.0;
   int64_t kernels_timed = 0;
   CU(s, cudaEventRecord(s->ev_run0, s->stream));
   CU(s, cudaMemsetAsync(s->status, 0, sizeof(int), s->stream));
@@ -1050,10 +1098,17 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
       bool any = false;
       for (int r = 0; r < s->nrep; r++) any = any || s->rebuild_h[r];
       if (any) {
+        CU(s, cudaEventRecord(s->ev_b0, s->stream));
         if (shape != HOT_NONE && !last && (rc = hot_unpack(s, shape))) return rc;
-        if ((rc = rebuild_flagged(s))) return rc;
-        if (shape != HOT_NONE && !last && (rc = hot_pack(s, shape))) return rc;
+        bool sorted = false;
+        if ((rc = rebuild_flagged(s, &sorted))) return rc;
+        if (shape != HOT_NONE && !last && sorted && (rc = hot_pack(s, shape))) return rc;
         CU(s, cudaMemsetAsync(s->rebuild, 0, sizeof(int) * s->nrep, s->stream));
+        CU(s, cudaEventRecord(s->ev_b1, s->stream));
+        CU(s, cudaEventSynchronize(s->ev_b1));
+        float bms = 0.f;
+        CU(s, cudaEventElapsedTime(&bms, s->ev_b0, s->ev_b1));
+        rebuild_ms += bms;
       }
     }
     if (driver) {
@@ -1082,6 +1137,7 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
     stats->device_ms = run_ms;
     stats->step_kernel_ms = kernel_ms;
     stats->step_kernels = kernels_timed;
+    stats->rebuild_ms = rebuild_ms;
   }
   if (st & ST_NONFINITE) return fail(s, SG_ERR_NONFINITE, "non-finite particle position detected");
   return SG_OK;

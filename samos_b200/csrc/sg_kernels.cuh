@@ -802,7 +802,7 @@ __global__ void k_rb_gather(const Replica* __restrict__ reps, const int* __restr
                             const int* __restrict__ rebuild, const int* __restrict__ perm,
                             Dyn src, Dyn dst, Stat ssrc, Stat sdst) {
   const int r = my_replica(blk_rep);
-  if (!rebuild[r]) return;
+  if (rebuild[r] != 2) return;
   const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
@@ -818,7 +818,7 @@ __global__ void k_rb_gather(const Replica* __restrict__ reps, const int* __restr
 __global__ void k_rb_copyback(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                               const int* __restrict__ rebuild, Dyn tmpd, Dyn d, Stat tmps, Stat st) {
   const int r = my_replica(blk_rep);
-  if (!rebuild[r]) return;
+  if (rebuild[r] != 2) return;
   const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
@@ -828,36 +828,18 @@ __global__ void k_rb_copyback(const Replica* __restrict__ reps, const int* __res
   st.r[k] = tmps.r[k]; st.mass[k] = tmps.mass[k]; st.type[k] = tmps.type[k]; st.id[k] = tmps.id[k];
 }
 
-constexpr int NB_LOCAL = 96;  // per-thread staging for the ordered list build
+constexpr int NB_LOCAL = 48;  // lower-id (or, on the N^2 path, each side's) neighbours staged per thread
 
-// ordered full-list build.  Cell path: the reference's 27-cell stencil with
+// Ordered full-list build.  Cell path: the reference's 27-cell stencil with
 // periodic index wrap (duplicates kept when a dimension has 2 cells, as in
-// cell_list.cpp:52-63); higher-id neighbours stay in visiting order.  N^2
-// path: each distinct neighbour cell once, higher ids sorted ascending
-// (build_nsq appends in ascending i).  Lower-id neighbours ascending in both.
-__global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                           const int* __restrict__ rebuild, Dyn d, Stat st, NbList nl,
-                           const int* __restrict__ pcell, const int* __restrict__ cstart,
-                           const int* __restrict__ ccnt, int* __restrict__ status, int* __restrict__ maxnb) {
-  const int r = my_replica(blk_rep);
-  if (!rebuild[r]) return;
-  const Replica& R = reps[r];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
-  if (k - R.off >= R.n) return;
-  // cell of this particle (positions are already in cell-sorted slots; the
-  // cell index is recomputed from the wrapped position)
-  const double x = d.x[k], y = d.y[k], z = d.z[k];
-  const int myid = st.id[k];
-  int a, b, c;
-  cell_of(R, x, y, z, a, b, c);
-  int lo_id[NB_LOCAL], lo_slot[NB_LOCAL];
-  int up_id[NB_LOCAL], up_slot[NB_LOCAL];
-  int nlo = 0, nup = 0;
-  bool overflow = false;
-  const int base0 = cstart[R.cell_off];
-  // stencil offsets: reference order; on the N^2 path skip repeated cells
-  int seen[27];
-  int nseen = 0;
+// cell_list.cpp:52-63); higher-id neighbours are written in visiting order by
+// a second sweep.  N^2 path: each distinct neighbour cell once, higher ids
+// sorted ascending (build_nsq appends in ascending i).  Lower-id neighbours
+// ascending in both.  rebuild[r] == 2: the particle arrays were just put in
+// cell order, so cell c's q-th particle sits at its segment slot directly;
+// rebuild[r] == 1: the slot comes from the cell-ordered index `cslot`.
+__device__ __forceinline__ int build_stencil(const Replica& R, int a, int b, int c, int* cells) {
+  int ncells = 0;
   for (int ox = -1; ox <= 1; ox++)
     for (int oy = -1; oy <= 1; oy++)
       for (int oz = -1; oz <= 1; oz++) {
@@ -866,54 +848,95 @@ __global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restri
         if (ib < 0) ib = R.cny - 1; else if (ib == R.cny) ib = 0;
         if (ic < 0) ic = R.cnz - 1; else if (ic == R.cnz) ic = 0;
         const int cl = R.cny * R.cnz * ia + R.cnz * ib + ic;
-        if (!R.use_cell) {
-          bool dup = false;
-          for (int q = 0; q < nseen; q++) dup = dup || (seen[q] == cl);
-          if (dup) continue;
-          seen[nseen++] = cl;
-        }
-        const int cg = R.cell_off + cl;
-        const int s0 = R.off + cstart[cg] - base0;
-        const int n = ccnt[cg];
-        for (int q = 0; q < n; q++) {
-          const int j = s0 + q;
-          const int jid = st.id[j];
-          if (jid == myid) continue;
-          double dx, dy, dz;
-          if (myid < jid) { dx = x - d.x[j]; dy = y - d.y[j]; dz = z - d.z[j]; }
-          else { dx = d.x[j] - x; dy = d.y[j] - y; dz = d.z[j] - z; }
-          apply_periodic(R, dx, dy, dz);
-          const double d2 = dx * dx + dy * dy + dz * dz;
-          if (d2 < R.cut2) {
-            if (jid < myid) {
-              if (nlo < NB_LOCAL) { lo_id[nlo] = jid; lo_slot[nlo] = j; nlo++; } else overflow = true;
-            } else {
-              if (nup < NB_LOCAL) { up_id[nup] = jid; up_slot[nup] = j; nup++; } else overflow = true;
-            }
-          }
+        bool dup = false;
+        if (!R.use_cell)
+          for (int q = 0; q < ncells; q++) dup = dup || (cells[q] == cl);
+        if (!dup) cells[ncells++] = cl;
+      }
+  return ncells;
+}
+
+__global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                           const int* __restrict__ rebuild, Dyn d, Stat st, NbList nl,
+                           const int* __restrict__ cslot, const int* __restrict__ cstart,
+                           const int* __restrict__ ccnt, int* __restrict__ status, int* __restrict__ maxnb) {
+  const int r = my_replica(blk_rep);
+  const int mode = rebuild[r];
+  if (!mode) return;
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  const double x = d.x[k], y = d.y[k], z = d.z[k];
+  const int myid = st.id[k];
+  int a, b, c;
+  cell_of(R, x, y, z, a, b, c);
+  int cells[27];
+  const int ncells = build_stencil(R, a, b, c, cells);
+  const int base0 = cstart[R.cell_off];
+  unsigned long long lo[NB_LOCAL], up[NB_LOCAL];  // (id << 32) | slot
+  int nlo = 0, nup = 0;
+  bool overflow = false;
+  // sweep 1: lower-id neighbours (and, on the N^2 path, higher-id ones)
+  for (int m = 0; m < ncells; m++) {
+    const int cg = R.cell_off + cells[m];
+    const int s0 = R.off + cstart[cg] - base0, n = ccnt[cg];
+    for (int q = 0; q < n; q++) {
+      const int j = mode == 2 ? s0 + q : cslot[s0 + q];
+      const int jid = st.id[j];
+      if (jid == myid) continue;
+      double dx, dy, dz;
+      if (myid < jid) { dx = x - d.x[j]; dy = y - d.y[j]; dz = z - d.z[j]; }
+      else { dx = d.x[j] - x; dy = d.y[j] - y; dz = d.z[j] - z; }
+      apply_periodic(R, dx, dy, dz);
+      if (dx * dx + dy * dy + dz * dz < R.cut2) {
+        const unsigned long long key = ((unsigned long long)(unsigned)jid << 32) | (unsigned)j;
+        if (jid < myid) { if (nlo < NB_LOCAL) lo[nlo] = key; nlo++; }
+        else {
+          if (!R.use_cell && nup < NB_LOCAL) up[nup] = key;
+          nup++;
         }
       }
-  // stable insertion sorts by id
-  for (int i = 1; i < nlo; i++) {
-    int ki = lo_id[i], ks = lo_slot[i], m = i - 1;
-    while (m >= 0 && lo_id[m] > ki) { lo_id[m + 1] = lo_id[m]; lo_slot[m + 1] = lo_slot[m]; m--; }
-    lo_id[m + 1] = ki; lo_slot[m + 1] = ks;
-  }
-  if (!R.use_cell) {
-    for (int i = 1; i < nup; i++) {
-      int ki = up_id[i], ks = up_slot[i], m = i - 1;
-      while (m >= 0 && up_id[m] > ki) { up_id[m + 1] = up_id[m]; up_slot[m + 1] = up_slot[m]; m--; }
-      up_id[m + 1] = ki; up_slot[m + 1] = ks;
     }
   }
+  if (nlo > NB_LOCAL || (!R.use_cell && nup > NB_LOCAL)) overflow = true;
   const int total = nlo + nup;
   atomicMax(maxnb, total);
   if (total > nl.cap || overflow) {
     atomicOr(status, ST_OVERFLOW);
     nl.cnt[k] = 0; nl.lo[k] = 0;
   } else {
-    for (int q = 0; q < nlo; q++) nl.nb[(size_t)q * nl.stride + k] = lo_slot[q];
-    for (int q = 0; q < nup; q++) nl.nb[(size_t)(nlo + q) * nl.stride + k] = up_slot[q];
+    for (int i = 1; i < nlo; i++) {  // insertion sort by id (keys are unique per duplicate-free id)
+      const unsigned long long v = lo[i];
+      int m = i - 1;
+      while (m >= 0 && (lo[m] >> 32) > (v >> 32)) { lo[m + 1] = lo[m]; m--; }
+      lo[m + 1] = v;
+    }
+    for (int q = 0; q < nlo; q++) nl.nb[(size_t)q * nl.stride + k] = (int)(unsigned)(lo[q] & 0xffffffffull);
+    if (!R.use_cell) {
+      for (int i = 1; i < nup; i++) {
+        const unsigned long long v = up[i];
+        int m = i - 1;
+        while (m >= 0 && (up[m] >> 32) > (v >> 32)) { up[m + 1] = up[m]; m--; }
+        up[m + 1] = v;
+      }
+      for (int q = 0; q < nup; q++)
+        nl.nb[(size_t)(nlo + q) * nl.stride + k] = (int)(unsigned)(up[q] & 0xffffffffull);
+    } else {
+      // sweep 2: higher-id neighbours in stencil visiting order
+      int w = nlo;
+      for (int m = 0; m < ncells; m++) {
+        const int cg = R.cell_off + cells[m];
+        const int s0 = R.off + cstart[cg] - base0, n = ccnt[cg];
+        for (int q = 0; q < n; q++) {
+          const int j = mode == 2 ? s0 + q : cslot[s0 + q];
+          const int jid = st.id[j];
+          if (jid <= myid) continue;
+          double dx = x - d.x[j], dy = y - d.y[j], dz = z - d.z[j];
+          apply_periodic(R, dx, dy, dz);
+          if (dx * dx + dy * dy + dz * dz < R.cut2) nl.nb[(size_t)(w++) * nl.stride + k] = j;
+        }
+      }
+    }
     nl.cnt[k] = total; nl.lo[k] = nlo;
   }
   nl.ox[k] = x; nl.oy[k] = y; nl.oz[k] = z;

@@ -38,7 +38,7 @@ class RunStats(C.Structure):
     _fields_ = [("steps_done", C.c_int64), ("nlist_builds", C.c_int64),
                 ("kernel_launches", C.c_int64), ("max_neighbours", C.c_int32),
                 ("status", C.c_int32), ("device_ms", C.c_double), ("step_kernel_ms", C.c_double),
-                ("step_kernels", C.c_int64)]
+                ("step_kernels", C.c_int64), ("rebuild_ms", C.c_double)]
 
 
 def library_path() -> str:
@@ -72,6 +72,7 @@ def load() -> C.CDLL:
         "sg_add_align": (I, [P, I, D, D, dp, I]),
         "sg_add_external": (I, [P, I, D, dp, I]),
         "sg_add_constraint": (I, [P, I, dp]),
+        "sg_add_constraint_per_replica": (I, [P, I, dp, dp]),
         "sg_add_integrator": (I, [P, I, dp, dp]),
         "sg_set_replica_param": (I, [P, I, I, I, I, D]),
         "sg_compute": (I, [P, D]),
@@ -197,6 +198,14 @@ class Engine:
         p = np.zeros(8)
         p[:len(params)] = params
         self._check(self.lib.sg_add_constraint(self.h, int(kind), _dptr(p)))
+
+    def add_constraint_per_replica(self, kind, params, value0):
+        p = np.zeros(8)
+        p[:len(params)] = params
+        v = np.ascontiguousarray(value0, dtype=np.float64)
+        if v.shape != (len(self.n),):
+            raise ValueError("one value per replica expected")
+        self._check(self.lib.sg_add_constraint_per_replica(self.h, int(kind), _dptr(p), _dptr(v)))
 
     def add_integrator(self, kind, params, temperature=None):
         p = np.zeros(INT_NPARAM)
