@@ -181,6 +181,48 @@ int  sg_set_path(sg_system* s, int path);
 int  sg_set_variant(sg_system* s, int variant);
 int  sg_get_variant(const sg_system* s);
 
+/* ---- device view (for kernels that work on the engine's state) -----------
+ * No reference counterpart.  Device pointers into the handle's current
+ * structure-of-arrays store (slot order) and neighbour lists, valid until the
+ * next call that runs, rebuilds or reconfigures.  Replica r owns slots
+ * [offset[r], offset[r] + n[r]); slot k holds particle id[k].  Neighbour q of
+ * slot k is slot nb[q * nb_stride + k] for q < nb_cnt[k].  After writing
+ * positions through the view call sg_positions_changed(), which rebuilds the
+ * neighbour lists before the next step.                                     */
+typedef struct {
+  double *x_device, *y_device, *z_device, *nx_device, *ny_device, *nz_device;
+  double *vx_device, *vy_device, *vz_device, *fx_device, *fy_device, *fz_device;
+  const double* radius_device;
+  const int32_t *id_device, *nb_device, *nb_cnt_device;
+  int32_t *ix_device, *iy_device;
+  int32_t nb_stride, slots;
+} sg_view;
+int  sg_get_view(sg_system* s, sg_view* out);
+int  sg_replica_slots(const sg_system* s, int replica, int32_t* offset, int32_t* n);
+int  sg_positions_changed(sg_system* s);
+/* cudaMemcpy with direction inferred from the pointers (helper for callers
+ * that hold device pointers from a view).                                   */
+int  sg_memcpy(void* dst, const void* src, int64_t bytes);
+
+/* ---- learned FIRE warm start (no reference counterpart) ------------------
+ * Message-passing network over the engine's neighbour lists (see
+ * samos_b200/csrc/sg_ml.cu for the architecture).  All buffers are device
+ * memory owned by the caller; box[2*slot] = (Lx, Ly) of the slot's replica,
+ * 0 for slots that are not part of the current batch.                      */
+int  sg_mlp_param_count(void);
+int  sg_mlp_edge_blocks(void);
+int  sg_mlp_part_floats(void);
+int  sg_mlp_prepare(const float* params, void* W1b16, void* W1bT16, void* Wpq16, void* WpqT16, void* stream);
+int  sg_mlp_forward(const sg_view* v, const double* box, double rc, const float* params, const void* W1bT16,
+                    const void* WpqT16, void* s16, void* h16, float* PQ, float* disp, void* stream);
+int  sg_mlp_backward(const sg_view* v, const double* box, double rc, const float* params, const void* W1b16,
+                     const void* Wpq16, const void* s16, const void* h16, const float* PQ, const float* disp,
+                     const float* target, float inv_n, float* gPQ, void* gPQ16, float* gh, void* gpre16, float* gs,
+                     float* part, float* red, float* loss_part, float* grad, void* stream);
+int  sg_mlp_adam(float* params, const float* grad, float* m, float* v, int n, float lr, float beta1, float beta2,
+                 float eps, int step, void* stream);
+int  sg_mlp_apply(const sg_view* v, const double* box, const float* disp, int32_t* ix, int32_t* iy, void* stream);
+
 /* ---- evaluation without allocation -------------------------------------
  * No counterpart in the reference: an addition of this library for callers
  * that cannot call cudaMalloc -- code running inside another framework's

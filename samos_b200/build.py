@@ -45,7 +45,8 @@ def build_engine(force: bool = False) -> str:
     srcs = _sources(CSRC, (".cu", ".cuh")) + [os.path.join(INCLUDE, "samos_gpu.h")]
     if force or _stale(ENGINE_SO, srcs):
         _run([NVCC, *NVCC_FLAGS, *ARCH, f"-I{INCLUDE}", "-o", ENGINE_SO,
-              os.path.join(CSRC, "sg_engine.cu"), os.path.join(CSRC, "sg_static.cu")])
+              os.path.join(CSRC, "sg_engine.cu"), os.path.join(CSRC, "sg_static.cu"),
+              os.path.join(CSRC, "sg_ml.cu")])
     return ENGINE_SO
 
 

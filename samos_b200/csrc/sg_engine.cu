@@ -69,6 +69,7 @@ struct sg_system {
   double *epart = nullptr, *fire_part = nullptr, *alpha_mix = nullptr, *Rn = nullptr;
   double dt_global = 0.0;
   bool e1_applied = false;
+  bool forces_fresh = false;  // forces equal those the next start-of-step pass would compute
   bool configured_nlist_once = false;
   int64_t launches = 0;
   int64_t builds_run = 0;
@@ -352,6 +353,7 @@ int sg_upload(sg_system* s, int replica, const char* field, const void* host) {
   }
   CU(s, cudaStreamSynchronize(s->stream));
   s->e1_applied = false;
+  s->forces_fresh = false;
   return SG_OK;
 }
 
@@ -427,6 +429,7 @@ static constexpr int kSortEvery = 8;
 
 static int rebuild_flagged(sg_system* s, bool* sorted) {
   const int nb = s->nblocks;
+  s->forces_fresh = false;
   bool any_sort = false;
   for (int r = 0; r < s->nrep; r++) {
     if (!s->rebuild_h[r]) continue;
@@ -742,7 +745,7 @@ int sg_set_replica_param(sg_system* s, int replica, int cls, int comp, int slot,
 // ---------------------------------------------------------------------------
 int sg_enforce(sg_system* s) {
   if (!s) return SG_ERR_ARG;
-  k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st);
+  k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, nullptr);
   LAUNCH_CHECK(s);
   CU(s, cudaStreamSynchronize(s->stream));
   return SG_OK;
@@ -777,12 +780,28 @@ static bool fused_program(const Program& P) {
 }
 
 // one unfused integration step (reference phase order, in place)
+// True when the start-of-step force pass would reproduce the forces of the
+// previous step's FIRE pass bit for bit: periodic plane only (the enforce
+// leaves positions unchanged), no aligners or external potentials (forces
+// then depend on positions alone) and no neighbour-list rebuild in between.
+static bool fire_forces_reusable(const sg_system* s) {
+  const Program& P = s->prog;
+  if (P.nalign || P.next || P.ncons != 1 || P.cons[0].kind != CONS_PLANE) return false;
+  for (int c = 0; c < P.ninteg; c++)
+    if (P.integ[c].kind != INT_FIRE) return false;
+  for (const Replica& R : s->reps_h)
+    if (!R.periodic || !(R.cons_p[0] > R.zlo && R.cons_p[0] <= R.zhi)) return false;
+  return true;
+}
+
 static int step_unfused(sg_system* s, bool energy, bool driver) {
   const int nb = s->nblocks;
-  k_enforce<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st);
+  k_enforce<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, driver ? s->clk : nullptr);
   LAUNCH_CHECK(s);
-  int rc = launch_force(s, s->dt_global, false, true, true, energy);
-  if (rc) return rc;
+  int rc = SG_OK;
+  if (!(s->forces_fresh && fire_forces_reusable(s)))
+    if ((rc = launch_force(s, s->dt_global, false, true, true, energy))) return rc;
+  s->forces_fresh = false;
   for (int c = 0; c < s->prog.ninteg; c++) {
     const IntegComp& ic = s->prog.integ[c];
     if (ic.kind == INT_LANGEVIN) {
@@ -795,6 +814,7 @@ static int step_unfused(sg_system* s, bool energy, bool driver) {
       k_fire_a<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st);
       LAUNCH_CHECK(s);
       if ((rc = launch_force(s, 0.0, true, true, true, true))) return rc;
+      s->forces_fresh = true;
       k_fire_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, s->fire_part, nb);
       LAUNCH_CHECK(s);
       k_fire_c<<<(s->nrep + 127) / 128, 128, 0, s->stream>>>(s->prog, s->reps, s->clk, s->rep_blk0, s->rep_nblk,
@@ -1040,6 +1060,7 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
   if (!s->nl.nb) { int rc = nlist_alloc(s, 1); if (rc) return rc; }
   const bool fused = fused_program(s->prog);
   const int shape = fused ? hot_shape(s) : HOT_NONE;
+  s->forces_fresh = false;
   if (shape != HOT_NONE) { int rc = hot_alloc(s, shape); if (rc) return rc; }
   s->abp_on = shape != HOT_NONE && abp_program(s) && s->force_generic == 0;
   if (s->abp_on) { int rc = abp_upload(s); if (rc) return rc; }
@@ -1062,7 +1083,7 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
     if (shape != HOT_NONE) {
       if (t == 0) {
         if (!s->e1_applied) {
-          k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st);
+          k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, nullptr);
           LAUNCH_CHECK(s);
         }
         if ((rc = hot_pack(s, shape))) return rc;
@@ -1071,7 +1092,7 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
       s->e1_applied = !last;
     } else if (fused) {
       if (!s->e1_applied) {
-        k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st);
+        k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, nullptr);
         LAUNCH_CHECK(s);
       }
       rc = step_fused(s, !last, last);
@@ -1111,7 +1132,7 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
         rebuild_ms += bms;
       }
     }
-    if (driver) {
+    if (driver && ((t & 15) == 15 || t == steps)) {  // converged replicas are frozen on the device
       if ((rc = pull_clk(s))) return rc;
       bool all = true;
       for (int r = 0; r < s->nrep; r++) all = all && s->clk_h[r].fire_conv_step >= 0;
@@ -1156,6 +1177,41 @@ int sg_minimize(sg_system* s, int64_t max_steps, int64_t* converged, sg_run_stat
   rc = push_clk(s);
   if (rc) return rc;
   return run_impl(s, max_steps, stats, true, converged);
+}
+
+int sg_get_view(sg_system* s, sg_view* v) {
+  if (!s || !v) return SG_ERR_ARG;
+  if (!s->nl.nb) { int rc = nlist_alloc(s, 1); if (rc) return rc; }
+  v->x_device = s->cur.x; v->y_device = s->cur.y; v->z_device = s->cur.z;
+  v->nx_device = s->cur.nx; v->ny_device = s->cur.ny; v->nz_device = s->cur.nz;
+  v->vx_device = s->cur.vx; v->vy_device = s->cur.vy; v->vz_device = s->cur.vz;
+  v->fx_device = s->cur.fx; v->fy_device = s->cur.fy; v->fz_device = s->cur.fz;
+  v->radius_device = s->st.r;
+  v->id_device = s->st.id; v->nb_device = s->nl.nb; v->nb_cnt_device = s->nl.cnt;
+  v->ix_device = s->cur.ix; v->iy_device = s->cur.iy;
+  v->nb_stride = s->nl.stride; v->slots = s->slots;
+  CU(s, cudaStreamSynchronize(s->stream));
+  return SG_OK;
+}
+
+int sg_replica_slots(const sg_system* s, int replica, int32_t* offset, int32_t* n) {
+  if (!s || replica < 0 || replica >= s->nrep || !offset || !n) return SG_ERR_ARG;
+  *offset = s->off[replica];
+  *n = s->n[replica];
+  return SG_OK;
+}
+
+int sg_memcpy(void* dst, const void* src, int64_t bytes) {
+  if (bytes < 0 || (!dst && bytes) || (!src && bytes)) return SG_ERR_ARG;
+  return cudaMemcpy(dst, src, (size_t)bytes, cudaMemcpyDefault) == cudaSuccess ? SG_OK : SG_ERR_CUDA;
+}
+
+int sg_positions_changed(sg_system* s) {
+  if (!s) return SG_ERR_ARG;
+  CU(s, cudaDeviceSynchronize());
+  s->e1_applied = false;
+  s->forces_fresh = false;
+  return s->has_nlist ? sg_build_nlist(s) : SG_OK;
 }
 
 int sg_set_variant(sg_system* s, int variant) {

@@ -273,10 +273,12 @@ __device__ __forceinline__ bool finite3(double a, double b, double c) {
 
 // Constrainer::enforce on every particle (samos.cpp:887-888)
 __global__ void k_enforce(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                          Dyn d, Stat st) {
-  const Replica& R = reps[my_replica(blk_rep)];
+                          Dyn d, Stat st, const Clock* __restrict__ frozen) {
+  const int r = my_replica(blk_rep);
+  const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
+  if (frozen && frozen[r].fire_conv_step >= 0) return;  // minimiser stopped this replica
   Part p;
   load_dyn(d, k, p);
   p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
@@ -292,7 +294,10 @@ __global__ void k_force(Program P, const Replica* __restrict__ reps, const int* 
                         int use_fire_dt, int with_pair, int with_align, double* epart, int nblocks) {
   const int r = my_replica(blk_rep);
   const Replica& R = reps[r];
-  if (use_fire_dt) dt = clk[r].fire_dt;
+  if (use_fire_dt) {
+    if (clk[r].fire_conv_step >= 0) return;  // converged replica: whole block exits (partials kept)
+    dt = clk[r].fire_dt;
+  }
   const int k = blockIdx.x * BLOCK + threadIdx.x;
   double e[MAX_PAIR + MAX_ALIGN];
 #pragma unroll

@@ -1,0 +1,553 @@
+// sg_ml.cu -- learned FIRE warm start: a two-layer message-passing network
+// over the engine's neighbour lists that predicts each particle's
+// displacement to its relaxed position.  No reference counterpart (this is
+// the learned part of the project).
+//
+// Network (width 64, edges with r < rc; e_ij = (r, a_i, a_j, a_i + a_j - r),
+// d_ij the minimum-image vector from i to j):
+//   s_i  = sum_j relu(W1a e_ij + b1a)                       edge kernel, FP32
+//   h_i  = relu(s_i W1b + b1b)                              BF16 tensor cores
+//   [P|Q] = h Wpq                                           BF16 tensor cores
+//   z_ij = relu(P_i + Q_j + W2e e_ij + b2),  w_ij = z_ij . w2 + c
+//   disp_i = sum_j w_ij d_ij / r_ij                         edge kernel, FP32
+// The 64-wide products are node-level (the first edge layer is summed before
+// W1b, the second is split into P_i + Q_j), so the tensor-core GEMMs are
+// [slots x 64] x [64 x 64|128] with FP32 accumulation (mma.sync m16n8k16 BF16).
+// Activations s, h and the GEMM operands of the backward pass are BF16.
+#include "samos_gpu.h"
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace {
+
+constexpr int F = 64;          // hidden width
+constexpr int NP_W1A = 0, NP_B1A = 256, NP_W1B = 320, NP_B1B = 4416, NP_WPQ = 4480, NP_B2 = 12672,
+              NP_W2E = 12736, NP_W2 = 12992, NP_C = 13056, NP_TOTAL = 13057;
+constexpr int EDGE_WARPS = 8;  // warps per block in the edge kernels
+constexpr int EDGE_BLOCKS = 148 * 8;
+
+__device__ __forceinline__ float bf(const __nv_bfloat16 v) { return __bfloat162float(v); }
+
+__device__ __forceinline__ bool edge_vec(const sg_view& V, const double* box, int i, int j, double rc, float* e,
+                                         float& ux, float& uy, float ai) {
+  const double Lx = box[2 * i], Ly = box[2 * i + 1];
+  double dx = V.x_device[j] - V.x_device[i], dy = V.y_device[j] - V.y_device[i];
+  if (dx > 0.5 * Lx) dx -= Lx; else if (dx < -0.5 * Lx) dx += Lx;
+  if (dy > 0.5 * Ly) dy -= Ly; else if (dy < -0.5 * Ly) dy += Ly;
+  const double r = sqrt(dx * dx + dy * dy);
+  if (!(r < rc) || r == 0.0) return false;
+  const float aj = (float)V.radius_device[j];
+  e[0] = (float)r; e[1] = ai; e[2] = aj; e[3] = ai + aj - (float)r;
+  ux = (float)(dx / r); uy = (float)(dy / r);
+  return true;
+}
+
+// ---- layer 1 edges: s_i = sum_j relu(W1a e + b1a), stored BF16 ----------------
+__global__ void k_ml_l1(sg_view V, const double* __restrict__ box, double rc, const float* __restrict__ P,
+                        __nv_bfloat16* __restrict__ s16) {
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  float w[2][4], b[2];
+  for (int h = 0; h < 2; h++) {
+    const int f = lane + 32 * h;
+    for (int d = 0; d < 4; d++) w[h][d] = P[NP_W1A + 4 * f + d];
+    b[h] = P[NP_B1A + f];
+  }
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < V.slots; i += nw) {
+    float acc[2] = {0.f, 0.f};
+    if (box[2 * i] > 0.0) {
+      const float ai = (float)V.radius_device[i];
+      const int cnt = V.nb_cnt_device[i];
+      for (int q = 0; q < cnt; q++) {
+        const int j = V.nb_device[(size_t)q * V.nb_stride + i];
+        float e[4], ux, uy;
+        if (!edge_vec(V, box, i, j, rc, e, ux, uy, ai)) continue;
+        for (int h = 0; h < 2; h++) {
+          const float z = w[h][0] * e[0] + w[h][1] * e[1] + w[h][2] * e[2] + w[h][3] * e[3] + b[h];
+          acc[h] += fmaxf(z, 0.f);
+        }
+      }
+    }
+    s16[(size_t)i * F + lane] = __float2bfloat16_rn(acc[0]);
+    s16[(size_t)i * F + lane + 32] = __float2bfloat16_rn(acc[1]);
+  }
+}
+
+// ---- BF16 tensor-core GEMM: C[m][n] = sum_k A[m][k] Bt[n][k] (+bias, relu) ------
+// One warp: 16 rows x N; Bt staged in shared memory.  Rows with box == 0
+// (padding slots) are written as zero.
+__device__ __forceinline__ uint32_t pack2(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+__device__ __forceinline__ void mma16816(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+template <int K, int N>
+__global__ void __launch_bounds__(128) k_ml_gemm(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ Bt,
+                                                 int M, const float* __restrict__ bias, int relu,
+                                                 const double* __restrict__ box, float* __restrict__ C32,
+                                                 __nv_bfloat16* __restrict__ C16) {
+  __shared__ __align__(16) __nv_bfloat16 sB[N * K];
+  for (int t = threadIdx.x; t < N * K / 2; t += blockDim.x)
+    reinterpret_cast<uint32_t*>(sB)[t] = reinterpret_cast<const uint32_t*>(Bt)[t];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int row0 = (blockIdx.x * 4 + (threadIdx.x >> 5)) * 16;
+  if (row0 >= M) return;
+  float acc[N / 8][4];
+#pragma unroll
+  for (int nt = 0; nt < N / 8; nt++) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+  const int ra = min(row0 + g, M - 1), rb = min(row0 + g + 8, M - 1);
+#pragma unroll
+  for (int kt = 0; kt < K / 16; kt++) {
+    const int k0 = kt * 16 + 2 * t;
+    const uint32_t a0 = pack2(A + (size_t)ra * K + k0);
+    const uint32_t a1 = pack2(A + (size_t)rb * K + k0);
+    const uint32_t a2 = pack2(A + (size_t)ra * K + k0 + 8);
+    const uint32_t a3 = pack2(A + (size_t)rb * K + k0 + 8);
+#pragma unroll
+    for (int nt = 0; nt < N / 8; nt++) {
+      const int n = nt * 8 + g;
+      const uint32_t b0 = pack2(sB + n * K + k0);
+      const uint32_t b1 = pack2(sB + n * K + k0 + 8);
+      mma16816(acc[nt], a0, a1, a2, a3, b0, b1);
+    }
+  }
+#pragma unroll
+  for (int nt = 0; nt < N / 8; nt++) {
+    const int n = nt * 8 + 2 * t;
+    for (int half = 0; half < 2; half++) {
+      const int row = row0 + g + 8 * half;
+      if (row >= M) continue;
+      const bool valid = box[2 * row] > 0.0;
+      for (int c = 0; c < 2; c++) {
+        float v = acc[nt][2 * half + c];
+        if (bias) v += bias[n + c];
+        if (relu) v = fmaxf(v, 0.f);
+        if (!valid) v = 0.f;
+        if (C32) C32[(size_t)row * N + n + c] = v;
+        if (C16) C16[(size_t)row * N + n + c] = __float2bfloat16_rn(v);
+      }
+    }
+  }
+}
+
+// ---- weight gradient: W[k][n] = sum_m X[m][k] G[m][n] ---------------------------
+// Fixed grid; every block reduces a contiguous row range into its own
+// [K x N] partial (deterministic), k_ml_reduce sums the partials in order.
+// Warp w of 4 owns the n-slice [32 * (w % (N/32)), +32) and, when N == 64,
+// every other 16-row chunk.
+template <int K, int N>
+__global__ void __launch_bounds__(128) k_ml_wgrad(const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ G,
+                                                  int M, float* __restrict__ partial) {
+  constexpr int SLICES = N / 32, REPL = 4 / SLICES;  // warps per slice
+  __shared__ __align__(16) __nv_bfloat16 sX[4][16 * K];
+  __shared__ __align__(16) __nv_bfloat16 sG[4][16 * N];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int slice = warp % SLICES, rep = warp / SLICES;
+  const int rows_per_block = (M + gridDim.x - 1) / gridDim.x;
+  const int m_begin = blockIdx.x * rows_per_block, m_end = min(M, m_begin + rows_per_block);
+  float acc[K / 16][4][4];
+#pragma unroll
+  for (int a = 0; a < K / 16; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b][0] = acc[a][b][1] = acc[a][b][2] = acc[a][b][3] = 0.f;
+  for (int c0 = m_begin + 16 * rep; c0 < m_end; c0 += 16 * REPL) {
+    // stage this warp's 16-row chunk of X and G
+    for (int idx = lane; idx < 16 * K; idx += 32) {
+      const int rr = idx / K, kk = idx % K, m = c0 + rr;
+      sX[warp][idx] = m < m_end ? X[(size_t)m * K + kk] : __float2bfloat16_rn(0.f);
+    }
+    for (int idx = lane; idx < 16 * N; idx += 32) {
+      const int rr = idx / N, nn = idx % N, m = c0 + rr;
+      sG[warp][idx] = m < m_end ? G[(size_t)m * N + nn] : __float2bfloat16_rn(0.f);
+    }
+    __syncwarp();
+    // A = X^T chunk: A[kf][row]; B = G chunk: B[row][n]
+#pragma unroll
+    for (int mt = 0; mt < K / 16; mt++) {
+      const int kf = mt * 16 + g;
+      __nv_bfloat162 p0, p1, p2, p3;
+      p0.x = sX[warp][(2 * t) * K + kf];         p0.y = sX[warp][(2 * t + 1) * K + kf];
+      p1.x = sX[warp][(2 * t) * K + kf + 8];     p1.y = sX[warp][(2 * t + 1) * K + kf + 8];
+      p2.x = sX[warp][(2 * t + 8) * K + kf];     p2.y = sX[warp][(2 * t + 9) * K + kf];
+      p3.x = sX[warp][(2 * t + 8) * K + kf + 8]; p3.y = sX[warp][(2 * t + 9) * K + kf + 8];
+      const uint32_t a0 = *reinterpret_cast<uint32_t*>(&p0), a1 = *reinterpret_cast<uint32_t*>(&p1);
+      const uint32_t a2 = *reinterpret_cast<uint32_t*>(&p2), a3 = *reinterpret_cast<uint32_t*>(&p3);
+#pragma unroll
+      for (int nt = 0; nt < 4; nt++) {
+        const int n = slice * 32 + nt * 8 + g;
+        __nv_bfloat162 q0, q1;
+        q0.x = sG[warp][(2 * t) * N + n];     q0.y = sG[warp][(2 * t + 1) * N + n];
+        q1.x = sG[warp][(2 * t + 8) * N + n]; q1.y = sG[warp][(2 * t + 9) * N + n];
+        mma16816(acc[mt][nt], a0, a1, a2, a3, *reinterpret_cast<uint32_t*>(&q0), *reinterpret_cast<uint32_t*>(&q1));
+      }
+    }
+    __syncwarp();
+  }
+  // each slice is owned by REPL warps: the first writes, the others add in order
+  float* out = partial + (size_t)blockIdx.x * K * N;
+  for (int r = 0; r < REPL; r++) {
+    if (rep == r) {
+#pragma unroll
+      for (int mt = 0; mt < K / 16; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+          const int kf = mt * 16 + g, n = slice * 32 + nt * 8 + 2 * t;
+          float* o0 = out + kf * N + n;
+          float* o1 = out + (kf + 8) * N + n;
+          if (r == 0) {
+            o0[0] = acc[mt][nt][0]; o0[1] = acc[mt][nt][1]; o1[0] = acc[mt][nt][2]; o1[1] = acc[mt][nt][3];
+          } else {
+            o0[0] += acc[mt][nt][0]; o0[1] += acc[mt][nt][1]; o1[0] += acc[mt][nt][2]; o1[1] += acc[mt][nt][3];
+          }
+        }
+    }
+    __syncthreads();
+  }
+}
+
+// out[i] += sum_b partial[b][i]   (fixed order)
+__global__ void k_ml_reduce(const float* __restrict__ partial, int nblk, int len, float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= len) return;
+  float s = 0.f;
+  for (int b = 0; b < nblk; b++) s += partial[(size_t)b * len + i];
+  out[i] += s;
+}
+
+// ---- layer 2 edges (forward): disp_i --------------------------------------------
+__global__ void k_ml_l2(sg_view V, const double* __restrict__ box, double rc, const float* __restrict__ P,
+                        const float* __restrict__ PQ, float* __restrict__ disp) {
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  float we[2][4], b2[2], w2[2];
+  for (int h = 0; h < 2; h++) {
+    const int f = lane + 32 * h;
+    for (int d = 0; d < 4; d++) we[h][d] = P[NP_W2E + 4 * f + d];
+    b2[h] = P[NP_B2 + f];
+    w2[h] = P[NP_W2 + f];
+  }
+  const float c = P[NP_C];
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < V.slots; i += nw) {
+    float dx = 0.f, dy = 0.f;
+    if (box[2 * i] > 0.0) {
+      const float ai = (float)V.radius_device[i];
+      const float Pi0 = PQ[(size_t)i * 2 * F + lane], Pi1 = PQ[(size_t)i * 2 * F + lane + 32];
+      const int cnt = V.nb_cnt_device[i];
+      for (int q = 0; q < cnt; q++) {
+        const int j = V.nb_device[(size_t)q * V.nb_stride + i];
+        float e[4], ux, uy;
+        if (!edge_vec(V, box, i, j, rc, e, ux, uy, ai)) continue;
+        const float Qj0 = PQ[(size_t)j * 2 * F + F + lane], Qj1 = PQ[(size_t)j * 2 * F + F + lane + 32];
+        const float z0 = Pi0 + Qj0 + we[0][0] * e[0] + we[0][1] * e[1] + we[0][2] * e[2] + we[0][3] * e[3] + b2[0];
+        const float z1 = Pi1 + Qj1 + we[1][0] * e[0] + we[1][1] * e[1] + we[1][2] * e[2] + we[1][3] * e[3] + b2[1];
+        float part = fmaxf(z0, 0.f) * w2[0] + fmaxf(z1, 0.f) * w2[1];
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        const float w = part + c;
+        dx += w * ux; dy += w * uy;
+      }
+    }
+    if (lane == 0) { disp[2 * i] = dx; disp[2 * i + 1] = dy; }
+  }
+}
+
+// ---- layer 2 edges (backward) -------------------------------------------------
+// gPQ must be zero on entry: the P half of row i is written by i's warp, the Q
+// half of row j receives atomic contributions from every i that has j as a
+// neighbour.  Per-block partials of (gW2e, gb2, gw2, gc) go to part[block].
+constexpr int L2_GRAD = 256 + 64 + 64 + 1;  // W2e, b2, w2, c
+__global__ void k_ml_l2_bwd(sg_view V, const double* __restrict__ box, double rc, const float* __restrict__ P,
+                            const float* __restrict__ PQ, const float* __restrict__ disp,
+                            const float* __restrict__ target, float inv_n, float* __restrict__ gPQ,
+                            float* __restrict__ part, float* __restrict__ loss_part) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  float we[2][4], b2[2], w2[2];
+  for (int h = 0; h < 2; h++) {
+    const int f = lane + 32 * h;
+    for (int d = 0; d < 4; d++) we[h][d] = P[NP_W2E + 4 * f + d];
+    b2[h] = P[NP_B2 + f];
+    w2[h] = P[NP_W2 + f];
+  }
+  const float c = P[NP_C];
+  float gWe[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}}, gb2[2] = {0.f, 0.f}, gw2[2] = {0.f, 0.f};
+  float gc = 0.f, lsum = 0.f;
+  for (int i = blockIdx.x * (blockDim.x >> 5) + warp; i < V.slots; i += nw) {
+    if (!(box[2 * i] > 0.0)) continue;
+    const float ddx = disp[2 * i] - target[2 * i], ddy = disp[2 * i + 1] - target[2 * i + 1];
+    lsum += ddx * ddx + ddy * ddy;
+    const float gdx = 2.f * ddx * inv_n, gdy = 2.f * ddy * inv_n;
+    const float ai = (float)V.radius_device[i];
+    const float Pi0 = PQ[(size_t)i * 2 * F + lane], Pi1 = PQ[(size_t)i * 2 * F + lane + 32];
+    float gP0 = 0.f, gP1 = 0.f;
+    const int cnt = V.nb_cnt_device[i];
+    for (int q = 0; q < cnt; q++) {
+      const int j = V.nb_device[(size_t)q * V.nb_stride + i];
+      float e[4], ux, uy;
+      if (!edge_vec(V, box, i, j, rc, e, ux, uy, ai)) continue;
+      const float Qj0 = PQ[(size_t)j * 2 * F + F + lane], Qj1 = PQ[(size_t)j * 2 * F + F + lane + 32];
+      const float z0 = Pi0 + Qj0 + we[0][0] * e[0] + we[0][1] * e[1] + we[0][2] * e[2] + we[0][3] * e[3] + b2[0];
+      const float z1 = Pi1 + Qj1 + we[1][0] * e[0] + we[1][1] * e[1] + we[1][2] * e[2] + we[1][3] * e[3] + b2[1];
+      const float a0 = fmaxf(z0, 0.f), a1 = fmaxf(z1, 0.f);
+      const float gw = gdx * ux + gdy * uy;  // d loss / d w_ij
+      gw2[0] += gw * a0; gw2[1] += gw * a1;
+      if (lane == 0) gc += gw;
+      const float gz0 = z0 > 0.f ? gw * w2[0] : 0.f, gz1 = z1 > 0.f ? gw * w2[1] : 0.f;
+      gb2[0] += gz0; gb2[1] += gz1;
+      for (int d = 0; d < 4; d++) { gWe[0][d] += gz0 * e[d]; gWe[1][d] += gz1 * e[d]; }
+      gP0 += gz0; gP1 += gz1;
+      atomicAdd(&gPQ[(size_t)j * 2 * F + F + lane], gz0);
+      atomicAdd(&gPQ[(size_t)j * 2 * F + F + lane + 32], gz1);
+    }
+    gPQ[(size_t)i * 2 * F + lane] = gP0;
+    gPQ[(size_t)i * 2 * F + lane + 32] = gP1;
+  }
+  // block reduction of the weight-gradient partials (fixed order over warps)
+  __shared__ float sp[EDGE_WARPS][L2_GRAD];
+  for (int h = 0; h < 2; h++) {
+    const int f = lane + 32 * h;
+    for (int d = 0; d < 4; d++) sp[warp][4 * f + d] = gWe[h][d];
+    sp[warp][256 + f] = gb2[h];
+    sp[warp][320 + f] = gw2[h];
+  }
+  for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+  if (lane == 0) sp[warp][384] = gc;
+  __shared__ float sl[EDGE_WARPS];
+  if (lane == 0) sl[warp] = lsum;
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < L2_GRAD; idx += blockDim.x) {
+    float s = 0.f;
+    for (int w = 0; w < EDGE_WARPS; w++) s += sp[w][idx];
+    part[(size_t)blockIdx.x * L2_GRAD + idx] = s;
+  }
+  if (threadIdx.x == 0) {
+    float s = 0.f;
+    for (int w = 0; w < EDGE_WARPS; w++) s += sl[w];
+    loss_part[blockIdx.x] = s;
+  }
+}
+
+// gpre = gh * (h > 0) (BF16) and per-block column partials of gpre (gb1b)
+__global__ void k_ml_relu_bwd(int M, const float* __restrict__ gh, const __nv_bfloat16* __restrict__ h16,
+                              __nv_bfloat16* __restrict__ gpre16, float* __restrict__ part) {
+  const int f = threadIdx.x & 63, rsub = threadIdx.x >> 6;  // 256 threads: 4 rows per pass
+  float acc = 0.f;
+  const int rows_per_block = (M + gridDim.x - 1) / gridDim.x;
+  const int m0 = blockIdx.x * rows_per_block, m1 = min(M, m0 + rows_per_block);
+  for (int m = m0 + rsub; m < m1; m += 4) {
+    const float g = bf(h16[(size_t)m * F + f]) > 0.f ? gh[(size_t)m * F + f] : 0.f;
+    const __nv_bfloat16 gb = __float2bfloat16_rn(g);
+    gpre16[(size_t)m * F + f] = gb;
+    acc += bf(gb);
+  }
+  __shared__ float s[4][64];
+  s[rsub][f] = acc;
+  __syncthreads();
+  if (threadIdx.x < 64) part[(size_t)blockIdx.x * 64 + threadIdx.x] = s[0][f] + s[1][f] + s[2][f] + s[3][f];
+}
+
+// ---- layer 1 edges (backward): gW1a, gb1a partials ------------------------------
+constexpr int L1_GRAD = 256 + 64;
+__global__ void k_ml_l1_bwd(sg_view V, const double* __restrict__ box, double rc, const float* __restrict__ P,
+                            const float* __restrict__ gs, float* __restrict__ part) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  float w[2][4], b[2];
+  for (int h = 0; h < 2; h++) {
+    const int f = lane + 32 * h;
+    for (int d = 0; d < 4; d++) w[h][d] = P[NP_W1A + 4 * f + d];
+    b[h] = P[NP_B1A + f];
+  }
+  float gW[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}}, gb[2] = {0.f, 0.f};
+  for (int i = blockIdx.x * (blockDim.x >> 5) + warp; i < V.slots; i += nw) {
+    if (!(box[2 * i] > 0.0)) continue;
+    const float ai = (float)V.radius_device[i];
+    const float gs0 = gs[(size_t)i * F + lane], gs1 = gs[(size_t)i * F + lane + 32];
+    const int cnt = V.nb_cnt_device[i];
+    for (int q = 0; q < cnt; q++) {
+      const int j = V.nb_device[(size_t)q * V.nb_stride + i];
+      float e[4], ux, uy;
+      if (!edge_vec(V, box, i, j, rc, e, ux, uy, ai)) continue;
+      const float z0 = w[0][0] * e[0] + w[0][1] * e[1] + w[0][2] * e[2] + w[0][3] * e[3] + b[0];
+      const float z1 = w[1][0] * e[0] + w[1][1] * e[1] + w[1][2] * e[2] + w[1][3] * e[3] + b[1];
+      const float g0 = z0 > 0.f ? gs0 : 0.f, g1 = z1 > 0.f ? gs1 : 0.f;
+      gb[0] += g0; gb[1] += g1;
+      for (int d = 0; d < 4; d++) { gW[0][d] += g0 * e[d]; gW[1][d] += g1 * e[d]; }
+    }
+  }
+  __shared__ float sp[EDGE_WARPS][L1_GRAD];
+  for (int h = 0; h < 2; h++) {
+    const int f = lane + 32 * h;
+    for (int d = 0; d < 4; d++) sp[warp][4 * f + d] = gW[h][d];
+    sp[warp][256 + f] = gb[h];
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < L1_GRAD; idx += blockDim.x) {
+    float s = 0.f;
+    for (int ww = 0; ww < EDGE_WARPS; ww++) s += sp[ww][idx];
+    part[(size_t)blockIdx.x * L1_GRAD + idx] = s;
+  }
+}
+
+// add the reduced small-gradient vectors into the flat gradient buffer
+__global__ void k_ml_place(const float* __restrict__ src, int len, float* __restrict__ dst, int off_d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < len) dst[off_d + i] += src[i];
+}
+
+__global__ void k_ml_to_bf16(const float* __restrict__ a, __nv_bfloat16* __restrict__ b, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = __float2bfloat16_rn(a[i]);
+}
+
+__global__ void k_ml_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                          float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi; v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// BF16 copies of the GEMM weights: W1b [64x64], W1b^T, Wpq [64x128], Wpq^T
+__global__ void k_ml_bf16_weights(const float* __restrict__ p, __nv_bfloat16* W1b, __nv_bfloat16* W1bT,
+                                  __nv_bfloat16* Wpq, __nv_bfloat16* WpqT) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < F * F) {
+    const int k = i / F, n = i % F;
+    const __nv_bfloat16 v = __float2bfloat16_rn(p[NP_W1B + i]);
+    W1b[i] = v;
+    W1bT[n * F + k] = v;
+  }
+  if (i < F * 2 * F) {
+    const int k = i / (2 * F), n = i % (2 * F);
+    const __nv_bfloat16 v = __float2bfloat16_rn(p[NP_WPQ + i]);
+    Wpq[i] = v;
+    WpqT[n * F + k] = v;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int sg_mlp_param_count(void) { return NP_TOTAL; }
+int sg_mlp_edge_blocks(void) { return EDGE_BLOCKS; }
+int sg_mlp_part_floats(void) { return 148 * F * 2 * F > EDGE_BLOCKS * L2_GRAD ? 148 * F * 2 * F : EDGE_BLOCKS * L2_GRAD; }
+
+int sg_mlp_prepare(const float* params, void* W1b16, void* W1bT16, void* Wpq16, void* WpqT16, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_ml_bf16_weights<<<(F * 2 * F + 255) / 256, 256, 0, st>>>(
+      params, (__nv_bfloat16*)W1b16, (__nv_bfloat16*)W1bT16, (__nv_bfloat16*)Wpq16, (__nv_bfloat16*)WpqT16);
+  return cudaGetLastError() == cudaSuccess ? SG_OK : SG_ERR_CUDA;
+}
+
+int sg_mlp_forward(const sg_view* V, const double* box, double rc, const float* params, const void* W1bT16,
+                   const void* WpqT16, void* s16, void* h16, float* PQ, float* disp, void* stream) {
+  if (!V || !box || !params) return SG_ERR_ARG;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int M = V->slots;
+  k_ml_l1<<<EDGE_BLOCKS, 32 * EDGE_WARPS, 0, st>>>(*V, box, rc, params, (__nv_bfloat16*)s16);
+  const int gb = (M + 63) / 64;
+  k_ml_gemm<F, F><<<gb, 128, 0, st>>>((const __nv_bfloat16*)s16, (const __nv_bfloat16*)W1bT16, M,
+                                       params + NP_B1B, 1, box, nullptr, (__nv_bfloat16*)h16);
+  k_ml_gemm<F, 2 * F><<<gb, 128, 0, st>>>((const __nv_bfloat16*)h16, (const __nv_bfloat16*)WpqT16, M, nullptr, 0,
+                                           box, PQ, nullptr);
+  k_ml_l2<<<EDGE_BLOCKS, 32 * EDGE_WARPS, 0, st>>>(*V, box, rc, params, PQ, disp);
+  return cudaGetLastError() == cudaSuccess ? SG_OK : SG_ERR_CUDA;
+}
+
+// Gradients are ADDED to grad[NP_TOTAL] (zero it first).  work: gPQ [M x 128]
+// fp32, gPQ16 [M x 128] bf16, gh [M x 64] fp32, gpre16 [M x 64] bf16, gs
+// [M x 64] fp32, part >= sg_mlp_part_floats() floats, red >= 512 floats,
+// loss_part >= sg_mlp_edge_blocks() floats (per-block partial sums of
+// |disp - target|^2).
+int sg_mlp_backward(const sg_view* V, const double* box, double rc, const float* params, const void* W1b16,
+                    const void* Wpq16, const void* s16, const void* h16, const float* PQ, const float* disp,
+                    const float* target, float inv_n, float* gPQ, void* gPQ16, float* gh, void* gpre16, float* gs,
+                    float* part, float* red, float* loss_part, float* grad, void* stream) {
+  if (!V || !box || !params || !grad) return SG_ERR_ARG;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int M = V->slots;
+  cudaMemsetAsync(gPQ, 0, sizeof(float) * (size_t)M * 2 * F, st);
+  // layer 2 edges
+  k_ml_l2_bwd<<<EDGE_BLOCKS, 32 * EDGE_WARPS, 0, st>>>(*V, box, rc, params, PQ, disp, target, inv_n, gPQ, part,
+                                                       loss_part);
+  cudaMemsetAsync(red, 0, sizeof(float) * L2_GRAD, st);
+  k_ml_reduce<<<(L2_GRAD + 255) / 256, 256, 0, st>>>(part, EDGE_BLOCKS, L2_GRAD, red);
+  k_ml_place<<<1, 256, 0, st>>>(red, 256, grad, NP_W2E);
+  k_ml_place<<<1, 64, 0, st>>>(red + 256, 64, grad, NP_B2);
+  k_ml_place<<<1, 64, 0, st>>>(red + 320, 64, grad, NP_W2);
+  k_ml_place<<<1, 1, 0, st>>>(red + 384, 1, grad, NP_C);
+  // gPQ -> bf16 for the GEMMs
+  {
+    const size_t len = (size_t)M * 2 * F;
+    k_ml_to_bf16<<<(unsigned)((len + 255) / 256), 256, 0, st>>>(gPQ, (__nv_bfloat16*)gPQ16, len);
+  }
+  // gWpq = h^T gPQ
+  constexpr int WG_BLOCKS = 148;
+  k_ml_wgrad<F, 2 * F><<<WG_BLOCKS, 128, 0, st>>>((const __nv_bfloat16*)h16, (const __nv_bfloat16*)gPQ16, M, part);
+  k_ml_reduce<<<(F * 2 * F + 255) / 256, 256, 0, st>>>(part, WG_BLOCKS, F * 2 * F, grad + NP_WPQ);
+  // gh = gPQ Wpq^T
+  const int gb = (M + 63) / 64;
+  k_ml_gemm<2 * F, F><<<gb, 128, 0, st>>>((const __nv_bfloat16*)gPQ16, (const __nv_bfloat16*)Wpq16, M, nullptr, 0, box,
+                                           gh, nullptr);
+  // through relu(s W1b + b1b)
+  k_ml_relu_bwd<<<WG_BLOCKS, 256, 0, st>>>(M, gh, (const __nv_bfloat16*)h16, (__nv_bfloat16*)gpre16, part);
+  k_ml_reduce<<<1, 64, 0, st>>>(part, WG_BLOCKS, F, grad + NP_B1B);
+  k_ml_wgrad<F, F><<<WG_BLOCKS, 128, 0, st>>>((const __nv_bfloat16*)s16, (const __nv_bfloat16*)gpre16, M, part);
+  k_ml_reduce<<<(F * F + 255) / 256, 256, 0, st>>>(part, WG_BLOCKS, F * F, grad + NP_W1B);
+  // gs = gpre W1b^T
+  k_ml_gemm<F, F><<<gb, 128, 0, st>>>((const __nv_bfloat16*)gpre16, (const __nv_bfloat16*)W1b16, M, nullptr, 0, box, gs,
+                                       nullptr);
+  // layer 1 edges
+  k_ml_l1_bwd<<<EDGE_BLOCKS, 32 * EDGE_WARPS, 0, st>>>(*V, box, rc, params, gs, part);
+  cudaMemsetAsync(red, 0, sizeof(float) * L1_GRAD, st);
+  k_ml_reduce<<<(L1_GRAD + 255) / 256, 256, 0, st>>>(part, EDGE_BLOCKS, L1_GRAD, red);
+  k_ml_place<<<1, 256, 0, st>>>(red, 256, grad, NP_W1A);
+  k_ml_place<<<1, 64, 0, st>>>(red + 256, 64, grad, NP_B1A);
+  return cudaGetLastError() == cudaSuccess ? SG_OK : SG_ERR_CUDA;
+}
+
+// x += dx, y += dy for the slots with box > 0 (scale 1), wrapped back into
+// the periodic box with the image flags updated, as enforce_periodic would.
+__global__ void k_ml_apply(sg_view V, const double* __restrict__ box, const float* __restrict__ disp,
+                           int* __restrict__ ix, int* __restrict__ iy) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V.slots) return;
+  const double Lx = box[2 * i], Ly = box[2 * i + 1];
+  if (!(Lx > 0.0)) return;
+  double x = V.x_device[i] + (double)disp[2 * i], y = V.y_device[i] + (double)disp[2 * i + 1];
+  if (x <= -0.5 * Lx) { x += Lx; ix[i]--; } else if (x > 0.5 * Lx) { x -= Lx; ix[i]++; }
+  if (y <= -0.5 * Ly) { y += Ly; iy[i]--; } else if (y > 0.5 * Ly) { y -= Ly; iy[i]++; }
+  V.x_device[i] = x;
+  V.y_device[i] = y;
+}
+
+int sg_mlp_adam(float* params, const float* grad, float* m, float* v, int n, float lr, float beta1, float beta2,
+                float eps, int step, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+  k_ml_adam<<<(n + 255) / 256, 256, 0, st>>>(params, grad, m, v, n, lr, beta1, beta2, eps, c1, c2);
+  return cudaGetLastError() == cudaSuccess ? SG_OK : SG_ERR_CUDA;
+}
+
+int sg_mlp_apply(const sg_view* V, const double* box, const float* disp, int* ix, int* iy, void* stream) {
+  if (!V || !box || !disp) return SG_ERR_ARG;
+  k_ml_apply<<<(V->slots + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(*V, box, disp, ix, iy);
+  return cudaGetLastError() == cudaSuccess ? SG_OK : SG_ERR_CUDA;
+}
+
+}  // extern "C"
+

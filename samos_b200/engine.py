@@ -34,6 +34,12 @@ class EngineError(RuntimeError):
         self.code = code
 
 
+class View(C.Structure):
+    _fields_ = [(f, C.c_void_p) for f in ("x", "y", "z", "nx", "ny", "nz", "vx", "vy", "vz", "fx", "fy", "fz",
+                                           "radius", "id", "nb", "nb_cnt", "ix", "iy")] + \
+               [("nb_stride", C.c_int32), ("slots", C.c_int32)]
+
+
 class RunStats(C.Structure):
     _fields_ = [("steps_done", C.c_int64), ("nlist_builds", C.c_int64),
                 ("kernel_launches", C.c_int64), ("max_neighbours", C.c_int32),
@@ -85,6 +91,10 @@ def load() -> C.CDLL:
         "sg_set_profiling": (I, [P, I]),
         "sg_set_device": (I, [I]),
         "sg_set_path": (I, [P, I]),
+        "sg_get_view": (I, [P, C.POINTER(View)]),
+        "sg_replica_slots": (I, [P, I, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+        "sg_positions_changed": (I, [P]),
+        "sg_memcpy": (I, [P, P, I64]),
         "sg_set_variant": (I, [P, I]),
         "sg_get_variant": (I, [P]),
         "sg_compute_static": (I, [I, D, D, D, I, D, D] + [P] * 7 + [D, D, I, I, D, D] + [P] * 6 + [P]),
@@ -142,8 +152,11 @@ class Engine:
 
     # -- configuration -----------------------------------------------------
     def set_box(self, lx, ly, lz, periodic=True, replica=None):
+        if not hasattr(self, "boxes"):
+            self.boxes = [None] * len(self.n)
         for r in (range(len(self.n)) if replica is None else [replica]):
             self._check(self.lib.sg_set_box(self.h, r, lx, ly, lz, int(bool(periodic))))
+            self.boxes[r] = (float(lx), float(ly), float(lz), bool(periodic))
 
     def set_timestep(self, dt):
         self._check(self.lib.sg_set_timestep(self.h, float(dt)))
@@ -255,6 +268,20 @@ class Engine:
     def set_path(self, path: int) -> None:
         """0 automatic, 1 generic SoA kernels, 2 packed kernels unspecialised."""
         self._check(self.lib.sg_set_path(self.h, int(path)))
+
+    def view(self) -> View:
+        """Device pointers into the current state and neighbour lists (see sg_view)."""
+        v = View()
+        self._check(self.lib.sg_get_view(self.h, C.byref(v)))
+        return v
+
+    def replica_slots(self, replica: int):
+        off, n = C.c_int32(), C.c_int32()
+        self._check(self.lib.sg_replica_slots(self.h, replica, C.byref(off), C.byref(n)))
+        return off.value, n.value
+
+    def positions_changed(self) -> None:
+        self._check(self.lib.sg_positions_changed(self.h))
 
     def set_variant(self, v: int) -> None:
         """Pin a step-kernel variant (0..4) or re-enable autotuning (-1)."""

@@ -55,3 +55,38 @@ def sphere_ensemble(reps: list[SphereReplica], k: float = 10.0, rcut: float = 2.
         eng.set_replica_param(i, 4, 0, 2, r.nu)
         eng.set_replica_param(i, 4, 0, 5, float(r.seed))
     return eng
+
+
+def quench_disks(n: int, phi: float, seed: int, radii=(1.0, 1.4)):
+    """Bidisperse disks (50:50) at uniform random positions in a square periodic
+    box of packing fraction phi -- the quench that FIRE relaxes."""
+    rng = np.random.default_rng(seed)
+    r = np.where(np.arange(n) % 2 == 0, radii[0], radii[1]).astype(np.float64)
+    rng.shuffle(r)
+    L = float(np.sqrt(np.sum(np.pi * r * r) / phi))
+    th = rng.uniform(0.0, 2.0 * np.pi, n)
+    parts = dict(x=rng.uniform(-L / 2, L / 2, n), y=rng.uniform(-L / 2, L / 2, n), z=np.zeros(n),
+                 vx=np.zeros(n), vy=np.zeros(n), vz=np.zeros(n),
+                 nx=np.cos(th), ny=np.sin(th), nz=np.zeros(n), radius=r)
+    return parts, L
+
+
+def plane_fire_ensemble(insts, k: float = 1.0, rcut: float = 2.8, pad: float = 0.3, dt: float = 0.01,
+                        dt_max: float = 0.2, fmax: float = 1e-10, device: int | None = None) -> E.Engine:
+    """FIRE minimisation of many periodic-plane systems (soft repulsion on the
+    particle radii) in one engine; insts = [(parts, L), ...]."""
+    eng = E.Engine([len(p["x"]) for p, _ in insts], device=device)
+    for i, (parts, L) in enumerate(insts):
+        eng.set_box(L, L, 10.0, periodic=True, replica=i)
+        for f, v in parts.items():
+            eng.upload(f, v, replica=i)
+    eng.set_nlist(rcut, pad)
+    kind, cp = resolve_constraint("plane", {})
+    eng.add_constraint(kind, cp)
+    pair = resolve_pair("soft", {"k": repr(k), "use_particle_radii": ""}, 1, rcut)
+    eng.add_pair(pair.kind, pair.glob, pair.table.reshape(-1), pair.use_radii, False, False, False,
+                 pair.phase_value)
+    eng.set_timestep(dt)
+    ikind, ip, temp = resolve_integrator("fire", {"dt_max": repr(dt_max), "fmax_tolerance": repr(fmax)}, dt)
+    eng.add_integrator(ikind, ip, temp)
+    return eng

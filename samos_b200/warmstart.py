@@ -1,0 +1,192 @@
+"""Learned FIRE warm start.
+
+A two-layer message-passing network (hidden width 64, neighbours within
+rc = 2.8; kernels in csrc/sg_ml.cu) predicts, from a quenched configuration,
+each particle's displacement to its FIRE minimum.  Training data are
+quench-then-FIRE relaxations run by the engine's own GPU FIRE; training runs
+the project's forward/backward kernels (BF16 tensor-core GEMMs, FP32
+accumulation) with Adam.  At use, the predicted displacement is applied only
+where it lowers a replica's energy; otherwise that replica starts from its
+quench (plain FIRE is the fallback).
+
+Device memory for parameters and activations is held in torch tensors
+(allocation and plumbing only; every computation is a call into
+libsamos_gpu.so).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+import torch
+
+from . import engine as E
+
+F = 64
+OFF = dict(W1a=(0, (64, 4)), b1a=(256, (64,)), W1b=(320, (64, 64)), b1b=(4416, (64,)), Wpq=(4480, (64, 128)),
+           b2=(12672, (64,)), W2e=(12736, (64, 4)), w2=(12992, (64,)), c=(13056, (1,)))
+
+
+def _p(t: torch.Tensor | None):
+    return C.c_void_p(0) if t is None else C.c_void_p(t.data_ptr())
+
+
+def _bind(lib):
+    P, I, D, Fl = C.c_void_p, C.c_int, C.c_double, C.c_float
+    vp = C.POINTER(E.View)
+    sig = {
+        "sg_mlp_param_count": (I, []), "sg_mlp_edge_blocks": (I, []), "sg_mlp_part_floats": (I, []),
+        "sg_mlp_prepare": (I, [P] * 6),
+        "sg_mlp_forward": (I, [vp, P, D, P, P, P, P, P, P, P, P]),
+        "sg_mlp_backward": (I, [vp, P, D, P, P, P, P, P, P, P, P, Fl, P, P, P, P, P, P, P, P, P, P]),
+        "sg_mlp_adam": (I, [P, P, P, P, I, Fl, Fl, Fl, Fl, I, P]),
+        "sg_mlp_apply": (I, [vp, P, P, P, P, P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype, f.argtypes = res, args
+    return lib
+
+
+def _ok(rc, what):
+    if rc != 0:
+        raise E.EngineError(rc, what)
+
+
+class WarmStartNet:
+    def __init__(self, seed: int = 0, rc: float = 2.8, device: str = "cuda"):
+        self.lib = _bind(E.load())
+        self.rc = float(rc)
+        self.dev = torch.device(device)
+        n = self.lib.sg_mlp_param_count()
+        self.params = torch.zeros(n, dtype=torch.float32, device=self.dev)
+        self.m = torch.zeros_like(self.params)
+        self.v = torch.zeros_like(self.params)
+        self.grad = torch.zeros_like(self.params)
+        self.W1b16 = torch.zeros(F * F, dtype=torch.bfloat16, device=self.dev)
+        self.W1bT16 = torch.zeros_like(self.W1b16)
+        self.Wpq16 = torch.zeros(F * 2 * F, dtype=torch.bfloat16, device=self.dev)
+        self.WpqT16 = torch.zeros_like(self.Wpq16)
+        self.step = 0
+        self._ws = {}
+        self.set_params(self.init_params(seed))
+
+    @staticmethod
+    def init_params(seed: int) -> np.ndarray:
+        """Uniform fan-in initialisation; the output weights start small."""
+        rng = np.random.default_rng(seed)
+        p = np.zeros(13057, np.float32)
+        def put(name, fan_in, scale=1.0):
+            off, shape = OFF[name]
+            b = scale / np.sqrt(fan_in)
+            p[off:off + int(np.prod(shape))] = rng.uniform(-b, b, int(np.prod(shape)))
+        put("W1a", 4); put("b1a", 4); put("W1b", 64); put("b1b", 64); put("Wpq", 64)
+        put("b2", 64); put("W2e", 4); put("w2", 64, 0.1)
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        self.params.copy_(torch.from_numpy(np.asarray(p, np.float32)))
+        self._refresh()
+
+    def get_params(self) -> np.ndarray:
+        return self.params.detach().cpu().numpy().copy()
+
+    def _refresh(self):
+        _ok(self.lib.sg_mlp_prepare(_p(self.params), _p(self.W1b16), _p(self.W1bT16), _p(self.Wpq16),
+                                    _p(self.WpqT16), None), "sg_mlp_prepare")
+
+    def _work(self, slots: int):
+        if slots not in self._ws:
+            d = self.dev
+            nb = self.lib.sg_mlp_edge_blocks()
+            self._ws[slots] = dict(
+                s16=torch.zeros(slots * F, dtype=torch.bfloat16, device=d),
+                h16=torch.zeros(slots * F, dtype=torch.bfloat16, device=d),
+                PQ=torch.zeros(slots * 2 * F, dtype=torch.float32, device=d),
+                disp=torch.zeros(slots * 2, dtype=torch.float32, device=d),
+                gPQ=torch.zeros(slots * 2 * F, dtype=torch.float32, device=d),
+                gPQ16=torch.zeros(slots * 2 * F, dtype=torch.bfloat16, device=d),
+                gh=torch.zeros(slots * F, dtype=torch.float32, device=d),
+                gpre16=torch.zeros(slots * F, dtype=torch.bfloat16, device=d),
+                gs=torch.zeros(slots * F, dtype=torch.float32, device=d),
+                part=torch.zeros(self.lib.sg_mlp_part_floats(), dtype=torch.float32, device=d),
+                red=torch.zeros(512, dtype=torch.float32, device=d),
+                loss=torch.zeros(nb, dtype=torch.float32, device=d))
+        return self._ws[slots]
+
+    # -- graph helpers ---------------------------------------------------------------
+    def box_array(self, eng: E.Engine, replicas=None) -> torch.Tensor:
+        """(Lx, Ly) per slot of the selected replicas, 0 elsewhere."""
+        view = eng.view()
+        box = np.zeros(view.slots * 2)
+        for r in (range(len(eng.n)) if replicas is None else replicas):
+            off, n = eng.replica_slots(r)
+            lx, ly, _, _ = eng.boxes[r]
+            box[2 * off:2 * (off + n):2] = lx
+            box[2 * off + 1:2 * (off + n):2] = ly
+        return torch.from_numpy(box).to(self.dev)
+
+    def slot_ids(self, eng: E.Engine) -> np.ndarray:
+        view = eng.view()
+        ids = np.zeros(view.slots, np.int32)
+        _ok(self.lib.sg_memcpy(ids.ctypes.data_as(C.c_void_p), C.c_void_p(view.id), ids.nbytes), "ids")
+        return ids
+
+    def slot_targets(self, eng: E.Engine, targets: list[np.ndarray]) -> torch.Tensor:
+        """Per-replica (n, 2) arrays in particle-id order -> slot-ordered float32."""
+        ids = self.slot_ids(eng)
+        t = np.zeros(len(ids) * 2, np.float32)
+        for r, tr in enumerate(targets):
+            off, n = eng.replica_slots(r)
+            sl = ids[off:off + n]
+            t[2 * off:2 * (off + n):2] = tr[sl, 0]
+            t[2 * off + 1:2 * (off + n):2] = tr[sl, 1]
+        return torch.from_numpy(t).to(self.dev)
+
+    # -- network ----------------------------------------------------------------------
+    def forward(self, eng: E.Engine, box: torch.Tensor) -> torch.Tensor:
+        view = eng.view()
+        w = self._work(view.slots)
+        _ok(self.lib.sg_mlp_forward(C.byref(view), _p(box), self.rc, _p(self.params), _p(self.W1bT16),
+                                    _p(self.WpqT16), _p(w["s16"]), _p(w["h16"]), _p(w["PQ"]), _p(w["disp"]), None),
+            "sg_mlp_forward")
+        return w["disp"]
+
+    def loss_and_grad(self, eng: E.Engine, box: torch.Tensor, target: torch.Tensor, n_valid: int) -> float:
+        """Mean squared displacement error; gradient into self.grad (overwritten)."""
+        view = eng.view()
+        w = self._work(view.slots)
+        self.forward(eng, box)
+        self.grad.zero_()
+        _ok(self.lib.sg_mlp_backward(C.byref(view), _p(box), self.rc, _p(self.params), _p(self.W1b16),
+                                     _p(self.Wpq16), _p(w["s16"]), _p(w["h16"]), _p(w["PQ"]), _p(w["disp"]),
+                                     _p(target), 1.0 / n_valid, _p(w["gPQ"]), _p(w["gPQ16"]), _p(w["gh"]),
+                                     _p(w["gpre16"]), _p(w["gs"]), _p(w["part"]), _p(w["red"]), _p(w["loss"]),
+                                     _p(self.grad), None), "sg_mlp_backward")
+        return float(w["loss"].sum().item()) / n_valid
+
+    def adam_step(self, lr: float = 1e-3, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8) -> None:
+        self.step += 1
+        _ok(self.lib.sg_mlp_adam(_p(self.params), _p(self.grad), _p(self.m), _p(self.v), self.params.numel(),
+                                 lr, beta1, beta2, eps, self.step, None), "sg_mlp_adam")
+        self._refresh()
+
+    def apply(self, eng: E.Engine, box: torch.Tensor, disp: torch.Tensor) -> None:
+        view = eng.view()
+        _ok(self.lib.sg_mlp_apply(C.byref(view), _p(box), _p(disp), C.c_void_p(view.ix), C.c_void_p(view.iy),
+                                  None), "sg_mlp_apply")
+        torch.cuda.synchronize()
+        eng.positions_changed()
+
+    def save(self, path: str) -> None:
+        np.savez(path, params=self.get_params(), rc=self.rc)
+
+    def load(self, path: str) -> None:
+        d = np.load(path)
+        self.rc = float(d["rc"])
+        self.set_params(d["params"])
+
+
+def min_image(d: np.ndarray, L: float) -> np.ndarray:
+    return d - L * np.round(d / L)
