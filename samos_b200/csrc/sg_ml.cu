@@ -284,7 +284,7 @@ __global__ void k_ml_l2_bwd(sg_view V, const double* __restrict__ box, double rc
   for (int i = blockIdx.x * (blockDim.x >> 5) + warp; i < V.slots; i += nw) {
     if (!(box[2 * i] > 0.0)) continue;
     const float ddx = disp[2 * i] - target[2 * i], ddy = disp[2 * i + 1] - target[2 * i + 1];
-    lsum += ddx * ddx + ddy * ddy;
+    if (lane == 0) lsum += ddx * ddx + ddy * ddy;
     const float gdx = 2.f * ddx * inv_n, gdy = 2.f * ddy * inv_n;
     const float ai = (float)V.radius_device[i];
     const float Pi0 = PQ[(size_t)i * 2 * F + lane], Pi1 = PQ[(size_t)i * 2 * F + lane + 32];

@@ -190,3 +190,118 @@ class WarmStartNet:
 
 def min_image(d: np.ndarray, L: float) -> np.ndarray:
     return d - L * np.round(d / L)
+
+
+# -- data: quench-then-FIRE relaxations on the GPU ---------------------------------------
+class Batch:
+    """One engine holding `R` quenched systems, with their relaxation targets
+    (displacement quench -> FIRE minimum, slot order) kept on the device."""
+
+    def __init__(self, net: WarmStartNet, insts, k: float = 1.0, dt: float = 0.01, dt_max: float = 0.2,
+                 fmax: float = 1e-10, max_steps: int = 200000):
+        from .ensemble import plane_fire_ensemble
+        self.insts = insts
+        self.eng = plane_fire_ensemble(insts, k=k, dt=dt, dt_max=dt_max, fmax=fmax)
+        self.eng.build_nlist()
+        t0 = time.perf_counter()
+        self.conv, st = self.eng.minimize(max_steps)
+        self.fire_s = time.perf_counter() - t0
+        self.fire_device_ms = st.device_ms
+        self.energy = np.array([self.eng.energy(0, 0, r) for r in range(len(insts))])
+        targets = []
+        for r, (parts, L) in enumerate(insts):
+            fx, fy = self.eng.download("x", r), self.eng.download("y", r)
+            targets.append(np.stack([min_image(fx - parts["x"], L), min_image(fy - parts["y"], L)], 1))
+        self.targets = targets
+        restore_quench(self.eng, insts)
+        self.box = net.box_array(self.eng)
+        self.target = net.slot_targets(self.eng, targets)
+        self.n_valid = int(sum(len(p["x"]) for p, _ in insts))
+
+
+def restore_quench(eng: E.Engine, insts, replicas=None) -> None:
+    """Put the quench positions (and zero velocities) back into the engine."""
+    for r in (range(len(insts)) if replicas is None else replicas):
+        parts, _ = insts[r]
+        for f in ("x", "y", "vx", "vy"):
+            eng.upload(f, parts[f], replica=r)
+        z = np.zeros(len(parts["x"]), np.int32)
+        eng.upload("ix", z, replica=r)
+        eng.upload("iy", z, replica=r)
+    eng.positions_changed()
+
+
+def quench_set(count: int, n_lo: int, n_hi: int, phi_lo: float, phi_hi: float, seed: int):
+    """`count` quenches; N log-uniform in [n_lo, n_hi] (fixed if equal), phi uniform."""
+    from .ensemble import quench_disks
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = n_lo if n_lo == n_hi else int(round(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi)))))
+        n += n % 2
+        out.append(quench_disks(n, float(rng.uniform(phi_lo, phi_hi)), int(rng.integers(1 << 31))))
+    return out
+
+
+def train(net: WarmStartNet, batches, steps: int, lr: float = 2e-3, lr_end: float = 1e-4, log_every: int = 0):
+    """Adam on the mean squared displacement error, cycling through the
+    batches; the learning rate decays geometrically from lr to lr_end."""
+    hist = []
+    for s in range(steps):
+        b = batches[s % len(batches)]
+        cur = lr * (lr_end / lr) ** (s / max(1, steps - 1))
+        loss = net.loss_and_grad(b.eng, b.box, b.target, b.n_valid)
+        net.adam_step(cur)
+        hist.append(loss)
+        if log_every and s % log_every == 0:
+            print(f"step {s} loss {loss:.5f} lr {cur:.2e}", flush=True)
+    return hist
+
+
+def mean_target_sq(batch: Batch) -> float:
+    """Loss of the zero displacement (the quench itself) on a batch."""
+    return float(sum(np.sum(t * t) for t in batch.targets)) / batch.n_valid
+
+
+def eval_loss(net: WarmStartNet, batch: Batch) -> float:
+    disp = net.forward(batch.eng, batch.box)
+    d = disp.view(-1, 2) - batch.target.view(-1, 2)
+    return float((d * d).sum().item()) / batch.n_valid
+
+
+# -- use: warm-started FIRE with plain FIRE as the fallback ----------------------------
+def relax(insts, net: WarmStartNet | None, k: float = 1.0, dt: float = 0.01, dt_max: float = 0.2,
+          fmax: float = 1e-10, max_steps: int = 400000) -> dict:
+    """Relax every instance to Fmax < fmax in one engine.  With a network,
+    the predicted displacement is applied first, and every replica whose
+    energy it raises goes back to its quench (plain FIRE).  Returns per-replica
+    steps, final energies and the device time of inference + minimisation."""
+    from .ensemble import plane_fire_ensemble
+    eng = plane_fire_ensemble(insts, k=k, dt=dt, dt_max=dt_max, fmax=fmax)
+    eng.build_nlist()
+    R = len(insts)
+    start = torch.cuda.Event(enable_timing=True)
+    mid = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    fallback = np.zeros(R, bool)
+    if net is not None:
+        eng.compute(dt)
+        e0 = np.array([eng.energy(0, 0, r) for r in range(R)])
+        box = net.box_array(eng)
+        disp = net.forward(eng, box)
+        net.apply(eng, box, disp)
+        eng.compute(dt)
+        e1 = np.array([eng.energy(0, 0, r) for r in range(R)])
+        fallback = e1 > e0
+        if fallback.any():
+            restore_quench(eng, insts, np.nonzero(fallback)[0])
+    mid.record()
+    torch.cuda.synchronize()
+    warm_ms = start.elapsed_time(mid)
+    conv, st = eng.minimize(max_steps)
+    energy = np.array([eng.energy(0, 0, r) for r in range(R)])
+    out = dict(steps=conv, energy=energy, fire_ms=st.device_ms, warm_ms=warm_ms, fallback=fallback,
+               total_ms=warm_ms + st.device_ms)
+    eng.close()
+    return out
