@@ -135,6 +135,22 @@ int  sg_add_constraint_per_replica(sg_system* s, int kind, const double* params,
  * Integrators must be added in std::map key order (type + "_" + group).     */
 int  sg_add_integrator(sg_system* s, int kind, const double* params,
                        const double* temperature_value);
+
+/* Multi-segment conf files (src/samos.cpp:864-972 runs once per `run`
+ * command with whatever the plugin maps hold at that point).
+ * sg_insert_integrator: like sg_add_integrator, at position `pos` of the
+ *   integrator sequence, so the host can keep std::map key order
+ *   (samos.cpp:899-900) when integrators are added between runs.
+ * sg_disable_integrator: the `disable` command (samos.cpp, "disable"
+ *   branch: the integrator is erased from the map); later integrators keep
+ *   their noise streams.
+ * sg_clear_forces: drop every pair potential, aligner and external
+ *   potential (they hold no state); the host re-adds the current set in map
+ *   order before a run.                                                   */
+int  sg_insert_integrator(sg_system* s, int pos, int kind, const double* params, const double* temperature_value);
+int  sg_disable_integrator(sg_system* s, int index);
+int  sg_clear_forces(sg_system* s);
+
 /* Per-replica override of one numeric parameter (batched ensembles):
  * cls 0 pair global, 1 aligner {0:J,1:rcut}, 2 external alpha,
  * 3 constraint {0: zpos|r}, 4 integrator params[] (slot 5 = seed).          */
@@ -150,6 +166,12 @@ int  sg_enforce(sg_system* s);
 /* `run steps` (src/samos.cpp:864-972): steps+1 integration steps with the
  * skin-triggered neighbour-list rebuilds of samos.cpp:944-966.              */
 int  sg_run(sg_system* s, int64_t steps, sg_run_stats* stats);
+/* `steps` (>= 1) further integration steps of the current run, with the
+ * run-step counter (Value schedules, samos.cpp:881) continuing: a host that
+ * reads the state every k steps (dumps, logs: samos.cpp:905-940) splits a
+ * `run` into sg_run(k - 1) followed by sg_run_continue(k) calls, with the
+ * same results as one sg_run.                                               */
+int  sg_run_continue(sg_system* s, int64_t steps, sg_run_stats* stats);
 /* FIRE minimisation driver: run until every replica's FIRE integrator has
  * converged or max_steps integration steps; converged[r] (may be NULL) gets
  * the step count per replica or -1.                                         */

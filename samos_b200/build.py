@@ -56,11 +56,11 @@ def build_host(force: bool = False) -> str | None:
     cpp = _sources(HOST, (".cpp",))
     if not cpp:
         return None
-    target = os.path.join(PKG, "samos_b200_run")
+    target = os.path.join(PKG, "samos-gpu")
     srcs = cpp + _sources(HOST, (".hpp",)) + [ENGINE_SO]
     if force or _stale(target, srcs):
         _run(["g++", "-std=c++17", "-O2", f"-I{INCLUDE}", "-o", target, *cpp,
-              f"-L{PKG}", "-lsamos_gpu", f"-Wl,-rpath,{PKG}", "-Wl,-rpath,$ORIGIN"])
+              f"-L{PKG}", "-lsamos_gpu", "-Wl,-rpath,$ORIGIN"])
     return target
 
 

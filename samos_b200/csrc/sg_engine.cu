@@ -717,6 +717,57 @@ int sg_add_integrator(sg_system* s, int kind, const double* params, const double
   return push_clk(s);
 }
 
+// Move integrator `from` to position `to` (program entry, per-replica
+// parameters, seed and noise counter move together).
+static void move_integrator(sg_system* s, int from, int to) {
+  Program& P = s->prog;
+  while (from != to) {
+    const int a = from, b = from < to ? from + 1 : from - 1;
+    std::swap(P.integ[a], P.integ[b]);
+    for (int r = 0; r < s->nrep; r++) {
+      Replica& R = s->reps_h[r];
+      for (int i = 0; i < INT_NPARAM; i++) std::swap(R.integ_p[a][i], R.integ_p[b][i]);
+      std::swap(R.seed[a], R.seed[b]);
+      std::swap(s->clk_h[r].ctr[a], s->clk_h[r].ctr[b]);
+    }
+    from = b;
+  }
+}
+
+int sg_insert_integrator(sg_system* s, int pos, int kind, const double* params, const double* temp) {
+  if (!s) return SG_ERR_ARG;
+  if (pos < 0 || pos > s->prog.ninteg) return fail(s, SG_ERR_ARG, "sg_insert_integrator: bad position");
+  int rc = pull_clk(s);
+  if (rc) return rc;
+  if ((rc = sg_add_integrator(s, kind, params, temp))) return rc;
+  move_integrator(s, s->prog.ninteg - 1, pos);
+  if ((rc = push_reps(s))) return rc;
+  return push_clk(s);
+}
+
+int sg_disable_integrator(sg_system* s, int index) {
+  if (!s) return SG_ERR_ARG;
+  if (index < 0 || index >= s->prog.ninteg) return fail(s, SG_ERR_ARG, "sg_disable_integrator: no such integrator");
+  int rc = pull_clk(s);
+  if (rc) return rc;
+  move_integrator(s, index, s->prog.ninteg - 1);
+  s->prog.ninteg--;
+  s->e1_applied = false;
+  s->forces_fresh = false;
+  if ((rc = push_reps(s))) return rc;
+  return push_clk(s);
+}
+
+int sg_clear_forces(sg_system* s) {
+  if (!s) return SG_ERR_ARG;
+  CU(s, cudaStreamSynchronize(s->stream));
+  Program& P = s->prog;
+  P.npair = P.nalign = P.next = 0;
+  s->pair_tab_h.clear(); s->align_tab_h.clear(); s->ext_tab_h.clear();
+  s->forces_fresh = false;
+  return SG_OK;
+}
+
 int sg_set_replica_param(sg_system* s, int replica, int cls, int comp, int slot, double value) {
   if (!s || replica < 0 || replica >= s->nrep) return fail(s, SG_ERR_ARG, "sg_set_replica_param: bad replica");
   Replica& R = s->reps_h[replica];
@@ -1050,7 +1101,8 @@ static int step_hot(sg_system* s, int shape, bool apply_e1, bool last, bool ener
   return SG_OK;
 }
 
-static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool driver, int64_t* conv_out) {
+static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool driver, int64_t* conv_out,
+                    bool cont = false) {
   if (!s || steps < 0) return SG_ERR_ARG;
   if (s->prog.ninteg == 0) return fail(s, SG_ERR_STATE, "Integrator has not been defined");
   if (s->prog.ncons == 0) return fail(s, SG_ERR_STATE, "Constraint has not been defined");
@@ -1069,8 +1121,9 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
   int64_t kernels_timed = 0;
   CU(s, cudaEventRecord(s->ev_run0, s->stream));
   CU(s, cudaMemsetAsync(s->status, 0, sizeof(int), s->stream));
-  // run-step counters restart with every `run` (samos.cpp:881)
-  {
+  // run-step counters restart with every `run` (samos.cpp:881); a
+  // continued segment keeps counting
+  if (!cont) {
     int rc = pull_clk(s);
     if (rc) return rc;
     for (int r = 0; r < s->nrep; r++) s->clk_h[r].run_step = 0;
@@ -1165,6 +1218,11 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
 }
 
 int sg_run(sg_system* s, int64_t steps, sg_run_stats* stats) { return run_impl(s, steps, stats, false, nullptr); }
+
+int sg_run_continue(sg_system* s, int64_t steps, sg_run_stats* stats) {
+  if (!s || steps < 1) return SG_ERR_ARG;
+  return run_impl(s, steps - 1, stats, false, nullptr, true);
+}
 
 int sg_minimize(sg_system* s, int64_t max_steps, int64_t* converged, sg_run_stats* stats) {
   if (!s) return SG_ERR_ARG;

@@ -278,7 +278,6 @@ __global__ void k_ml_l2_bwd(sg_view V, const double* __restrict__ box, double rc
     b2[h] = P[NP_B2 + f];
     w2[h] = P[NP_W2 + f];
   }
-  const float c = P[NP_C];
   float gWe[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}}, gb2[2] = {0.f, 0.f}, gw2[2] = {0.f, 0.f};
   float gc = 0.f, lsum = 0.f;
   for (int i = blockIdx.x * (blockDim.x >> 5) + warp; i < V.slots; i += nw) {

@@ -1,0 +1,387 @@
+// runner.cpp -- the command loop of src/samos.cpp for the hot-path
+// commands, over the C ABI.  Command order rules and error messages follow
+// the reference (samos.cpp:176-1400): a box before `input`, `input` before
+// constraints, potentials and integrators, a constraint before integrators,
+// and a constraint plus an integrator before `run`.
+//
+// Plugins are kept in std::maps keyed as the reference keys them (pair and
+// external potentials and aligners by type, integrators by type_group).
+// Before each `run` the stateless force terms are handed to the engine in
+// map order; integrators are inserted at their map position when created
+// and removed by `disable`, so their noise streams persist across runs as the
+// reference's RNG objects do.
+#include <cmath>
+#include <cstdio>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+
+#include "samos_host.hpp"
+
+namespace samos_host {
+
+namespace {
+
+int64_t to_i64(const std::string& s, const char* what) {
+  char* end = nullptr;
+  const long long v = std::strtoll(s.c_str(), &end, 10);
+  if (s.empty() || *end != '\0') throw HostError(std::string("Could not parse ") + what + " command.");
+  return v;
+}
+double to_dbl(const std::string& s, const char* what) {
+  char* end = nullptr;
+  const double v = std::strtod(s.c_str(), &end);
+  if (s.empty() || *end != '\0') throw HostError(std::string("Could not parse ") + what + " command.");
+  return v;
+}
+
+}  // namespace
+
+Samos::~Samos() {
+  if (h_) sg_destroy(h_);
+}
+
+void Samos::check(int rc, const char* what) const {
+  if (rc != SG_OK) {
+    const std::string why = h_ ? sg_last_error(h_) : sg_error_string(rc);
+    throw HostError(std::string(what) + ": " + sg_error_string(rc) + (why.empty() ? "" : " (" + why + ")"));
+  }
+}
+
+void Samos::need_system(const char* what) const {
+  if (!has_input_)
+    throw HostError(std::string("System has not been defined. Please define system using \"input\" command before ") +
+                    what + ".");
+}
+
+void Samos::ensure_engine() {
+  if (h_ || opt_.check_only) return;
+  check(sg_set_device(opt_.device), "sg_set_device");
+  const int32_t n = (int32_t)parts_.size();
+  check(sg_create(1, &n, parts_.ntypes, &h_), "sg_create");
+  check(sg_set_box(h_, 0, lx_, ly_, lz_, periodic_ ? 1 : 0), "sg_set_box");
+  auto up = [&](const char* f, const void* p) { check(sg_upload(h_, 0, f, p), "sg_upload"); };
+  up("x", parts_.x.data()); up("y", parts_.y.data()); up("z", parts_.z.data());
+  up("vx", parts_.vx.data()); up("vy", parts_.vy.data()); up("vz", parts_.vz.data());
+  up("nx", parts_.nx.data()); up("ny", parts_.ny.data()); up("nz", parts_.nz.data());
+  up("omega", parts_.omega.data()); up("radius", parts_.radius.data()); up("mass", parts_.mass.data());
+  up("type", parts_.type.data());
+  up("ix", parts_.ix.data()); up("iy", parts_.iy.data()); up("iz", parts_.iz.data());
+}
+
+void Samos::execute_file(const std::string& conf_path) {
+  std::ifstream in(conf_path);
+  if (!in) throw HostError("Could not open configuration file " + conf_path);
+  const size_t slash = conf_path.find_last_of('/');
+  base_dir_ = slash == std::string::npos ? "" : conf_path.substr(0, slash + 1);
+  std::string line;
+  int no = 1;
+  while (std::getline(in, line)) {
+    execute_line(line, no);
+    no++;
+  }
+}
+
+void Samos::execute_line(const std::string& raw, int line_no) {
+  const std::string line = trim(raw);
+  if (line.empty() || line[0] == '#') return;
+  std::string cmd, rest, type, ptext;
+  split_command(line, cmd, rest);
+  Params p;
+  auto params_of = [&](const std::string& text, const char* what) {
+    if (!parse_params(text.empty() ? "{}" : text, p))
+      throw HostError(std::string("Error parsing ") + what + " parameters at line " + std::to_string(line_no) + ".");
+  };
+  auto typed = [&](const char* what) {
+    if (!split_type_params(rest, type, ptext))
+      throw HostError(std::string("Error parsing ") + what + " command at line " + std::to_string(line_no) + ".");
+    params_of(ptext, what);
+  };
+
+  if (cmd == "messages") {
+    return;  // host messages go to stderr here
+  } else if (cmd == "box") {  // samos.cpp:186-230
+    typed("box");
+    if (type == "periodic") periodic_ = true;
+    else if (type == "fixed") periodic_ = false;
+    else throw HostError("Unknown box type.");
+    lx_ = p.count("lx") ? to_dbl(p["lx"], "box") : 10.0;  // DEFAULT_LX (defaults.hpp:36-38)
+    ly_ = p.count("ly") ? to_dbl(p["ly"], "box") : 10.0;
+    lz_ = p.count("lz") ? to_dbl(p["lz"], "box") : 10.0;
+    has_box_ = true;
+  } else if (cmd == "input") {  // samos.cpp:240-265
+    if (!has_box_) throw HostError("Simulation box not defined.");
+    const std::string name = trim(rest);
+    parts_ = read_particles(name.size() && name[0] == '/' ? name : base_dir_ + name);
+    has_input_ = true;
+    ensure_engine();
+  } else if (cmd == "nlist") {  // samos.cpp:540-560
+    need_system("creating neighbour list");
+    params_of(rest, "neighbour list");
+    nl_rcut_ = p.count("rcut") ? to_dbl(p["rcut"], "nlist") : 3.0;  // DEFAULT_CUTOFF / DEFAULT_PADDING
+    nl_pad_ = p.count("pad") ? to_dbl(p["pad"], "nlist") : 0.5;
+    has_nlist_ = true;
+    if (h_) check(sg_set_nlist(h_, nl_rcut_, nl_pad_), "sg_set_nlist");
+  } else if (cmd == "constraint") {  // samos.cpp:498-530
+    need_system("adding constraint");
+    typed("constraint");
+    ConstraintSpec c = resolve_constraint(type, p);
+    constraints_.push_back(c);
+    if (h_) check(sg_add_constraint(h_, c.kind, c.params), "sg_add_constraint");
+  } else if (cmd == "pair_potential") {  // samos.cpp:332-380
+    need_system("adding pair potential");
+    typed("pair potential");
+    if (!has_nlist_) {  // samos.cpp:347-352: a default neighbour list
+      nl_rcut_ = 3.0; nl_pad_ = 0.5; has_nlist_ = true;
+      if (h_) check(sg_set_nlist(h_, nl_rcut_, nl_pad_), "sg_set_nlist");
+    }
+    pairs_[type] = resolve_pair(type, p, parts_.ntypes, nl_rcut_);
+  } else if (cmd == "pair_param") {
+    if (pairs_.empty()) throw HostError("No pair potentials defined.");
+    typed("pair parameters");
+    auto it = pairs_.find(type);
+    if (it == pairs_.end()) throw HostError("Pair potential " + type + " has not been defined.");
+    apply_pair_param(it->second, p, parts_.ntypes);
+  } else if (cmd == "pair_align") {
+    need_system("adding pair alignment");
+    typed("pair alignment");
+    if (!has_nlist_) {
+      nl_rcut_ = 3.0; nl_pad_ = 0.5; has_nlist_ = true;
+      if (h_) check(sg_set_nlist(h_, nl_rcut_, nl_pad_), "sg_set_nlist");
+    }
+    aligns_[type] = resolve_align(type, p, parts_.ntypes, nl_rcut_);
+  } else if (cmd == "align_param") {
+    if (aligns_.empty()) throw HostError("No pair alignment defined.");
+    typed("alignment parameters");
+    auto it = aligns_.find(type);
+    if (it == aligns_.end()) throw HostError("Pair alignment " + type + " has not been defined.");
+    apply_align_param(it->second, p, parts_.ntypes);
+  } else if (cmd == "external") {
+    need_system("adding external potential");
+    typed("external potential");
+    externals_[type] = resolve_external(type, p, parts_.ntypes);
+  } else if (cmd == "external_param") {
+    typed("external potential parameters");
+    auto it = externals_.find(type);
+    if (it == externals_.end()) throw HostError("External potential " + type + " has not been defined.");
+    apply_external_param(it->second, p, parts_.ntypes);
+  } else if (cmd == "timestep") {  // samos.cpp:1332-1350
+    need_system("setting the integrator time step");
+    dt_ = to_dbl(trim(rest), "timestep");
+    if (h_) check(sg_set_timestep(h_, dt_), "sg_set_timestep");
+  } else if (cmd == "integrator") {  // samos.cpp:640-700
+    need_system("adding integrator");
+    if (constraints_.empty()) throw HostError("Constraint not defined.");
+    typed("integrator");
+    const std::string key = type + "_" + (p.count("group") ? p["group"] : std::string("all"));
+    if (integrators_.count(key))
+      throw HostError("Integrator of type " + type + " (for group " + key.substr(type.size() + 1) +
+                      ") already exists. You need to disable the old one first.");
+    IntegratorSpec s = resolve_integrator(type, p, dt_);
+    integrators_[key] = s;
+    int pos = 0;
+    for (const auto& kv : integrators_) {
+      if (kv.first == key) break;
+      pos++;
+    }
+    committed_integ_.insert(committed_integ_.begin() + pos, key);
+    if (h_) check(sg_insert_integrator(h_, pos, s.kind, s.params, s.temperature), "sg_insert_integrator");
+  } else if (cmd == "disable") {  // samos.cpp:1143-1180
+    if (integrators_.empty()) throw HostError("Integrator not defined.");
+    typed("disable");
+    const std::string key = type + "_" + (p.count("group") ? p["group"] : std::string("all"));
+    auto it = integrators_.find(key);
+    if (it == integrators_.end()) throw HostError("Trying to disable non-existent integrator.");
+    int pos = 0;
+    for (const auto& k : committed_integ_) {
+      if (k == key) break;
+      pos++;
+    }
+    integrators_.erase(it);
+    committed_integ_.erase(committed_integ_.begin() + pos);
+    if (h_) check(sg_disable_integrator(h_, pos), "sg_disable_integrator");
+  } else if (cmd == "run") {  // samos.cpp:837-972
+    need_system("running");
+    if (constraints_.empty()) throw HostError("Constraint not defined.");
+    if (integrators_.empty()) throw HostError("Integrator not defined.");
+    cmd_run(to_i64(trim(rest), "run"));
+  } else if (cmd == "dump") {
+    need_system("adding dumps");
+    cmd_dump(rest);
+  } else if (cmd == "log") {
+    need_system("adding logs");
+    cmd_log(rest);
+  } else if (cmd == "group") {
+    throw HostError("Particle groups other than 'all' are not part of the GPU path.");
+  } else {
+    throw HostError("Command " + cmd + " (line " + std::to_string(line_no) + ") is not part of the GPU path.");
+  }
+}
+
+void Samos::commit_forces() {
+  if (!h_) return;
+  check(sg_clear_forces(h_), "sg_clear_forces");
+  for (const auto& kv : pairs_) {
+    const PairSpec& s = kv.second;
+    check(sg_add_pair(h_, s.kind, s.glob, s.table.data(), s.use_radii, s.phase_in, s.shifted, s.has_pair_params,
+                      s.phase_value),
+          "sg_add_pair");
+  }
+  for (const auto& kv : aligns_) {
+    const AlignSpec& s = kv.second;
+    check(sg_add_align(h_, s.kind, s.J, s.rcut, s.table.data(), s.has_pair_params), "sg_add_align");
+  }
+  for (const auto& kv : externals_) {
+    const ExternalSpec& s = kv.second;
+    check(sg_add_external(h_, s.kind, s.alpha, s.type_alpha.data(), s.has_params), "sg_add_external");
+  }
+}
+
+void Samos::cmd_run(int64_t steps) {
+  if (!opt_.quiet) std::fprintf(stderr, "Starting simulation run for %lld steps.\n", (long long)steps);
+  if (opt_.check_only) { steps_run_ += steps + 1; return; }
+  commit_forces();
+  // dumps and logs read the state every `freq` steps: the run is split at
+  // those steps (sg_run(k) executes k+1 steps; sg_run_continue(k) k more).
+  int64_t every = 0;
+  for (const auto& d : dumps_) every = every ? std::min(every, d.freq) : d.freq;
+  for (const auto& l : logs_) every = every ? std::min(every, l.freq) : l.freq;
+  sg_run_stats st{};
+  if (!every || every > steps) {
+    check(sg_run(h_, steps, &st), "sg_run");
+    steps_run_ += steps + 1;
+  } else {
+    int64_t done = 0;
+    const int64_t total = steps + 1;
+    while (done < total) {
+      const int64_t seg = std::min(every, total - done);
+      if (done == 0) check(sg_run(h_, seg - 1, &st), "sg_run");
+      else check(sg_run_continue(h_, seg, &st), "sg_run_continue");
+      done += seg;
+      steps_run_ += seg;
+      write_dumps(steps_run_, done == total);
+    }
+  }
+  if (!opt_.quiet)
+    std::fprintf(stderr, "Run of %lld steps done: %lld neighbour-list builds, %.3f ms on the device.\n",
+                 (long long)(steps + 1), (long long)st.nlist_builds, st.device_ms);
+}
+
+void Samos::cmd_dump(const std::string& rest) {
+  std::string name, ptext;
+  if (!split_type_params(rest, name, ptext)) throw HostError("Error parsing dump command.");
+  Params p;
+  if (!parse_params(ptext, p)) throw HostError("Error parsing dump parameters.");
+  Dump d;
+  d.name = name;
+  d.type = p.count("type") ? p["type"] : "input";
+  if (d.type != "input" && d.type != "full") throw HostError("Dump type " + d.type + " is not part of the GPU path.");
+  d.start = p.count("start") ? to_i64(p["start"], "dump") : 0;
+  d.freq = p.count("freq") ? to_i64(p["freq"], "dump") : 1;
+  d.multi = p.count("multi") != 0;
+  if (d.freq <= 0) throw HostError("Dump frequency has to be positive.");
+  dumps_.push_back(d);
+}
+
+void Samos::cmd_log(const std::string& rest) {
+  std::string name, ptext;
+  if (!split_type_params(rest, name, ptext)) throw HostError("Error parsing log command.");
+  Params p;
+  if (!parse_params(ptext, p)) throw HostError("Error parsing log parameters.");
+  Log l;
+  l.name = name;
+  l.freq = p.count("freq") ? to_i64(p["freq"], "log") : 1;
+  if (l.freq <= 0) throw HostError("Log frequency has to be positive.");
+  std::string what = p.count("what") ? p["what"] : "";
+  // logger columns the engine reduces (logger.cpp:49-77); '+'-separated here
+  std::stringstream ss(what);
+  std::string c;
+  while (std::getline(ss, c, '+'))
+    if (!c.empty()) {
+      if (c != "soft_energy" && c != "lj_energy" && c != "morse_energy" && c != "gaussian_energy" &&
+          c != "polar_align" && c != "nematic_align" && c != "velocity")
+        throw HostError("Log column " + c + " is not part of the GPU path.");
+      l.cols.push_back(c);
+    }
+  logs_.push_back(l);
+  std::FILE* f = std::fopen(l.name.c_str(), "w");
+  if (!f) throw HostError("Cannot open log file " + l.name);
+  std::fprintf(f, "# step");
+  for (const auto& col : l.cols) std::fprintf(f, " %s", col.c_str());
+  std::fprintf(f, "\n");
+  std::fclose(f);
+}
+
+void Samos::write_dumps(int64_t step, bool) {
+  bool any = false;
+  for (const auto& d : dumps_) any = any || (step >= d.start && step % d.freq == 0);
+  for (const auto& l : logs_) any = any || step % l.freq == 0;
+  if (!any) return;
+  auto down = [&](const char* f, void* p) { check(sg_download(h_, 0, f, p), "sg_download"); };
+  down("x", parts_.x.data()); down("y", parts_.y.data()); down("z", parts_.z.data());
+  down("vx", parts_.vx.data()); down("vy", parts_.vy.data()); down("vz", parts_.vz.data());
+  down("nx", parts_.nx.data()); down("ny", parts_.ny.data()); down("nz", parts_.nz.data());
+  down("omega", parts_.omega.data());
+  down("ix", parts_.ix.data()); down("iy", parts_.iy.data()); down("iz", parts_.iz.data());
+  for (const auto& d : dumps_) {
+    if (step < d.start || step % d.freq) continue;
+    char num[32];
+    std::snprintf(num, sizeof num, "_%010lld", (long long)step);
+    write_input_dump(d.multi ? d.name + num + ".dat" : d.name + ".dat", parts_);
+  }
+  for (const auto& l : logs_) {
+    if (step % l.freq) continue;
+    std::FILE* f = std::fopen(l.name.c_str(), "a");
+    if (!f) throw HostError("Cannot open log file " + l.name);
+    std::fprintf(f, "%lld", (long long)step);
+    for (const auto& c : l.cols) {
+      double v = 0.0;
+      if (c == "velocity") {  // log_velocity.hpp:56-65: mean speed
+        for (size_t i = 0; i < parts_.size(); i++)
+          v += std::sqrt(parts_.vx[i] * parts_.vx[i] + parts_.vy[i] * parts_.vy[i] + parts_.vz[i] * parts_.vz[i]);
+        v /= (double)parts_.size();
+      } else {
+        const bool align = c == "polar_align" || c == "nematic_align";
+        const std::string want = align ? c.substr(0, c.find('_')) : c.substr(0, c.find('_'));
+        int comp = 0;
+        bool found = false;
+        if (align) {
+          for (const auto& kv : aligns_) { if (kv.first == want) { found = true; break; } comp++; }
+        } else {
+          for (const auto& kv : pairs_) { if (kv.first == want) { found = true; break; } comp++; }
+        }
+        if (!found) throw HostError("Log column " + c + " names a term that is not defined.");
+        check(sg_energy(h_, 0, align ? 1 : 0, comp, &v), "sg_energy");
+        v /= (double)parts_.size();  // per particle, as the reference's loggers report
+      }
+      std::fprintf(f, " %.12g", v);
+    }
+    std::fprintf(f, "\n");
+    std::fclose(f);
+  }
+}
+
+std::string Samos::describe() const {
+  std::ostringstream o;
+  o << "particles " << parts_.size() << " ntypes " << parts_.ntypes << "\n";
+  o << "box " << (periodic_ ? "periodic" : "fixed") << " " << lx_ << " " << ly_ << " " << lz_ << "\n";
+  if (has_nlist_) o << "nlist " << nl_rcut_ << " " << nl_pad_ << "\n";
+  for (const auto& c : constraints_) o << "constraint " << c.kind << " " << c.params[0] << "\n";
+  for (const auto& kv : pairs_) {
+    o << "pair " << kv.first << " " << kv.second.kind;
+    for (int i = 0; i < SG_PAIR_NPARAM; i++) o << " " << kv.second.glob[i];
+    o << " radii " << kv.second.use_radii << "\n";
+  }
+  for (const auto& kv : aligns_) o << "align " << kv.first << " " << kv.second.J << " " << kv.second.rcut << "\n";
+  for (const auto& kv : externals_) o << "external " << kv.first << " " << kv.second.alpha << "\n";
+  for (const auto& key : committed_integ_) {
+    const IntegratorSpec& s = integrators_.at(key);
+    o << "integrator " << key << " " << s.kind;
+    for (int i = 0; i < 12; i++) o << " " << s.params[i];
+    o << "\n";
+  }
+  o << "steps " << steps_run_ << "\n";
+  return o.str();
+}
+
+}  // namespace samos_host
