@@ -208,6 +208,51 @@ def batched_leg(n_rep=256, warm=30, steps=50, seed=7, device=0):
                        "256 one-at-a-time runs)", serial_wall_s=t_wall)
 
 
+def ml_leg(count=48, seed=4242, device=0):
+    """Learned FIRE warm start vs plain FIRE (to Fmax < 1e-10, FP64) on `count`
+    fresh quenches (N log-uniform in [1024, 16384], phi uniform in [0.84, 0.90]),
+    with the network trained by `python -m samos_b200.warmstart train` on 2,000
+    GPU-FIRE relaxations at N = 4096 (samos_b200/data/warmstart_c5.npz)."""
+    path = os.path.join(ROOT, "samos_b200", "data", "warmstart_c5.npz")
+    if not os.path.exists(path):
+        return {"unavailable": "no trained warm-start parameters (samos_b200/data/warmstart_c5.npz)"}
+    import torch
+    torch.cuda.set_device(device)
+    from samos_b200.warmstart import WarmStartNet, quench_set, relax, summarize
+    net = WarmStartNet(device=f"cuda:{device}")
+    net.load(path)
+    insts = quench_set(count, 1024, 16384, 0.84, 0.90, seed=seed)
+    plain = relax(insts, None)
+    warm = relax(insts, net)
+    rep = summarize(plain, warm, insts)
+    rep["timing"] = "CUDA events on the engine stream: inference + apply + fallback + minimisation (warm), minimisation (plain)"
+    return rep
+
+
+def step_kernel_name(variant):
+    """The fused step kernel the autotuner kept for the headline program
+    (soft + nematic + brownian on a periodic plane)."""
+    if variant == 5:
+        return "k_abp_flat<plane,nematic>"
+    return f"k_abp_step<plane,nematic,variant={variant}>"
+
+
+def measured_traffic(kernel, n_part):
+    """DRAM bytes per launch of the step kernel from the committed ncu
+    summary (`dram_bytes_per_particle_step:` line, scaled to this system
+    size), or None when no summary covers this kernel variant."""
+    path = os.path.join(ROOT, "profiles", "k_abp_step_plane_nematic.md")
+    if not os.path.exists(path):
+        return None
+    per = {}
+    for line in open(path):
+        if line.startswith("dram_bytes_per_particle_step"):
+            # dram_bytes_per_particle_step[<kernel>]: <bytes>
+            key = line.split("[", 1)[1].split("]", 1)[0]
+            per[key] = float(line.rsplit(":", 1)[1])
+    return per[kernel] * n_part if kernel in per else None
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -256,6 +301,7 @@ def main():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-serial replica leg")
+    ap.add_argument("--no-ml", action="store_true", help="skip the learned FIRE warm-start leg")
     ap.add_argument("--particles", type=int, default=N_PART,
                     help="system size (profiling runs use a smaller system of the same density)")
     args = ap.parse_args()
@@ -292,6 +338,7 @@ def main():
     with ClockSampler(local) as clocks:
         st = eng.run(args.steps - 1)
     launches = eng.kernel_launches() - launches0
+    variant = eng.variant()
     t_ms = max_over_ranks(st.device_ms, ws)
     value = ws * n_part * args.steps / (t_ms * 1e-3)
 
@@ -307,10 +354,8 @@ def main():
     except OSError:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
-    if os.path.exists(tf):
-        traffic = json.load(open(tf)).get("bytes_per_launch_4M")
+    kernel = step_kernel_name(variant)
+    traffic = measured_traffic(kernel, n_part)
 
     # end to end through the C ABI with host buffers
     barrier(ws)
@@ -336,6 +381,9 @@ def main():
     if ws == 1 and not args.no_batched and args.particles == N_PART:
         eng.close()
         batched = batched_leg(device=local)
+    ml = None
+    if ws == 1 and not args.no_ml and args.particles == N_PART:
+        ml = ml_leg(device=local)
 
     if rank == 0:
         line = dict(
@@ -345,9 +393,9 @@ def main():
             config=dict(workload=WORKLOAD if n_part == N_PART else WORKLOAD.replace("4,194,304", f"{n_part:,}"),
                         n_particles=n_part, box=L, parallelism=f"replicas x{ws}",
                         l2="state resident in HBM, 1.4 GB per buffer set >> 126 MB L2 (no flush needed)",
-                        nlist_builds_timed=st.nlist_builds, kernel_variant=eng.variant()),
+                        nlist_builds_timed=st.nlist_builds, kernel_variant=variant),
             roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
-                          traffic=traffic, kernel="k_step_brownian", kernel_ms=k_ms,
+                          traffic=traffic, kernel=kernel, kernel_ms=k_ms,
                           algorithmic_bytes_per_particle_step=BYTES_PER_PARTICLE_STEP,
                           peak_source="MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"),
             e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
@@ -356,6 +404,7 @@ def main():
             clocks=clocks.summary(),
             cpu_baseline=cpu,
             batched=batched,
+            fire_warm_start=ml,
         )
         print(json.dumps(line), flush=True)
     if eng.h:

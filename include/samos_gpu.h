@@ -38,7 +38,7 @@ enum { SG_ALIGN_POLAR = 0, SG_ALIGN_NEMATIC = 1, SG_ALIGN_VICSEK = 2 };
 enum { SG_EXT_SELF_PROPULSION = 0 };
 enum { SG_CONS_NONE = 0, SG_CONS_PLANE = 1, SG_CONS_SPHERE = 2 };
 enum { SG_INT_BROWNIAN = 0, SG_INT_BROWNIAN_POS = 1, SG_INT_BROWNIAN_ALIGN = 2,
-       SG_INT_LANGEVIN = 3, SG_INT_FIRE = 4 };
+       SG_INT_LANGEVIN = 3, SG_INT_FIRE = 4, SG_INT_NVE = 5 };
 enum { SG_VALUE_CONSTANT = 0, SG_VALUE_LINEAR = 1 };
 enum { SG_LANGEVIN_BAOAB = 0, SG_LANGEVIN_SPV = 1, SG_LANGEVIN_BBK = 2 };
 
@@ -131,6 +131,8 @@ int  sg_add_constraint_per_replica(sg_system* s, int kind, const double* params,
  *  langevin       : 0 dt, 5 seed, 9 gamma, 10 method
  *  fire           : 0 dt, 1 alpha, 2 alpha_scale, 3 f_tolerance, 4 e_tolerance,
  *                   6 dt_inc, 7 dt_dec, 8 dt_max, 9 min_neg_steps, 11 fmax_tolerance
+ *  nve            : 0 dt, 12 has_limit, 13 limit, 14 has_angle_limit, 15 angle_limit
+ *                   (integrator_nve.hpp:59-75)
  * temperature_value = {kind, min_val, max_val, steps} (Value, value.hpp).
  * Integrators must be added in std::map key order (type + "_" + group).     */
 int  sg_add_integrator(sg_system* s, int kind, const double* params,
@@ -172,6 +174,11 @@ int  sg_run(sg_system* s, int64_t steps, sg_run_stats* stats);
  * `run` into sg_run(k - 1) followed by sg_run_continue(k) calls, with the
  * same results as one sg_run.                                               */
 int  sg_run_continue(sg_system* s, int64_t steps, sg_run_stats* stats);
+/* The top of the next step up to the dumps and logs (samos.cpp:887-896):
+ * the start-of-step constraint enforce is applied now (and not again by the
+ * next sg_run / sg_run_continue), so downloads see what the reference's
+ * dumps see.  Follow with sg_compute for energies at that point.           */
+int  sg_begin_step(sg_system* s);
 /* FIRE minimisation driver: run until every replica's FIRE integrator has
  * converged or max_steps integration steps; converged[r] (may be NULL) gets
  * the step count per replica or -1.                                         */

@@ -1134,6 +1134,7 @@ void or_compute(or_system* s, double dt)
  *  langevin       : 0 dt, 5 seed, 9 gamma, 10 method
  *  fire           : 0 dt, 1 alpha, 2 alpha_scale, 3 f_tol, 4 e_tol, 6 dt_inc,
  *                   7 dt_dec, 8 dt_max, 9 min_neg_steps, 11 fmax_tol (<=0: off)
+ *  nve            : 0 dt, 12 has_limit, 13 limit, 14 has_angle_limit, 15 angle_limit
  * `tau` is the conf value; the flip probability dt/tau is formed here as in
  * integrator_brownian.hpp:139-147.
  */
@@ -1430,6 +1431,59 @@ static void integ_fire(or_system* s, or_integ* g)
   g->old_energy = E;
 }
 
+/* IntegratorNVE::integrate, integrators/integrator_nve.cpp:37-141.  The
+ * reference leaves m_has_limit / m_has_theta_limit / m_theta_limit
+ * uninitialised when `limit` / `angle_limit` are absent (integrator_nve.hpp
+ * constructor); here an absent limit is off, and the omega clamp of the last
+ * loop (guarded there by m_has_limit but reading m_theta_limit) applies only
+ * when both limits are given. */
+static void integ_nve(or_system* s, or_integ* g)
+{
+  int N = s->N;
+  double dt = g->dt, dt_2 = 0.5 * dt;
+  int has_limit = g->p[12] != 0.0, has_theta = g->p[14] != 0.0;
+  double limit = g->p[13], theta_limit = g->p[15];
+  for (int i = 0; i < N; i++) {
+    s->vx[i] += dt_2 * s->fx[i]; s->vy[i] += dt_2 * s->fy[i]; s->vz[i] += dt_2 * s->fz[i];
+    enforce_one(s, i);
+    s->omega[i] += dt_2 * project_torque(s, i);
+  }
+  for (int i = 0; i < N; i++) {
+    double dx = dt * s->vx[i], dy = dt * s->vy[i], dz = dt * s->vz[i];
+    if (has_limit) {
+      double dr = sqrt(dx * dx + dy * dy + dz * dz);
+      if (dr > limit) { dx = limit * dx / dr; dy = limit * dy / dr; dz = limit * dz / dr; }
+    }
+    s->x[i] += dx; s->y[i] += dy; s->z[i] += dz;
+    enforce_one(s, i);
+  }
+  for (int i = 0; i < N; i++) {
+    double dtheta = dt * s->omega[i];
+    if (has_theta && fabs(dtheta) > theta_limit) dtheta = (dtheta >= 0.0 ? 1.0 : -1.0) * theta_limit;  /* SIGN, integrator_nve.hpp:38 */
+    rotate_director(s, i, dtheta);
+  }
+  reset_forces(s);
+  reset_torques(s);
+  if (s->npairs + s->nexts) potential_compute(s, dt);
+  if (s->naligns) aligner_compute(s);
+  for (int i = 0; i < N; i++) {
+    s->vx[i] += dt_2 * s->fx[i]; s->vy[i] += dt_2 * s->fy[i]; s->vz[i] += dt_2 * s->fz[i];
+    if (has_limit) {
+      double v = sqrt(s->vx[i] * s->vx[i] + s->vy[i] * s->vy[i] + s->vz[i] * s->vz[i]);
+      if (v * dt > limit) {
+        s->vx[i] = s->vx[i] / v * limit / dt;
+        s->vy[i] = s->vy[i] / v * limit / dt;
+        s->vz[i] = s->vz[i] / v * limit / dt;
+      }
+    }
+    enforce_one(s, i);
+    s->omega[i] += dt_2 * project_torque(s, i);
+    if (has_limit && has_theta && fabs(s->omega[i]) * dt > theta_limit)
+      s->omega[i] = (s->omega[i] >= 0.0 ? 1.0 : -1.0) * theta_limit / dt;
+    s->age[i] += dt;
+  }
+}
+
 static void integrate(or_system* s, or_integ* g)
 {
   switch (g->kind) {
@@ -1444,6 +1498,7 @@ static void integrate(or_system* s, or_integ* g)
       }
       break;
     case OR_INT_FIRE: integ_fire(s, g); break;
+    case OR_INT_NVE: integ_nve(s, g); break;
   }
 }
 

@@ -673,7 +673,7 @@ int sg_add_constraint(sg_system* s, int kind, const double* params) {
 }
 
 int sg_add_integrator(sg_system* s, int kind, const double* params, const double* temp) {
-  if (!s || !params || kind < SG_INT_BROWNIAN || kind > SG_INT_FIRE) return fail(s, SG_ERR_ARG, "sg_add_integrator: bad kind");
+  if (!s || !params || kind < SG_INT_BROWNIAN || kind > SG_INT_NVE) return fail(s, SG_ERR_ARG, "sg_add_integrator: bad kind");
   Program& P = s->prog;
   if (P.ninteg >= MAX_INTEG) return fail(s, SG_ERR_ARG, "too many integrators");
   if (!(params[0] > 0.0)) return fail(s, SG_ERR_ARG, "integrator step size has to be larger than 0");
@@ -794,6 +794,17 @@ int sg_set_replica_param(sg_system* s, int replica, int cls, int comp, int slot,
 // ---------------------------------------------------------------------------
 // execution
 // ---------------------------------------------------------------------------
+int sg_begin_step(sg_system* s) {
+  if (!s) return SG_ERR_ARG;
+  if (!s->e1_applied) {
+    k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, nullptr);
+    LAUNCH_CHECK(s);
+    s->e1_applied = true;
+  }
+  CU(s, cudaStreamSynchronize(s->stream));
+  return SG_OK;
+}
+
 int sg_enforce(sg_system* s) {
   if (!s) return SG_ERR_ARG;
   k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, nullptr);
@@ -847,8 +858,10 @@ static bool fire_forces_reusable(const sg_system* s) {
 
 static int step_unfused(sg_system* s, bool energy, bool driver) {
   const int nb = s->nblocks;
-  k_enforce<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, driver ? s->clk : nullptr);
-  LAUNCH_CHECK(s);
+  if (!s->e1_applied) {  // samos.cpp:887-888 (already applied by sg_begin_step)
+    k_enforce<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, driver ? s->clk : nullptr);
+    LAUNCH_CHECK(s);
+  }
   int rc = SG_OK;
   if (!(s->forces_fresh && fire_forces_reusable(s)))
     if ((rc = launch_force(s, s->dt_global, false, true, true, energy))) return rc;
@@ -860,6 +873,12 @@ static int step_unfused(sg_system* s, bool energy, bool driver) {
       LAUNCH_CHECK(s);
       if ((rc = launch_force(s, s->reps_h[0].integ_p[c][0], false, true, false, true))) return rc;
       k_langevin_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, c, s->Rn);
+      LAUNCH_CHECK(s);
+    } else if (ic.kind == INT_NVE) {
+      k_nve_a<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, c);
+      LAUNCH_CHECK(s);
+      if ((rc = launch_force(s, s->reps_h[0].integ_p[c][0], false, true, true, true))) return rc;
+      k_nve_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, c);
       LAUNCH_CHECK(s);
     } else if (ic.kind == INT_FIRE) {
       k_fire_a<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st);

@@ -513,6 +513,74 @@ __global__ void k_langevin_b(Program P, const Replica* __restrict__ reps, const 
 }
 
 // ---------------------------------------------------------------------------
+// NVE (integrators/integrator_nve.cpp:37-141).  The first three loops act on
+// each particle alone, so one thread runs them in sequence; then the force
+// pass; then the last loop.  Limits: params 12 has_limit, 13 limit,
+// 14 has_angle_limit, 15 angle_limit (absent limits are off; the omega clamp
+// of the last loop needs both, the reference reading an unset angle limit
+// there).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double sign_of(double x) { return x >= 0.0 ? 1.0 : -1.0; }  // integrator_nve.hpp:38
+
+__global__ void k_nve_a(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep, Dyn d, Stat st,
+                        int c) {
+  const int r = my_replica(blk_rep);
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  Part p;
+  load_dyn(d, k, p);
+  p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
+  const double* ip = R.integ_p[c];
+  const double dt = ip[0], dt_2 = 0.5 * dt;
+  const bool has_limit = ip[12] != 0.0, has_theta = ip[14] != 0.0;
+  const double limit = ip[13], theta_limit = ip[15];
+  p.vx += dt_2 * p.fx; p.vy += dt_2 * p.fy; p.vz += dt_2 * p.fz;  // nve.cpp:49-55
+  enforce_all(P, R, p);
+  p.omega += dt_2 * project_torque(P, R, p);
+  double dx = dt * p.vx, dy = dt * p.vy, dz = dt * p.vz;  // nve.cpp:57-76
+  if (has_limit) {
+    const double dr = sqrt(dx * dx + dy * dy + dz * dz);
+    if (dr > limit) { dx = limit * dx / dr; dy = limit * dy / dr; dz = limit * dz / dr; }
+  }
+  p.x += dx; p.y += dy; p.z += dz;
+  enforce_all(P, R, p);
+  double dtheta = dt * p.omega;  // nve.cpp:78-86
+  if (has_theta && fabs(dtheta) > theta_limit) dtheta = sign_of(dtheta) * theta_limit;
+  rotate_director(P, R, p, dtheta);
+  store_dyn(d, k, p);
+}
+
+__global__ void k_nve_b(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep, Dyn d, Stat st,
+                        int c) {
+  const int r = my_replica(blk_rep);
+  const Replica& R = reps[r];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  Part p;
+  load_dyn(d, k, p);
+  p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
+  const double* ip = R.integ_p[c];
+  const double dt = ip[0], dt_2 = 0.5 * dt;
+  const bool has_limit = ip[12] != 0.0, has_theta = ip[14] != 0.0;
+  const double limit = ip[13], theta_limit = ip[15];
+  p.vx += dt_2 * p.fx; p.vy += dt_2 * p.fy; p.vz += dt_2 * p.fz;  // nve.cpp:93-120
+  if (has_limit) {
+    const double v = sqrt(p.vx * p.vx + p.vy * p.vy + p.vz * p.vz);
+    if (v * dt > limit) {
+      p.vx = p.vx / v * limit / dt;
+      p.vy = p.vy / v * limit / dt;
+      p.vz = p.vz / v * limit / dt;
+    }
+  }
+  enforce_all(P, R, p);
+  p.omega += dt_2 * project_torque(P, R, p);
+  if (has_limit && has_theta && fabs(p.omega) * dt > theta_limit) p.omega = sign_of(p.omega) * theta_limit / dt;
+  p.age += dt;
+  store_dyn(d, k, p);
+}
+
+// ---------------------------------------------------------------------------
 // FIRE (integrators/integrator_fire.cpp:34-148)
 // ---------------------------------------------------------------------------
 // first half: half kick, drift, enforce, omega, director rotation (49-66)

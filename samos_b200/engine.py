@@ -19,7 +19,7 @@ PAIR = {"soft": 0, "lj": 1, "morse": 2, "gaussian": 3}
 ALIGN = {"polar": 0, "nematic": 1, "vicsek": 2}
 EXTERNAL = {"self_propulsion": 0}
 CONSTRAINT = {"none": 0, "plane": 1, "sphere": 2}
-INTEGRATOR = {"brownian": 0, "brownian_pos": 1, "brownian_align": 2, "langevin": 3, "fire": 4}
+INTEGRATOR = {"brownian": 0, "brownian_pos": 1, "brownian_align": 2, "langevin": 3, "fire": 4, "nve": 5}
 PAIR_NPARAM = 8
 INT_NPARAM = 16
 
@@ -84,6 +84,11 @@ def load() -> C.CDLL:
         "sg_compute": (I, [P, D]),
         "sg_enforce": (I, [P]),
         "sg_run": (I, [P, I64, C.POINTER(RunStats)]),
+        "sg_run_continue": (I, [P, I64, C.POINTER(RunStats)]),
+        "sg_begin_step": (I, [P]),
+        "sg_insert_integrator": (I, [P, I, I, dp, dp]),
+        "sg_disable_integrator": (I, [P, I]),
+        "sg_clear_forces": (I, [P]),
         "sg_minimize": (I, [P, I64, C.POINTER(I64), C.POINTER(RunStats)]),
         "sg_energy": (I, [P, I, I, I, dp]),
         "sg_fire_state": (I, [P, I, dp]),
@@ -225,6 +230,26 @@ class Engine:
         p[:len(params)] = params
         t = _arr(temperature)
         self._check(self.lib.sg_add_integrator(self.h, int(kind), _dptr(p), _dptr(t)))
+
+    def insert_integrator(self, pos, kind, params, temperature=None):
+        p = np.zeros(INT_NPARAM)
+        p[:len(params)] = params
+        t = _arr(temperature)
+        self._check(self.lib.sg_insert_integrator(self.h, int(pos), int(kind), _dptr(p), _dptr(t)))
+
+    def disable_integrator(self, index):
+        self._check(self.lib.sg_disable_integrator(self.h, int(index)))
+
+    def clear_forces(self):
+        self._check(self.lib.sg_clear_forces(self.h))
+
+    def run_continue(self, steps: int) -> "RunStats":
+        st = RunStats()
+        self._check(self.lib.sg_run_continue(self.h, int(steps), C.byref(st)))
+        return st
+
+    def begin_step(self):
+        self._check(self.lib.sg_begin_step(self.h))
 
     def set_replica_param(self, replica, cls, comp, slot, value):
         self._check(self.lib.sg_set_replica_param(self.h, replica, cls, comp, slot, float(value)))

@@ -235,6 +235,10 @@ IntegratorSpec resolve_integrator(const std::string& name, const Params& p, doub
     q[6] = get(p, "dt_inc", 1.1); q[7] = get(p, "dt_dec", 0.5); q[8] = get(p, "dt_max", 1.0);
     q[9] = has(p, "min_neg_steps") ? (double)to_int("min_neg_steps", p.at("min_neg_steps")) : 5.0;
     q[11] = get(p, "fmax_tolerance", 0.0);
+  } else if (name == "nve") {  // integrator_nve.hpp:59-75 (no params_ok there)
+    s.kind = SG_INT_NVE;
+    if (has(p, "limit")) { q[12] = 1.0; q[13] = get(p, "limit", 0.0); }
+    if (has(p, "angle_limit")) { q[14] = 1.0; q[15] = get(p, "angle_limit", 0.0); }
   } else {
     throw HostError("Integrator " + name + " is not part of the GPU path.");
   }

@@ -10,6 +10,7 @@
 // map order; integrators are inserted at their map position when created
 // and removed by `disable`, so their noise streams persist across runs as the
 // reference's RNG objects do.
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <fstream>
@@ -241,30 +242,41 @@ void Samos::cmd_run(int64_t steps) {
   if (!opt_.quiet) std::fprintf(stderr, "Starting simulation run for %lld steps.\n", (long long)steps);
   if (opt_.check_only) { steps_run_ += steps + 1; return; }
   commit_forces();
-  // dumps and logs read the state every `freq` steps: the run is split at
-  // those steps (sg_run(k) executes k+1 steps; sg_run_continue(k) k more).
-  int64_t every = 0;
-  for (const auto& d : dumps_) every = every ? std::min(every, d.freq) : d.freq;
-  for (const auto& l : logs_) every = every ? std::min(every, l.freq) : l.freq;
-  sg_run_stats st{};
-  if (!every || every > steps) {
-    check(sg_run(h_, steps, &st), "sg_run");
-    steps_run_ += steps + 1;
-  } else {
-    int64_t done = 0;
-    const int64_t total = steps + 1;
-    while (done < total) {
-      const int64_t seg = std::min(every, total - done);
-      if (done == 0) check(sg_run(h_, seg - 1, &st), "sg_run");
-      else check(sg_run_continue(h_, seg, &st), "sg_run_continue");
-      done += seg;
-      steps_run_ += seg;
-      write_dumps(steps_run_, done == total);
+  // Iterations t = 0..steps (samos.cpp:878) with the global step counter
+  // time_step = steps_run_ + t.  Dumps and logs act at the top of an
+  // iteration (samos.cpp:895-898), so the run is split there: sg_run for the
+  // first segment, sg_run_continue for the others (same bits as one sg_run).
+  auto next_due = [&](int64_t T) {  // first global step > T with a dump or log
+    int64_t best = INT64_MAX;
+    for (const auto& d : dumps_) {
+      int64_t a = std::max(d.start, T + 1);
+      a = (a + d.freq - 1) / d.freq * d.freq;
+      best = std::min(best, a);
     }
+    for (const auto& l : logs_) best = std::min(best, (T + 1 + l.freq - 1) / l.freq * l.freq);
+    return best;
+  };
+  auto due = [&](int64_t T) { return next_due(T - 1) == T; };
+  const int64_t total = steps + 1;
+  int64_t t = 0, builds = 0;
+  double ms = 0.0;
+  bool started = false;
+  while (t < total) {
+    if (due(steps_run_)) report(steps_run_);
+    const int64_t nd = next_due(steps_run_);
+    const int64_t len = std::min(total - t, nd - steps_run_);
+    sg_run_stats st{};
+    if (!started) check(sg_run(h_, len - 1, &st), "sg_run");
+    else check(sg_run_continue(h_, len, &st), "sg_run_continue");
+    started = true;
+    builds += st.nlist_builds;
+    ms += st.device_ms;
+    steps_run_ += len;
+    t += len;
   }
   if (!opt_.quiet)
     std::fprintf(stderr, "Run of %lld steps done: %lld neighbour-list builds, %.3f ms on the device.\n",
-                 (long long)(steps + 1), (long long)st.nlist_builds, st.device_ms);
+                 (long long)total, (long long)builds, ms);
 }
 
 void Samos::cmd_dump(const std::string& rest) {
@@ -312,11 +324,13 @@ void Samos::cmd_log(const std::string& rest) {
   std::fclose(f);
 }
 
-void Samos::write_dumps(int64_t step, bool) {
-  bool any = false;
-  for (const auto& d : dumps_) any = any || (step >= d.start && step % d.freq == 0);
-  for (const auto& l : logs_) any = any || step % l.freq == 0;
-  if (!any) return;
+void Samos::report(int64_t step) {
+  check(sg_begin_step(h_), "sg_begin_step");
+  bool energies = false;
+  for (const auto& l : logs_)
+    if (step % l.freq == 0)
+      for (const auto& c : l.cols) energies = energies || c != "velocity";
+  if (energies) check(sg_compute(h_, dt_), "sg_compute");
   auto down = [&](const char* f, void* p) { check(sg_download(h_, 0, f, p), "sg_download"); };
   down("x", parts_.x.data()); down("y", parts_.y.data()); down("z", parts_.z.data());
   down("vx", parts_.vx.data()); down("vy", parts_.vy.data()); down("vz", parts_.vz.data());
@@ -324,7 +338,7 @@ void Samos::write_dumps(int64_t step, bool) {
   down("omega", parts_.omega.data());
   down("ix", parts_.ix.data()); down("iy", parts_.iy.data()); down("iz", parts_.iz.data());
   for (const auto& d : dumps_) {
-    if (step < d.start || step % d.freq) continue;
+    if (step < d.start || step % d.freq) continue;  // Dump::dump, dump.cpp:351-360
     char num[32];
     std::snprintf(num, sizeof num, "_%010lld", (long long)step);
     write_input_dump(d.multi ? d.name + num + ".dat" : d.name + ".dat", parts_);

@@ -112,7 +112,7 @@ class Samos {
   void cmd_run(int64_t steps);
   void cmd_dump(const std::string& rest);
   void cmd_log(const std::string& rest);
-  void write_dumps(int64_t step, bool final_step);
+  void report(int64_t step);  // dumps and logs at the top of global step `step`
   void check(int rc, const char* what) const;
 
   RunOptions opt_;
@@ -134,7 +134,7 @@ class Samos {
   std::vector<Dump> dumps_;
   struct Log { std::string name; int64_t freq = 1; std::vector<std::string> cols; };
   std::vector<Log> logs_;
-  int64_t steps_run_ = 0;
+  int64_t steps_run_ = 0;  // the reference's time_step
 };
 
 }  // namespace samos_host

@@ -260,6 +260,11 @@ def resolve_integrator(name: str, params: dict, dt_global: float) -> tuple[int, 
         p[6] = _f(params, "dt_inc", 1.1); p[7] = _f(params, "dt_dec", 0.5)
         p[8] = _f(params, "dt_max", 1.0); p[9] = float(int(params["min_neg_steps"])) if "min_neg_steps" in params else 5.0
         p[11] = _f(params, "fmax_tolerance", 0.0)
+    elif name == "nve":  # integrator_nve.hpp:59-75 (no params_ok there)
+        if "limit" in params:
+            p[12], p[13] = 1.0, float(params["limit"])
+        if "angle_limit" in params:
+            p[14], p[15] = 1.0, float(params["angle_limit"])
     else:
         raise PluginError(f"Integrator {name} is not part of the GPU path.")
     temp = _value(params.get("temperature_control", "constant"), params)

@@ -198,7 +198,7 @@ class Batch:
     (displacement quench -> FIRE minimum, slot order) kept on the device."""
 
     def __init__(self, net: WarmStartNet, insts, k: float = 1.0, dt: float = 0.01, dt_max: float = 0.2,
-                 fmax: float = 1e-10, max_steps: int = 200000):
+                 fmax: float = 1e-10, max_steps: int = 400000):
         from .ensemble import plane_fire_ensemble
         self.insts = insts
         self.eng = plane_fire_ensemble(insts, k=k, dt=dt, dt_max=dt_max, fmax=fmax)
@@ -305,3 +305,80 @@ def relax(insts, net: WarmStartNet | None, k: float = 1.0, dt: float = 0.01, dt_
                total_ms=warm_ms + st.device_ms)
     eng.close()
     return out
+
+
+# -- command line: the full train / evaluate pipeline --------------------------------------
+def summarize(plain: dict, warm: dict, insts) -> dict:
+    """Plain vs warm-started FIRE over the same instances."""
+    ok = (plain["steps"] > 0) & (warm["steps"] > 0)
+    rel = np.abs(warm["energy"] - plain["energy"]) / np.maximum(np.abs(plain["energy"]), 1e-300)
+    signed = (warm["energy"] - plain["energy"]) / np.maximum(np.abs(plain["energy"]), 1e-300)
+    n = np.array([len(p["x"]) for p, _ in insts])
+    return dict(
+        instances=len(insts), particles=int(n.sum()),
+        plain_s=plain["total_ms"] / 1e3, warm_s=warm["total_ms"] / 1e3,
+        speedup=plain["total_ms"] / warm["total_ms"],
+        inference_ms=warm["warm_ms"],
+        plain_steps_mean=float(plain["steps"][ok].mean()), warm_steps_mean=float(warm["steps"][ok].mean()),
+        plain_steps_max=int(plain["steps"].max()), warm_steps_max=int(warm["steps"].max()),
+        steps_ratio_median=float(np.median(plain["steps"][ok] / warm["steps"][ok])),
+        unconverged_plain=int((plain["steps"] < 0).sum()), unconverged_warm=int((warm["steps"] < 0).sum()),
+        fallback=int(warm["fallback"].sum()),
+        energy_rel_diff_median=float(np.median(rel[ok])), energy_rel_diff_max=float(rel[ok].max()),
+        energy_within_1e8=float(np.mean(rel[ok] < 1e-8)),
+        energy_warm_lower_frac=float(np.mean(signed[ok] < 0)),
+        energy_signed_rel_mean=float(signed[ok].mean()))
+
+
+def main(argv=None) -> int:
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="learned FIRE warm start: train on GPU-FIRE relaxations, evaluate")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--count", type=int, default=2000)
+    t.add_argument("--n", type=int, default=4096)
+    t.add_argument("--per-engine", type=int, default=500)
+    t.add_argument("--steps", type=int, default=2000)
+    t.add_argument("--seed", type=int, default=1)
+    t.add_argument("--out", required=True)
+    e = sub.add_parser("eval")
+    e.add_argument("--params", required=True)
+    e.add_argument("--count", type=int, default=512)
+    e.add_argument("--seed", type=int, default=99)
+    e.add_argument("--out")
+    a = ap.parse_args(argv)
+    if a.cmd == "train":
+        net = WarmStartNet(seed=a.seed)
+        data = quench_set(a.count + 64, a.n, a.n, 0.84, 0.90, seed=a.seed)
+        t0 = time.perf_counter()
+        batches = [Batch(net, data[i:i + a.per_engine]) for i in range(0, a.count, a.per_engine)]
+        held = Batch(net, data[a.count:])
+        gen_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        hist = train(net, batches, a.steps, log_every=max(1, a.steps // 10))
+        torch.cuda.synchronize()
+        train_s = time.perf_counter() - t0
+        net.save(a.out)
+        rep = dict(relaxations=a.count, n=a.n, generation_s=gen_s, fire_device_s=sum(b.fire_device_ms for b in batches) / 1e3,
+                   fire_steps_max=[int(b.conv.max()) for b in batches],
+                   unconverged=int(sum((b.conv < 0).sum() for b in batches)), adam_steps=a.steps, train_s=train_s,
+                   loss_first=hist[0], loss_last=float(np.mean(hist[-len(batches):])),
+                   held_out_quench_loss=mean_target_sq(held), held_out_loss=eval_loss(net, held))
+        print(json.dumps(rep), flush=True)
+        return 0
+    net = WarmStartNet()
+    net.load(a.params)
+    insts = quench_set(a.count, 1024, 16384, 0.84, 0.90, seed=a.seed)
+    plain = relax(insts, None)
+    warm = relax(insts, net)
+    rep = summarize(plain, warm, insts)
+    print(json.dumps(rep), flush=True)
+    if a.out:
+        np.savez(a.out, plain_steps=plain["steps"], warm_steps=warm["steps"], plain_energy=plain["energy"],
+                 warm_energy=warm["energy"], fallback=warm["fallback"])
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -196,6 +196,18 @@ def test_trajectory_langevin(method):
     assert_traj(e, o, ("x", "y", "vx", "vy"))
 
 
+@pytest.mark.parametrize("limits", [{"limit": "0.0001"}, {}, {"limit": "0.001", "angle_limit": "0.0005"}])
+def test_trajectory_nve(limits):
+    # the relaxation stage of the example configurations: nve with a
+    # displacement limit over overlapping soft disks with a polar aligner
+    n = 1000
+    parts, L = plane_disks(n, 0.6, seed=10)
+    e, o = run_both(n, parts, (L, L, 10.0), 299, nlist=(2.4, 0.3),
+                    pairs=[("soft", {"k": "1.0"})], aligns=[("polar", {"J": "1.0"})], dt=1e-3,
+                    integrators=[("nve", dict(limits))])
+    assert_traj(e, o, ("x", "y", "vx", "vy", "nx", "ny", "omega"))
+
+
 def test_fire_matches_oracle():
     n = 600
     parts, L = plane_disks(n, 0.86, seed=11, bidisperse=(1.0, 1.4))

@@ -162,6 +162,7 @@ def python_run(parts, L, segments):
                 pairs=[("soft", {"k": "10.0", "use_particle_radii": ""})], aligns=[("polar", {"J": "0.1"})],
                 dt=1e-3, integrators=segments[0])
     sim.run(segments[1])
+    e.enforce()  # the start-of-step enforce a dump at the next step sees
     return {f: e.download(f) for f in ("x", "y", "nx", "ny")}
 
 
@@ -171,10 +172,12 @@ def read_dump(path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("dump_freq", [481, 37])
-def test_host_run_matches_python_binding(tmp_path, dump_freq):
-    # `run 480` is 481 steps = 13 x 37: with freq 37 the host runs 13
-    # segments (sg_run + 12 sg_run_continue) and the last dump is the end state
+@pytest.mark.parametrize("dump_freq,last_dump", [(400, 400), (37, 444)])
+def test_host_run_matches_python_binding(tmp_path, dump_freq, last_dump):
+    # `run 480` is iterations 0..480; a dump acts at the top of an iteration
+    # (after that step's constraint enforce), so the last dump written is at
+    # the last multiple of the frequency <= 480, and the host splits the run
+    # there (sg_run, then sg_run_continue).
     parts, L = plane_parts(900, 50.0, seed=9)
     write_particles(tmp_path / "p.dat", parts)
     dump = f"dump out {{ type=input; start=0; freq={dump_freq} }}\n"
@@ -185,6 +188,59 @@ def test_host_run_matches_python_binding(tmp_path, dump_freq):
     assert r.returncode == 0, r.stderr
     got = read_dump(tmp_path / "out.dat")
     want = python_run(parts, L, ([("brownian_pos", {"seed": "7", "mu": "1.0"}),
-                                  ("brownian_align", {"seed": "8", "nu": "0.1", "mur": "1.0"})], 480))
+                                  ("brownian_align", {"seed": "8", "nu": "0.1", "mur": "1.0"})], last_dump - 1))
     for f in ("x", "y", "nx", "ny"):
         np.testing.assert_array_equal(got[f], want[f], err_msg=f)
+
+
+@pytest.mark.gpu
+def test_host_disable_and_new_integrator_between_runs(tmp_path):
+    # the example configurations' pattern: relax with nve {limit}, disable it,
+    # then run Brownian dynamics; the host must drive the engine exactly as
+    # the same ABI calls made directly (integrator inserted at its map position)
+    from samos_b200 import Engine, engine as E
+    parts, L = plane_parts(700, 45.0, seed=12)
+    write_particles(tmp_path / "p.dat", parts)
+    conf = ("box periodic { lx = 45.0;  ly = 45.0;  lz = 10.0 }\ninput p.dat\nnlist { rcut = 2.4; pad = 0.3 }\n"
+            "constraint plane { }\npair_potential soft { k = 1.0 }\npair_align polar { J = 1.0 }\n"
+            "timestep 0.001\nintegrator nve { limit = 0.0001 }\nrun 199\ndisable nve { group = all }\n"
+            "external self_propulsion { alpha = 1.0 }\ntimestep 0.01\n"
+            "integrator brownian_pos { seed = 1;  mu = 1.0; group = all }\n"
+            "integrator brownian_align { seed = 1;  mur = 1.0; nu = 0.1; group = all }\n"
+            "dump out { type=input; start=0; freq=50 }\nrun 249\n")
+    (tmp_path / "c.conf").write_text(conf)
+    r = subprocess.run([BIN, "--quiet", str(tmp_path / "c.conf")], capture_output=True, text=True, timeout=600,
+                       cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    got = read_dump(tmp_path / "out.dat")  # written at global step 400 (top of the run's iteration 200)
+
+    e = Engine(len(parts["x"]))
+    e.set_box(45.0, 45.0, 10.0, True)
+    for f in ("x", "y", "z", "nx", "ny", "nz", "radius"):
+        e.upload(f, parts[f])
+    e.set_nlist(2.4, 0.3)
+    kind, cp = PL.resolve_constraint("plane", {})
+    e.add_constraint(kind, cp)
+    soft = PL.resolve_pair("soft", {"k": "1.0"}, 1, 2.4)
+    polar = PL.resolve_align("polar", {"J": "1.0"}, 1, 2.4)
+    sp = PL.resolve_external("self_propulsion", {"alpha": "1.0"}, 1)
+    e.set_timestep(0.001)
+    e.add_pair(soft.kind, soft.glob, soft.table.reshape(-1), soft.use_radii, False, False, False, soft.phase_value)
+    e.add_align(polar.kind, polar.J, polar.rcut, polar.table.reshape(-1), False)
+    k, p, t = PL.resolve_integrator("nve", {"limit": "0.0001"}, 0.001)
+    e.insert_integrator(0, k, p, t)
+    e.run(199)
+    e.disable_integrator(0)
+    e.set_timestep(0.01)
+    e.clear_forces()
+    e.add_pair(soft.kind, soft.glob, soft.table.reshape(-1), soft.use_radii, False, False, False, soft.phase_value)
+    e.add_align(polar.kind, polar.J, polar.rcut, polar.table.reshape(-1), False)
+    e.add_external(sp.kind, sp.alpha, sp.type_alpha, sp.has_params)
+    k, p, t = PL.resolve_integrator("brownian_pos", {"seed": "1", "mu": "1.0", "group": "all"}, 0.01)
+    e.insert_integrator(0, k, p, t)
+    k, p, t = PL.resolve_integrator("brownian_align", {"seed": "1", "mur": "1.0", "nu": "0.1", "group": "all"}, 0.01)
+    e.insert_integrator(0, k, p, t)  # "brownian_align_all" < "brownian_pos_all"
+    e.run(199)                       # global steps 200..399
+    e.begin_step()                   # the dump at global step 400 sees the next step's enforce
+    for f in ("x", "y", "nx", "ny"):
+        np.testing.assert_array_equal(got[f], e.download(f), err_msg=f)

@@ -170,3 +170,30 @@ def test_run_executes_steps_plus_one():
     sim.run(9)  # samos.cpp:878 runs t = 0..9
     assert o.download("x")[0] == pytest.approx(10 * 0.01, rel=1e-14)
     assert o.download("age")[0] == pytest.approx(10 * 0.01, rel=1e-14)
+
+
+def test_nve_limit_clamps_displacement_and_speed():
+    # free particle, v = (3, 4, 0), dt = 0.1, limit = 0.2 (integrator_nve.cpp:57-76, 96-105):
+    # the drift 0.5 is cut to 0.2 along v, and |v| dt = 0.5 > 0.2 cuts v to 0.2 / dt
+    parts, box = two(8.0)
+    parts["vx"] = np.array([3.0, 0.0]); parts["vy"] = np.array([4.0, 0.0]); parts["vz"] = np.zeros(2)
+    o = OracleSystem(2)
+    sim = drive(o, parts, box, constraint=("plane", {}), dt=0.1, integrators=[("nve", {"limit": "0.2"})])
+    sim.run(0)
+    assert o.download("x")[0] == pytest.approx(0.12, abs=1e-15)
+    assert o.download("y")[0] == pytest.approx(0.16, abs=1e-15)
+    assert o.download("vx")[0] == pytest.approx(1.2, abs=1e-14)
+    assert o.download("vy")[0] == pytest.approx(1.6, abs=1e-14)
+    # the resting particle does not move
+    assert o.download("x")[1] == 8.0 and o.download("vx")[1] == 0.0
+
+
+def test_nve_without_limit_is_velocity_verlet():
+    parts, box = two(1.5, r=(1.0, 1.0))  # overlapping soft disks push apart symmetrically
+    o = OracleSystem(2)
+    sim = drive(o, parts, box, constraint=("plane", {}), pairs=[("soft", {"k": "1", "use_particle_radii": ""})],
+                dt=0.01, integrators=[("nve", {})])
+    sim.run(99)
+    x, vx = o.download("x"), o.download("vx")
+    assert x[0] < 0.0 < 1.5 < x[1]
+    assert vx[0] == -vx[1]  # momentum conserved exactly by the symmetric update
