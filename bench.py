@@ -302,6 +302,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-serial replica leg")
     ap.add_argument("--no-ml", action="store_true", help="skip the learned FIRE warm-start leg")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="pin the step-kernel variant instead of autotuning (profiling runs: ncu distorts the tuner's timings)")
     ap.add_argument("--particles", type=int, default=N_PART,
                     help="system size (profiling runs use a smaller system of the same density)")
     args = ap.parse_args()
@@ -330,6 +332,8 @@ def main():
     configure(sim, parts, L)
 
     # warm-up (untimed); the engine's autotuner picks the step-kernel variant here
+    if args.variant >= 0:
+        eng.set_variant(args.variant)
     sim.run(args.warmup - 1)
 
     # timed region: K steps with inputs resident in HBM (state 1.4 GB >> 126 MB L2)

@@ -31,9 +31,152 @@ struct AbpParams {
 
 // Tuning variants (chunk of neighbour records fetched ahead, min blocks/SM):
 // the engine's autotuner times them on the live system and keeps the fastest.
-constexpr int ABP_NVARIANT = 6;  // 0-4 per-particle sweep, 5 flattened sweep
+constexpr int ABP_NVARIANT = 8;  // 0-4 per-particle sweep, 5 flattened sweep, 6-7 staged (cp.async) sweep
 __host__ __device__ constexpr int abp_chunk(int v) { return v == 0 ? 4 : v == 1 ? 4 : v == 2 ? 2 : v == 3 ? 2 : 8; }
 __host__ __device__ constexpr int abp_minb(int v) { return v == 0 ? 5 : v == 1 ? 4 : v == 2 ? 6 : v == 3 ? 4 : 3; }
+
+// One neighbour's pair term of the specialised program: soft repulsion
+// (PairSoftPotential::compute, pair_soft_potential.cpp:79-104) and the polar /
+// nematic torque (pair_polar_aligner.cpp, pair_nematic_aligner.cpp), gathered
+// from the particle's side: F -= ff d, tau += J' (n_i x n_j).  `count_e`: the
+// neighbour has the higher id, so the half-list energy counts this pair here.
+template <int SHAPE, int ALIGN, bool ENERGY>
+__device__ __forceinline__ void abp_pair_term(const AbpParams& S, double x, double y, double z, double nx, double ny,
+                                              double nz, double ri, const D4& g, const D4& h, double rj, bool count_e,
+                                              double& fx, double& fy, double& fz, double& tx, double& ty, double& tz,
+                                              double& epair, double& ealign) {
+  constexpr bool PLANE = SHAPE == HOT_PLANE;
+    double dx = g.x - x, dy = g.y - y, dz = 0.0;
+    if (!PLANE) dz = g.z - z;
+    if (S.periodic) {
+      if (dx > S.xhi) dx -= S.Lx; else if (dx < S.xlo) dx += S.Lx;
+      if (dy > S.yhi) dy -= S.Ly; else if (dy < S.ylo) dy += S.Ly;
+      if (!PLANE) { if (dz > S.zhi) dz -= S.Lz; else if (dz < S.zlo) dz += S.Lz; }
+    }
+    const double r_sq = PLANE ? dx * dx + dy * dy : dx * dx + dy * dy + dz * dz;
+    // PairSoftPotential::compute, pair_soft_potential.cpp:79-104
+    const double sig = S.use_radii ? ri + rj : S.a;
+    // r_sq >= sig^2 (1 + 2^-40) implies sqrt(r_sq) >= sig after rounding:
+    // no contact, so the square root can be skipped without changing a bit
+    const double rd = r_sq < sig * sig * (1.0 + 0x1p-40) ? sqrt(r_sq) : sig;
+    if (rd < sig) {
+      const double diff = sig - rd;
+      double ff;
+      if (rd > 0.0) ff = S.k * diff / rd; else ff = S.k * diff;
+      fx -= ff * dx; fy -= ff * dy;
+      if (!PLANE) fz -= ff * dz;
+      if (ENERGY && count_e) epair += 0.5 * S.k * diff * diff;
+    }
+    if (ALIGN != ABP_ALIGN_NONE && r_sq <= S.rc2) {
+      double onx, ony, onz;
+      if (PLANE) { onx = g.z; ony = g.w; onz = 0.0; }
+      else { onx = h.x; ony = h.y; onz = h.z; }
+      if (PLANE) {
+        const double tau_z = nx * ony - ny * onx;
+        if (ALIGN == ALIGN_POLAR) {
+          tz += S.J * tau_z;
+          if (ENERGY && count_e) ealign += -2.0 * S.J * (nx * onx + ny * ony);
+        } else {
+          const double cd = nx * onx + ny * ony;
+          tz += S.J * cd * tau_z;
+          if (ENERGY && count_e) ealign += -2.0 * S.J * (2.0 * cd * cd - 1.0);
+        }
+      } else {
+        const double tau_x = ny * onz - nz * ony;
+        const double tau_y = nz * onx - nx * onz;
+        const double tau_z = nx * ony - ny * onx;
+        if (ALIGN == ALIGN_POLAR) {
+          tx += S.J * tau_x; ty += S.J * tau_y; tz += S.J * tau_z;
+          if (ENERGY && count_e) ealign += -2.0 * S.J * (nx * onx + ny * ony + nz * onz);
+        } else {
+          const double cd = nx * onx + ny * ony + nz * onz;
+          tx += S.J * cd * tau_x; ty += S.J * cd * tau_y; tz += S.J * cd * tau_z;
+          if (ENERGY && count_e) ealign += -2.0 * S.J * (2.0 * cd * cd - 1.0);
+        }
+      }
+    }
+}
+
+// Integration tail of the specialised program: self-propulsion, the
+// Brownian update (integrator_brownian.cpp:57-121), enforce, torque
+// projection, rotation, skin test (neighbour_list.cpp:278-302), the next
+// step's enforce, and the stores.
+template <int SHAPE, bool SP>
+__device__ __forceinline__ void abp_finish(const AbpParams& S, int r, int k, double x, double y, double z, double nx,
+                                           double ny, double nz, double ri, double fx, double fy, double fz, double tx,
+                                           double ty, double tz, double g_rot, double g_x, double g_y, double g_z,
+                                           double T, uint64_t gid, uint64_t s_base, double ox, double oy, double oz,
+                                           double age0, D4* __restrict__ Gout, D4* __restrict__ Hout, Dyn& d,
+                                           int* __restrict__ rebuild, int* __restrict__ status, int apply_e1,
+                                           int last) {
+  constexpr bool PLANE = SHAPE == HOT_PLANE;
+  if (SP) { fx += S.alpha * nx; fy += S.alpha * ny; if (!PLANE) fz += S.alpha * nz; }
+
+  // ---- IntegratorBrownian::integrate (integrator_brownian.cpp:57-121) ----
+  Hp p;
+  p.x = x; p.y = y; p.z = z; p.nx = nx; p.ny = ny; p.nz = nz;
+  p.vx = 0.0; p.vy = 0.0; p.vz = 0.0;
+  if (S.nematic) {
+    // the velocity flip of velocity_align is overwritten below (v = fd)
+    if (noise_uniform(S.seed, s_base + gid) < S.flip) { p.nx = -p.nx; p.ny = -p.ny; p.nz = -p.nz; }
+  }
+  double fd_x = S.v0 * p.nx + S.mu * fx;
+  double fd_y = S.v0 * p.ny + S.mu * fy;
+  double fd_z = S.v0 * p.nz + S.mu * fz;
+  p.vx = fd_x; p.vy = fd_y; p.vz = fd_z;
+  p.x += S.dt * fd_x; p.y += S.dt * fd_y;
+  if (!PLANE) p.z += S.dt * fd_z;
+  if (T > 0.0) {
+    const double B = sqrt(2.0 * S.mu * T), sqrt_dt = sqrt(S.dt);
+    const double fr_x = B * g_x, fr_y = B * g_y;
+    p.vx += fr_x; p.vy += fr_y;
+    p.x += sqrt_dt * fr_x; p.y += sqrt_dt * fr_y;
+    if (!PLANE) { const double fr_z = B * g_z; p.vz += fr_z; p.z += sqrt_dt * fr_z; }
+  }
+  int dix = 0, diy = 0;
+  const ShapeGeom Rb{S.xlo, S.xhi, S.Lx, S.ylo, S.yhi, S.Ly, S.Rs};
+  hot_enforce<SHAPE>(Rb, p, dix, diy);
+  if (PLANE) p.vz = 0.0;
+  p.tx = tx; p.ty = ty; p.tz = tz;
+  p.omega = S.mur * hot_project_torque<SHAPE>(Rb, p);
+  const double dtheta = S.dt * p.omega + S.stoch * g_rot;
+  hot_rotate<SHAPE>(Rb, p, dtheta, S.velocity != 0);
+  const double age = age0 + S.dt;
+
+  // ---- skin test, NeighbourList::need_update (neighbour_list.cpp:278-302)
+  {
+    double ddx = ox - p.x, ddy = oy - p.y, ddz = PLANE ? 0.0 : oz - p.z;
+    if (S.periodic) {
+      if (ddx > S.xhi) ddx -= S.Lx; else if (ddx < S.xlo) ddx += S.Lx;
+      if (ddy > S.yhi) ddy -= S.Ly; else if (ddy < S.ylo) ddy += S.Ly;
+      if (!PLANE) { if (ddz > S.zhi) ddz -= S.Lz; else if (ddz < S.zlo) ddz += S.Lz; }
+    }
+    const double d2 = PLANE ? ddx * ddx + ddy * ddy : ddx * ddx + ddy * ddy + ddz * ddz;
+    if (!(d2 < S.pad2q)) {
+      if (rebuild[r] == 0) atomicOr(&rebuild[r], 1);
+    }
+  }
+  if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) atomicOr(status, ST_NONFINITE);
+  if (apply_e1) hot_enforce<SHAPE>(Rb, p, dix, diy);
+
+  // ---- stores ---------------------------------------------------------------
+  if (PLANE) {
+    stg4(Gout + k, D4{p.x, p.y, p.nx, p.ny});
+    d.vx[k] = p.vx; d.vy[k] = p.vy;
+  } else {
+    stg4(Gout + k, D4{p.x, p.y, p.z, ri});
+    stg4(Hout + k, D4{p.nx, p.ny, p.nz, 0.0});
+    d.vx[k] = p.vx; d.vy[k] = p.vy; d.vz[k] = p.vz;
+  }
+  d.age[k] = age;
+  if (dix) d.ix[k] += dix;
+  if (diy) d.iy[k] += diy;
+  if (last) {
+    d.omega[k] = p.omega;
+    d.fx[k] = fx; d.fy[k] = fy; d.fz[k] = PLANE ? 0.0 : fz;
+    d.tx[k] = tx; d.ty[k] = ty; d.tz[k] = tz;
+  }
+}
 
 template <int SHAPE, int ALIGN, bool SP, bool ENERGY, int VAR>
 __global__ void __launch_bounds__(BLOCK, abp_minb(VAR))
@@ -110,125 +253,13 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
       for (int u = 0; u < CH; u++) {
         const int q = q0 + u;
         if (q < cnt) {
-          double dx = gg[u].x - x, dy = gg[u].y - y, dz = 0.0;
-          if (!PLANE) dz = gg[u].z - z;
-          if (S.periodic) {
-            if (dx > S.xhi) dx -= S.Lx; else if (dx < S.xlo) dx += S.Lx;
-            if (dy > S.yhi) dy -= S.Ly; else if (dy < S.ylo) dy += S.Ly;
-            if (!PLANE) { if (dz > S.zhi) dz -= S.Lz; else if (dz < S.zlo) dz += S.Lz; }
-          }
-          const double r_sq = PLANE ? dx * dx + dy * dy : dx * dx + dy * dy + dz * dz;
-          // PairSoftPotential::compute, pair_soft_potential.cpp:79-104
-          const double rj = PLANE ? rr[u] : gg[u].w;
-          const double sig = S.use_radii ? ri + rj : S.a;
-          // r_sq >= sig^2 (1 + 2^-40) implies sqrt(r_sq) >= sig after rounding:
-          // no contact, so the square root can be skipped without changing a bit
-          const double rd = r_sq < sig * sig * (1.0 + 0x1p-40) ? sqrt(r_sq) : sig;
-          if (rd < sig) {
-            const double diff = sig - rd;
-            double ff;
-            if (rd > 0.0) ff = S.k * diff / rd; else ff = S.k * diff;
-            fx -= ff * dx; fy -= ff * dy;
-            if (!PLANE) fz -= ff * dz;
-            if (ENERGY && q >= lo) epair += 0.5 * S.k * diff * diff;
-          }
-          if (ALIGN != ABP_ALIGN_NONE && r_sq <= S.rc2) {
-            double onx, ony, onz;
-            if (PLANE) { onx = gg[u].z; ony = gg[u].w; onz = 0.0; }
-            else { onx = hh[u].x; ony = hh[u].y; onz = hh[u].z; }
-            if (PLANE) {
-              const double tau_z = nx * ony - ny * onx;
-              if (ALIGN == ALIGN_POLAR) {
-                tz += S.J * tau_z;
-                if (ENERGY && q >= lo) ealign += -2.0 * S.J * (nx * onx + ny * ony);
-              } else {
-                const double cd = nx * onx + ny * ony;
-                tz += S.J * cd * tau_z;
-                if (ENERGY && q >= lo) ealign += -2.0 * S.J * (2.0 * cd * cd - 1.0);
-              }
-            } else {
-              const double tau_x = ny * onz - nz * ony;
-              const double tau_y = nz * onx - nx * onz;
-              const double tau_z = nx * ony - ny * onx;
-              if (ALIGN == ALIGN_POLAR) {
-                tx += S.J * tau_x; ty += S.J * tau_y; tz += S.J * tau_z;
-                if (ENERGY && q >= lo) ealign += -2.0 * S.J * (nx * onx + ny * ony + nz * onz);
-              } else {
-                const double cd = nx * onx + ny * ony + nz * onz;
-                tx += S.J * cd * tau_x; ty += S.J * cd * tau_y; tz += S.J * cd * tau_z;
-                if (ENERGY && q >= lo) ealign += -2.0 * S.J * (2.0 * cd * cd - 1.0);
-              }
-            }
-          }
+          abp_pair_term<SHAPE, ALIGN, ENERGY>(S, x, y, z, nx, ny, nz, ri, gg[u], hh[u], PLANE ? rr[u] : gg[u].w,
+                                              q >= lo, fx, fy, fz, tx, ty, tz, epair, ealign);
         }
       }
     }
-    if (SP) { fx += S.alpha * nx; fy += S.alpha * ny; if (!PLANE) fz += S.alpha * nz; }
-
-    // ---- IntegratorBrownian::integrate (integrator_brownian.cpp:57-121) ----
-    Hp p;
-    p.x = x; p.y = y; p.z = z; p.nx = nx; p.ny = ny; p.nz = nz;
-    p.vx = 0.0; p.vy = 0.0; p.vz = 0.0;
-    if (S.nematic) {
-      // the velocity flip of velocity_align is overwritten below (v = fd)
-      if (noise_uniform(S.seed, s_base + gid) < S.flip) { p.nx = -p.nx; p.ny = -p.ny; p.nz = -p.nz; }
-    }
-    double fd_x = S.v0 * p.nx + S.mu * fx;
-    double fd_y = S.v0 * p.ny + S.mu * fy;
-    double fd_z = S.v0 * p.nz + S.mu * fz;
-    p.vx = fd_x; p.vy = fd_y; p.vz = fd_z;
-    p.x += S.dt * fd_x; p.y += S.dt * fd_y;
-    if (!PLANE) p.z += S.dt * fd_z;
-    if (T > 0.0) {
-      const double B = sqrt(2.0 * S.mu * T), sqrt_dt = sqrt(S.dt);
-      const double fr_x = B * g_x, fr_y = B * g_y;
-      p.vx += fr_x; p.vy += fr_y;
-      p.x += sqrt_dt * fr_x; p.y += sqrt_dt * fr_y;
-      if (!PLANE) { const double fr_z = B * g_z; p.vz += fr_z; p.z += sqrt_dt * fr_z; }
-    }
-    int dix = 0, diy = 0;
-    const ShapeGeom Rb{S.xlo, S.xhi, S.Lx, S.ylo, S.yhi, S.Ly, S.Rs};
-    hot_enforce<SHAPE>(Rb, p, dix, diy);
-    if (PLANE) p.vz = 0.0;
-    p.tx = tx; p.ty = ty; p.tz = tz;
-    p.omega = S.mur * hot_project_torque<SHAPE>(Rb, p);
-    const double dtheta = S.dt * p.omega + S.stoch * g_rot;
-    hot_rotate<SHAPE>(Rb, p, dtheta, S.velocity != 0);
-    const double age = age0 + S.dt;
-
-    // ---- skin test, NeighbourList::need_update (neighbour_list.cpp:278-302)
-    {
-      double ddx = ox - p.x, ddy = oy - p.y, ddz = PLANE ? 0.0 : oz - p.z;
-      if (S.periodic) {
-        if (ddx > S.xhi) ddx -= S.Lx; else if (ddx < S.xlo) ddx += S.Lx;
-        if (ddy > S.yhi) ddy -= S.Ly; else if (ddy < S.ylo) ddy += S.Ly;
-        if (!PLANE) { if (ddz > S.zhi) ddz -= S.Lz; else if (ddz < S.zlo) ddz += S.Lz; }
-      }
-      const double d2 = PLANE ? ddx * ddx + ddy * ddy : ddx * ddx + ddy * ddy + ddz * ddz;
-      if (!(d2 < S.pad2q)) {
-        if (rebuild[r] == 0) atomicOr(&rebuild[r], 1);
-      }
-    }
-    if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) atomicOr(status, ST_NONFINITE);
-    if (apply_e1) hot_enforce<SHAPE>(Rb, p, dix, diy);
-
-    // ---- stores ---------------------------------------------------------------
-    if (PLANE) {
-      stg4(Gout + k, D4{p.x, p.y, p.nx, p.ny});
-      d.vx[k] = p.vx; d.vy[k] = p.vy;
-    } else {
-      stg4(Gout + k, D4{p.x, p.y, p.z, ri});
-      stg4(Hout + k, D4{p.nx, p.ny, p.nz, 0.0});
-      d.vx[k] = p.vx; d.vy[k] = p.vy; d.vz[k] = p.vz;
-    }
-    d.age[k] = age;
-    if (dix) d.ix[k] += dix;
-    if (diy) d.iy[k] += diy;
-    if (last) {
-      d.omega[k] = p.omega;
-      d.fx[k] = fx; d.fy[k] = fy; d.fz[k] = PLANE ? 0.0 : fz;
-      d.tx[k] = tx; d.ty[k] = ty; d.tz[k] = tz;
-    }
+    abp_finish<SHAPE, SP>(S, r, k, x, y, z, nx, ny, nz, ri, fx, fy, fz, tx, ty, tz, g_rot, g_x, g_y, g_z, T, gid,
+                          s_base, ox, oy, oz, age0, Gout, Hout, d, rebuild, status, apply_e1, last);
   }
   if (ENERGY) {
     double ev[MAX_PAIR + MAX_ALIGN];
@@ -240,6 +271,151 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Staged variant: each thread's neighbour records are copied into shared
+// memory with cp.async (no registers held by loads in flight), CH records per
+// stage, two stages in flight, while the previous stage is evaluated.  The
+// pair term and the integration tail are the same functions as above, so the
+// bits are those of k_abp_step.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// One stage: per record slot u, 16-byte chunks laid out lane-consecutive
+// ([chunk][thread]), so a warp's shared loads are conflict-free.
+template <int SHAPE, int ALIGN, int CH>
+struct StagedBuf {
+  static constexpr int NCHUNK = SHAPE == HOT_PLANE ? 2 : (ALIGN != ABP_ALIGN_NONE ? 4 : 2);
+  double2 c[2][CH][NCHUNK][BLOCK];
+  double r[SHAPE == HOT_PLANE ? 2 : 1][SHAPE == HOT_PLANE ? CH : 1][BLOCK];
+};
+
+template <int SHAPE, int ALIGN, bool SP, bool ENERGY, int CH, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB)
+k_abp_staged(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, const Clock* __restrict__ clk,
+             const D4* __restrict__ Gin, D4* __restrict__ Gout, const D4* __restrict__ Hin, D4* __restrict__ Hout,
+             Dyn d, Stat st, NbList nl, int* __restrict__ rebuild, int* __restrict__ status, int apply_e1, int last,
+             double* epart, int nblocks) {
+  constexpr bool PLANE = SHAPE == HOT_PLANE;
+  using SB = StagedBuf<SHAPE, ALIGN, CH>;
+  constexpr int NC = SB::NCHUNK;
+  extern __shared__ __align__(16) unsigned char staged_smem[];
+  SB& B = *reinterpret_cast<SB*>(staged_smem);
+  __shared__ AbpParams S;
+  __shared__ uint64_t s_base;
+  __shared__ int s_step;
+  const int r = blk_rep[blockIdx.x];
+  {
+    constexpr int NW = (int)(sizeof(AbpParams) / 8);
+    if (threadIdx.x < NW)
+      reinterpret_cast<unsigned long long*>(&S)[threadIdx.x] =
+          reinterpret_cast<const unsigned long long*>(prm + r)[threadIdx.x];
+    if (threadIdx.x == 0) { s_base = clk[r].ctr[0]; s_step = clk[r].run_step; }
+  }
+  __syncthreads();
+  const int t = threadIdx.x;
+  const int k = blockIdx.x * BLOCK + t;
+  double epair = 0.0, ealign = 0.0;
+  if (k - S.off < S.n) {
+    double x, y, z, nx, ny, nz, ri;
+    {
+      const D4 g = ldg4(Gin + k);
+      x = g.x; y = g.y;
+      if (PLANE) { z = 0.0; nx = g.z; ny = g.w; nz = 0.0; ri = st.r[k]; }
+      else { z = g.z; ri = g.w; const D4 h = ldg4(Hin + k); nx = h.x; ny = h.y; nz = h.z; }
+    }
+    const int cnt = nl.cnt[k], lo = nl.lo[k];
+    const uint64_t gid = (uint64_t)st.id[k];
+    const double ox = nl.ox[k], oy = nl.oy[k], oz = PLANE ? 0.0 : nl.oz[k];
+    const double age0 = d.age[k];
+    const double* rr_src = st.r;
+    auto issue = [&](int stage, int q0) {
+#pragma unroll
+      for (int u = 0; u < CH; u++) {
+        const int q = q0 + u;
+        if (q < cnt) {
+          const int j = __ldg(nl.nb + (size_t)q * nl.stride + k);
+          const double2* gsrc = reinterpret_cast<const double2*>(Gin + j);
+          cp_async16(&B.c[stage][u][0][t], gsrc);
+          cp_async16(&B.c[stage][u][1][t], gsrc + 1);
+          if (PLANE) {
+            if (S.use_radii) cp_async8(&B.r[stage][u][t], rr_src + j);
+          } else if (ALIGN != ABP_ALIGN_NONE) {
+            const double2* hsrc = reinterpret_cast<const double2*>(Hin + j);
+            cp_async16(&B.c[stage][u][2][t], hsrc);
+            cp_async16(&B.c[stage][u][3][t], hsrc + 1);
+          }
+        }
+      }
+      cp_async_commit();
+    };
+
+    double fx = 0.0, fy = 0.0, fz = 0.0, tx = 0.0, ty = 0.0, tz = 0.0;
+    const double T = value_get(S.temp, s_step);
+    uint64_t base = s_base;
+    if (S.nematic) base += (uint64_t)S.n;
+    const int D = T > 0.0 ? 4 : 1;
+    const uint64_t c0 = base + gid * (uint64_t)D;
+    issue(0, 0);
+    // the noise is pure ALU work: it runs while the first stage is in flight
+    double g_rot = noise_gauss(S.seed, c0 + (uint64_t)(D - 1)), g_x = 0.0, g_y = 0.0, g_z = 0.0;
+    if (T > 0.0) {
+      g_x = noise_gauss(S.seed, c0 + 0);
+      g_y = noise_gauss(S.seed, c0 + 1);
+      if (!PLANE) g_z = noise_gauss(S.seed, c0 + 2);
+    }
+    int stage = 0;
+    for (int q0 = 0; q0 < cnt; q0 += CH) {
+      issue(stage ^ 1, q0 + CH);  // next stage (an empty group past the end)
+      cp_async_wait<1>();         // this thread's copies of `stage` have landed
+#pragma unroll
+      for (int u = 0; u < CH; u++) {
+        const int q = q0 + u;
+        if (q < cnt) {
+          const double2 a = B.c[stage][u][0][t], b = B.c[stage][u][1][t];
+          D4 g{a.x, a.y, b.x, b.y}, h{0.0, 0.0, 0.0, 0.0};
+          double rj;
+          if (PLANE) rj = S.use_radii ? B.r[stage][u][t] : 1.0;
+          else {
+            rj = g.w;
+            if (ALIGN != ABP_ALIGN_NONE) {
+              const double2 c = B.c[stage][u][2][t], e = B.c[stage][u][3][t];
+              h = D4{c.x, c.y, e.x, e.y};
+            }
+          }
+          abp_pair_term<SHAPE, ALIGN, ENERGY>(S, x, y, z, nx, ny, nz, ri, g, h, rj, q >= lo, fx, fy, fz, tx, ty, tz,
+                                              epair, ealign);
+        }
+      }
+      stage ^= 1;
+    }
+    cp_async_wait<0>();
+    abp_finish<SHAPE, SP>(S, r, k, x, y, z, nx, ny, nz, ri, fx, fy, fz, tx, ty, tz, g_rot, g_x, g_y, g_z, T, gid,
+                          s_base, ox, oy, oz, age0, Gout, Hout, d, rebuild, status, apply_e1, last);
+  }
+  if (ENERGY) {
+    double ev[MAX_PAIR + MAX_ALIGN];
+#pragma unroll
+    for (int i = 0; i < MAX_PAIR + MAX_ALIGN; i++) ev[i] = 0.0;
+    ev[0] = epair;
+    ev[MAX_PAIR] = ealign;
+    block_reduce_store<MAX_PAIR + MAX_ALIGN>(ev, epart, nblocks);
+  }
+}
+
+template <int SHAPE, int ALIGN, int CH>
+constexpr size_t staged_smem_bytes() { return sizeof(StagedBuf<SHAPE, ALIGN, CH>); }
 
 // ---------------------------------------------------------------------------
 // Flattened variant: a warp's (particle, neighbour) items are laid out

@@ -1042,16 +1042,35 @@ static void launch_abp_v(sg_system* s, bool apply_e1, bool last) {
       s->status, apply_e1 ? 1 : 0, last ? 1 : 0, s->epart, s->nblocks);
 }
 
+// cudaFuncSetAttribute is per device: remember, per kernel, the devices it
+// has been raised on.
+template <typename K>
+static void raise_smem(K kernel, size_t smem, unsigned* done_mask, int device) {
+  const unsigned bit = 1u << (device & 31);
+  if (!(*done_mask & bit)) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    *done_mask |= bit;
+  }
+}
+
 template <int SHAPE, int ALIGN, bool SP, bool ENERGY>
 static void launch_abp_flat(sg_system* s, bool apply_e1, bool last) {
   const int b = s->hot_buf;
   constexpr size_t smem = flat_smem_bytes<SHAPE, ENERGY>();
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_abp_flat<SHAPE, ALIGN, SP, ENERGY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  static unsigned done = 0;
+  raise_smem(k_abp_flat<SHAPE, ALIGN, SP, ENERGY>, smem, &done, s->device);
   k_abp_flat<SHAPE, ALIGN, SP, ENERGY><<<s->nblocks, BLOCK, smem, s->stream>>>(
+      s->abp, s->blk_rep, s->clk, s->G[b], s->G[1 - b], s->H[b], s->H[1 - b], s->cur, s->st, s->nl, s->rebuild,
+      s->status, apply_e1 ? 1 : 0, last ? 1 : 0, s->epart, s->nblocks);
+}
+
+template <int SHAPE, int ALIGN, bool SP, bool ENERGY, int CH, int MINB>
+static void launch_abp_staged(sg_system* s, bool apply_e1, bool last) {
+  const int b = s->hot_buf;
+  constexpr size_t smem = staged_smem_bytes<SHAPE, ALIGN, CH>();
+  static unsigned done = 0;
+  raise_smem(k_abp_staged<SHAPE, ALIGN, SP, ENERGY, CH, MINB>, smem, &done, s->device);
+  k_abp_staged<SHAPE, ALIGN, SP, ENERGY, CH, MINB><<<s->nblocks, BLOCK, smem, s->stream>>>(
       s->abp, s->blk_rep, s->clk, s->G[b], s->G[1 - b], s->H[b], s->H[1 - b], s->cur, s->st, s->nl, s->rebuild,
       s->status, apply_e1 ? 1 : 0, last ? 1 : 0, s->epart, s->nblocks);
 }
@@ -1061,6 +1080,8 @@ static void launch_abp3(sg_system* s, bool apply_e1, bool last, bool energy) {
   if (energy) { launch_abp_v<SHAPE, ALIGN, SP, true, 1>(s, apply_e1, last); return; }
   switch (s->abp_variant) {
     case 5: launch_abp_flat<SHAPE, ALIGN, SP, false>(s, apply_e1, last); break;
+    case 6: launch_abp_staged<SHAPE, ALIGN, SP, false, 4, 4>(s, apply_e1, last); break;
+    case 7: launch_abp_staged<SHAPE, ALIGN, SP, false, 4, 5>(s, apply_e1, last); break;
     case 0: launch_abp_v<SHAPE, ALIGN, SP, false, 0>(s, apply_e1, last); break;
     case 1: launch_abp_v<SHAPE, ALIGN, SP, false, 1>(s, apply_e1, last); break;
     case 2: launch_abp_v<SHAPE, ALIGN, SP, false, 2>(s, apply_e1, last); break;
