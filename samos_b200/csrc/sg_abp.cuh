@@ -9,6 +9,9 @@
 // The arithmetic per term is the reference's (see sg_kernels.cuh), so results
 // are bit-identical to the generic kernels.
 #pragma once
+#include <climits>
+#include <cstddef>
+
 #include "sg_hot.cuh"
 
 namespace sg {
@@ -31,7 +34,7 @@ struct AbpParams {
 
 // Tuning variants (chunk of neighbour records fetched ahead, min blocks/SM):
 // the engine's autotuner times them on the live system and keeps the fastest.
-constexpr int ABP_NVARIANT = 8;  // 0-4 per-particle sweep, 5 flattened sweep, 6-7 staged (cp.async) sweep
+constexpr int ABP_NVARIANT = 9;  // 0-4 per-particle sweep, 5 flattened, 6-7 staged (cp.async), 8 shared-memory tile
 __host__ __device__ constexpr int abp_chunk(int v) { return v == 0 ? 4 : v == 1 ? 4 : v == 2 ? 2 : v == 3 ? 2 : 8; }
 __host__ __device__ constexpr int abp_minb(int v) { return v == 0 ? 5 : v == 1 ? 4 : v == 2 ? 6 : v == 3 ? 4 : 3; }
 
@@ -416,6 +419,234 @@ k_abp_staged(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep,
 
 template <int SHAPE, int ALIGN, int CH>
 constexpr size_t staged_smem_bytes() { return sizeof(StagedBuf<SHAPE, ALIGN, CH>); }
+using StagedBufSphere4 = StagedBuf<HOT_SPHERE, ALIGN_POLAR, 4>;
+static_assert(offsetof(StagedBufSphere4, c) == 0, "16-byte cp.async targets come first");
+
+// ---------------------------------------------------------------------------
+// Tile variant: slots are in cell order, so the neighbours of a block's 128
+// particles are a few hundred records from a handful of nearby cells.  After
+// every neighbour-list build, k_tile_prep lists each block's distinct
+// neighbour slots (ascending) and rewrites the lists as positions in that
+// set (16-bit); the step kernel then copies the block's records into shared
+// memory once (cp.async, while the Gaussian draws are computed) and every
+// pair term reads shared memory.  Blocks whose neighbour slots span more than
+// TILE_WIN slots or hold more than TILE_MAX distinct records (periodic wrap,
+// unsorted lists) keep the global gather (tile_n = -1).  The pair term and
+// the tail are the functions above, in list order: same bits.
+// ---------------------------------------------------------------------------
+constexpr int TILE_WIN = 16384;  // slot window per block (bitmap bits)
+constexpr int TILE_MAX = 640;    // distinct neighbour records staged per block
+constexpr int TILE_QMAX = 24;    // list ranks whose positions are staged (deeper ranks read global memory)
+
+__global__ void __launch_bounds__(BLOCK)
+k_tile_prep(const Replica* __restrict__ reps, const int* __restrict__ blk_rep, NbList nl, int* __restrict__ tile_n,
+            int* __restrict__ tile_slot, uint16_t* __restrict__ nbpos, const int* __restrict__ blist = nullptr) {
+  __shared__ uint32_t bm[TILE_WIN / 32];
+  __shared__ int woff[TILE_WIN / 32];
+  __shared__ int s_min, s_max, s_total;
+  __shared__ int wsum[BLOCK / 32];
+  const int b = blist ? blist[blockIdx.x] : (int)blockIdx.x, t = threadIdx.x, k = b * BLOCK + t;
+  const Replica& R = reps[blk_rep[b]];
+  const int cnt = (k - R.off < R.n) ? nl.cnt[k] : 0;
+  if (t == 0) { s_min = INT_MAX; s_max = -1; }
+  __syncthreads();
+  int mn = INT_MAX, mx = -1;
+  for (int q = 0; q < cnt; q++) {
+    const int j = nl.nb[(size_t)q * nl.stride + k];
+    mn = min(mn, j); mx = max(mx, j);
+  }
+  if (mx >= 0) { atomicMin(&s_min, mn); atomicMax(&s_max, mx); }
+  __syncthreads();
+  const int lo = s_min, hi = s_max;
+  if (hi < 0) { if (t == 0) tile_n[b] = 0; return; }
+  if (hi - lo + 1 > TILE_WIN) { if (t == 0) tile_n[b] = -1; return; }
+  constexpr int WPT = TILE_WIN / 32 / BLOCK;  // bitmap words per thread
+  for (int w = 0; w < WPT; w++) bm[t * WPT + w] = 0u;
+  __syncthreads();
+  for (int q = 0; q < cnt; q++) {
+    const int d = nl.nb[(size_t)q * nl.stride + k] - lo;
+    atomicOr(&bm[d >> 5], 1u << (d & 31));
+  }
+  __syncthreads();
+  int pc[WPT], mine = 0;
+  for (int w = 0; w < WPT; w++) { pc[w] = __popc(bm[t * WPT + w]); mine += pc[w]; }
+  // exclusive scan of `mine` over the block
+  const int lane = t & 31, warp = t >> 5;
+  int incl = mine;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  int base = incl - mine;
+  for (int w = 0; w < warp; w++) base += wsum[w];
+  if (t == BLOCK - 1) s_total = base + mine;
+  for (int w = 0; w < WPT; w++) { woff[t * WPT + w] = base; base += pc[w]; }
+  __syncthreads();
+  const int total = s_total;
+  if (total > TILE_MAX) { if (t == 0) tile_n[b] = -1; return; }
+  for (int w = 0; w < WPT; w++) {
+    uint32_t bits = bm[t * WPT + w];
+    int pos = woff[t * WPT + w];
+    while (bits) {
+      const int l = __ffs(bits) - 1;
+      tile_slot[(size_t)b * TILE_MAX + pos++] = lo + (t * WPT + w) * 32 + l;
+      bits &= bits - 1u;
+    }
+  }
+  for (int q = 0; q < cnt; q++) {
+    const size_t at = (size_t)q * nl.stride + k;
+    const int d = nl.nb[at] - lo, w = d >> 5;
+    nbpos[at] = (uint16_t)(woff[w] + __popc(bm[w] & ((1u << (d & 31)) - 1u)));
+  }
+  if (t == 0) tile_n[b] = total;
+}
+
+template <int SHAPE, int ALIGN>
+struct TileBuf {
+  static constexpr int NCHUNK = SHAPE == HOT_PLANE ? 2 : (ALIGN != ABP_ALIGN_NONE ? 4 : 2);
+  double2 c[NCHUNK][TILE_MAX];
+  double r[SHAPE == HOT_PLANE ? TILE_MAX : 2];     // even count: keeps `pos` 16-byte aligned
+  uint16_t pos[TILE_QMAX][BLOCK];  // the block's list positions, rank-major (16-byte cp.async targets)
+};
+using TileBufPlane = TileBuf<HOT_PLANE, ALIGN_POLAR>;
+using TileBufSphere = TileBuf<HOT_SPHERE, ALIGN_POLAR>;
+using TileBufSphereNoAlign = TileBuf<HOT_SPHERE, ABP_ALIGN_NONE>;
+static_assert(offsetof(TileBufPlane, pos) % 16 == 0, "tile positions must be 16-byte aligned");
+static_assert(offsetof(TileBufSphere, pos) % 16 == 0, "tile positions must be 16-byte aligned");
+static_assert(offsetof(TileBufSphereNoAlign, pos) % 16 == 0, "tile positions must be 16-byte aligned");
+template <int SHAPE, int ALIGN>
+constexpr size_t tile_smem_bytes() { return sizeof(TileBuf<SHAPE, ALIGN>); }
+
+template <int SHAPE, int ALIGN, bool SP, bool ENERGY, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB)
+k_abp_tile(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, const Clock* __restrict__ clk,
+           const D4* __restrict__ Gin, D4* __restrict__ Gout, const D4* __restrict__ Hin, D4* __restrict__ Hout,
+           Dyn d, Stat st, NbList nl, int* __restrict__ rebuild, int* __restrict__ status, int apply_e1, int last,
+           double* epart, int nblocks, const int* __restrict__ tile_n, const int* __restrict__ tile_slot,
+           const uint16_t* __restrict__ nbpos) {
+  constexpr bool PLANE = SHAPE == HOT_PLANE;
+  using TB = TileBuf<SHAPE, ALIGN>;
+  extern __shared__ __align__(16) unsigned char tile_smem[];
+  TB& B = *reinterpret_cast<TB*>(tile_smem);
+  __shared__ AbpParams S;
+  __shared__ uint64_t s_base;
+  __shared__ int s_step;
+  const int r = blk_rep[blockIdx.x];
+  {
+    constexpr int NW = (int)(sizeof(AbpParams) / 8);
+    if (threadIdx.x < NW)
+      reinterpret_cast<unsigned long long*>(&S)[threadIdx.x] =
+          reinterpret_cast<const unsigned long long*>(prm + r)[threadIdx.x];
+    if (threadIdx.x == 0) { s_base = clk[r].ctr[0]; s_step = clk[r].run_step; }
+  }
+  __syncthreads();
+  const int t = threadIdx.x;
+  const int k = blockIdx.x * BLOCK + t;
+  const int nt = tile_n[blockIdx.x];
+  __shared__ int s_qmax;
+  const bool active = k - S.off < S.n;
+  const int cnt = active ? nl.cnt[k] : 0;
+  if (t == 0) s_qmax = 0;
+  __syncthreads();
+  if (cnt > 0) atomicMax(&s_qmax, cnt);
+  __syncthreads();
+  const int qst = min(s_qmax, TILE_QMAX);  // list ranks staged
+  if (nt > 0) {  // stage the block's distinct neighbour records and list positions
+    const uint16_t* prow = nbpos + (size_t)blockIdx.x * BLOCK;
+    for (int c = t; c < qst * (BLOCK / 8); c += BLOCK) {  // 16-byte pieces: 8 positions
+      const int q = c / (BLOCK / 8), piece = c % (BLOCK / 8);
+      cp_async16(&B.pos[q][piece * 8], prow + (size_t)q * nl.stride + piece * 8);
+    }
+    const int* slots = tile_slot + (size_t)blockIdx.x * TILE_MAX;
+    for (int u = t; u < nt; u += BLOCK) {
+      const int j = slots[u];
+      const double2* gs = reinterpret_cast<const double2*>(Gin + j);
+      cp_async16(&B.c[0][u], gs);
+      cp_async16(&B.c[1][u], gs + 1);
+      if (PLANE) {
+        if (S.use_radii) cp_async8(&B.r[u], st.r + j);
+      } else if (ALIGN != ABP_ALIGN_NONE) {
+        const double2* hs = reinterpret_cast<const double2*>(Hin + j);
+        cp_async16(&B.c[2][u], hs);
+        cp_async16(&B.c[3][u], hs + 1);
+      }
+    }
+    cp_async_commit();
+  }
+  double x = 0.0, y = 0.0, z = 0.0, nx = 0.0, ny = 0.0, nz = 0.0, ri = 0.0, ox = 0.0, oy = 0.0, oz = 0.0, age0 = 0.0;
+  int lo = 0;
+  uint64_t gid = 0;
+  double g_rot = 0.0, g_x = 0.0, g_y = 0.0, g_z = 0.0;
+  const double T = value_get(S.temp, s_step);
+  if (active) {
+    const D4 g = ldg4(Gin + k);
+    x = g.x; y = g.y;
+    if (PLANE) { nx = g.z; ny = g.w; ri = st.r[k]; }
+    else { z = g.z; ri = g.w; const D4 h = ldg4(Hin + k); nx = h.x; ny = h.y; nz = h.z; }
+    lo = nl.lo[k];
+    gid = (uint64_t)st.id[k];
+    ox = nl.ox[k]; oy = nl.oy[k];
+    if (!PLANE) oz = nl.oz[k];
+    age0 = d.age[k];
+    // the Gaussian draws: pure ALU work while the records are in flight
+    uint64_t base = s_base;
+    if (S.nematic) base += (uint64_t)S.n;
+    const int D = T > 0.0 ? 4 : 1;
+    const uint64_t c0 = base + gid * (uint64_t)D;
+    g_rot = noise_gauss(S.seed, c0 + (uint64_t)(D - 1));
+    if (T > 0.0) {
+      g_x = noise_gauss(S.seed, c0 + 0);
+      g_y = noise_gauss(S.seed, c0 + 1);
+      if (!PLANE) g_z = noise_gauss(S.seed, c0 + 2);
+    }
+  }
+  if (nt > 0) cp_async_wait<0>();
+  __syncthreads();
+  double epair = 0.0, ealign = 0.0;
+  if (active) {
+    double fx = 0.0, fy = 0.0, fz = 0.0, tx = 0.0, ty = 0.0, tz = 0.0;
+    for (int q = 0; q < cnt; q++) {
+      const size_t at = (size_t)q * nl.stride + k;
+      D4 g, h{0.0, 0.0, 0.0, 0.0};
+      double rj;
+      if (nt >= 0) {
+        const int u = q < TILE_QMAX ? B.pos[q][t] : nbpos[at];
+        const double2 a = B.c[0][u], c = B.c[1][u];
+        g = D4{a.x, a.y, c.x, c.y};
+        if (PLANE) rj = S.use_radii ? B.r[u] : 1.0;
+        else {
+          rj = g.w;
+          if (ALIGN != ABP_ALIGN_NONE) {
+            const double2 e = B.c[2][u], f = B.c[3][u];
+            h = D4{e.x, e.y, f.x, f.y};
+          }
+        }
+      } else {
+        const int j = __ldg(nl.nb + at);
+        g = ldg4(Gin + j);
+        if (PLANE) rj = S.use_radii ? __ldg(st.r + j) : 1.0;
+        else {
+          rj = g.w;
+          if (ALIGN != ABP_ALIGN_NONE) h = ldg4(Hin + j);
+        }
+      }
+      abp_pair_term<SHAPE, ALIGN, ENERGY>(S, x, y, z, nx, ny, nz, ri, g, h, rj, q >= lo, fx, fy, fz, tx, ty, tz,
+                                          epair, ealign);
+    }
+    abp_finish<SHAPE, SP>(S, r, k, x, y, z, nx, ny, nz, ri, fx, fy, fz, tx, ty, tz, g_rot, g_x, g_y, g_z, T, gid,
+                          s_base, ox, oy, oz, age0, Gout, Hout, d, rebuild, status, apply_e1, last);
+  }
+  if (ENERGY) {
+    double ev[MAX_PAIR + MAX_ALIGN];
+#pragma unroll
+    for (int i = 0; i < MAX_PAIR + MAX_ALIGN; i++) ev[i] = 0.0;
+    ev[0] = epair;
+    ev[MAX_PAIR] = ealign;
+    block_reduce_store<MAX_PAIR + MAX_ALIGN>(ev, epart, nblocks);
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Flattened variant: a warp's (particle, neighbour) items are laid out

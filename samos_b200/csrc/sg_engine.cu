@@ -64,6 +64,11 @@ struct sg_system {
   int ncell_total = 0;
   int *pcell = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
   int *tmp = nullptr, *perm = nullptr, *scan_bsum = nullptr;
+  CellSeg* segs = nullptr;            // cell ranges of the replicas being rebuilt
+  std::vector<CellSeg> segs_h;
+  int* blist = nullptr;               // blocks of the replicas being rebuilt (null: every block)
+  std::vector<int> blist_h;
+  int nblist = 0;
   int *rebuild = nullptr, *status = nullptr, *maxnb = nullptr;
   int* rebuild_h = nullptr;  // pinned
   double *epart = nullptr, *fire_part = nullptr, *alpha_mix = nullptr, *Rn = nullptr;
@@ -85,13 +90,21 @@ struct sg_system {
   std::vector<std::vector<double>> pair_tab_h, align_tab_h, ext_tab_h;
   AbpParams* abp = nullptr;
   bool abp_on = false;
+  // shared-memory tile variant: per-block distinct neighbour slots and the
+  // lists rewritten as positions in them (k_tile_prep), valid until the next
+  // list build
+  int* tile_n = nullptr;
+  int* tile_slot = nullptr;
+  uint16_t* nbpos = nullptr;
+  int nbpos_cap = 0;
+  bool tile_valid = false;
   int abp_variant = 1;
   // autotuner: every variant yields the same bits, so candidates are timed on
   // the run's own first steps (CUDA events around the step kernel)
   bool tuned = false;
   int tune_trial = 0;
-  double tune_ms[8] = {0};
-  int tune_n[8] = {0};
+  double tune_ms[ABP_NVARIANT] = {0};
+  int tune_n[ABP_NVARIANT] = {0};
   cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
   int hot_buf = 0;
   int force_generic = 0;  // testing aid: keep the generic SoA kernels
@@ -427,6 +440,27 @@ static int nlist_alloc(sg_system* s, int cap) {
 // was re-sorted.
 static constexpr int kSortEvery = 8;
 
+// Blocks of the flagged replicas (s->rebuild_h): the particle passes of a
+// rebuild launch over these only.  When every replica is flagged the list is
+// left null and the passes cover the whole grid.
+static int prepare_blist(sg_system* s) {
+  s->blist_h.clear();
+  bool all = true;
+  for (int r = 0; r < s->nrep; r++) {
+    if (!s->rebuild_h[r]) { all = false; continue; }
+    for (int b = 0; b < s->rep_nblk_h[r]; b++) s->blist_h.push_back(s->rep_blk0_h[r] + b);
+  }
+  s->nblist = all ? s->nblocks : (int)s->blist_h.size();
+  if (all || s->nblist == 0) return SG_OK;
+  if (!s->blist) {
+    s->blist = s->mem.alloc<int>(s->nblocks);
+    if (!s->blist) { s->mem.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "block list"); }
+  }
+  CU(s, cudaMemcpyAsync(s->blist, s->blist_h.data(), sizeof(int) * s->nblist, cudaMemcpyHostToDevice, s->stream));
+  return SG_OK;
+}
+static const int* blist_of(const sg_system* s) { return s->nblist == s->nblocks ? nullptr : s->blist; }
+
 static int rebuild_flagged(sg_system* s, bool* sorted) {
   const int nb = s->nblocks;
   s->forces_fresh = false;
@@ -439,40 +473,69 @@ static int rebuild_flagged(sg_system* s, bool* sorted) {
   }
   if (sorted) *sorted = any_sort;
   CU(s, cudaMemcpyAsync(s->rebuild, s->rebuild_h, sizeof(int) * s->nrep, cudaMemcpyHostToDevice, s->stream));
+  {
+    int rc = prepare_blist(s);
+    if (rc) return rc;
+  }
+  const int* bl = blist_of(s);
+  const int ng = s->nblist;
+  // cell ranges of the flagged replicas (the cell passes touch only these)
+  s->segs_h.clear();
+  int nvirt = 0;
+  for (int r = 0; r < s->nrep; r++) {
+    if (!s->rebuild_h[r]) continue;
+    const Replica& R = s->reps_h[r];
+    s->segs_h.push_back(CellSeg{R.cell_off, R.ncell, nvirt, 0});
+    nvirt += R.ncell;
+  }
+  const int nseg = (int)s->segs_h.size();
+  if (nseg == 0) return SG_OK;
+  CU(s, cudaMemcpyAsync(s->segs, s->segs_h.data(), sizeof(CellSeg) * nseg, cudaMemcpyHostToDevice, s->stream));
   for (int attempt = 0; attempt < 4; attempt++) {
-    CU(s, cudaMemsetAsync(s->cell_cnt, 0, sizeof(int) * (size_t)s->ncell_total, s->stream));
-    CU(s, cudaMemsetAsync(s->cell_fill, 0, sizeof(int) * (size_t)s->ncell_total, s->stream));
+    k_seg_zero<<<std::min((nvirt + 255) / 256, 148 * 16), 256, 0, s->stream>>>(s->segs, nseg, nvirt, s->cell_cnt,
+                                                                                  s->cell_fill);
+    LAUNCH_CHECK(s);
     CU(s, cudaMemsetAsync(s->status, 0, sizeof(int), s->stream));
     CU(s, cudaMemsetAsync(s->maxnb, 0, sizeof(int), s->stream));
-    k_rb_bin<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->pcell, s->cell_cnt);
+    k_rb_bin<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->pcell, s->cell_cnt, bl);
     LAUNCH_CHECK(s);
-    const int nscan = (s->ncell_total + SCAN_TILE - 1) / SCAN_TILE;
-    k_scan_a<<<nscan, SCAN_T, 0, s->stream>>>(s->cell_cnt, s->ncell_total, s->scan_bsum);
+    const int nscan = (nvirt + SCAN_TILE - 1) / SCAN_TILE;
+    k_scan_a<<<nscan, SCAN_T, 0, s->stream>>>(s->cell_cnt, nvirt, s->segs, nseg, s->scan_bsum);
     LAUNCH_CHECK(s);
     k_scan_b<<<1, SCAN_T, 0, s->stream>>>(s->scan_bsum, nscan);
     LAUNCH_CHECK(s);
-    k_scan_c<<<nscan, SCAN_T, 0, s->stream>>>(s->cell_cnt, s->ncell_total, s->scan_bsum, s->cell_start);
+    k_scan_c<<<nscan, SCAN_T, 0, s->stream>>>(s->cell_cnt, nvirt, s->segs, nseg, s->scan_bsum, s->cell_start);
     LAUNCH_CHECK(s);
-    k_rb_scatter<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->pcell, s->cell_start, s->cell_fill, s->tmp);
+    k_rb_scatter<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->pcell, s->cell_start, s->cell_fill, s->tmp,
+                                            bl);
     LAUNCH_CHECK(s);
-    k_rb_rank<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->pcell, s->cell_start, s->cell_cnt,
-                                          s->tmp, s->st.id, s->perm);
+    k_rb_rank<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->pcell, s->cell_start, s->cell_cnt,
+                                          s->tmp, s->st.id, s->perm, bl);
     LAUNCH_CHECK(s);
     if (any_sort) {
-      k_rb_gather<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->perm, s->cur, s->alt, s->st,
-                                               s->st_alt);
+      k_rb_gather<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->perm, s->cur, s->alt, s->st,
+                                               s->st_alt, bl);
       LAUNCH_CHECK(s);
-      k_rb_copyback<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->alt, s->cur, s->st_alt, s->st);
+      k_rb_copyback<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->alt, s->cur, s->st_alt, s->st, bl);
       LAUNCH_CHECK(s);
     }
-    k_rb_build<<<nb, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->st, s->nl, s->perm,
-                                           s->cell_start, s->cell_cnt, s->status, s->maxnb);
+    k_rb_build<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->st, s->nl, s->perm,
+                                           s->cell_start, s->cell_cnt, s->status, s->maxnb, bl);
     LAUNCH_CHECK(s);
     int st = 0, mx = 0;
     CU(s, cudaMemcpyAsync(&st, s->status, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     CU(s, cudaMemcpyAsync(&mx, s->maxnb, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     CU(s, cudaStreamSynchronize(s->stream));
     if (!(st & ST_OVERFLOW)) {
+      // tile data: re-derived for the rebuilt blocks (the others keep theirs);
+      // a grown list capacity invalidates every block's positions
+      if (s->tile_n && s->tile_valid) {
+        if (s->nbpos_cap < s->nl.cap) s->tile_valid = false;
+        else {
+          k_tile_prep<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->nl, s->tile_n, s->tile_slot, s->nbpos, bl);
+          LAUNCH_CHECK(s);
+        }
+      }
       s->builds_run++;
       s->maxnb_seen = std::max(s->maxnb_seen, mx);
       for (int r = 0; r < s->nrep; r++)
@@ -520,6 +583,7 @@ int sg_set_nlist(sg_system* s, double rcut, double pad) {
   s->cell_start = m.alloc<int>(cell_off);
   s->cell_fill = m.alloc<int>(cell_off);
   s->scan_bsum = m.alloc<int>((cell_off + SCAN_TILE - 1) / SCAN_TILE + 1);
+  if (!s->segs) s->segs = m.alloc<CellSeg>(s->nrep);
   if (m.err != cudaSuccess) { m.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "cell list allocation failed"); }
   int rc = push_reps(s);
   if (rc) return rc;
@@ -949,22 +1013,29 @@ static int hot_alloc(sg_system* s, int shape) {
   return SG_OK;
 }
 
-static int hot_pack(sg_system* s, int shape) {
+// whole grid, or (flagged = true) the blocks of the replicas being rebuilt
+static int hot_pack(sg_system* s, int shape, bool flagged = false) {
+  const int ng = flagged ? s->nblist : s->nblocks;
+  const int* bl = flagged ? blist_of(s) : nullptr;
+  if (ng == 0) return SG_OK;
   if (shape == HOT_PLANE)
-    k_hot_pack<HOT_PLANE><<<s->nblocks, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->st, s->G[s->hot_buf], nullptr);
+    k_hot_pack<HOT_PLANE><<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->st, s->G[s->hot_buf], nullptr, bl);
   else
-    k_hot_pack<HOT_SPHERE><<<s->nblocks, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->st, s->G[s->hot_buf],
-                                                                s->H[s->hot_buf]);
+    k_hot_pack<HOT_SPHERE><<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->st, s->G[s->hot_buf],
+                                                        s->H[s->hot_buf], bl);
   LAUNCH_CHECK(s);
   return SG_OK;
 }
 
-static int hot_unpack(sg_system* s, int shape) {
+static int hot_unpack(sg_system* s, int shape, bool flagged = false) {
+  const int ng = flagged ? s->nblist : s->nblocks;
+  const int* bl = flagged ? blist_of(s) : nullptr;
+  if (ng == 0) return SG_OK;
   if (shape == HOT_PLANE)
-    k_hot_unpack<HOT_PLANE><<<s->nblocks, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->G[s->hot_buf], nullptr);
+    k_hot_unpack<HOT_PLANE><<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->G[s->hot_buf], nullptr, bl);
   else
-    k_hot_unpack<HOT_SPHERE><<<s->nblocks, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->G[s->hot_buf],
-                                                                  s->H[s->hot_buf]);
+    k_hot_unpack<HOT_SPHERE><<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->G[s->hot_buf],
+                                                          s->H[s->hot_buf], bl);
   LAUNCH_CHECK(s);
   return SG_OK;
 }
@@ -1075,6 +1146,36 @@ static void launch_abp_staged(sg_system* s, bool apply_e1, bool last) {
       s->status, apply_e1 ? 1 : 0, last ? 1 : 0, s->epart, s->nblocks);
 }
 
+// (Re)derive the tile data from the current lists (after any list build).
+static int tile_prep(sg_system* s) {
+  DevBuf& m = s->mem;
+  if (!s->tile_n) {
+    s->tile_n = m.alloc<int>(s->nblocks);
+    s->tile_slot = m.alloc<int>((size_t)s->nblocks * TILE_MAX);
+  }
+  if (s->nbpos_cap < s->nl.cap) {
+    m.release(s->nbpos);
+    s->nbpos = m.alloc<uint16_t>((size_t)s->nl.cap * s->nl.stride);
+    s->nbpos_cap = s->nl.cap;
+  }
+  if (m.err != cudaSuccess) { m.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "tile buffers"); }
+  k_tile_prep<<<s->nblocks, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->nl, s->tile_n, s->tile_slot, s->nbpos);
+  LAUNCH_CHECK(s);
+  s->tile_valid = true;
+  return SG_OK;
+}
+
+template <int SHAPE, int ALIGN, bool SP, bool ENERGY, int MINB>
+static void launch_abp_tile(sg_system* s, bool apply_e1, bool last) {
+  const int b = s->hot_buf;  // tile data prepared by step_hot
+  constexpr size_t smem = tile_smem_bytes<SHAPE, ALIGN>();
+  static unsigned done = 0;
+  raise_smem(k_abp_tile<SHAPE, ALIGN, SP, ENERGY, MINB>, smem, &done, s->device);
+  k_abp_tile<SHAPE, ALIGN, SP, ENERGY, MINB><<<s->nblocks, BLOCK, smem, s->stream>>>(
+      s->abp, s->blk_rep, s->clk, s->G[b], s->G[1 - b], s->H[b], s->H[1 - b], s->cur, s->st, s->nl, s->rebuild,
+      s->status, apply_e1 ? 1 : 0, last ? 1 : 0, s->epart, s->nblocks, s->tile_n, s->tile_slot, s->nbpos);
+}
+
 template <int SHAPE, int ALIGN, bool SP>
 static void launch_abp3(sg_system* s, bool apply_e1, bool last, bool energy) {
   if (energy) { launch_abp_v<SHAPE, ALIGN, SP, true, 1>(s, apply_e1, last); return; }
@@ -1082,6 +1183,7 @@ static void launch_abp3(sg_system* s, bool apply_e1, bool last, bool energy) {
     case 5: launch_abp_flat<SHAPE, ALIGN, SP, false>(s, apply_e1, last); break;
     case 6: launch_abp_staged<SHAPE, ALIGN, SP, false, 4, 4>(s, apply_e1, last); break;
     case 7: launch_abp_staged<SHAPE, ALIGN, SP, false, 4, 5>(s, apply_e1, last); break;
+    case 8: launch_abp_tile<SHAPE, ALIGN, SP, false, 5>(s, apply_e1, last); break;
     case 0: launch_abp_v<SHAPE, ALIGN, SP, false, 0>(s, apply_e1, last); break;
     case 1: launch_abp_v<SHAPE, ALIGN, SP, false, 1>(s, apply_e1, last); break;
     case 2: launch_abp_v<SHAPE, ALIGN, SP, false, 2>(s, apply_e1, last); break;
@@ -1112,6 +1214,10 @@ static int step_hot(sg_system* s, int shape, bool apply_e1, bool last, bool ener
   if (tuning) {
     s->abp_variant = (s->tune_trial / (TUNE_REPS + 1)) % ABP_NVARIANT;
     CU(s, cudaEventRecord(s->ev_t0, s->stream));
+  }
+  if (s->abp_on && !energy && s->abp_variant == 8 && !s->tile_valid) {
+    int rc = tile_prep(s);
+    if (rc) return rc;
   }
   if (s->profile) CU(s, cudaEventRecord(s->ev_k0, s->stream));
   if (s->abp_on) {
@@ -1213,10 +1319,11 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
       for (int r = 0; r < s->nrep; r++) any = any || s->rebuild_h[r];
       if (any) {
         CU(s, cudaEventRecord(s->ev_b0, s->stream));
-        if (shape != HOT_NONE && !last && (rc = hot_unpack(s, shape))) return rc;
+        if ((rc = prepare_blist(s))) return rc;
+        if (shape != HOT_NONE && !last && (rc = hot_unpack(s, shape, true))) return rc;
         bool sorted = false;
         if ((rc = rebuild_flagged(s, &sorted))) return rc;
-        if (shape != HOT_NONE && !last && sorted && (rc = hot_pack(s, shape))) return rc;
+        if (shape != HOT_NONE && !last && sorted && (rc = hot_pack(s, shape, true))) return rc;
         CU(s, cudaMemsetAsync(s->rebuild, 0, sizeof(int) * s->nrep, s->stream));
         CU(s, cudaEventRecord(s->ev_b1, s->stream));
         CU(s, cudaEventSynchronize(s->ev_b1));
@@ -1316,7 +1423,7 @@ int sg_set_variant(sg_system* s, int variant) {
   if (!s || variant < -1 || variant >= ABP_NVARIANT) return SG_ERR_ARG;
   if (variant < 0) {  // re-tune on the next run
     s->tuned = false; s->tune_trial = 0;
-    for (int v = 0; v < 8; v++) { s->tune_ms[v] = 0.0; s->tune_n[v] = 0; }
+    for (int v = 0; v < ABP_NVARIANT; v++) { s->tune_ms[v] = 0.0; s->tune_n[v] = 0; }
     return SG_OK;
   }
   s->abp_variant = variant;

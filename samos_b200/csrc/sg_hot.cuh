@@ -38,9 +38,10 @@ enum { HOT_NONE = 0, HOT_PLANE = 1, HOT_SPHERE = 2 };
 // ---------------------------------------------------------------------------
 template <int SHAPE>
 __global__ void k_hot_pack(const Replica* __restrict__ reps, const int* __restrict__ blk_rep, Dyn d, Stat st,
-                           D4* __restrict__ G, D4* __restrict__ H) {
-  const Replica& R = reps[my_replica(blk_rep)];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+                           D4* __restrict__ G, D4* __restrict__ H, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const Replica& R = reps[blk_rep[bid_]];
+  const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   if (SHAPE == HOT_PLANE) {
     stg4(G + k, D4{d.x[k], d.y[k], d.nx[k], d.ny[k]});
@@ -52,9 +53,10 @@ __global__ void k_hot_pack(const Replica* __restrict__ reps, const int* __restri
 
 template <int SHAPE>
 __global__ void k_hot_unpack(const Replica* __restrict__ reps, const int* __restrict__ blk_rep, Dyn d,
-                             const D4* __restrict__ G, const D4* __restrict__ H) {
-  const Replica& R = reps[my_replica(blk_rep)];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+                             const D4* __restrict__ G, const D4* __restrict__ H, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const Replica& R = reps[blk_rep[bid_]];
+  const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   const D4 g = ldg4(G + k);
   d.x[k] = g.x; d.y[k] = g.y;

@@ -733,11 +733,12 @@ __device__ __forceinline__ int cell_of(const Replica& R, double x, double y, dou
 // populate wrap (no image update) + cell index + count
 __global__ void k_rb_bin(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                          const int* __restrict__ rebuild, Dyn d, int* __restrict__ pcell,
-                         int* __restrict__ cell_cnt) {
-  const int r = my_replica(blk_rep);
+                         int* __restrict__ cell_cnt, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const int r = blk_rep[bid_];
   if (!rebuild[r]) return;
   const Replica& R = reps[r];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   double x = d.x[k], y = d.y[k], z = d.z[k];
   if (R.periodic) {
@@ -759,14 +760,37 @@ constexpr int SCAN_T = 1024;
 constexpr int SCAN_ITEMS = 4;
 constexpr int SCAN_TILE = SCAN_T * SCAN_ITEMS;
 
-__global__ void k_scan_a(const int* __restrict__ in, int n, int* __restrict__ bsum) {
+// The scan runs over the cells of the replicas being rebuilt only: their
+// cell ranges, concatenated, form a virtual array (CellSeg.vbase = offset of
+// the range in it).  Offsets within one replica's range are what the list
+// build uses, and those are the same as in a scan over every cell.
+struct CellSeg { int cell_off, ncell, vbase, pad; };
+
+__device__ __forceinline__ int seg_cell(const CellSeg* __restrict__ segs, int nseg, int v) {
+  int lo = 0, hi = nseg - 1;  // last segment with vbase <= v
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (segs[mid].vbase <= v) lo = mid; else hi = mid - 1;
+  }
+  return segs[lo].cell_off + (v - segs[lo].vbase);
+}
+
+__global__ void k_seg_zero(const CellSeg* __restrict__ segs, int nseg, int n, int* __restrict__ a, int* __restrict__ b) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const int g = seg_cell(segs, nseg, v);
+    a[g] = 0; b[g] = 0;
+  }
+}
+
+__global__ void k_scan_a(const int* __restrict__ in, int n, const CellSeg* __restrict__ segs, int nseg,
+                         int* __restrict__ bsum) {
   __shared__ int sh[SCAN_T / 32];
   const int base = blockIdx.x * SCAN_TILE;
   int s = 0;
 #pragma unroll
   for (int i = 0; i < SCAN_ITEMS; i++) {
     int idx = base + threadIdx.x * SCAN_ITEMS + i;
-    if (idx < n) s += in[idx];
+    if (idx < n) s += in[seg_cell(segs, nseg, idx)];
   }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
@@ -816,15 +840,17 @@ __global__ void k_scan_b(int* bsum, int nb) {
   }
 }
 
-__global__ void k_scan_c(const int* __restrict__ in, int n, const int* __restrict__ bsum, int* __restrict__ out) {
+__global__ void k_scan_c(const int* __restrict__ in, int n, const CellSeg* __restrict__ segs, int nseg,
+                         const int* __restrict__ bsum, int* __restrict__ out) {
   __shared__ int shw[32];
   const int base = blockIdx.x * SCAN_TILE;
-  int v[SCAN_ITEMS];
+  int v[SCAN_ITEMS], g[SCAN_ITEMS];
   int s = 0;
 #pragma unroll
   for (int i = 0; i < SCAN_ITEMS; i++) {
     int idx = base + threadIdx.x * SCAN_ITEMS + i;
-    v[i] = idx < n ? in[idx] : 0;
+    g[i] = idx < n ? seg_cell(segs, nseg, idx) : 0;
+    v[i] = idx < n ? in[g[i]] : 0;
     s += v[i];
   }
   int tot;
@@ -832,7 +858,7 @@ __global__ void k_scan_c(const int* __restrict__ in, int n, const int* __restric
 #pragma unroll
   for (int i = 0; i < SCAN_ITEMS; i++) {
     int idx = base + threadIdx.x * SCAN_ITEMS + i;
-    if (idx < n) out[idx] = ex;
+    if (idx < n) out[g[i]] = ex;
     ex += v[i];
   }
 }
@@ -840,11 +866,12 @@ __global__ void k_scan_c(const int* __restrict__ in, int n, const int* __restric
 // unordered placement into the cell segments
 __global__ void k_rb_scatter(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                              const int* __restrict__ rebuild, const int* __restrict__ pcell,
-                             const int* __restrict__ cstart, int* __restrict__ cfill, int* __restrict__ tmp) {
-  const int r = my_replica(blk_rep);
+                             const int* __restrict__ cstart, int* __restrict__ cfill, int* __restrict__ tmp, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const int r = blk_rep[bid_];
   if (!rebuild[r]) return;
   const Replica& R = reps[r];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   const int cg = R.cell_off + pcell[k];
   const int pos = cstart[cg] - cstart[R.cell_off] + atomicAdd(&cfill[cg], 1);
@@ -855,11 +882,12 @@ __global__ void k_rb_scatter(const Replica* __restrict__ reps, const int* __rest
 __global__ void k_rb_rank(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                           const int* __restrict__ rebuild, const int* __restrict__ pcell,
                           const int* __restrict__ cstart, const int* __restrict__ ccnt,
-                          const int* __restrict__ tmp, const int* __restrict__ id, int* __restrict__ perm) {
-  const int r = my_replica(blk_rep);
+                          const int* __restrict__ tmp, const int* __restrict__ id, int* __restrict__ perm, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const int r = blk_rep[bid_];
   if (!rebuild[r]) return;
   const Replica& R = reps[r];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   const int cg = R.cell_off + pcell[k];
   const int s0 = R.off + cstart[cg] - cstart[R.cell_off];
@@ -873,11 +901,12 @@ __global__ void k_rb_rank(const Replica* __restrict__ reps, const int* __restric
 // gather all particle arrays into the permuted order (dst = src[perm])
 __global__ void k_rb_gather(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                             const int* __restrict__ rebuild, const int* __restrict__ perm,
-                            Dyn src, Dyn dst, Stat ssrc, Stat sdst) {
-  const int r = my_replica(blk_rep);
+                            Dyn src, Dyn dst, Stat ssrc, Stat sdst, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const int r = blk_rep[bid_];
   if (rebuild[r] != 2) return;
   const Replica& R = reps[r];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   const int o = perm[k];
   Part p;
@@ -889,11 +918,12 @@ __global__ void k_rb_gather(const Replica* __restrict__ reps, const int* __restr
 
 // copy back (dst -> src) for the rebuilt replicas
 __global__ void k_rb_copyback(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                              const int* __restrict__ rebuild, Dyn tmpd, Dyn d, Stat tmps, Stat st) {
-  const int r = my_replica(blk_rep);
+                              const int* __restrict__ rebuild, Dyn tmpd, Dyn d, Stat tmps, Stat st, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const int r = blk_rep[bid_];
   if (rebuild[r] != 2) return;
   const Replica& R = reps[r];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   Part p;
   load_dyn(tmpd, k, p);
@@ -932,12 +962,13 @@ __device__ __forceinline__ int build_stencil(const Replica& R, int a, int b, int
 __global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                            const int* __restrict__ rebuild, Dyn d, Stat st, NbList nl,
                            const int* __restrict__ cslot, const int* __restrict__ cstart,
-                           const int* __restrict__ ccnt, int* __restrict__ status, int* __restrict__ maxnb) {
-  const int r = my_replica(blk_rep);
+                           const int* __restrict__ ccnt, int* __restrict__ status, int* __restrict__ maxnb, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const int r = blk_rep[bid_];
   const int mode = rebuild[r];
   if (!mode) return;
   const Replica& R = reps[r];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   const double x = d.x[k], y = d.y[k], z = d.z[k];
   const int myid = st.id[k];

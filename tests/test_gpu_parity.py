@@ -254,10 +254,29 @@ def test_hot_kernels_match_generic_kernels_bitwise(shape):
         np.testing.assert_array_equal(out[2].download(f), ref, err_msg=f + " (packed vs generic)")
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
-def test_every_tuning_variant_gives_identical_bits(variant):
-    n = 3000
-    parts, L = plane_disks(n, 0.8, seed=22, bidisperse=(1.0, 1.4))
+VARIANT_CASES = {
+    # the headline program, slow motion (no rebuild in 120 steps)
+    "plane_nematic": dict(n=3000, phi=0.8, v0="0.3", dt=5e-4, steps=120, align=("nematic", {"J": "0.5"}), sp=False),
+    # fast motion: list-only rebuilds and full re-sorts (every 8th build) inside the run
+    "plane_polar_fast": dict(n=3000, phi=0.7, v0="3.0", dt=5e-3, steps=200, align=("polar", {"J": "0.2"}), sp=False),
+    # sphere with polar alignment and self-propulsion
+    "sphere_polar_sp": dict(n=3000, phi=None, v0="1.0", dt=1e-3, steps=120, align=("polar", {"J": "0.2"}), sp=True),
+}
+
+
+@pytest.mark.parametrize("case", sorted(VARIANT_CASES))
+@pytest.mark.parametrize("variant", list(range(9)))
+def test_every_tuning_variant_gives_identical_bits(variant, case):
+    c = VARIANT_CASES[case]
+    n = c["n"]
+    if c["phi"] is None:
+        parts, R = sphere_disks(n, seed=23)
+        box, periodic, cons = (2 * R + 10,) * 3, False, ("sphere", {"r": repr(R)})
+        pairs = [("soft", {"k": "10"})]
+    else:
+        parts, L = plane_disks(n, c["phi"], seed=22, bidisperse=(1.0, 1.4))
+        box, periodic, cons = (L, L, 10.0), True, ("plane", {})
+        pairs = [("soft", {"k": "10", "use_particle_radii": ""})]
     outs = []
     for v in (variant, -2):
         e = Engine(n)
@@ -265,13 +284,17 @@ def test_every_tuning_variant_gives_identical_bits(variant):
             e.set_variant(v)
         else:
             e.set_path(1)
-        sim = drive(e, parts, (L, L, 10.0), nlist=(2.8, 0.3), pairs=[("soft", {"k": "10", "use_particle_radii": ""})],
-                    aligns=[("nematic", {"J": "0.5"})], dt=5e-4,
-                    integrators=[("brownian", {"v0": "0.3", "nu": "0.1", "seed": "1"})])
-        sim.run(120)
-        outs.append(e)
-    for f in ("x", "y", "nx", "ny", "vx", "vy", "fx", "fy", "tau_z", "omega", "age", "ix", "iy"):
-        np.testing.assert_array_equal(outs[0].download(f), outs[1].download(f), err_msg=f)
+        sim = drive(e, parts, box, periodic=periodic, nlist=(2.8, 0.3), constraint=cons, pairs=pairs,
+                    aligns=[c["align"]], externals=[("self_propulsion", {"alpha": "0.5"})] if c["sp"] else [],
+                    dt=c["dt"], integrators=[("brownian", {"v0": c["v0"], "nu": "0.1", "seed": "1"})])
+        st = sim.run(c["steps"])
+        outs.append((e, st))
+    if case == "plane_polar_fast":
+        assert outs[0][1].nlist_builds >= 9  # at least one full re-sort besides list-only builds
+    fields = ["x", "y", "z", "nx", "ny", "nz", "vx", "vy", "vz", "fx", "fy", "fz", "tau_x", "tau_y", "tau_z", "omega",
+              "age", "ix", "iy"]
+    for f in fields:
+        np.testing.assert_array_equal(outs[0][0].download(f), outs[1][0].download(f), err_msg=f)
 
 
 def test_trajectory_vicsek_generic_fused_path():
