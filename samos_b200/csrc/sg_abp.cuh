@@ -312,7 +312,6 @@ k_abp_staged(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep,
              double* epart, int nblocks) {
   constexpr bool PLANE = SHAPE == HOT_PLANE;
   using SB = StagedBuf<SHAPE, ALIGN, CH>;
-  constexpr int NC = SB::NCHUNK;
   extern __shared__ __align__(16) unsigned char staged_smem[];
   SB& B = *reinterpret_cast<SB*>(staged_smem);
   __shared__ AbpParams S;

@@ -462,7 +462,6 @@ static int prepare_blist(sg_system* s) {
 static const int* blist_of(const sg_system* s) { return s->nblist == s->nblocks ? nullptr : s->blist; }
 
 static int rebuild_flagged(sg_system* s, bool* sorted) {
-  const int nb = s->nblocks;
   s->forces_fresh = false;
   bool any_sort = false;
   for (int r = 0; r < s->nrep; r++) {
