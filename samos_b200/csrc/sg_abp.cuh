@@ -192,6 +192,7 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
   __shared__ uint64_t s_base;
   __shared__ int s_step;
   const int r = blk_rep[blockIdx.x];
+  if (clk[r].halt) return;  // batched stepping: a rebuild is pending (same value for the whole block)
   {
     constexpr int NW = (int)(sizeof(AbpParams) / 8);
     static_assert(sizeof(AbpParams) % 8 == 0, "AbpParams must be 8-byte granular");
@@ -318,6 +319,7 @@ k_abp_staged(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep,
   __shared__ uint64_t s_base;
   __shared__ int s_step;
   const int r = blk_rep[blockIdx.x];
+  if (clk[r].halt) return;  // batched stepping: a rebuild is pending (same value for the whole block)
   {
     constexpr int NW = (int)(sizeof(AbpParams) / 8);
     if (threadIdx.x < NW)
@@ -533,6 +535,7 @@ k_abp_tile(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
   __shared__ uint64_t s_base;
   __shared__ int s_step;
   const int r = blk_rep[blockIdx.x];
+  if (clk[r].halt) return;  // batched stepping: a rebuild is pending (same value for the whole block)
   {
     constexpr int NW = (int)(sizeof(AbpParams) / 8);
     if (threadIdx.x < NW)
@@ -687,6 +690,7 @@ k_abp_flat(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
   __shared__ uint64_t s_base;
   __shared__ int s_step;
   const int r = blk_rep[blockIdx.x];
+  if (clk[r].halt) return;  // batched stepping: a rebuild is pending (same value for the whole block)
   {
     constexpr int NW = (int)(sizeof(AbpParams) / 8);
     if (threadIdx.x < NW)

@@ -80,7 +80,8 @@ struct Clock {
   int run_step, time_step;
   uint64_t ctr[MAX_INTEG];     // noise counter base per integrator
   double fire_dt, fire_alpha, fire_old_e;
-  int fire_last_neg, fire_converged, fire_conv_step, pad;
+  int fire_last_neg, fire_converged, fire_conv_step;
+  int halt;  // batched stepping: set after a step that flagged a rebuild; later step kernels return at once
   double fire_P, fire_F, fire_V, fire_E, fire_Fmax2;
 };
 

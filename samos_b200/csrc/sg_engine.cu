@@ -70,6 +70,9 @@ struct sg_system {
   std::vector<int> blist_h;
   int nblist = 0;
   int *rebuild = nullptr, *status = nullptr, *maxnb = nullptr;
+  int *bstatus = nullptr;   // list-build status (overflow), separate from the run's status word
+  int *exec_cnt = nullptr;  // steps executed in a batch (batched stepping)
+  int64_t since_rebuild = 0, last_gap = 8;  // batch length follows the steps between rebuilds
   int* rebuild_h = nullptr;  // pinned
   double *epart = nullptr, *fire_part = nullptr, *alpha_mix = nullptr, *Rn = nullptr;
   double dt_global = 0.0;
@@ -226,6 +229,8 @@ int sg_create(int n_replicas, const int32_t* n_particles, int ntypes, sg_system*
             alloc_stat(m, s->st, s->slots) && alloc_stat(m, s->st_alt, s->slots);
   s->rebuild = m.alloc<int>(n_replicas);
   s->status = m.alloc<int>(1);
+  s->bstatus = m.alloc<int>(1);
+  s->exec_cnt = m.alloc<int>(1);
   s->maxnb = m.alloc<int>(1);
   s->epart = m.alloc<double>((size_t)(MAX_PAIR + MAX_ALIGN) * s->nblocks);
   s->fire_part = m.alloc<double>((size_t)4 * s->nblocks);
@@ -494,7 +499,7 @@ static int rebuild_flagged(sg_system* s, bool* sorted) {
     k_seg_zero<<<std::min((nvirt + 255) / 256, 148 * 16), 256, 0, s->stream>>>(s->segs, nseg, nvirt, s->cell_cnt,
                                                                                   s->cell_fill);
     LAUNCH_CHECK(s);
-    CU(s, cudaMemsetAsync(s->status, 0, sizeof(int), s->stream));
+    CU(s, cudaMemsetAsync(s->bstatus, 0, sizeof(int), s->stream));
     CU(s, cudaMemsetAsync(s->maxnb, 0, sizeof(int), s->stream));
     k_rb_bin<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->pcell, s->cell_cnt, bl);
     LAUNCH_CHECK(s);
@@ -519,10 +524,10 @@ static int rebuild_flagged(sg_system* s, bool* sorted) {
       LAUNCH_CHECK(s);
     }
     k_rb_build<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->st, s->nl, s->perm,
-                                           s->cell_start, s->cell_cnt, s->status, s->maxnb, bl);
+                                           s->cell_start, s->cell_cnt, s->bstatus, s->maxnb, bl);
     LAUNCH_CHECK(s);
     int st = 0, mx = 0;
-    CU(s, cudaMemcpyAsync(&st, s->status, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CU(s, cudaMemcpyAsync(&st, s->bstatus, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     CU(s, cudaMemcpyAsync(&mx, s->maxnb, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     CU(s, cudaStreamSynchronize(s->stream));
     if (!(st & ST_OVERFLOW)) {
@@ -1246,6 +1251,69 @@ static int step_hot(sg_system* s, int shape, bool apply_e1, bool last, bool ener
   return SG_OK;
 }
 
+// Rebuild the lists of the replicas flagged in s->rebuild_h (already read
+// back), keeping the packed records in step (mid-run: unpack / re-pack the
+// rebuilt replicas around the build).
+static int rebuild_pending(sg_system* s, int shape, bool last, double* rebuild_ms) {
+  bool any = false;
+  for (int r = 0; r < s->nrep; r++) any = any || s->rebuild_h[r];
+  if (!any) return SG_OK;
+  s->last_gap = std::max<int64_t>(1, s->since_rebuild);
+  s->since_rebuild = 0;
+  int rc;
+  CU(s, cudaEventRecord(s->ev_b0, s->stream));
+  if ((rc = prepare_blist(s))) return rc;
+  if (shape != HOT_NONE && !last && (rc = hot_unpack(s, shape, true))) return rc;
+  bool sorted = false;
+  if ((rc = rebuild_flagged(s, &sorted))) return rc;
+  if (shape != HOT_NONE && !last && sorted && (rc = hot_pack(s, shape, true))) return rc;
+  CU(s, cudaMemsetAsync(s->rebuild, 0, sizeof(int) * s->nrep, s->stream));
+  CU(s, cudaEventRecord(s->ev_b1, s->stream));
+  CU(s, cudaEventSynchronize(s->ev_b1));
+  float bms = 0.f;
+  CU(s, cudaEventElapsedTime(&bms, s->ev_b0, s->ev_b1));
+  *rebuild_ms += bms;
+  return SG_OK;
+}
+
+// K non-final steps on the packed path, enqueued without waiting (the caller
+// keeps K at or below half the last gap between rebuilds, since a longer
+// batch would mostly enqueue halted launches, and steps one at a time when
+// that is 1): each
+// step kernel returns at once when an earlier step of the batch flagged a
+// rebuild (Clock::halt, set by k_tail_batch), so the host learns after the
+// batch how many steps ran, puts the double-buffer index right, rebuilds and
+// goes on from there.  Results are those of stepping one at a time.
+static constexpr int64_t kBatch = 32;
+
+static int run_batch(sg_system* s, int shape, int64_t K, bool needs_nl, int64_t* executed, double* rebuild_ms) {
+  const int b0 = s->hot_buf;
+  CU(s, cudaMemsetAsync(s->exec_cnt, 0, sizeof(int), s->stream));
+  for (int64_t i = 0; i < K; i++) {
+    int rc = step_hot(s, shape, true, false, false);
+    if (rc) return rc;
+    k_tail_batch<<<1, 256, 0, s->stream>>>(s->prog, s->reps, s->clk, s->nrep, s->rebuild, s->exec_cnt);
+    LAUNCH_CHECK(s);
+  }
+  int ex = 0;
+  CU(s, cudaMemcpyAsync(&ex, s->exec_cnt, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  if (needs_nl)
+    CU(s, cudaMemcpyAsync(s->rebuild_h, s->rebuild, sizeof(int) * s->nrep, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  if (ex < 1 || ex > K) return fail(s, SG_ERR_CUDA, "batched stepping: inconsistent step count");
+  s->hot_buf = b0 ^ (int)(ex & 1);
+  s->e1_applied = true;
+  *executed = ex;
+  s->since_rebuild += ex;
+  if (!needs_nl) return SG_OK;
+  bool any = false;
+  for (int r = 0; r < s->nrep; r++) any = any || s->rebuild_h[r];
+  if (!any) return SG_OK;
+  k_set_halt<<<(s->nrep + 127) / 128, 128, 0, s->stream>>>(s->clk, s->nrep, 0);
+  LAUNCH_CHECK(s);
+  return rebuild_pending(s, shape, false, rebuild_ms);
+}
+
 static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool driver, int64_t* conv_out,
                     bool cont = false) {
   if (!s || steps < 0) return SG_ERR_ARG;
@@ -1271,13 +1339,23 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
   if (!cont) {
     int rc = pull_clk(s);
     if (rc) return rc;
-    for (int r = 0; r < s->nrep; r++) s->clk_h[r].run_step = 0;
+    for (int r = 0; r < s->nrep; r++) { s->clk_h[r].run_step = 0; s->clk_h[r].halt = 0; }
     if ((rc = push_clk(s))) return rc;
   }
   int64_t done = 0;
   for (int64_t t = 0; t <= steps; t++) {
     const bool last = (t == steps);
     int rc;
+    // batched stepping: steps enqueued kBatch at a time with no host round
+    // trip, the first step that flags a rebuild halting the rest (same bits)
+    const int64_t K = std::min<int64_t>(needs_nl ? std::min<int64_t>(kBatch, s->last_gap / 2) : kBatch, steps - t);
+    if (shape != HOT_NONE && t > 0 && !last && K > 1 && !driver && !s->profile && (!s->abp_on || s->tuned)) {
+      int64_t ex = 0;
+      if ((rc = run_batch(s, shape, K, needs_nl, &ex, &rebuild_ms))) return rc;
+      done += ex;
+      t += ex - 1;
+      continue;
+    }
     if (shape != HOT_NONE) {
       if (t == 0) {
         if (!s->e1_applied) {
@@ -1311,25 +1389,11 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
       kernel_ms += ms;
       kernels_timed++;
     }
+    s->since_rebuild++;
     if (needs_nl) {
       CU(s, cudaMemcpyAsync(s->rebuild_h, s->rebuild, sizeof(int) * s->nrep, cudaMemcpyDeviceToHost, s->stream));
       CU(s, cudaStreamSynchronize(s->stream));
-      bool any = false;
-      for (int r = 0; r < s->nrep; r++) any = any || s->rebuild_h[r];
-      if (any) {
-        CU(s, cudaEventRecord(s->ev_b0, s->stream));
-        if ((rc = prepare_blist(s))) return rc;
-        if (shape != HOT_NONE && !last && (rc = hot_unpack(s, shape, true))) return rc;
-        bool sorted = false;
-        if ((rc = rebuild_flagged(s, &sorted))) return rc;
-        if (shape != HOT_NONE && !last && sorted && (rc = hot_pack(s, shape, true))) return rc;
-        CU(s, cudaMemsetAsync(s->rebuild, 0, sizeof(int) * s->nrep, s->stream));
-        CU(s, cudaEventRecord(s->ev_b1, s->stream));
-        CU(s, cudaEventSynchronize(s->ev_b1));
-        float bms = 0.f;
-        CU(s, cudaEventElapsedTime(&bms, s->ev_b0, s->ev_b1));
-        rebuild_ms += bms;
-      }
+      if ((rc = rebuild_pending(s, shape, last, &rebuild_ms))) return rc;
     }
     if (driver && ((t & 15) == 15 || t == steps)) {  // converged replicas are frozen on the device
       if ((rc = pull_clk(s))) return rc;

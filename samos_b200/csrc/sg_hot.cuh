@@ -177,6 +177,7 @@ k_hot_step(Program P, const Replica* __restrict__ reps, const int* __restrict__ 
            int* __restrict__ rebuild, int* __restrict__ status, double dt_global, int apply_e1, int last,
            double* epart, int nblocks) {
   const int r = my_replica(blk_rep);
+  if (clk[r].halt) return;  // batched stepping: a rebuild is pending
   const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
   double e[MAX_PAIR + MAX_ALIGN];

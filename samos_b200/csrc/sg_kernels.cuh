@@ -381,17 +381,47 @@ __host__ __device__ inline uint64_t langevin_draws(const IntegComp& ic, const do
 }
 
 // per-replica clock advance after one integration step
-__global__ void k_tail(Program P, const Replica* __restrict__ reps, Clock* clk, int nrep) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= nrep) return;
-  Clock& C = clk[r];
+// end-of-step bookkeeping of replica r: noise counters and step counters
+__device__ __forceinline__ void tail_one(const Program& P, const Replica& R, Clock& C) {
   for (int c = 0; c < P.ninteg; c++) {
     const IntegComp& ic = P.integ[c];
-    if (ic.kind == INT_LANGEVIN) C.ctr[c] += langevin_draws(ic, reps[r].integ_p[c], C.run_step, reps[r].n);
-    else C.ctr[c] += draws_per_call(ic, C.run_step, reps[r].n);
+    if (ic.kind == INT_LANGEVIN) C.ctr[c] += langevin_draws(ic, R.integ_p[c], C.run_step, R.n);
+    else C.ctr[c] += draws_per_call(ic, C.run_step, R.n);
   }
   C.run_step++;
   C.time_step++;
+}
+
+__global__ void k_tail(Program P, const Replica* __restrict__ reps, Clock* clk, int nrep) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrep) return;
+  tail_one(P, reps[r], clk[r]);
+}
+
+// Tail of one step of a batch enqueued without host synchronisation (one
+// block).  If an earlier step of the batch flagged a rebuild, the step just
+// enqueued did nothing (its kernel saw the halt) and neither does this.
+// Otherwise the step counts as executed, and if it flagged a rebuild every
+// replica is halted until the host has rebuilt the lists.
+__global__ void k_tail_batch(Program P, const Replica* __restrict__ reps, Clock* clk, int nrep,
+                             const int* __restrict__ rebuild, int* __restrict__ executed) {
+  __shared__ int halted, any;
+  if (threadIdx.x == 0) { halted = clk[0].halt; any = 0; }
+  __syncthreads();
+  if (halted) return;
+  for (int r = threadIdx.x; r < nrep; r += blockDim.x) {
+    tail_one(P, reps[r], clk[r]);
+    if (rebuild[r]) atomicOr(&any, 1);
+  }
+  __syncthreads();
+  if (any)
+    for (int r = threadIdx.x; r < nrep; r += blockDim.x) clk[r].halt = 1;
+  if (threadIdx.x == 0) (*executed)++;
+}
+
+__global__ void k_set_halt(Clock* clk, int nrep, int v) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < nrep) clk[r].halt = v;
 }
 
 // ---------------------------------------------------------------------------
