@@ -1010,7 +1010,9 @@ __global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restri
   unsigned long long lo[NB_LOCAL], up[NB_LOCAL];  // (id << 32) | slot
   int nlo = 0, nup = 0;
   bool overflow = false;
-  // sweep 1: lower-id neighbours (and, on the N^2 path, higher-id ones)
+  // One sweep: lower-id neighbours as (id, slot) keys, sorted below; on the
+  // cell path the higher-id ones are kept in stencil visiting order (the
+  // reference's list[i] order), on the N^2 path as keys sorted by id.
   for (int m = 0; m < ncells; m++) {
     const int cg = R.cell_off + cells[m];
     const int s0 = R.off + cstart[cg] - base0, n = ccnt[cg];
@@ -1025,10 +1027,7 @@ __global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restri
       if (dx * dx + dy * dy + dz * dz < R.cut2) {
         const unsigned long long key = ((unsigned long long)(unsigned)jid << 32) | (unsigned)j;
         if (jid < myid) { if (nlo < NB_LOCAL) lo[nlo] = key; nlo++; }
-        else {
-          if (!R.use_cell && nup < NB_LOCAL) up[nup] = key;
-          nup++;
-        }
+        else { if (nup < NB_LOCAL) up[nup] = key; nup++; }
       }
     }
   }
@@ -1039,7 +1038,7 @@ __global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restri
     atomicOr(status, ST_OVERFLOW);
     nl.cnt[k] = 0; nl.lo[k] = 0;
   } else {
-    for (int i = 1; i < nlo; i++) {  // insertion sort by id (keys are unique per duplicate-free id)
+    for (int i = 1; i < nlo; i++) {  // insertion sort by id (stable: equal ids keep their order)
       const unsigned long long v = lo[i];
       int m = i - 1;
       while (m >= 0 && (lo[m] >> 32) > (v >> 32)) { lo[m + 1] = lo[m]; m--; }
@@ -1055,8 +1054,12 @@ __global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restri
       }
       for (int q = 0; q < nup; q++)
         nl.nb[(size_t)(nlo + q) * nl.stride + k] = (int)(unsigned)(up[q] & 0xffffffffull);
+    } else if (nup <= NB_LOCAL) {
+      for (int q = 0; q < nup; q++)
+        nl.nb[(size_t)(nlo + q) * nl.stride + k] = (int)(unsigned)(up[q] & 0xffffffffull);
     } else {
-      // sweep 2: higher-id neighbours in stencil visiting order
+      // more higher-id neighbours than the local array holds: a second sweep
+      // writes them in stencil visiting order straight into the list
       int w = nlo;
       for (int m = 0; m < ncells; m++) {
         const int cg = R.cell_off + cells[m];
