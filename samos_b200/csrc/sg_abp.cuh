@@ -34,9 +34,37 @@ struct AbpParams {
 
 // Tuning variants (chunk of neighbour records fetched ahead, min blocks/SM):
 // the engine's autotuner times them on the live system and keeps the fastest.
-constexpr int ABP_NVARIANT = 9;  // 0-4 per-particle sweep, 5 flattened, 6-7 staged (cp.async), 8 shared-memory tile
-__host__ __device__ constexpr int abp_chunk(int v) { return v == 0 ? 4 : v == 1 ? 4 : v == 2 ? 2 : v == 3 ? 2 : 8; }
-__host__ __device__ constexpr int abp_minb(int v) { return v == 0 ? 5 : v == 1 ? 4 : v == 2 ? 6 : v == 3 ? 4 : 3; }
+// 0-4 per-particle sweep, 5 flattened, 6-7 staged (cp.async), 8 shared-memory
+// tile, 9-10 per-particle sweep with lanes assigned in neighbour-count order
+constexpr int ABP_NVARIANT = 11;
+__host__ __device__ constexpr int abp_chunk(int v) {
+  return v == 0 ? 4 : v == 1 ? 4 : v == 2 ? 2 : v == 3 ? 2 : v == 9 ? 2 : v == 10 ? 4 : 8;
+}
+__host__ __device__ constexpr int abp_minb(int v) {
+  return v == 0 ? 5 : v == 1 ? 4 : v == 2 ? 6 : v == 3 ? 4 : v == 9 ? 6 : v == 10 ? 5 : 3;
+}
+__host__ __device__ constexpr bool abp_ordered(int v) { return v == 9 || v == 10; }
+
+// Lane order of a block for the ordered variants: its particles sorted by
+// neighbour count, largest first (ties by slot), so each warp's 32 lanes have
+// similar list lengths and the warp's sweep is not set by one long list.
+// Padding slots go last.  Each particle's own arithmetic is unchanged.
+__global__ void __launch_bounds__(BLOCK)
+k_lane_order(const Replica* __restrict__ reps, const int* __restrict__ blk_rep, NbList nl,
+             uint8_t* __restrict__ order, const int* __restrict__ blist = nullptr) {
+  __shared__ int sc[BLOCK];
+  const int b = blist ? blist[blockIdx.x] : (int)blockIdx.x, t = threadIdx.x, k = b * BLOCK + t;
+  const Replica& R = reps[blk_rep[b]];
+  const int c = (k - R.off < R.n) ? nl.cnt[k] : -1;
+  sc[t] = c;
+  __syncthreads();
+  int rank = 0;
+  for (int u = 0; u < BLOCK; u++) {
+    const int cu = sc[u];
+    rank += (cu > c || (cu == c && u < t)) ? 1 : 0;
+  }
+  order[(size_t)b * BLOCK + rank] = (uint8_t)t;
+}
 
 // One neighbour's pair term of the specialised program: soft repulsion
 // (PairSoftPotential::compute, pair_soft_potential.cpp:79-104) and the polar /
@@ -186,7 +214,7 @@ __global__ void __launch_bounds__(BLOCK, abp_minb(VAR))
 k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, const Clock* __restrict__ clk,
            const D4* __restrict__ Gin, D4* __restrict__ Gout, const D4* __restrict__ Hin, D4* __restrict__ Hout,
            Dyn d, Stat st, NbList nl, int* __restrict__ rebuild, int* __restrict__ status, int apply_e1, int last,
-           double* epart, int nblocks) {
+           double* epart, int nblocks, const uint8_t* __restrict__ lane_order = nullptr) {
   constexpr bool PLANE = SHAPE == HOT_PLANE;
   __shared__ AbpParams S;
   __shared__ uint64_t s_base;
@@ -203,7 +231,9 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
     if (threadIdx.x == 0) { s_base = clk[r].ctr[0]; s_step = clk[r].run_step; }
   }
   __syncthreads();
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  static_assert(!(abp_ordered(VAR) && ENERGY), "the ordered variants change the block's energy summation order");
+  const int k = blockIdx.x * BLOCK +
+                (abp_ordered(VAR) ? (int)lane_order[(size_t)blockIdx.x * BLOCK + threadIdx.x] : (int)threadIdx.x);
   double epair = 0.0, ealign = 0.0;
   if (k - S.off < S.n) {
     // ---- own state ----------------------------------------------------------

@@ -101,6 +101,9 @@ struct sg_system {
   uint16_t* nbpos = nullptr;
   int nbpos_cap = 0;
   bool tile_valid = false;
+  // ordered variants: per-block lane order by neighbour count (k_lane_order)
+  uint8_t* lane_order = nullptr;
+  bool order_valid = false;
   int abp_variant = 1;
   // autotuner: every variant yields the same bits, so candidates are timed on
   // the run's own first steps (CUDA events around the step kernel)
@@ -533,6 +536,10 @@ static int rebuild_flagged(sg_system* s, bool* sorted) {
     if (!(st & ST_OVERFLOW)) {
       // tile data: re-derived for the rebuilt blocks (the others keep theirs);
       // a grown list capacity invalidates every block's positions
+      if (s->lane_order && s->order_valid) {
+        k_lane_order<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->nl, s->lane_order, bl);
+        LAUNCH_CHECK(s);
+      }
       if (s->tile_n && s->tile_valid) {
         if (s->nbpos_cap < s->nl.cap) s->tile_valid = false;
         else {
@@ -1114,7 +1121,7 @@ static void launch_abp_v(sg_system* s, bool apply_e1, bool last) {
   const int b = s->hot_buf;
   k_abp_step<SHAPE, ALIGN, SP, ENERGY, VAR><<<s->nblocks, BLOCK, 0, s->stream>>>(
       s->abp, s->blk_rep, s->clk, s->G[b], s->G[1 - b], s->H[b], s->H[1 - b], s->cur, s->st, s->nl, s->rebuild,
-      s->status, apply_e1 ? 1 : 0, last ? 1 : 0, s->epart, s->nblocks);
+      s->status, apply_e1 ? 1 : 0, last ? 1 : 0, s->epart, s->nblocks, s->lane_order);
 }
 
 // cudaFuncSetAttribute is per device: remember, per kernel, the devices it
@@ -1188,6 +1195,8 @@ static void launch_abp3(sg_system* s, bool apply_e1, bool last, bool energy) {
     case 6: launch_abp_staged<SHAPE, ALIGN, SP, false, 4, 4>(s, apply_e1, last); break;
     case 7: launch_abp_staged<SHAPE, ALIGN, SP, false, 4, 5>(s, apply_e1, last); break;
     case 8: launch_abp_tile<SHAPE, ALIGN, SP, false, 5>(s, apply_e1, last); break;
+    case 9: launch_abp_v<SHAPE, ALIGN, SP, false, 9>(s, apply_e1, last); break;
+    case 10: launch_abp_v<SHAPE, ALIGN, SP, false, 10>(s, apply_e1, last); break;
     case 0: launch_abp_v<SHAPE, ALIGN, SP, false, 0>(s, apply_e1, last); break;
     case 1: launch_abp_v<SHAPE, ALIGN, SP, false, 1>(s, apply_e1, last); break;
     case 2: launch_abp_v<SHAPE, ALIGN, SP, false, 2>(s, apply_e1, last); break;
@@ -1222,6 +1231,15 @@ static int step_hot(sg_system* s, int shape, bool apply_e1, bool last, bool ener
   if (s->abp_on && !energy && s->abp_variant == 8 && !s->tile_valid) {
     int rc = tile_prep(s);
     if (rc) return rc;
+  }
+  if (s->abp_on && !energy && abp_ordered(s->abp_variant) && !s->order_valid) {
+    if (!s->lane_order) {
+      s->lane_order = s->mem.alloc<uint8_t>((size_t)s->nblocks * BLOCK);
+      if (!s->lane_order) { s->mem.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "lane order"); }
+    }
+    k_lane_order<<<s->nblocks, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->nl, s->lane_order);
+    LAUNCH_CHECK(s);
+    s->order_valid = true;
   }
   if (s->profile) CU(s, cudaEventRecord(s->ev_k0, s->stream));
   if (s->abp_on) {
