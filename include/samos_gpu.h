@@ -38,7 +38,7 @@ enum { SG_ALIGN_POLAR = 0, SG_ALIGN_NEMATIC = 1, SG_ALIGN_VICSEK = 2 };
 enum { SG_EXT_SELF_PROPULSION = 0 };
 enum { SG_CONS_NONE = 0, SG_CONS_PLANE = 1, SG_CONS_SPHERE = 2 };
 enum { SG_INT_BROWNIAN = 0, SG_INT_BROWNIAN_POS = 1, SG_INT_BROWNIAN_ALIGN = 2,
-       SG_INT_LANGEVIN = 3, SG_INT_FIRE = 4, SG_INT_NVE = 5 };
+       SG_INT_LANGEVIN = 3, SG_INT_FIRE = 4, SG_INT_NVE = 5, SG_INT_VICSEK = 6 };
 enum { SG_VALUE_CONSTANT = 0, SG_VALUE_LINEAR = 1 };
 enum { SG_LANGEVIN_BAOAB = 0, SG_LANGEVIN_SPV = 1, SG_LANGEVIN_BBK = 2 };
 
@@ -133,6 +133,7 @@ int  sg_add_constraint_per_replica(sg_system* s, int kind, const double* params,
  *                   6 dt_inc, 7 dt_dec, 8 dt_max, 9 min_neg_steps, 11 fmax_tolerance
  *  nve            : 0 dt, 12 has_limit, 13 limit, 14 has_angle_limit, 15 angle_limit
  *                   (integrator_nve.hpp:59-75)
+ *  vicsek         : 0 dt, 1 v0, 2 eta, 3 mu, 5 seed (integrator_vicsek.hpp:55-105)
  * temperature_value = {kind, min_val, max_val, steps} (Value, value.hpp).
  * Integrators must be added in std::map key order (type + "_" + group).     */
 int  sg_add_integrator(sg_system* s, int kind, const double* params,

@@ -1135,6 +1135,7 @@ void or_compute(or_system* s, double dt)
  *  fire           : 0 dt, 1 alpha, 2 alpha_scale, 3 f_tol, 4 e_tol, 6 dt_inc,
  *                   7 dt_dec, 8 dt_max, 9 min_neg_steps, 11 fmax_tol (<=0: off)
  *  nve            : 0 dt, 12 has_limit, 13 limit, 14 has_angle_limit, 15 angle_limit
+ *  vicsek         : 0 dt, 1 v0, 2 eta, 3 mu, 5 seed
  * `tau` is the conf value; the flip probability dt/tau is formed here as in
  * integrator_brownian.hpp:139-147.
  */
@@ -1484,6 +1485,30 @@ static void integ_nve(or_system* s, or_integ* g)
   }
 }
 
+/* IntegratorVicsek::integrate, integrators/integrator_vicsek.cpp:44-82:
+ * velocity along the aligner's (normalised) torque vector plus mobility
+ * times force, a uniform random rotation of the velocity in the tangent plane
+ * of width eta*sqrt(dt), then the position update. */
+static void integ_vicsek(or_system* s, or_integ* g)
+{
+  int N = s->N;
+  double dt = g->dt, v0 = g->p[1], eta = g->p[2], mu = g->p[3];
+  double noise = eta * sqrt(dt);
+  for (int i = 0; i < N; i++) {
+    s->vx[i] = v0 * s->tx[i] + mu * s->fx[i];
+    s->vy[i] = v0 * s->ty[i] + mu * s->fy[i];
+    s->vz[i] = v0 * s->tz[i] + mu * s->fz[i];
+    enforce_one(s, i);
+    double theta = 2.0 * noise * 3.14159265358979323846 * (rng_drnd(&g->rng) - 0.5);
+    rotate_velocity(s, i, theta);
+    s->x[i] += dt * s->vx[i];
+    s->y[i] += dt * s->vy[i];
+    s->z[i] += dt * s->vz[i];
+    enforce_one(s, i);
+    s->age[i] += dt;
+  }
+}
+
 static void integrate(or_system* s, or_integ* g)
 {
   switch (g->kind) {
@@ -1499,6 +1524,7 @@ static void integrate(or_system* s, or_integ* g)
       break;
     case OR_INT_FIRE: integ_fire(s, g); break;
     case OR_INT_NVE: integ_nve(s, g); break;
+    case OR_INT_VICSEK: integ_vicsek(s, g); break;
   }
 }
 

@@ -36,7 +36,7 @@ enum { OR_ALIGN_POLAR = 0, OR_ALIGN_NEMATIC = 1, OR_ALIGN_VICSEK = 2 };
 enum { OR_EXT_SELF_PROPULSION = 0 };
 enum { OR_CONS_NONE = 0, OR_CONS_PLANE = 1, OR_CONS_SPHERE = 2 };
 enum { OR_INT_BROWNIAN = 0, OR_INT_BROWNIAN_POS = 1, OR_INT_BROWNIAN_ALIGN = 2,
-       OR_INT_LANGEVIN = 3, OR_INT_FIRE = 4, OR_INT_NVE = 5 };
+       OR_INT_LANGEVIN = 3, OR_INT_FIRE = 4, OR_INT_NVE = 5, OR_INT_VICSEK = 6 };
 enum { OR_VALUE_CONSTANT = 0, OR_VALUE_LINEAR = 1 };
 enum { OR_LANGEVIN_BAOAB = 0, OR_LANGEVIN_SPV = 1, OR_LANGEVIN_BBK = 2 };
 

@@ -26,7 +26,7 @@ constexpr int BLOCK = 128;          // particle slots per block; replicas are pa
 enum { PAIR_SOFT = 0, PAIR_LJ = 1, PAIR_MORSE = 2, PAIR_GAUSSIAN = 3 };
 enum { ALIGN_POLAR = 0, ALIGN_NEMATIC = 1, ALIGN_VICSEK = 2 };
 enum { CONS_NONE = 0, CONS_PLANE = 1, CONS_SPHERE = 2 };
-enum { INT_BROWNIAN = 0, INT_BROWNIAN_POS = 1, INT_BROWNIAN_ALIGN = 2, INT_LANGEVIN = 3, INT_FIRE = 4, INT_NVE = 5 };
+enum { INT_BROWNIAN = 0, INT_BROWNIAN_POS = 1, INT_BROWNIAN_ALIGN = 2, INT_LANGEVIN = 3, INT_FIRE = 4, INT_NVE = 5, INT_VICSEK = 6 };
 enum { LANGEVIN_BAOAB = 0, LANGEVIN_SPV = 1, LANGEVIN_BBK = 2 };
 
 // device status word bits

@@ -748,7 +748,7 @@ int sg_add_constraint(sg_system* s, int kind, const double* params) {
 }
 
 int sg_add_integrator(sg_system* s, int kind, const double* params, const double* temp) {
-  if (!s || !params || kind < SG_INT_BROWNIAN || kind > SG_INT_NVE) return fail(s, SG_ERR_ARG, "sg_add_integrator: bad kind");
+  if (!s || !params || kind < SG_INT_BROWNIAN || kind > SG_INT_VICSEK) return fail(s, SG_ERR_ARG, "sg_add_integrator: bad kind");
   Program& P = s->prog;
   if (P.ninteg >= MAX_INTEG) return fail(s, SG_ERR_ARG, "too many integrators");
   if (!(params[0] > 0.0)) return fail(s, SG_ERR_ARG, "integrator step size has to be larger than 0");
@@ -911,7 +911,8 @@ int sg_compute(sg_system* s, double dt) {
 
 static bool fused_program(const Program& P) {
   for (int c = 0; c < P.ninteg; c++)
-    if (P.integ[c].kind != INT_BROWNIAN && P.integ[c].kind != INT_BROWNIAN_POS && P.integ[c].kind != INT_BROWNIAN_ALIGN)
+    if (P.integ[c].kind != INT_BROWNIAN && P.integ[c].kind != INT_BROWNIAN_POS && P.integ[c].kind != INT_BROWNIAN_ALIGN &&
+        P.integ[c].kind != INT_VICSEK)
       return false;
   return true;
 }
@@ -1004,6 +1005,8 @@ static int hot_shape(const sg_system* s) {
   if (s->force_generic == 1 || !fused_program(P) || P.ncons != 1) return HOT_NONE;
   for (int c = 0; c < P.nalign; c++)
     if (P.align[c].kind == ALIGN_VICSEK) return HOT_NONE;
+  for (int c = 0; c < P.ninteg; c++)
+    if (P.integ[c].kind == INT_VICSEK) return HOT_NONE;  // generic fused kernel only
   for (int c = 0; c < P.npair; c++)
     if (P.pair[c].phase_in) return HOT_NONE;
   if (P.cons[0].kind == CONS_PLANE) {

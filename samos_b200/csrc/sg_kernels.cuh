@@ -239,6 +239,25 @@ __device__ __forceinline__ void integ_brownian_align(const Program& P, const Rep
   rotate_director(P, R, p, dtheta);
 }
 
+// IntegratorVicsek::integrate, integrators/integrator_vicsek.cpp:44-82: the
+// velocity follows the (normalised) Vicsek torque vector, v0 tau + mu F, and
+// is turned by a uniform angle of width eta sqrt(dt); one uniform draw per
+// particle.
+__device__ __forceinline__ void integ_vicsek(const Program& P, const Replica& R, const double* ip, uint32_t seed,
+                                             uint64_t base, Part& p) {
+  const double dt = ip[0], v0 = ip[1], eta = ip[2], mu = ip[3];
+  const double noise = eta * sqrt(dt);
+  p.vx = v0 * p.tx + mu * p.fx;
+  p.vy = v0 * p.ty + mu * p.fy;
+  p.vz = v0 * p.tz + mu * p.fz;
+  enforce_all(P, R, p);
+  const double theta = 2.0 * noise * 3.14159265358979323846 * (noise_uniform(seed, base + (uint64_t)p.id) - 0.5);
+  rotate_velocity(P, R, p, theta);
+  p.x += dt * p.vx; p.y += dt * p.vy; p.z += dt * p.vz;
+  enforce_all(P, R, p);
+  p.age += dt;
+}
+
 // noise draws consumed per call by integrator c of a replica of n particles
 __host__ __device__ inline uint64_t draws_per_call(const IntegComp& ic, int run_step, int n) {
   double T = value_get(ic.temp, run_step);
@@ -246,6 +265,7 @@ __host__ __device__ inline uint64_t draws_per_call(const IntegComp& ic, int run_
     case INT_BROWNIAN: return (uint64_t)n * ((ic.nematic ? 1u : 0u) + (T > 0.0 ? 4u : 1u));
     case INT_BROWNIAN_POS: return T > 0.0 ? (uint64_t)n * 3u : 0u;
     case INT_BROWNIAN_ALIGN: return (uint64_t)n * ((ic.nematic ? 1u : 0u) + 1u);
+    case INT_VICSEK: return (uint64_t)n;
     default: return 0u;
   }
 }
@@ -345,6 +365,8 @@ k_step_brownian(Program P, const Replica* __restrict__ reps, const int* __restri
         integ_brownian_pos(P, R, ic, R.integ_p[c], R.seed[c], base, run_step, p);
       else if (ic.kind == INT_BROWNIAN_ALIGN)
         integ_brownian_align(P, R, ic, R.integ_p[c], R.seed[c], base, R.n, p);
+      else if (ic.kind == INT_VICSEK)
+        integ_vicsek(P, R, R.integ_p[c], R.seed[c], base, p);
     }
     if (need_update(R, nl, k, p)) {
       if (rebuild[r] == 0) atomicOr(&rebuild[r], 1);

@@ -19,7 +19,7 @@ PAIR = {"soft": 0, "lj": 1, "morse": 2, "gaussian": 3}
 ALIGN = {"polar": 0, "nematic": 1, "vicsek": 2}
 EXTERNAL = {"self_propulsion": 0}
 CONSTRAINT = {"none": 0, "plane": 1, "sphere": 2}
-INTEGRATOR = {"brownian": 0, "brownian_pos": 1, "brownian_align": 2, "langevin": 3, "fire": 4, "nve": 5}
+INTEGRATOR = {"brownian": 0, "brownian_pos": 1, "brownian_align": 2, "langevin": 3, "fire": 4, "nve": 5, "vicsek": 6}
 PAIR_NPARAM = 8
 INT_NPARAM = 16
 

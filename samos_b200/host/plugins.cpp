@@ -235,6 +235,9 @@ IntegratorSpec resolve_integrator(const std::string& name, const Params& p, doub
     q[6] = get(p, "dt_inc", 1.1); q[7] = get(p, "dt_dec", 0.5); q[8] = get(p, "dt_max", 1.0);
     q[9] = has(p, "min_neg_steps") ? (double)to_int("min_neg_steps", p.at("min_neg_steps")) : 5.0;
     q[11] = get(p, "fmax_tolerance", 0.0);
+  } else if (name == "vicsek") {  // integrator_vicsek.hpp:55-105 (no params_ok there)
+    s.kind = SG_INT_VICSEK;
+    q[1] = get(p, "v0", 1.0); q[2] = get(p, "eta", 0.1); q[3] = get(p, "mu", 0.0); q[5] = seed();
   } else if (name == "nve") {  // integrator_nve.hpp:59-75 (no params_ok there)
     s.kind = SG_INT_NVE;
     if (has(p, "limit")) { q[12] = 1.0; q[13] = get(p, "limit", 0.0); }

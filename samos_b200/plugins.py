@@ -260,6 +260,9 @@ def resolve_integrator(name: str, params: dict, dt_global: float) -> tuple[int, 
         p[6] = _f(params, "dt_inc", 1.1); p[7] = _f(params, "dt_dec", 0.5)
         p[8] = _f(params, "dt_max", 1.0); p[9] = float(int(params["min_neg_steps"])) if "min_neg_steps" in params else 5.0
         p[11] = _f(params, "fmax_tolerance", 0.0)
+    elif name == "vicsek":  # integrator_vicsek.hpp:55-105 (no params_ok there)
+        p[1] = _f(params, "v0", 1.0); p[2] = _f(params, "eta", 0.1); p[3] = _f(params, "mu", 0.0)
+        p[5] = float(int(params["seed"])) if "seed" in params else 0.0
     elif name == "nve":  # integrator_nve.hpp:59-75 (no params_ok there)
         if "limit" in params:
             p[12], p[13] = 1.0, float(params["limit"])

@@ -297,6 +297,20 @@ def test_every_tuning_variant_gives_identical_bits(variant, case):
         np.testing.assert_array_equal(outs[0][0].download(f), outs[1][0].download(f), err_msg=f)
 
 
+def test_trajectory_vicsek_model():
+    # the Vicsek integrator with the Vicsek aligner (and a soft repulsion
+    # through the mobility), on the generic fused kernel
+    n = 1500
+    parts, L = plane_disks(n, 0.4, seed=14)
+    rng = np.random.default_rng(14)
+    th = rng.uniform(0, 2 * np.pi, n)
+    parts["vx"], parts["vy"] = np.cos(th), np.sin(th)
+    e, o = run_both(n, parts, (L, L, 10.0), 299, nlist=(2.4, 0.3),
+                    pairs=[("soft", {"k": "10", "use_particle_radii": ""})], aligns=[("vicsek", {"rcut": "2.0"})],
+                    dt=1e-2, integrators=[("vicsek", {"v0": "0.5", "eta": "0.3", "mu": "0.1", "seed": "5"})])
+    assert_traj(e, o, ("x", "y", "vx", "vy"))
+
+
 def test_trajectory_vicsek_generic_fused_path():
     n = 1200
     parts, L = plane_disks(n, 0.5, seed=12)

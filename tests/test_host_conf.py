@@ -128,6 +128,18 @@ def test_command_order_rules(tmp_path):
     assert r.returncode == 1 and "non-existent integrator" in r.stderr
 
 
+def test_vicsek_and_nve_integrators_parse(tmp_path):
+    conf = CONF.replace("integrator brownian_pos { seed = 7; mu = 1.0 }\nintegrator brownian_align { seed = 8; nu = 0.1, mur = 1.0 }\n",
+                        "integrator vicsek { v0 = 0.5; eta = 0.3; seed = 2 }\n")
+    r = check(tmp_path, conf)
+    assert r.returncode == 0, r.stderr
+    row = parse_describe(r.stdout)["integrator"][0]
+    _, p, _ = PL.resolve_integrator("vicsek", {"v0": "0.5", "eta": "0.3", "seed": "2"}, 1e-3)
+    assert row[0] == "vicsek_all" and [float(v) for v in row[2:]] == list(p[:12])
+    r = check(tmp_path, conf + "disable vicsek { }\nintegrator nve { limit = 0.001 }\nrun 5\n")
+    assert r.returncode == 0, r.stderr
+
+
 def test_old_input_formats(tmp_path):
     parts, _ = plane_parts(50)
     for style in ("hash", "old"):

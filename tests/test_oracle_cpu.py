@@ -197,3 +197,19 @@ def test_nve_without_limit_is_velocity_verlet():
     x, vx = o.download("x"), o.download("vx")
     assert x[0] < 0.0 < 1.5 < x[1]
     assert vx[0] == -vx[1]  # momentum conserved exactly by the symmetric update
+
+
+def test_vicsek_integrator_follows_the_aligned_velocity():
+    # integrator_vicsek.cpp:62-80 with eta = 0: v = v0 tau, tau the normalised
+    # sum of the velocities around (here the particle's own, (3, 4) -> (0.6, 0.8))
+    parts, box = two(8.0)
+    parts["vx"] = np.array([3.0, 0.0]); parts["vy"] = np.array([4.0, 1.0]); parts["vz"] = np.zeros(2)
+    o = OracleSystem(2)
+    sim = drive(o, parts, box, constraint=("plane", {}), aligns=[("vicsek", {"rcut": "1.0"})], dt=0.1,
+                integrators=[("vicsek", {"v0": "0.5", "eta": "0", "seed": "3"})])
+    sim.run(0)
+    assert o.download("vx")[0] == pytest.approx(0.3, abs=1e-15)
+    assert o.download("vy")[0] == pytest.approx(0.4, abs=1e-15)
+    assert o.download("x")[0] == pytest.approx(0.03, abs=1e-15)
+    assert o.download("y")[0] == pytest.approx(0.04, abs=1e-15)
+    assert o.download("y")[1] == pytest.approx(0.05, abs=1e-15)  # (0, 1) -> v0 * (0, 1) * dt
