@@ -260,12 +260,28 @@ def dist_env():
     return ws, rank, local
 
 
+def pg_backend():
+    """NCCL between the GPUs of a node; gloo where no GPU is visible (the
+    multi-process plumbing is exercised on CPU that way)."""
+    import torch
+    return "nccl" if torch.cuda.is_available() else "gloo"
+
+
+def init_ranks(local):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    dist.init_process_group(pg_backend(), timeout=timedelta(seconds=120))
+
+
 def max_over_ranks(x, ws):
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -309,11 +325,7 @@ def main():
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if ws > 1:
-        import torch
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        init_ranks(local)
     if args.impl == "reference":
         rc = run_reference_arm(args, ws, rank)
         if ws > 1:

@@ -69,6 +69,10 @@ struct sg_system {
   int* blist = nullptr;               // blocks of the replicas being rebuilt (null: every block)
   std::vector<int> blist_h;
   int nblist = 0;
+  // minimiser: blocks of the replicas that have not converged (null: every block)
+  int* act = nullptr;
+  std::vector<int> act_h;
+  int nact = 0;
   int *rebuild = nullptr, *status = nullptr, *maxnb = nullptr;
   int *bstatus = nullptr;   // list-build status (overflow), separate from the run's status word
   int *exec_cnt = nullptr;  // steps executed in a batch (batched stepping)
@@ -888,13 +892,15 @@ int sg_enforce(sg_system* s) {
   return SG_OK;
 }
 
-static int launch_force(sg_system* s, double dt, bool fire_dt, bool with_pair, bool with_align, bool energy) {
+static int launch_force(sg_system* s, double dt, bool fire_dt, bool with_pair, bool with_align, bool energy,
+                        int ng = -1, const int* bl = nullptr) {
+  if (ng < 0) ng = s->nblocks;
   if (energy)
-    k_force<true><<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, s->nl, dt,
-                                                       fire_dt, with_pair, with_align, s->epart, s->nblocks);
+    k_force<true><<<ng, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, s->nl, dt,
+                                               fire_dt, with_pair, with_align, s->epart, s->nblocks, bl);
   else
-    k_force<false><<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, s->nl, dt,
-                                                        fire_dt, with_pair, with_align, s->epart, s->nblocks);
+    k_force<false><<<ng, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, s->nl, dt,
+                                                fire_dt, with_pair, with_align, s->epart, s->nblocks, bl);
   LAUNCH_CHECK(s);
   return SG_OK;
 }
@@ -934,13 +940,18 @@ static bool fire_forces_reusable(const sg_system* s) {
 
 static int step_unfused(sg_system* s, bool energy, bool driver) {
   const int nb = s->nblocks;
+  // the minimiser launches the per-particle passes over the blocks of the
+  // replicas still running (converged replicas are frozen, their blocks would
+  // only return)
+  const int* al = driver && s->nact < nb ? s->act : nullptr;
+  const int na = driver ? s->nact : nb;
   if (!s->e1_applied) {  // samos.cpp:887-888 (already applied by sg_begin_step)
-    k_enforce<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, driver ? s->clk : nullptr);
+    k_enforce<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, driver ? s->clk : nullptr, al);
     LAUNCH_CHECK(s);
   }
   int rc = SG_OK;
   if (!(s->forces_fresh && fire_forces_reusable(s)))
-    if ((rc = launch_force(s, s->dt_global, false, true, true, energy))) return rc;
+    if ((rc = launch_force(s, s->dt_global, false, true, true, energy, na, al))) return rc;
   s->forces_fresh = false;
   for (int c = 0; c < s->prog.ninteg; c++) {
     const IntegComp& ic = s->prog.integ[c];
@@ -957,24 +968,24 @@ static int step_unfused(sg_system* s, bool energy, bool driver) {
       k_nve_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, c);
       LAUNCH_CHECK(s);
     } else if (ic.kind == INT_FIRE) {
-      k_fire_a<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st);
+      k_fire_a<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, al);
       LAUNCH_CHECK(s);
-      if ((rc = launch_force(s, 0.0, true, true, true, true))) return rc;
+      if ((rc = launch_force(s, 0.0, true, true, true, true, na, al))) return rc;
       s->forces_fresh = true;
-      k_fire_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, s->fire_part, nb);
+      k_fire_b<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, s->fire_part, nb, al);
       LAUNCH_CHECK(s);
       k_fire_c<<<(s->nrep + 127) / 128, 128, 0, s->stream>>>(s->prog, s->reps, s->clk, s->rep_blk0, s->rep_nblk,
                                                              s->fire_part, s->epart, nb, s->nrep, c, driver ? 1 : 0,
                                                              s->alpha_mix);
       LAUNCH_CHECK(s);
-      k_fire_d<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alpha_mix);
+      k_fire_d<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alpha_mix, al);
       LAUNCH_CHECK(s);
     } else {
       return fail(s, SG_ERR_UNSUPPORTED, "mixing Brownian-family integrators with Langevin/FIRE is not supported");
     }
   }
   if (s->has_nlist) {
-    k_skin<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->nl, s->rebuild, s->status);
+    k_skin<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->nl, s->rebuild, s->status, al);
     LAUNCH_CHECK(s);
   }
   return SG_OK;
@@ -1335,6 +1346,22 @@ static int run_batch(sg_system* s, int shape, int64_t K, bool needs_nl, int64_t*
   return rebuild_pending(s, shape, false, rebuild_ms);
 }
 
+// Blocks of the replicas whose minimiser has not converged (from clk_h).
+static int refresh_active(sg_system* s) {
+  s->act_h.clear();
+  for (int r = 0; r < s->nrep; r++)
+    if (s->clk_h[r].fire_conv_step < 0)
+      for (int b = 0; b < s->rep_nblk_h[r]; b++) s->act_h.push_back(s->rep_blk0_h[r] + b);
+  s->nact = (int)s->act_h.size();
+  if (s->nact == s->nblocks || s->nact == 0) return SG_OK;
+  if (!s->act) {
+    s->act = s->mem.alloc<int>(s->nblocks);
+    if (!s->act) { s->mem.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "active block list"); }
+  }
+  CU(s, cudaMemcpyAsync(s->act, s->act_h.data(), sizeof(int) * s->nact, cudaMemcpyHostToDevice, s->stream));
+  return SG_OK;
+}
+
 static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool driver, int64_t* conv_out,
                     bool cont = false) {
   if (!s || steps < 0) return SG_ERR_ARG;
@@ -1421,6 +1448,7 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
       bool all = true;
       for (int r = 0; r < s->nrep; r++) all = all && s->clk_h[r].fire_conv_step >= 0;
       if (all) break;
+      if ((rc = refresh_active(s))) return rc;
     }
   }
   CU(s, cudaEventRecord(s->ev_run1, s->stream));
@@ -1465,6 +1493,7 @@ int sg_minimize(sg_system* s, int64_t max_steps, int64_t* converged, sg_run_stat
   for (int r = 0; r < s->nrep; r++) s->clk_h[r].fire_conv_step = -1;
   rc = push_clk(s);
   if (rc) return rc;
+  s->nact = s->nblocks;
   return run_impl(s, max_steps, stats, true, converged);
 }
 

@@ -136,7 +136,7 @@ __device__ void compute_ft(const Program& P, const Replica& R, const Dyn& d, con
 
 // block reduction of up to NV doubles into out[v * nblocks + blockIdx.x]
 template <int NV>
-__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out, int nblocks) {
+__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out, int nblocks, int slot = -1) {
   __shared__ double sh[NV][BLOCK / 32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
@@ -149,7 +149,7 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out,
   if (threadIdx.x < NV) {
     double s = 0.0;
     for (int i = 0; i < BLOCK / 32; i++) s += sh[threadIdx.x][i];
-    out[(size_t)threadIdx.x * nblocks + blockIdx.x] = s;
+    out[(size_t)threadIdx.x * nblocks + (slot < 0 ? (int)blockIdx.x : slot)] = s;
   }
 }
 
@@ -293,10 +293,11 @@ __device__ __forceinline__ bool finite3(double a, double b, double c) {
 
 // Constrainer::enforce on every particle (samos.cpp:887-888)
 __global__ void k_enforce(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                          Dyn d, Stat st, const Clock* __restrict__ frozen) {
-  const int r = my_replica(blk_rep);
+                          Dyn d, Stat st, const Clock* __restrict__ frozen, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const int r = blk_rep[bid_];
   const Replica& R = reps[r];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   if (frozen && frozen[r].fire_conv_step >= 0) return;  // minimiser stopped this replica
   Part p;
@@ -311,14 +312,15 @@ __global__ void k_enforce(Program P, const Replica* __restrict__ reps, const int
 template <bool ENERGY>
 __global__ void k_force(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                         const Clock* __restrict__ clk, Dyn d, Stat st, NbList nl, double dt,
-                        int use_fire_dt, int with_pair, int with_align, double* epart, int nblocks) {
-  const int r = my_replica(blk_rep);
+                        int use_fire_dt, int with_pair, int with_align, double* epart, int nblocks, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const int r = blk_rep[bid_];
   const Replica& R = reps[r];
   if (use_fire_dt) {
     if (clk[r].fire_conv_step >= 0) return;  // converged replica: whole block exits (partials kept)
     dt = clk[r].fire_dt;
   }
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  const int k = bid_ * BLOCK + threadIdx.x;
   double e[MAX_PAIR + MAX_ALIGN];
 #pragma unroll
   for (int i = 0; i < MAX_PAIR + MAX_ALIGN; i++) e[i] = 0.0;
@@ -332,7 +334,7 @@ __global__ void k_force(Program P, const Replica* __restrict__ reps, const int* 
     if (with_pair) { d.fx[k] = me.fx; d.fy[k] = me.fy; d.fz[k] = me.fz; }
     if (with_align) { d.tx[k] = me.tx; d.ty[k] = me.ty; d.tz[k] = me.tz; }
   }
-  if (ENERGY) block_reduce_store<MAX_PAIR + MAX_ALIGN>(e, epart, nblocks);
+  if (ENERGY) block_reduce_store<MAX_PAIR + MAX_ALIGN>(e, epart, nblocks, bid_);
 }
 
 // Fused Brownian-family step: F, tau from the current buffer, integrators in
@@ -380,10 +382,11 @@ k_step_brownian(Program P, const Replica* __restrict__ reps, const int* __restri
 
 // Skin test over all particles of the current buffer (unfused path)
 __global__ void k_skin(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                       Dyn d, NbList nl, int* __restrict__ rebuild, int* __restrict__ status) {
-  const int r = my_replica(blk_rep);
+                       Dyn d, NbList nl, int* __restrict__ rebuild, int* __restrict__ status, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const int r = blk_rep[bid_];
   const Replica& R = reps[r];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   Part p;
   p.x = d.x[k]; p.y = d.y[k]; p.z = d.z[k];
@@ -637,10 +640,11 @@ __global__ void k_nve_b(Program P, const Replica* __restrict__ reps, const int* 
 // ---------------------------------------------------------------------------
 // first half: half kick, drift, enforce, omega, director rotation (49-66)
 __global__ void k_fire_a(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                         const Clock* __restrict__ clk, Dyn d, Stat st) {
-  const int r = my_replica(blk_rep);
+                         const Clock* __restrict__ clk, Dyn d, Stat st, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const int r = blk_rep[bid_];
   const Replica& R = reps[r];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   if (clk[r].fire_conv_step >= 0) return;  // frozen after convergence (driver mode)
   Part p;
@@ -659,10 +663,11 @@ __global__ void k_fire_a(Program P, const Replica* __restrict__ reps, const int*
 
 // second half kick + P, |F|^2, |v|^2, max|F|^2 partials (79-94)
 __global__ void k_fire_b(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                         const Clock* __restrict__ clk, Dyn d, Stat st, double* part, int nblocks) {
-  const int r = my_replica(blk_rep);
+                         const Clock* __restrict__ clk, Dyn d, Stat st, double* part, int nblocks, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const int r = blk_rep[bid_];
   const Replica& R = reps[r];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  const int k = bid_ * BLOCK + threadIdx.x;
   double v[3] = {0.0, 0.0, 0.0};
   double fmax2 = 0.0;
   const bool frozen = clk[r].fire_conv_step >= 0;
@@ -681,7 +686,7 @@ __global__ void k_fire_b(Program P, const Replica* __restrict__ reps, const int*
     p.omega += dt_2 * project_torque(P, R, p);
     store_dyn(d, k, p);
   }
-  block_reduce_store<3>(v, part, nblocks);
+  block_reduce_store<3>(v, part, nblocks, bid_);
   // max reduction (exact in any order)
   for (int o = 16; o > 0; o >>= 1) fmax2 = fmax(fmax2, __shfl_down_sync(0xffffffffu, fmax2, o));
   __shared__ double shm[BLOCK / 32];
@@ -690,7 +695,7 @@ __global__ void k_fire_b(Program P, const Replica* __restrict__ reps, const int*
   if (threadIdx.x == 0) {
     double m = 0.0;
     for (int i = 0; i < BLOCK / 32; i++) m = fmax(m, shm[i]);
-    part[(size_t)3 * nblocks + blockIdx.x] = m;
+    part[(size_t)3 * nblocks + bid_] = m;
   }
 }
 
@@ -749,10 +754,11 @@ __global__ void k_fire_c(Program P, const Replica* __restrict__ reps, Clock* clk
 // FIRE velocity mixing (110-121) with the pre-update alpha, then the
 // P <= 0 restart that zeroes the velocities (131-142).
 __global__ void k_fire_d(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                         const Clock* __restrict__ clk, Dyn d, const double* alpha_mix) {
-  const int r = my_replica(blk_rep);
+                         const Clock* __restrict__ clk, Dyn d, const double* alpha_mix, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const int r = blk_rep[bid_];
   const Replica& R = reps[r];
-  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   const Clock& C = clk[r];
   if (C.fire_converged || C.fire_conv_step >= 0) return;

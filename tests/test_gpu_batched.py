@@ -54,3 +54,25 @@ def test_batched_replica_matches_oracle():
     for f in ("x", "y", "z", "nx", "ny", "nz"):
         err = np.max(np.abs(batched.download(f, replica=1) - o.download(f)))
         assert err <= 1e-9, (f, err)
+
+
+def test_batched_fire_matches_one_at_a_time():
+    # replicas converge at different iterations; the minimiser then launches
+    # only the blocks of the replicas still running: results must be those of
+    # each replica minimised alone
+    from samos_b200.ensemble import plane_fire_ensemble, quench_disks
+    insts = [quench_disks(n, phi, seed) for n, phi, seed in ((300, 0.85, 1), (520, 0.88, 2), (800, 0.86, 3),
+                                                            (256, 0.90, 4))]
+    eng = plane_fire_ensemble(insts, fmax=1e-10)
+    eng.build_nlist()
+    conv, _ = eng.minimize(400000)
+    assert (conv > 0).all() and len(set(conv.tolist())) > 1
+    for r, inst in enumerate(insts):
+        one = plane_fire_ensemble([inst], fmax=1e-10)
+        one.build_nlist()
+        c1, _ = one.minimize(400000)
+        assert c1[0] == conv[r]
+        for f in ("x", "y", "vx", "vy"):
+            np.testing.assert_array_equal(one.download(f), eng.download(f, replica=r), err_msg=f"{f} replica {r}")
+        one.close()
+    eng.close()
