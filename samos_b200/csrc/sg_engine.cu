@@ -1362,6 +1362,46 @@ static int refresh_active(sg_system* s) {
   return SG_OK;
 }
 
+// The minimiser's iterations, K at a time with no host round trip between
+// them (same halt mechanism as run_batch: an iteration whose skin test flags a
+// rebuild halts the ones enqueued after it).  Afterwards the host rebuilds if
+// needed and polls convergence; *all_done reports that every replica has
+// converged.
+static int run_fire_batch(sg_system* s, int64_t K, bool needs_nl, int64_t* executed, double* rebuild_ms,
+                          bool* all_done) {
+  CU(s, cudaMemsetAsync(s->exec_cnt, 0, sizeof(int), s->stream));
+  for (int64_t i = 0; i < K; i++) {
+    int rc = step_unfused(s, false, true);
+    if (rc) return rc;
+    k_tail_batch<<<1, 256, 0, s->stream>>>(s->prog, s->reps, s->clk, s->nrep, s->rebuild, s->exec_cnt);
+    LAUNCH_CHECK(s);
+  }
+  int ex = 0;
+  CU(s, cudaMemcpyAsync(&ex, s->exec_cnt, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  if (needs_nl)
+    CU(s, cudaMemcpyAsync(s->rebuild_h, s->rebuild, sizeof(int) * s->nrep, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  if (ex < 1 || ex > K) return fail(s, SG_ERR_CUDA, "batched iterations: inconsistent step count");
+  *executed = ex;
+  s->since_rebuild += ex;
+  s->e1_applied = false;
+  int rc;
+  if (needs_nl) {
+    bool any = false;
+    for (int r = 0; r < s->nrep; r++) any = any || s->rebuild_h[r];
+    if (any) {
+      k_set_halt<<<(s->nrep + 127) / 128, 128, 0, s->stream>>>(s->clk, s->nrep, 0);
+      LAUNCH_CHECK(s);
+      if ((rc = rebuild_pending(s, HOT_NONE, false, rebuild_ms))) return rc;
+    }
+  }
+  if ((rc = pull_clk(s))) return rc;
+  bool all = true;
+  for (int r = 0; r < s->nrep; r++) all = all && s->clk_h[r].fire_conv_step >= 0;
+  *all_done = all;
+  return all ? SG_OK : refresh_active(s);
+}
+
 static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool driver, int64_t* conv_out,
                     bool cont = false) {
   if (!s || steps < 0) return SG_ERR_ARG;
@@ -1397,6 +1437,15 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
     // batched stepping: steps enqueued kBatch at a time with no host round
     // trip, the first step that flags a rebuild halting the rest (same bits)
     const int64_t K = std::min<int64_t>(needs_nl ? std::min<int64_t>(kBatch, s->last_gap / 2) : kBatch, steps - t);
+    if (driver && t > 0 && !last && K > 1 && !s->profile) {
+      int64_t ex = 0;
+      bool all = false;
+      if ((rc = run_fire_batch(s, std::min<int64_t>(K, 16), needs_nl, &ex, &rebuild_ms, &all))) return rc;
+      done += ex;
+      t += ex - 1;
+      if (all) break;
+      continue;
+    }
     if (shape != HOT_NONE && t > 0 && !last && K > 1 && !driver && !s->profile && (!s->abp_on || s->tuned)) {
       int64_t ex = 0;
       if ((rc = run_batch(s, shape, K, needs_nl, &ex, &rebuild_ms))) return rc;

@@ -299,7 +299,7 @@ __global__ void k_enforce(Program P, const Replica* __restrict__ reps, const int
   const Replica& R = reps[r];
   const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
-  if (frozen && frozen[r].fire_conv_step >= 0) return;  // minimiser stopped this replica
+  if (frozen && (frozen[r].fire_conv_step >= 0 || frozen[r].halt)) return;  // minimiser stopped / batch halted
   Part p;
   load_dyn(d, k, p);
   p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
@@ -315,6 +315,7 @@ __global__ void k_force(Program P, const Replica* __restrict__ reps, const int* 
                         int use_fire_dt, int with_pair, int with_align, double* epart, int nblocks, const int* __restrict__ blist = nullptr) {
   const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
   const int r = blk_rep[bid_];
+  if (clk[r].halt) return;  // batched iterations: a rebuild is pending
   const Replica& R = reps[r];
   if (use_fire_dt) {
     if (clk[r].fire_conv_step >= 0) return;  // converged replica: whole block exits (partials kept)
@@ -646,7 +647,7 @@ __global__ void k_fire_a(Program P, const Replica* __restrict__ reps, const int*
   const Replica& R = reps[r];
   const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
-  if (clk[r].fire_conv_step >= 0) return;  // frozen after convergence (driver mode)
+  if (clk[r].fire_conv_step >= 0 || clk[r].halt) return;  // frozen after convergence / batch halted
   Part p;
   load_dyn(d, k, p);
   p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
@@ -670,6 +671,7 @@ __global__ void k_fire_b(Program P, const Replica* __restrict__ reps, const int*
   const int k = bid_ * BLOCK + threadIdx.x;
   double v[3] = {0.0, 0.0, 0.0};
   double fmax2 = 0.0;
+  if (clk[r].halt) return;  // batched iterations: a rebuild is pending (k_fire_c skips too)
   const bool frozen = clk[r].fire_conv_step >= 0;
   if (k - R.off < R.n && !frozen) {
     Part p;
@@ -708,7 +710,7 @@ __global__ void k_fire_c(Program P, const Replica* __restrict__ reps, Clock* clk
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nrep) return;
   Clock& C = clk[r];
-  if (C.fire_conv_step >= 0) return;
+  if (C.fire_conv_step >= 0 || C.halt) return;
   const Replica& R = reps[r];
   const double* ip = R.integ_p[c];
   double Ps = 0.0, Fn = 0.0, Vn = 0.0, Fm = 0.0, E = 0.0;
@@ -761,7 +763,7 @@ __global__ void k_fire_d(Program P, const Replica* __restrict__ reps, const int*
   const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   const Clock& C = clk[r];
-  if (C.fire_converged || C.fire_conv_step >= 0) return;
+  if (C.fire_converged || C.fire_conv_step >= 0 || C.halt) return;
   const double a = alpha_mix[r];
   const double inv_Fnorm = 1.0 / C.fire_F;
   const double fact_1 = 1.0 - a;
