@@ -171,7 +171,7 @@ def sphere_parts(n, seed):
                 nz=t[:, 2].copy(), radius=np.ones(n)), R
 
 
-def batched_leg(n_rep=256, warm=60, steps=100, seed=7, device=0):
+def batched_leg(n_rep=256, warm=80, steps=100, seed=7, device=0):
     """256 sphere systems, N log-uniform in [1024, 65536], R = sqrt(N/4), v0 ~ U[0.01,1],
     J ~ U[0,1], nu ~ logU[1e-3,1], own seeds; soft k=10 + polar, dt=1e-3."""
     from samos_b200 import Engine

@@ -35,15 +35,19 @@ struct AbpParams {
 // Tuning variants (chunk of neighbour records fetched ahead, min blocks/SM):
 // the engine's autotuner times them on the live system and keeps the fastest.
 // 0-4 per-particle sweep, 5 flattened, 6-7 staged (cp.async), 8 shared-memory
-// tile, 9-10 per-particle sweep with lanes assigned in neighbour-count order
-constexpr int ABP_NVARIANT = 11;
+// tile, 9-10 per-particle sweep with lanes assigned in neighbour-count order,
+// 11-14 ordered with the Gaussian draws taken before the sweep (fewer live
+// registers inside it), at rising occupancy
+constexpr int ABP_NVARIANT = 15;
 __host__ __device__ constexpr int abp_chunk(int v) {
-  return v == 0 ? 4 : v == 1 ? 4 : v == 2 ? 2 : v == 3 ? 2 : v == 9 ? 2 : v == 10 ? 4 : 8;
+  return v == 0 ? 4 : v == 1 ? 4 : v == 2 ? 2 : v == 3 ? 2 : v == 9 ? 2 : v == 10 ? 4 : v >= 11 ? 2 : 8;
 }
 __host__ __device__ constexpr int abp_minb(int v) {
-  return v == 0 ? 5 : v == 1 ? 4 : v == 2 ? 6 : v == 3 ? 4 : v == 9 ? 6 : v == 10 ? 5 : 3;
+  return v == 0 ? 5 : v == 1 ? 4 : v == 2 ? 6 : v == 3 ? 4 : v == 9 ? 6 : v == 10 ? 5 : v == 11 ? 6 : v == 12 ? 7
+       : v == 13 ? 8 : v == 14 ? 10 : 3;
 }
-__host__ __device__ constexpr bool abp_ordered(int v) { return v == 9 || v == 10; }
+__host__ __device__ constexpr bool abp_ordered(int v) { return v >= 9; }
+__host__ __device__ constexpr bool abp_prenoise(int v) { return v >= 11; }
 
 // Lane order of a block for the ordered variants: its particles sorted by
 // neighbour count, largest first (ties by slot), so each warp's 32 lanes have
@@ -259,6 +263,15 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
     if (S.nematic) base += (uint64_t)S.n;
     const int D = T > 0.0 ? 4 : 1;
     const uint64_t c0 = base + gid * (uint64_t)D;
+    if (abp_prenoise(VAR)) {
+      g_rot = noise_gauss(S.seed, c0 + (uint64_t)(D - 1));
+      if (T > 0.0) {
+        g_x = noise_gauss(S.seed, c0 + 0);
+        g_y = noise_gauss(S.seed, c0 + 1);
+        if (!PLANE) g_z = noise_gauss(S.seed, c0 + 2);
+      }
+      noise_done = true;
+    }
     for (int q0 = 0; q0 < cnt || !noise_done; q0 += CH) {
       int jj[CH];
       D4 gg[CH], hh[CH];

@@ -1211,6 +1211,10 @@ static void launch_abp3(sg_system* s, bool apply_e1, bool last, bool energy) {
     case 8: launch_abp_tile<SHAPE, ALIGN, SP, false, 5>(s, apply_e1, last); break;
     case 9: launch_abp_v<SHAPE, ALIGN, SP, false, 9>(s, apply_e1, last); break;
     case 10: launch_abp_v<SHAPE, ALIGN, SP, false, 10>(s, apply_e1, last); break;
+    case 11: launch_abp_v<SHAPE, ALIGN, SP, false, 11>(s, apply_e1, last); break;
+    case 12: launch_abp_v<SHAPE, ALIGN, SP, false, 12>(s, apply_e1, last); break;
+    case 13: launch_abp_v<SHAPE, ALIGN, SP, false, 13>(s, apply_e1, last); break;
+    case 14: launch_abp_v<SHAPE, ALIGN, SP, false, 14>(s, apply_e1, last); break;
     case 0: launch_abp_v<SHAPE, ALIGN, SP, false, 0>(s, apply_e1, last); break;
     case 1: launch_abp_v<SHAPE, ALIGN, SP, false, 1>(s, apply_e1, last); break;
     case 2: launch_abp_v<SHAPE, ALIGN, SP, false, 2>(s, apply_e1, last); break;
