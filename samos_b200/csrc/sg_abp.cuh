@@ -250,8 +250,6 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
     }
     const int cnt = nl.cnt[k], lo = nl.lo[k];
     const uint64_t gid = (uint64_t)st.id[k];
-    const double ox = nl.ox[k], oy = nl.oy[k], oz = PLANE ? 0.0 : nl.oz[k];
-    const double age0 = d.age[k];
 
     // ---- forces and torques ---------------------------------------------------
     double fx = 0.0, fy = 0.0, fz = 0.0, tx = 0.0, ty = 0.0, tz = 0.0;
@@ -305,6 +303,9 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
         }
       }
     }
+    // read only now: values the sweep does not need stay out of its registers
+    const double ox = nl.ox[k], oy = nl.oy[k], oz = PLANE ? 0.0 : nl.oz[k];
+    const double age0 = d.age[k];
     abp_finish<SHAPE, SP>(S, r, k, x, y, z, nx, ny, nz, ri, fx, fy, fz, tx, ty, tz, g_rot, g_x, g_y, g_z, T, gid,
                           s_base, ox, oy, oz, age0, Gout, Hout, d, rebuild, status, apply_e1, last);
   }

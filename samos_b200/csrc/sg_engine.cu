@@ -76,6 +76,7 @@ struct sg_system {
   int *rebuild = nullptr, *status = nullptr, *maxnb = nullptr;
   int *bstatus = nullptr;   // list-build status (overflow), separate from the run's status word
   int *exec_cnt = nullptr;  // steps executed in a batch (batched stepping)
+  int *fire_cnt = nullptr;  // per replica: blocks of k_fire_b done (the last one runs the FIRE control)
   int64_t since_rebuild = 0, last_gap = 8;  // batch length follows the steps between rebuilds
   int* rebuild_h = nullptr;  // pinned
   double *epart = nullptr, *fire_part = nullptr, *alpha_mix = nullptr, *Rn = nullptr;
@@ -238,6 +239,7 @@ int sg_create(int n_replicas, const int32_t* n_particles, int ntypes, sg_system*
   s->status = m.alloc<int>(1);
   s->bstatus = m.alloc<int>(1);
   s->exec_cnt = m.alloc<int>(1);
+  s->fire_cnt = m.alloc<int>(n_replicas);
   s->maxnb = m.alloc<int>(1);
   s->epart = m.alloc<double>((size_t)(MAX_PAIR + MAX_ALIGN) * s->nblocks);
   s->fire_part = m.alloc<double>((size_t)4 * s->nblocks);
@@ -950,6 +952,7 @@ static int step_unfused(sg_system* s, bool energy, bool driver) {
     LAUNCH_CHECK(s);
   }
   int rc = SG_OK;
+  bool skin_done = false;  // FIRE runs the skin test inside its last pass
   if (!(s->forces_fresh && fire_forces_reusable(s)))
     if ((rc = launch_force(s, s->dt_global, false, true, true, energy, na, al))) return rc;
   s->forces_fresh = false;
@@ -972,19 +975,19 @@ static int step_unfused(sg_system* s, bool energy, bool driver) {
       LAUNCH_CHECK(s);
       if ((rc = launch_force(s, 0.0, true, true, true, true, na, al))) return rc;
       s->forces_fresh = true;
-      k_fire_b<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, s->fire_part, nb, al);
+      k_fire_b<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, s->fire_part, nb,
+                                            s->rep_blk0, s->rep_nblk, s->epart, c, driver ? 1 : 0, s->alpha_mix,
+                                            s->fire_cnt, al);
       LAUNCH_CHECK(s);
-      k_fire_c<<<(s->nrep + 127) / 128, 128, 0, s->stream>>>(s->prog, s->reps, s->clk, s->rep_blk0, s->rep_nblk,
-                                                             s->fire_part, s->epart, nb, s->nrep, c, driver ? 1 : 0,
-                                                             s->alpha_mix);
+      k_fire_d<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alpha_mix, s->nl,
+                                            s->has_nlist ? 1 : 0, s->rebuild, s->status, al);
       LAUNCH_CHECK(s);
-      k_fire_d<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alpha_mix, al);
-      LAUNCH_CHECK(s);
+      skin_done = true;
     } else {
       return fail(s, SG_ERR_UNSUPPORTED, "mixing Brownian-family integrators with Langevin/FIRE is not supported");
     }
   }
-  if (s->has_nlist) {
+  if (s->has_nlist && !skin_done) {
     k_skin<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->nl, s->rebuild, s->status, al);
     LAUNCH_CHECK(s);
   }

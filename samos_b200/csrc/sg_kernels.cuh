@@ -662,9 +662,61 @@ __global__ void k_fire_a(Program P, const Replica* __restrict__ reps, const int*
   store_dyn(d, k, p);
 }
 
+// per replica: fixed-order sums over its blocks, convergence test and the
+// dt / alpha control (96-147).  alpha_mix[r] keeps the alpha the mixing step
+// must use (the value before this update).
+__device__ void fire_control(const Program& P, const Replica& R, Clock& C, int r, int c, const double* part,
+                             const double* epart, int nblocks, int b0, int nb, int driver, double* alpha_mix) {
+  if (C.fire_conv_step >= 0 || C.halt) return;
+  const double* ip = R.integ_p[c];
+  double Ps = 0.0, Fn = 0.0, Vn = 0.0, Fm = 0.0, E = 0.0;
+  for (int b = b0; b < b0 + nb; b++) {  // fixed order; other blocks' partials, so past L1
+    Ps += __ldcg(part + b); Fn += __ldcg(part + (size_t)nblocks + b); Vn += __ldcg(part + (size_t)2 * nblocks + b);
+    Fm = fmax(Fm, __ldcg(part + (size_t)3 * nblocks + b));
+  }
+  for (int pc = 0; pc < P.npair; pc++) {
+    double s = 0.0;
+    for (int b = b0; b < b0 + nb; b++) s += __ldcg(epart + (size_t)pc * nblocks + b);
+    E += s;
+  }
+  Fn = sqrt(Fn);
+  Vn = sqrt(Vn);
+  C.fire_P = Ps; C.fire_F = Fn; C.fire_V = Vn; C.fire_E = E; C.fire_Fmax2 = Fm;
+  const double sqrt_ndof = sqrt((double)(3 * R.n));
+  const double fmax_tol = ip[11];
+  const bool conv = (fmax_tol > 0.0) ? (sqrt(Fm) < fmax_tol)
+                                     : (Fn / sqrt_ndof < ip[3] && fabs(E - C.fire_old_e) < ip[4]);
+  if (conv) {
+    C.fire_converged = 1;
+    if (driver) C.fire_conv_step = C.run_step;
+    return;
+  }
+  alpha_mix[r] = C.fire_alpha;
+  if (Ps > 0.0) {
+    C.fire_last_neg++;
+    if (C.fire_last_neg > (int)ip[9]) {
+      double ndt = C.fire_dt * ip[6];
+      C.fire_dt = ndt < ip[8] ? ndt : ip[8];
+      C.fire_alpha *= ip[2];
+    }
+  } else {
+    C.fire_dt *= ip[7];
+    C.fire_alpha = ip[1];
+    C.fire_last_neg = 0;
+  }
+  C.fire_converged = 0;
+  C.fire_old_e = E;
+}
+
 // second half kick + P, |F|^2, |v|^2, max|F|^2 partials (79-94)
+// ... and, in the replica's last block to finish, the per-replica sums, the
+// convergence test and the dt / alpha control (96-147) of fire_control: the
+// blocks of a replica count themselves done on fire_cnt[r] after their
+// partials are visible, so the last one sees them all.
 __global__ void k_fire_b(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                         const Clock* __restrict__ clk, Dyn d, Stat st, double* part, int nblocks, const int* __restrict__ blist = nullptr) {
+                         Clock* __restrict__ clk, Dyn d, Stat st, double* part, int nblocks, const int* rep_blk0,
+                         const int* rep_nblk, const double* epart, int c, int driver, double* alpha_mix,
+                         int* __restrict__ fire_cnt, const int* __restrict__ blist = nullptr) {
   const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
   const int r = blk_rep[bid_];
   const Replica& R = reps[r];
@@ -699,80 +751,50 @@ __global__ void k_fire_b(Program P, const Replica* __restrict__ reps, const int*
     for (int i = 0; i < BLOCK / 32; i++) m = fmax(m, shm[i]);
     part[(size_t)3 * nblocks + bid_] = m;
   }
-}
-
-// per replica: fixed-order sums over its blocks, convergence test and the
-// dt / alpha control (96-147).  One thread per replica.  alpha_mix[r] keeps
-// the alpha the mixing step must use (the value before this update).
-__global__ void k_fire_c(Program P, const Replica* __restrict__ reps, Clock* clk, const int* __restrict__ rep_blk0,
-                         const int* __restrict__ rep_nblk, const double* part, const double* epart,
-                         int nblocks, int nrep, int c, int driver, double* alpha_mix) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= nrep) return;
-  Clock& C = clk[r];
-  if (C.fire_conv_step >= 0 || C.halt) return;
-  const Replica& R = reps[r];
-  const double* ip = R.integ_p[c];
-  double Ps = 0.0, Fn = 0.0, Vn = 0.0, Fm = 0.0, E = 0.0;
-  const int b0 = rep_blk0[r], nb = rep_nblk[r];
-  for (int b = b0; b < b0 + nb; b++) {
-    Ps += part[b]; Fn += part[(size_t)nblocks + b]; Vn += part[(size_t)2 * nblocks + b];
-    Fm = fmax(Fm, part[(size_t)3 * nblocks + b]);
+  if (frozen) return;  // whole block: a frozen replica takes no control step
+  __shared__ int amlast;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) amlast = atomicAdd(&fire_cnt[r], 1) == rep_nblk[r] - 1;
+  __syncthreads();
+  if (amlast && threadIdx.x == 0) {
+    __threadfence();
+    fire_control(P, R, clk[r], r, c, part, epart, nblocks, rep_blk0[r], rep_nblk[r], driver, alpha_mix);
+    fire_cnt[r] = 0;
   }
-  for (int pc = 0; pc < P.npair; pc++) {
-    double s = 0.0;
-    for (int b = b0; b < b0 + nb; b++) s += epart[(size_t)pc * nblocks + b];
-    E += s;
-  }
-  Fn = sqrt(Fn);
-  Vn = sqrt(Vn);
-  C.fire_P = Ps; C.fire_F = Fn; C.fire_V = Vn; C.fire_E = E; C.fire_Fmax2 = Fm;
-  const double sqrt_ndof = sqrt((double)(3 * R.n));
-  const double fmax_tol = ip[11];
-  const bool conv = (fmax_tol > 0.0) ? (sqrt(Fm) < fmax_tol)
-                                     : (Fn / sqrt_ndof < ip[3] && fabs(E - C.fire_old_e) < ip[4]);
-  if (conv) {
-    C.fire_converged = 1;
-    if (driver) C.fire_conv_step = C.run_step;
-    return;
-  }
-  alpha_mix[r] = C.fire_alpha;
-  if (Ps > 0.0) {
-    C.fire_last_neg++;
-    if (C.fire_last_neg > (int)ip[9]) {
-      double ndt = C.fire_dt * ip[6];
-      C.fire_dt = ndt < ip[8] ? ndt : ip[8];
-      C.fire_alpha *= ip[2];
-    }
-  } else {
-    C.fire_dt *= ip[7];
-    C.fire_alpha = ip[1];
-    C.fire_last_neg = 0;
-  }
-  C.fire_converged = 0;
-  C.fire_old_e = E;
 }
 
 // FIRE velocity mixing (110-121) with the pre-update alpha, then the
 // P <= 0 restart that zeroes the velocities (131-142).
 __global__ void k_fire_d(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                         const Clock* __restrict__ clk, Dyn d, const double* alpha_mix, const int* __restrict__ blist = nullptr) {
+                         const Clock* __restrict__ clk, Dyn d, const double* alpha_mix, NbList nl, int skin,
+                         int* __restrict__ rebuild, int* __restrict__ status, const int* __restrict__ blist = nullptr) {
   const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
   const int r = blk_rep[bid_];
   const Replica& R = reps[r];
   const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
   const Clock& C = clk[r];
-  if (C.fire_converged || C.fire_conv_step >= 0 || C.halt) return;
-  const double a = alpha_mix[r];
-  const double inv_Fnorm = 1.0 / C.fire_F;
-  const double fact_1 = 1.0 - a;
-  const double fact_2 = a * inv_Fnorm * C.fire_V;
-  double vx = fact_1 * d.vx[k] + fact_2 * d.fx[k];
-  double vy = fact_1 * d.vy[k] + fact_2 * d.fy[k];
-  double vz = fact_1 * d.vz[k] + fact_2 * d.fz[k];
-  if (!(C.fire_P > 0.0)) { vx = 0.0; vy = 0.0; vz = 0.0; }
-  d.vx[k] = vx; d.vy[k] = vy; d.vz[k] = vz;
+  if (C.fire_conv_step >= 0 || C.halt) return;  // frozen or halted: positions as the last skin test saw them
+  if (!C.fire_converged) {
+    const double a = alpha_mix[r];
+    const double inv_Fnorm = 1.0 / C.fire_F;
+    const double fact_1 = 1.0 - a;
+    const double fact_2 = a * inv_Fnorm * C.fire_V;
+    double vx = fact_1 * d.vx[k] + fact_2 * d.fx[k];
+    double vy = fact_1 * d.vy[k] + fact_2 * d.fy[k];
+    double vz = fact_1 * d.vz[k] + fact_2 * d.fz[k];
+    if (!(C.fire_P > 0.0)) { vx = 0.0; vy = 0.0; vz = 0.0; }
+    d.vx[k] = vx; d.vy[k] = vy; d.vz[k] = vz;
+  }
+  if (skin) {  // the step's skin test (neighbour_list.cpp:278-302), fused
+    Part p;
+    p.x = d.x[k]; p.y = d.y[k]; p.z = d.z[k];
+    if (need_update(R, nl, k, p)) {
+      if (rebuild[r] == 0) atomicOr(&rebuild[r], 1);
+    }
+    if (!finite3(p.x, p.y, p.z)) atomicOr(status, ST_NONFINITE);
+  }
 }
 
 // ---------------------------------------------------------------------------
