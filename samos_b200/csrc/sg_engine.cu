@@ -947,13 +947,17 @@ static int step_unfused(sg_system* s, bool energy, bool driver) {
   // only return)
   const int* al = driver && s->nact < nb ? s->act : nullptr;
   const int na = driver ? s->nact : nb;
-  if (!s->e1_applied) {  // samos.cpp:887-888 (already applied by sg_begin_step)
+  const bool reuse_forces = s->forces_fresh && fire_forces_reusable(s);
+  // FIRE alone with reused forces: the start-of-step enforce runs inside the
+  // first FIRE pass
+  const bool fuse_enforce = !s->e1_applied && reuse_forces && s->prog.ninteg == 1 && s->prog.integ[0].kind == INT_FIRE;
+  if (!s->e1_applied && !fuse_enforce) {  // samos.cpp:887-888 (already applied by sg_begin_step)
     k_enforce<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, driver ? s->clk : nullptr, al);
     LAUNCH_CHECK(s);
   }
   int rc = SG_OK;
   bool skin_done = false;  // FIRE runs the skin test inside its last pass
-  if (!(s->forces_fresh && fire_forces_reusable(s)))
+  if (!reuse_forces)
     if ((rc = launch_force(s, s->dt_global, false, true, true, energy, na, al))) return rc;
   s->forces_fresh = false;
   for (int c = 0; c < s->prog.ninteg; c++) {
@@ -971,7 +975,8 @@ static int step_unfused(sg_system* s, bool energy, bool driver) {
       k_nve_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, c);
       LAUNCH_CHECK(s);
     } else if (ic.kind == INT_FIRE) {
-      k_fire_a<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, al);
+      k_fire_a<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, fuse_enforce ? 1 : 0,
+                                            al);
       LAUNCH_CHECK(s);
       if ((rc = launch_force(s, 0.0, true, true, true, true, na, al))) return rc;
       s->forces_fresh = true;

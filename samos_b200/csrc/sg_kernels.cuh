@@ -641,7 +641,8 @@ __global__ void k_nve_b(Program P, const Replica* __restrict__ reps, const int* 
 // ---------------------------------------------------------------------------
 // first half: half kick, drift, enforce, omega, director rotation (49-66)
 __global__ void k_fire_a(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                         const Clock* __restrict__ clk, Dyn d, Stat st, const int* __restrict__ blist = nullptr) {
+                         const Clock* __restrict__ clk, Dyn d, Stat st, int pre_enforce,
+                         const int* __restrict__ blist = nullptr) {
   const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
   const int r = blk_rep[bid_];
   const Replica& R = reps[r];
@@ -651,6 +652,9 @@ __global__ void k_fire_a(Program P, const Replica* __restrict__ reps, const int*
   Part p;
   load_dyn(d, k, p);
   p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
+  // the step's start-of-step enforce (k_enforce), when no force pass lies
+  // between them (the forces of the previous iteration are reused)
+  if (pre_enforce) enforce_all(P, R, p);
   const double dt = clk[r].fire_dt;
   const double dt_2 = 0.5 * dt;
   p.vx += dt_2 * p.fx; p.vy += dt_2 * p.fy; p.vz += dt_2 * p.fz;
