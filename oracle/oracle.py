@@ -154,7 +154,7 @@ class OracleSystem:
         self.lib.or_add_external(self.h, int(kind), float(alpha), _p(t), int(has_params))
 
     def add_constraint(self, kind, params):
-        p = np.zeros(8)
+        p = np.zeros(9)
         p[:len(params)] = params
         self.lib.or_add_constraint(self.h, int(kind), _p(p))
         self.lib.or_enforce_all(self.h)  # samos.cpp:518-522

@@ -209,7 +209,8 @@ typedef struct {
 typedef struct {
   int kind;
   double zpos; int unlimited;      /* plane */
-  double r;                        /* sphere */
+  double r;                        /* sphere; cylinder r; torus c; ellipsoid a */
+  double b2, b3;                   /* torus a; ellipsoid b, c */
   int max_iter; double tol;
   double rescale; int rescale_steps, rescale_freq; double scale;
 } or_cons;
@@ -885,6 +886,10 @@ int or_add_constraint(or_system* s, int kind, const double* p)
   c->kind = kind;
   c->zpos = p ? p[0] : 0.0; c->unlimited = p ? (int)p[1] : 0;
   c->r = p ? p[0] : 1.0;
+  if (kind == OR_CONS_TORUS || kind == OR_CONS_ELLIPSOID) {  /* params[7], params[8] */
+    c->b2 = p ? p[7] : (kind == OR_CONS_TORUS ? 0.5 : 1.0);
+    c->b3 = p ? p[8] : 1.0;
+  }
   c->max_iter = p ? (int)p[2] : 100;
   c->tol = p ? p[3] : 1e-6;
   c->rescale = p ? p[4] : 1.0;
@@ -939,12 +944,104 @@ static void sphere_enforce(or_system* s, const or_cons* c, int i)
 
 /* Constrainer::enforce, constraints/constrainer.hpp:73-77; ConstraintNone,
    constraints/constraint_none.hpp:58-62 */
+/* ConstraintCylinder::enforce, constraints/constraint_cylinder.cpp:38-71:
+   radial projection onto radius r; the periodic wrap in z is the
+   constraint's own (no image-flag update). */
+static void cylinder_enforce(or_system* s, const or_cons* c, int i)
+{
+  double x = s->x[i], y = s->y[i];
+  double R = sqrt(x * x + y * y);
+  double sc = c->r / R;
+  s->x[i] *= sc; s->y[i] *= sc;
+  double Nx = s->x[i] / c->r, Ny = s->y[i] / c->r;
+  double v_dot_N = s->vx[i] * Nx + s->vy[i] * Ny;
+  double n_dot_N = s->nx[i] * Nx + s->ny[i] * Ny;
+  s->vx[i] -= v_dot_N * Nx; s->vy[i] -= v_dot_N * Ny;
+  s->nx[i] -= n_dot_N * Nx; s->ny[i] -= n_dot_N * Ny;
+  double inv_len = 1.0 / sqrt(s->nx[i] * s->nx[i] + s->ny[i] * s->ny[i] + s->nz[i] * s->nz[i]);
+  s->nx[i] *= inv_len; s->ny[i] *= inv_len; s->nz[i] *= inv_len;
+  if (s->periodic) {
+    if (s->z[i] > 0.5 * s->Lz) s->z[i] -= s->Lz;
+    else if (s->z[i] < -0.5 * s->Lz) s->z[i] += s->Lz;
+  }
+}
+
+/* compute_gradient / constraint_value of the implicit surfaces:
+   ConstraintTorus (constraint_torus.cpp: (c - sqrt(x^2+y^2))^2 + z^2 - a^2)
+   and ConstraintEllipsoid (constraint_ellipsoid.cpp: x^2/a^2 + y^2/b^2 + z^2/c^2 - 1) */
+static void implicit_gradient(const or_cons* c, double x, double y, double z, double* gx, double* gy, double* gz)
+{
+  if (c->kind == OR_CONS_TORUS) {
+    double sqr_xy = sqrt(x * x + y * y);
+    double fact = -2.0 * (c->r - sqr_xy) / sqr_xy;
+    *gx = x * fact; *gy = y * fact; *gz = 2.0 * z;
+  } else {
+    *gx = 2.0 * x / c->r / c->r; *gy = 2.0 * y / c->b2 / c->b2; *gz = 2.0 * z / c->b3 / c->b3;
+  }
+}
+
+static double implicit_value(const or_cons* c, double x, double y, double z)
+{
+  if (c->kind == OR_CONS_TORUS) {
+    double ft = c->r - sqrt(x * x + y * y);
+    return ft * ft + z * z - c->b2 * c->b2;
+  }
+  return x * x / c->r / c->r + y * y / c->b2 / c->b2 + z * z / c->b3 / c->b3 - 1.0;
+}
+
+/* compute_normal of each non-plane surface (the gradient normalised for the
+   implicit ones, constraint_torus.cpp / constraint_ellipsoid.cpp; x/r, y/r, 0
+   for the cylinder, constraint_cylinder.hpp:76-80) */
+static void surface_normal(or_system* s, const or_cons* c, int i, double* Nx, double* Ny, double* Nz)
+{
+  if (c->kind == OR_CONS_SPHERE) { *Nx = s->x[i] / c->r; *Ny = s->y[i] / c->r; *Nz = s->z[i] / c->r; }
+  else if (c->kind == OR_CONS_CYLINDER) { *Nx = s->x[i] / c->r; *Ny = s->y[i] / c->r; *Nz = 0.0; }
+  else {
+    implicit_gradient(c, s->x[i], s->y[i], s->z[i], Nx, Ny, Nz);
+    double len_N = sqrt(*Nx * *Nx + *Ny * *Ny + *Nz * *Nz);
+    *Nx /= len_N; *Ny /= len_N; *Nz /= len_N;
+  }
+  s->Nx[i] = *Nx; s->Ny[i] = *Ny; s->Nz[i] = *Nz;
+}
+
+/* Constraint::enforce, constraints/constraint.cpp:40-87: SHAKE iterations
+   along the gradient at the start point until |g| <= tol, then the tangent
+   projections of v and n, n normalised, and the periodic wrap. */
+static void implicit_enforce(or_system* s, const or_cons* c, int i)
+{
+  double ref_gx, ref_gy, ref_gz;
+  implicit_gradient(c, s->x[i], s->y[i], s->z[i], &ref_gx, &ref_gy, &ref_gz);
+  int iter = 0;
+  while (iter++ < c->max_iter) {
+    double gx, gy, gz;
+    implicit_gradient(c, s->x[i], s->y[i], s->z[i], &gx, &gy, &gz);
+    double sv = gx * ref_gx + gy * ref_gy + gz * ref_gz;
+    double g = implicit_value(c, s->x[i], s->y[i], s->z[i]);
+    double lambda = g / sv;
+    if (!(fabs(g) > c->tol)) break;
+    s->x[i] -= lambda * ref_gx;
+    s->y[i] -= lambda * ref_gy;
+    s->z[i] -= lambda * ref_gz;
+  }
+  double Nx, Ny, Nz;
+  surface_normal(s, c, i, &Nx, &Ny, &Nz);
+  double v_dot_N = s->vx[i] * Nx + s->vy[i] * Ny + s->vz[i] * Nz;
+  double n_dot_N = s->nx[i] * Nx + s->ny[i] * Ny + s->nz[i] * Nz;
+  s->vx[i] -= v_dot_N * Nx; s->vy[i] -= v_dot_N * Ny; s->vz[i] -= v_dot_N * Nz;
+  s->nx[i] -= n_dot_N * Nx; s->ny[i] -= n_dot_N * Ny; s->nz[i] -= n_dot_N * Nz;
+  double inv_len = 1.0 / sqrt(s->nx[i] * s->nx[i] + s->ny[i] * s->ny[i] + s->nz[i] * s->nz[i]);
+  s->nx[i] *= inv_len; s->ny[i] *= inv_len; s->nz[i] *= inv_len;
+  if (s->periodic) enforce_periodic(s, i);
+}
+
 static void enforce_one(or_system* s, int i)
 {
   for (int k = 0; k < s->ncons; k++) {
     const or_cons* c = &s->cons[k];
     if (c->kind == OR_CONS_PLANE) plane_enforce(s, c, i);
     else if (c->kind == OR_CONS_SPHERE) sphere_enforce(s, c, i);
+    else if (c->kind == OR_CONS_CYLINDER) cylinder_enforce(s, c, i);
+    else if (c->kind == OR_CONS_TORUS || c->kind == OR_CONS_ELLIPSOID) implicit_enforce(s, c, i);
     else if (s->periodic) enforce_periodic(s, i);
   }
 }
@@ -964,9 +1061,9 @@ static double project_torque(or_system* s, int i)
   for (int k = 0; k < s->ncons; k++) {
     const or_cons* c = &s->cons[k];
     if (c->kind == OR_CONS_PLANE) val += s->tz[i];
-    else if (c->kind == OR_CONS_SPHERE) {
-      double Nx = s->x[i] / c->r, Ny = s->y[i] / c->r, Nz = s->z[i] / c->r;
-      s->Nx[i] = Nx; s->Ny[i] = Ny; s->Nz[i] = Nz;
+    else if (c->kind != OR_CONS_NONE) {
+      double Nx, Ny, Nz;
+      surface_normal(s, c, i, &Nx, &Ny, &Nz);
       val += s->tx[i] * Nx + s->ty[i] * Ny + s->tz[i] * Nz;
     } else val += 0.0;
   }
@@ -987,9 +1084,9 @@ static void rotate_director(or_system* s, int i, double phi)
       double ny = Ryx * s->nx[i] + Ryy * s->ny[i];
       double len = sqrt(nx * nx + ny * ny);
       s->nx[i] = nx / len; s->ny[i] = ny / len;
-    } else if (c->kind == OR_CONS_SPHERE) {
-      double U = s->x[i] / c->r, V = s->y[i] / c->r, W = s->z[i] / c->r;
-      s->Nx[i] = U; s->Ny[i] = V; s->Nz[i] = W;
+    } else if (c->kind != OR_CONS_NONE) {
+      double U, V, W;
+      surface_normal(s, c, i, &U, &V, &W);
       double cs = cos(phi), sn = sin(phi);
       double pnx = s->nx[i], pny = s->ny[i], pnz = s->nz[i];
       double nx = U * (U * pnx + V * pny + W * pnz) * (1.0 - cs) + pnx * cs + (-W * pny + V * pnz) * sn;
@@ -1013,9 +1110,9 @@ static void rotate_velocity(or_system* s, int i, double phi)
       double vx = Rxx * s->vx[i] + Rxy * s->vy[i];
       double vy = Ryx * s->vx[i] + Ryy * s->vy[i];
       s->vx[i] = vx; s->vy[i] = vy;
-    } else if (c->kind == OR_CONS_SPHERE) {
-      double U = s->x[i] / c->r, V = s->y[i] / c->r, W = s->z[i] / c->r;
-      s->Nx[i] = U; s->Ny[i] = V; s->Nz[i] = W;
+    } else if (c->kind != OR_CONS_NONE) {
+      double U, V, W;
+      surface_normal(s, c, i, &U, &V, &W);
       double cs = cos(phi), sn = sin(phi);
       double pvx = s->vx[i], pvy = s->vy[i], pvz = s->vz[i];
       double vx = U * (U * pvx + V * pvy + W * pvz) * (1.0 - cs) + pvx * cs + (-W * pvy + V * pvz) * sn;

@@ -25,7 +25,7 @@ constexpr int BLOCK = 128;          // particle slots per block; replicas are pa
 
 enum { PAIR_SOFT = 0, PAIR_LJ = 1, PAIR_MORSE = 2, PAIR_GAUSSIAN = 3 };
 enum { ALIGN_POLAR = 0, ALIGN_NEMATIC = 1, ALIGN_VICSEK = 2 };
-enum { CONS_NONE = 0, CONS_PLANE = 1, CONS_SPHERE = 2 };
+enum { CONS_NONE = 0, CONS_PLANE = 1, CONS_SPHERE = 2, CONS_CYLINDER = 3, CONS_TORUS = 4, CONS_ELLIPSOID = 5 };
 enum { INT_BROWNIAN = 0, INT_BROWNIAN_POS = 1, INT_BROWNIAN_ALIGN = 2, INT_LANGEVIN = 3, INT_FIRE = 4, INT_NVE = 5, INT_VICSEK = 6 };
 enum { LANGEVIN_BAOAB = 0, LANGEVIN_SPV = 1, LANGEVIN_BBK = 2 };
 
@@ -44,7 +44,9 @@ __host__ __device__ inline double value_get(const Value& v, int step) {
 struct PairComp { int kind, use_radii, phase_in, shifted, has_pp; Value phase; const double* table; };
 struct AlignComp { int kind, has_pp; const double* table; };
 struct ExtComp { int kind, has_params; const double* type_alpha; };
-struct ConsComp { int kind, unlimited; };
+// b2, b3: torus tube radius a; ellipsoid b, c (the first shape parameter is
+// per replica, Replica::cons_p); max_iter, tol: the SHAKE projection
+struct ConsComp { int kind, unlimited, max_iter, pad; double b2, b3, tol; };
 struct IntegComp { int kind, method, nematic, velocity; Value temp; };
 
 // The configured component program, passed by value to every kernel.
@@ -294,6 +296,88 @@ __device__ __forceinline__ void sphere_enforce(double Rs, Part& p) {
   p.nx *= inv_len; p.ny *= inv_len; p.nz *= inv_len;
 }
 
+// ConstraintCylinder::enforce, constraints/constraint_cylinder.cpp:38-71 (its
+// own periodic wrap in z, without image flags)
+__device__ __forceinline__ void cylinder_enforce(const Replica& R, double rc, Part& p) {
+  double x = p.x, y = p.y;
+  double Rr = sqrt(x * x + y * y);
+  double sc = rc / Rr;
+  p.x *= sc; p.y *= sc;
+  double Nx = p.x / rc, Ny = p.y / rc;
+  double v_dot_N = p.vx * Nx + p.vy * Ny;
+  double n_dot_N = p.nx * Nx + p.ny * Ny;
+  p.vx -= v_dot_N * Nx; p.vy -= v_dot_N * Ny;
+  p.nx -= n_dot_N * Nx; p.ny -= n_dot_N * Ny;
+  double inv_len = 1.0 / sqrt(p.nx * p.nx + p.ny * p.ny + p.nz * p.nz);
+  p.nx *= inv_len; p.ny *= inv_len; p.nz *= inv_len;
+  if (R.periodic) {
+    if (p.z > R.zhi) p.z -= R.Lz;
+    else if (p.z < R.zlo) p.z += R.Lz;
+  }
+}
+
+// implicit surfaces: ConstraintTorus ((c - sqrt(x^2+y^2))^2 + z^2 - a^2,
+// constraint_torus.cpp) and ConstraintEllipsoid (x^2/a^2 + y^2/b^2 + z^2/c^2 - 1,
+// constraint_ellipsoid.cpp): gradient and value
+__host__ __device__ __forceinline__ void implicit_gradient(const ConsComp& C, double a0, double x, double y, double z,
+                                                  double& gx, double& gy, double& gz) {
+  if (C.kind == CONS_TORUS) {
+    double sqr_xy = sqrt(x * x + y * y);
+    double fact = -2.0 * (a0 - sqr_xy) / sqr_xy;
+    gx = x * fact; gy = y * fact; gz = 2.0 * z;
+  } else {
+    gx = 2.0 * x / a0 / a0; gy = 2.0 * y / C.b2 / C.b2; gz = 2.0 * z / C.b3 / C.b3;
+  }
+}
+__device__ __forceinline__ double implicit_value(const ConsComp& C, double a0, double x, double y, double z) {
+  if (C.kind == CONS_TORUS) {
+    double ft = a0 - sqrt(x * x + y * y);
+    return ft * ft + z * z - C.b2 * C.b2;
+  }
+  return x * x / a0 / a0 + y * y / C.b2 / C.b2 + z * z / C.b3 / C.b3 - 1.0;
+}
+
+// compute_normal of the curved surfaces (sphere x/R; cylinder x/r, y/r, 0,
+// constraint_cylinder.hpp:76-80; implicit: the normalised gradient)
+__host__ __device__ __forceinline__ void surface_normal(const ConsComp& C, double a0, const Part& p, double& Nx, double& Ny,
+                                               double& Nz) {
+  if (C.kind == CONS_SPHERE) { Nx = p.x / a0; Ny = p.y / a0; Nz = p.z / a0; }
+  else if (C.kind == CONS_CYLINDER) { Nx = p.x / a0; Ny = p.y / a0; Nz = 0.0; }
+  else {
+    implicit_gradient(C, a0, p.x, p.y, p.z, Nx, Ny, Nz);
+    double len_N = sqrt(Nx * Nx + Ny * Ny + Nz * Nz);
+    Nx /= len_N; Ny /= len_N; Nz /= len_N;
+  }
+}
+
+// Constraint::enforce, constraints/constraint.cpp:40-87 (SHAKE along the
+// gradient at the start point, then the tangent projections)
+__device__ __forceinline__ void implicit_enforce(const ConsComp& C, const Replica& R, double a0, Part& p) {
+  double ref_gx, ref_gy, ref_gz;
+  implicit_gradient(C, a0, p.x, p.y, p.z, ref_gx, ref_gy, ref_gz);
+  int iter = 0;
+  while (iter++ < C.max_iter) {
+    double gx, gy, gz;
+    implicit_gradient(C, a0, p.x, p.y, p.z, gx, gy, gz);
+    double sv = gx * ref_gx + gy * ref_gy + gz * ref_gz;
+    double g = implicit_value(C, a0, p.x, p.y, p.z);
+    double lambda = g / sv;
+    if (!(fabs(g) > C.tol)) break;
+    p.x -= lambda * ref_gx;
+    p.y -= lambda * ref_gy;
+    p.z -= lambda * ref_gz;
+  }
+  double Nx, Ny, Nz;
+  surface_normal(C, a0, p, Nx, Ny, Nz);
+  double v_dot_N = p.vx * Nx + p.vy * Ny + p.vz * Nz;
+  double n_dot_N = p.nx * Nx + p.ny * Ny + p.nz * Nz;
+  p.vx -= v_dot_N * Nx; p.vy -= v_dot_N * Ny; p.vz -= v_dot_N * Nz;
+  p.nx -= n_dot_N * Nx; p.ny -= n_dot_N * Ny; p.nz -= n_dot_N * Nz;
+  double inv_len = 1.0 / sqrt(p.nx * p.nx + p.ny * p.ny + p.nz * p.nz);
+  p.nx *= inv_len; p.ny *= inv_len; p.nz *= inv_len;
+  enforce_periodic(R, p);
+}
+
 // Constrainer::enforce (constrainer.hpp:73-77); ConstraintNone::enforce
 // (constraint_none.hpp:58-62)
 __device__ __forceinline__ void enforce_all(const Program& P, const Replica& R, Part& p) {
@@ -301,6 +385,8 @@ __device__ __forceinline__ void enforce_all(const Program& P, const Replica& R, 
     int kind = P.cons[c].kind;
     if (kind == CONS_PLANE) plane_enforce(R, R.cons_p[c], P.cons[c].unlimited, p);
     else if (kind == CONS_SPHERE) sphere_enforce(R.cons_p[c], p);
+    else if (kind == CONS_CYLINDER) cylinder_enforce(R, R.cons_p[c], p);
+    else if (kind == CONS_TORUS || kind == CONS_ELLIPSOID) implicit_enforce(P.cons[c], R, R.cons_p[c], p);
     else enforce_periodic(R, p);
   }
 }
@@ -314,9 +400,9 @@ __device__ __forceinline__ double project_torque(const Program& P, const Replica
   for (int c = 0; c < P.ncons; c++) {
     int kind = P.cons[c].kind;
     if (kind == CONS_PLANE) val += p.tz;
-    else if (kind == CONS_SPHERE) {
-      double Rs = R.cons_p[c];
-      double Nx = p.x / Rs, Ny = p.y / Rs, Nz = p.z / Rs;
+    else if (kind != CONS_NONE) {
+      double Nx, Ny, Nz;
+      surface_normal(P.cons[c], R.cons_p[c], p, Nx, Ny, Nz);
       val += p.tx * Nx + p.ty * Ny + p.tz * Nz;
     } else val += 0.0;
   }
@@ -335,9 +421,9 @@ __device__ __forceinline__ void rotate_director(const Program& P, const Replica&
       double ny = Ryx * p.nx + Ryy * p.ny;
       double len = sqrt(nx * nx + ny * ny);
       p.nx = nx / len; p.ny = ny / len;
-    } else if (kind == CONS_SPHERE) {
-      double Rs = R.cons_p[c];
-      double U = p.x / Rs, V = p.y / Rs, W = p.z / Rs;
+    } else if (kind != CONS_NONE) {
+      double U, V, W;
+      surface_normal(P.cons[c], R.cons_p[c], p, U, V, W);
       double cs = cos(phi), sn = sin(phi);
       double dot = U * p.nx + V * p.ny + W * p.nz;
       double nx = U * dot * (1.0 - cs) + p.nx * cs + (-W * p.ny + V * p.nz) * sn;
@@ -360,9 +446,9 @@ __device__ __forceinline__ void rotate_velocity(const Program& P, const Replica&
       double vx = Rxx * p.vx + Rxy * p.vy;
       double vy = Ryx * p.vx + Ryy * p.vy;
       p.vx = vx; p.vy = vy;
-    } else if (kind == CONS_SPHERE) {
-      double Rs = R.cons_p[c];
-      double U = p.x / Rs, V = p.y / Rs, W = p.z / Rs;
+    } else if (kind != CONS_NONE) {
+      double U, V, W;
+      surface_normal(P.cons[c], R.cons_p[c], p, U, V, W);
       double cs = cos(phi), sn = sin(phi);
       double dot = U * p.vx + V * p.vy + W * p.vz;
       double vx = U * dot * (1.0 - cs) + p.vx * cs + (-W * p.vy + V * p.vz) * sn;

@@ -406,9 +406,16 @@ int sg_download(sg_system* s, int replica, const char* field, void* host) {
     for (int c = 0; c < s->prog.ncons; c++) {
       if (s->prog.cons[c].kind == CONS_PLANE)
         for (int i = 0; i < n; i++) h[i] = comp == 2 ? 1.0 : 0.0;
-      else if (s->prog.cons[c].kind == CONS_SPHERE) {
-        double Rs = s->reps_h[replica].cons_p[c];
-        for (int k = 0; k < n; k++) h[ids[k]] = (comp == 0 ? X[k] : comp == 1 ? Y[k] : Z[k]) / Rs;
+      else if (s->prog.cons[c].kind != CONS_NONE) {  // compute_normal of the curved surfaces
+        const ConsComp& C = s->prog.cons[c];
+        const double a0 = s->reps_h[replica].cons_p[c];
+        for (int k = 0; k < n; k++) {
+          Part q;
+          q.x = X[k]; q.y = Y[k]; q.z = Z[k];
+          double N[3];
+          surface_normal(C, a0, q, N[0], N[1], N[2]);
+          h[ids[k]] = N[comp];
+        }
       }
     }
     return SG_OK;
@@ -720,15 +727,25 @@ int sg_add_external(sg_system* s, int kind, double alpha, const double* type_alp
   return push_reps(s);
 }
 
+// Program-level part of a constraint: kind, plane flag, the second and third
+// shape parameters (torus a; ellipsoid b, c: params[7], params[8]) and the
+// SHAKE settings of the implicit surfaces (maxiter params[2], tol params[3]).
+static void set_cons(ConsComp& C, int kind, const double* params) {
+  C.kind = kind;
+  C.unlimited = (kind == CONS_PLANE && params) ? (int)params[1] : 0;
+  C.max_iter = params ? (int)params[2] : 100;
+  C.tol = params ? params[3] : 1e-6;
+  C.b2 = (kind == CONS_TORUS || kind == CONS_ELLIPSOID) ? (params ? params[7] : (kind == CONS_TORUS ? 0.5 : 1.0)) : 0.0;
+  C.b3 = kind == CONS_ELLIPSOID ? (params ? params[8] : 1.0) : 0.0;
+}
+
 int sg_add_constraint_per_replica(sg_system* s, int kind, const double* params, const double* value0) {
-  if (!s || !value0 || kind < SG_CONS_NONE || kind > SG_CONS_SPHERE) return fail(s, SG_ERR_ARG, "bad constraint");
+  if (!s || !value0 || kind < SG_CONS_NONE || kind > SG_CONS_ELLIPSOID) return fail(s, SG_ERR_ARG, "bad constraint");
   Program& P = s->prog;
   if (P.ncons >= MAX_CONS) return fail(s, SG_ERR_ARG, "too many constraints");
   if (params && params[4] != 0.0 && params[4] != 1.0)
     return fail(s, SG_ERR_UNSUPPORTED, "constraint rescale is not supported by the GPU path");
-  ConsComp& C = P.cons[P.ncons];
-  C.kind = kind;
-  C.unlimited = (kind == CONS_PLANE && params) ? (int)params[1] : 0;
+  set_cons(P.cons[P.ncons], kind, params);
   for (int r = 0; r < s->nrep; r++) s->reps_h[r].cons_p[P.ncons] = value0[r];
   P.ncons++;
   int rc = push_reps(s);
@@ -737,16 +754,14 @@ int sg_add_constraint_per_replica(sg_system* s, int kind, const double* params, 
 }
 
 int sg_add_constraint(sg_system* s, int kind, const double* params) {
-  if (!s || kind < SG_CONS_NONE || kind > SG_CONS_SPHERE) return fail(s, SG_ERR_ARG, "sg_add_constraint: bad kind");
+  if (!s || kind < SG_CONS_NONE || kind > SG_CONS_ELLIPSOID) return fail(s, SG_ERR_ARG, "sg_add_constraint: bad kind");
   Program& P = s->prog;
   if (P.ncons >= MAX_CONS) return fail(s, SG_ERR_ARG, "too many constraints");
   if (params && params[4] != 0.0 && params[4] != 1.0)
     return fail(s, SG_ERR_UNSUPPORTED, "constraint rescale is not supported by the GPU path");
-  ConsComp& C = P.cons[P.ncons];
-  C.kind = kind;
-  C.unlimited = (kind == CONS_PLANE && params) ? (int)params[1] : 0;
+  set_cons(P.cons[P.ncons], kind, params);
   for (int r = 0; r < s->nrep; r++)
-    s->reps_h[r].cons_p[P.ncons] = params ? params[0] : (kind == CONS_SPHERE ? 1.0 : 0.0);
+    s->reps_h[r].cons_p[P.ncons] = params ? params[0] : (kind == CONS_PLANE || kind == CONS_NONE ? 0.0 : 1.0);
   P.ncons++;
   int rc = push_reps(s);
   if (rc) return rc;

@@ -18,7 +18,7 @@ _lib = None
 PAIR = {"soft": 0, "lj": 1, "morse": 2, "gaussian": 3}
 ALIGN = {"polar": 0, "nematic": 1, "vicsek": 2}
 EXTERNAL = {"self_propulsion": 0}
-CONSTRAINT = {"none": 0, "plane": 1, "sphere": 2}
+CONSTRAINT = {"none": 0, "plane": 1, "sphere": 2, "cylinder": 3, "torus": 4, "ellipsoid": 5}
 INTEGRATOR = {"brownian": 0, "brownian_pos": 1, "brownian_align": 2, "langevin": 3, "fire": 4, "nve": 5, "vicsek": 6}
 PAIR_NPARAM = 8
 INT_NPARAM = 16
@@ -213,12 +213,12 @@ class Engine:
         self._check(self.lib.sg_add_external(self.h, int(kind), float(alpha), _dptr(t), int(has_params)))
 
     def add_constraint(self, kind, params):
-        p = np.zeros(8)
+        p = np.zeros(9)
         p[:len(params)] = params
         self._check(self.lib.sg_add_constraint(self.h, int(kind), _dptr(p)))
 
     def add_constraint_per_replica(self, kind, params, value0):
-        p = np.zeros(8)
+        p = np.zeros(9)
         p[:len(params)] = params
         v = np.ascontiguousarray(value0, dtype=np.float64)
         if v.shape != (len(self.n),):

@@ -182,17 +182,22 @@ ConstraintSpec resolve_constraint(const std::string& name, const Params& p) {
   if (name == "none") s.kind = SG_CONS_NONE;
   else if (name == "plane") s.kind = SG_CONS_PLANE;
   else if (name == "sphere") s.kind = SG_CONS_SPHERE;
+  else if (name == "cylinder") s.kind = SG_CONS_CYLINDER;
+  else if (name == "torus") s.kind = SG_CONS_TORUS;
+  else if (name == "ellipsoid") s.kind = SG_CONS_ELLIPSOID;
   else throw HostError("Constraint " + name + " is not part of the GPU path.");
   if (has(p, "group") && p.at("group") != "all") throw HostError("Constraint groups other than 'all' are not part of the GPU path.");
   // Constraint base (constraint.hpp:56-120); tol is parsed as an int there (82)
   const double maxiter = has(p, "maxiter") ? to_int("maxiter", p.at("maxiter")) : 100.0;
   const double tol = has(p, "tol") ? (double)to_int("tol", p.at("tol")) : 1e-6;
-  double first = 0.0, unlimited = 0.0;
+  double first = 0.0, unlimited = 0.0, second = 0.0, third = 0.0;
   if (name == "plane") { first = get(p, "zpos", 0.0); unlimited = has(p, "unlimited") ? 1.0 : 0.0; }
-  else if (name == "sphere") first = get(p, "r", 1.0);
-  const double v[7] = {first, unlimited, maxiter, tol, get(p, "rescale", 1.0), get(p, "rescale_steps", 1000.0),
-                       get(p, "rescale_freq", 10.0)};
-  for (int i = 0; i < 7; i++) s.params[i] = v[i];
+  else if (name == "sphere" || name == "cylinder") first = get(p, "r", 1.0);
+  else if (name == "torus") { first = get(p, "c", 1.0); second = get(p, "a", 0.5); }  // constraint_torus.hpp
+  else if (name == "ellipsoid") { first = get(p, "a", 1.0); second = get(p, "b", 1.0); third = get(p, "c", 1.0); }
+  const double v[9] = {first, unlimited, maxiter, tol, get(p, "rescale", 1.0), get(p, "rescale_steps", 1000.0),
+                       get(p, "rescale_freq", 10.0), second, third};
+  for (int i = 0; i < 9; i++) s.params[i] = v[i];
   return s;
 }
 

@@ -70,7 +70,7 @@ struct ExternalSpec {
 };
 struct ConstraintSpec {
   int kind = 0;
-  double params[8] = {0};
+  double params[10] = {0};  // the 9 values of sg_add_constraint
 };
 struct IntegratorSpec {
   std::string name;

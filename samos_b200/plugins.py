@@ -193,8 +193,9 @@ def resolve_external(name: str, params: dict, ntypes: int) -> ExternalSpec:
 
 def resolve_constraint(name: str, params: dict) -> tuple[int, list[float]]:
     """constraint <name> {...} (constraint.hpp:56-120, constraint_plane.hpp,
-    constraint_sphere.hpp): returns (kind, [zpos|r, unlimited, maxiter, tol,
-    rescale, rescale_steps, rescale_freq])."""
+    constraint_sphere.hpp, constraint_cylinder.hpp, constraint_torus.hpp,
+    constraint_ellipsoid.hpp): returns (kind, [zpos|r|c|a, unlimited, maxiter,
+    tol, rescale, rescale_steps, rescale_freq, torus a|ellipsoid b, ellipsoid c])."""
     if name not in E.CONSTRAINT:
         raise PluginError(f"Constraint {name} is not part of the GPU path.")
     if "group" in params and params["group"] != "all":
@@ -204,15 +205,20 @@ def resolve_constraint(name: str, params: dict) -> tuple[int, list[float]]:
     rescale = _f(params, "rescale", 1.0)
     rescale_steps = _f(params, "rescale_steps", 1000.0)
     rescale_freq = _f(params, "rescale_freq", 10.0)
+    second, third = 0.0, 0.0
     if name == "plane":
         first = _f(params, "zpos", 0.0)
         unlimited = 1.0 if "unlimited" in params else 0.0
-    elif name == "sphere":
+    elif name in ("sphere", "cylinder"):  # constraint_sphere.hpp, constraint_cylinder.hpp:58-69
         first = _f(params, "r", 1.0)
         unlimited = 0.0
+    elif name == "torus":  # constraint_torus.hpp: c (1), a (0.5)
+        first, second, unlimited = _f(params, "c", 1.0), _f(params, "a", 0.5), 0.0
+    elif name == "ellipsoid":  # constraint_ellipsoid.hpp: a, b, c (1)
+        first, second, third, unlimited = _f(params, "a", 1.0), _f(params, "b", 1.0), _f(params, "c", 1.0), 0.0
     else:
         first, unlimited = 0.0, 0.0
-    return E.CONSTRAINT[name], [first, unlimited, maxiter, tol, rescale, rescale_steps, rescale_freq]
+    return E.CONSTRAINT[name], [first, unlimited, maxiter, tol, rescale, rescale_steps, rescale_freq, second, third]
 
 
 _INT_BASE = ["dt", "group", "temperature_control", "min_val", "max_val", "steps"]

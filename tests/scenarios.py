@@ -69,3 +69,27 @@ def drive(backend, parts, box, periodic=True, nlist=(2.4, 0.3), constraint=("pla
     for name, p in integrators:
         sim.integrator(name, dict(p))
     return sim
+
+
+def surface_disks(kind, n, seed=1, **shape):
+    """n particles scattered near a cylinder (r), torus (c, a) or ellipsoid
+    (a, b, c) around the origin, with random directors; the constraint
+    projects them on the surface when it is added."""
+    rng = np.random.default_rng(seed)
+    u, v = rng.uniform(0.0, 2.0 * np.pi, n), rng.uniform(0.0, 2.0 * np.pi, n)
+    if kind == "cylinder":
+        r, Lz = shape["r"], shape["Lz"]
+        x, y, z = r * np.cos(u), r * np.sin(u), rng.uniform(-Lz / 2, Lz / 2, n)
+    elif kind == "torus":
+        c, a = shape["c"], shape["a"]
+        x, y, z = (c + a * np.cos(v)) * np.cos(u), (c + a * np.cos(v)) * np.sin(u), a * np.sin(v)
+    else:
+        a, b, c = shape["a"], shape["b"], shape["c"]
+        w = rng.uniform(-1.0, 1.0, n)
+        s = np.sqrt(1.0 - w * w)
+        x, y, z = a * s * np.cos(u), b * s * np.sin(u), c * w
+    jitter = rng.normal(0.0, 0.05, (3, n))
+    d = rng.normal(size=(3, n))
+    d /= np.linalg.norm(d, axis=0)
+    return dict(x=x + jitter[0], y=y + jitter[1], z=z + jitter[2], vx=np.zeros(n), vy=np.zeros(n), vz=np.zeros(n),
+                nx=d[0], ny=d[1], nz=d[2], radius=np.full(n, 1.0))

@@ -12,7 +12,7 @@ import pytest
 
 from oracle.oracle import OracleSystem
 from samos_b200 import Engine
-from scenarios import drive, plane_disks, sphere_disks
+from scenarios import drive, plane_disks, sphere_disks, surface_disks
 
 pytestmark = pytest.mark.gpu
 
@@ -295,6 +295,22 @@ def test_every_tuning_variant_gives_identical_bits(variant, case):
               "age", "ix", "iy"]
     for f in fields:
         np.testing.assert_array_equal(outs[0][0].download(f), outs[1][0].download(f), err_msg=f)
+
+
+@pytest.mark.parametrize("kind,shape,box,n", [
+    ("cylinder", {"r": 10.0, "Lz": 60.0}, (40.0, 40.0, 60.0), 700),
+    ("torus", {"c": 20.0, "a": 8.0}, (70.0, 70.0, 30.0), 1500),
+    ("ellipsoid", {"a": 20.0, "b": 15.0, "c": 12.0}, (50.0, 40.0, 34.0), 800),
+])
+def test_trajectory_curved_constraints(kind, shape, box, n):
+    # active Brownian particles on a cylinder / torus / ellipsoid (the generic
+    # fused kernel), 300 steps against the oracle with the shared noise stream
+    parts = surface_disks(kind, n, seed=17, **shape)
+    conf = {k: repr(v) for k, v in shape.items() if k != "Lz"}
+    e, o = run_both(n, parts, box, 299, periodic=(kind == "cylinder"), nlist=(2.4, 0.3), constraint=(kind, conf),
+                    pairs=[("soft", {"k": "10"})], aligns=[("polar", {"J": "0.2"})], dt=1e-3,
+                    integrators=[("brownian", {"v0": "1.0", "nu": "0.1", "seed": "4"})])
+    assert_traj(e, o)
 
 
 def test_trajectory_vicsek_model():

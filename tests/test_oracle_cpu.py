@@ -9,7 +9,7 @@ import pytest
 
 from oracle.oracle import OracleSystem, noise_gauss, noise_log, noise_uniform
 from samos_b200 import engine as E
-from scenarios import drive, plane_disks, sphere_disks
+from scenarios import drive, plane_disks, sphere_disks, surface_disks
 
 
 def two(x2, y2=0.0, r=(1.0, 1.0), box=20.0, n1=(1.0, 0.0, 0.0), n2=(0.0, 1.0, 0.0)):
@@ -213,3 +213,36 @@ def test_vicsek_integrator_follows_the_aligned_velocity():
     assert o.download("x")[0] == pytest.approx(0.03, abs=1e-15)
     assert o.download("y")[0] == pytest.approx(0.04, abs=1e-15)
     assert o.download("y")[1] == pytest.approx(0.05, abs=1e-15)  # (0, 1) -> v0 * (0, 1) * dt
+
+
+@pytest.mark.parametrize("kind,shape,box", [
+    ("cylinder", {"r": 10.0, "Lz": 40.0}, (40.0, 40.0, 40.0)),
+    ("torus", {"c": 12.0, "a": 5.0}, (50.0, 50.0, 50.0)),
+    ("ellipsoid", {"a": 12.0, "b": 9.0, "c": 7.0}, (40.0, 40.0, 40.0)),
+])
+def test_curved_constraints_project_onto_their_surface(kind, shape, box):
+    # constraint_cylinder.cpp:38-71 (radial), Constraint::enforce SHAKE for
+    # the implicit torus and ellipsoid (constraint.cpp:40-87): positions on
+    # the surface, directors unit and tangent
+    parts = surface_disks(kind, 300, seed=5, **shape)
+    o = OracleSystem(300)
+    conf = {k: repr(v) for k, v in shape.items() if k != "Lz"}
+    drive(o, parts, box, periodic=(kind == "cylinder"), constraint=(kind, conf))
+    x, y, z = o.download("x"), o.download("y"), o.download("z")
+    n = np.stack([o.download("nx"), o.download("ny"), o.download("nz")], 1)
+    if kind == "cylinder":
+        assert np.allclose(np.hypot(x, y), shape["r"], rtol=1e-14)
+        N = np.stack([x / shape["r"], y / shape["r"], 0 * z], 1)
+    elif kind == "torus":
+        g = (shape["c"] - np.hypot(x, y)) ** 2 + z ** 2 - shape["a"] ** 2
+        assert np.abs(g).max() <= 1e-6
+        s = np.hypot(x, y)
+        N = np.stack([-2 * (shape["c"] - s) / s * x, -2 * (shape["c"] - s) / s * y, 2 * z], 1)
+        N /= np.linalg.norm(N, axis=1)[:, None]
+    else:
+        g = x ** 2 / shape["a"] ** 2 + y ** 2 / shape["b"] ** 2 + z ** 2 / shape["c"] ** 2 - 1.0
+        assert np.abs(g).max() <= 1e-6
+        N = np.stack([2 * x / shape["a"] ** 2, 2 * y / shape["b"] ** 2, 2 * z / shape["c"] ** 2], 1)
+        N /= np.linalg.norm(N, axis=1)[:, None]
+    assert np.allclose(np.linalg.norm(n, axis=1), 1.0, atol=1e-14)
+    assert np.abs(np.sum(n * N, 1)).max() <= 1e-6
