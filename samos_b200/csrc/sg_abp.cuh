@@ -270,20 +270,28 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
       }
       noise_done = true;
     }
+    // list entries of the first chunk; each iteration then fetches the next
+    // chunk's entries while its own records are in flight (index -> record
+    // would otherwise be two dependent memory latencies per chunk)
+    int jn[CH];
+#pragma unroll
+    for (int u = 0; u < CH; u++) jn[u] = u < cnt ? __ldg(nl.nb + (size_t)u * nl.stride + k) : k;
     for (int q0 = 0; q0 < cnt || !noise_done; q0 += CH) {
       int jj[CH];
       D4 gg[CH], hh[CH];
       double rr[CH];
 #pragma unroll
-      for (int u = 0; u < CH; u++) {
-        const int q = q0 + u;
-        jj[u] = q < cnt ? __ldg(nl.nb + (size_t)q * nl.stride + k) : k;
-      }
+      for (int u = 0; u < CH; u++) jj[u] = jn[u];
 #pragma unroll
       for (int u = 0; u < CH; u++) {
         gg[u] = ldg4(Gin + jj[u]);
         if (PLANE) rr[u] = S.use_radii ? __ldg(st.r + jj[u]) : 1.0;
         if (!PLANE && ALIGN != ABP_ALIGN_NONE) hh[u] = ldg4(Hin + jj[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < CH; u++) {
+        const int q = q0 + CH + u;
+        jn[u] = q < cnt ? __ldg(nl.nb + (size_t)q * nl.stride + k) : k;
       }
       if (!noise_done) {  // independent of the loads above: overlaps their latency
         g_rot = noise_gauss(S.seed, c0 + (uint64_t)(D - 1));
