@@ -234,6 +234,10 @@ def step_kernel_name(variant):
     (soft + nematic + brownian on a periodic plane)."""
     if variant == 5:
         return "k_abp_flat<plane,nematic>"
+    if variant in (6, 7):
+        return f"k_abp_staged<plane,nematic,variant={variant}>"
+    if variant == 8:
+        return "k_abp_tile<plane,nematic>"
     return f"k_abp_step<plane,nematic,variant={variant}>"
 
 

@@ -37,17 +37,24 @@ struct AbpParams {
 // 0-4 per-particle sweep, 5 flattened, 6-7 staged (cp.async), 8 shared-memory
 // tile, 9-10 per-particle sweep with lanes assigned in neighbour-count order,
 // 11-14 ordered with the Gaussian draws taken before the sweep (fewer live
-// registers inside it), at rising occupancy
-constexpr int ABP_NVARIANT = 15;
+// registers inside it), at rising occupancy; 15-16 the same with each
+// neighbour record fetched one iteration before it is used, at 6-12 blocks/SM
+constexpr int ABP_NVARIANT = 21;
 __host__ __device__ constexpr int abp_chunk(int v) {
-  return v == 0 ? 4 : v == 1 ? 4 : v == 2 ? 2 : v == 3 ? 2 : v == 9 ? 2 : v == 10 ? 4 : v >= 11 ? 2 : 8;
+  return v == 0 ? 4 : v == 1 ? 4 : v == 2 ? 2 : v == 3 ? 2 : v == 9 ? 2 : v == 10 ? 4 : v >= 15 ? 1 : v >= 11 ? 2 : 8;
 }
 __host__ __device__ constexpr int abp_minb(int v) {
   return v == 0 ? 5 : v == 1 ? 4 : v == 2 ? 6 : v == 3 ? 4 : v == 9 ? 6 : v == 10 ? 5 : v == 11 ? 6 : v == 12 ? 7
-       : v == 13 ? 8 : v == 14 ? 10 : 3;
+       : v == 13 ? 8 : v == 14 ? 10 : v == 15 ? 7 : v == 16 ? 6 : v == 17 ? 8 : v == 18 ? 9 : v == 19 ? 10 : v == 20 ? 12 : 3;
 }
 __host__ __device__ constexpr bool abp_ordered(int v) { return v >= 9; }
 __host__ __device__ constexpr bool abp_prenoise(int v) { return v >= 11; }
+__host__ __device__ constexpr bool abp_pipelined(int v) { return v >= 15; }
+
+// The variants the autotuner times (every one can still be pinned): those
+// that never won on the plane, sphere or replica workloads are left out.
+constexpr int ABP_TUNED[] = {0, 1, 2, 3, 8, 9, 10, 11, 12, 13, 15, 16, 17, 18};
+constexpr int ABP_NTUNED = (int)(sizeof(ABP_TUNED) / sizeof(ABP_TUNED[0]));
 
 // Lane order of a block for the ordered variants: its particles sorted by
 // neighbour count, largest first (ties by slot), so each warp's 32 lanes have
@@ -236,6 +243,7 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
   }
   __syncthreads();
   static_assert(!(abp_ordered(VAR) && ENERGY), "the ordered variants change the block's energy summation order");
+  static_assert(!abp_pipelined(VAR) || abp_prenoise(VAR), "the pipelined sweep takes the draws first");
   const int k = blockIdx.x * BLOCK +
                 (abp_ordered(VAR) ? (int)lane_order[(size_t)blockIdx.x * BLOCK + threadIdx.x] : (int)threadIdx.x);
   double epair = 0.0, ealign = 0.0;
@@ -273,6 +281,27 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
     // list entries of the first chunk; each iteration then fetches the next
     // chunk's entries while its own records are in flight (index -> record
     // would otherwise be two dependent memory latencies per chunk)
+    if constexpr (abp_pipelined(VAR)) {
+      // one neighbour per iteration: its record was requested during the
+      // previous iteration, the entry after it two iterations ahead
+      int jnext = 1 < cnt ? __ldg(nl.nb + (size_t)1 * nl.stride + k) : k;
+      const int j0 = 0 < cnt ? __ldg(nl.nb + k) : k;
+      D4 gcur = ldg4(Gin + j0), hcur{0.0, 0.0, 0.0, 0.0};
+      double rcur = PLANE ? (S.use_radii ? __ldg(st.r + j0) : 1.0) : 0.0;
+      if (!PLANE && ALIGN != ABP_ALIGN_NONE) hcur = ldg4(Hin + j0);
+      for (int q = 0; q < cnt; q++) {
+        const D4 g = gcur, h = hcur;
+        const double rj = PLANE ? rcur : g.w;
+        if (q + 1 < cnt) {
+          gcur = ldg4(Gin + jnext);
+          if (PLANE) rcur = S.use_radii ? __ldg(st.r + jnext) : 1.0;
+          if (!PLANE && ALIGN != ABP_ALIGN_NONE) hcur = ldg4(Hin + jnext);
+          jnext = q + 2 < cnt ? __ldg(nl.nb + (size_t)(q + 2) * nl.stride + k) : k;
+        }
+        abp_pair_term<SHAPE, ALIGN, ENERGY>(S, x, y, z, nx, ny, nz, ri, g, h, rj, q >= lo, fx, fy, fz, tx, ty, tz,
+                                            epair, ealign);
+      }
+    } else {
     int jn[CH];
 #pragma unroll
     for (int u = 0; u < CH; u++) jn[u] = u < cnt ? __ldg(nl.nb + (size_t)u * nl.stride + k) : k;
@@ -310,6 +339,7 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
                                               q >= lo, fx, fy, fz, tx, ty, tz, epair, ealign);
         }
       }
+    }
     }
     // read only now: values the sweep does not need stay out of its registers
     const double ox = nl.ox[k], oy = nl.oy[k], oz = PLANE ? 0.0 : nl.oz[k];

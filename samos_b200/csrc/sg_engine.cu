@@ -1238,6 +1238,12 @@ static void launch_abp3(sg_system* s, bool apply_e1, bool last, bool energy) {
     case 12: launch_abp_v<SHAPE, ALIGN, SP, false, 12>(s, apply_e1, last); break;
     case 13: launch_abp_v<SHAPE, ALIGN, SP, false, 13>(s, apply_e1, last); break;
     case 14: launch_abp_v<SHAPE, ALIGN, SP, false, 14>(s, apply_e1, last); break;
+    case 15: launch_abp_v<SHAPE, ALIGN, SP, false, 15>(s, apply_e1, last); break;
+    case 16: launch_abp_v<SHAPE, ALIGN, SP, false, 16>(s, apply_e1, last); break;
+    case 17: launch_abp_v<SHAPE, ALIGN, SP, false, 17>(s, apply_e1, last); break;
+    case 18: launch_abp_v<SHAPE, ALIGN, SP, false, 18>(s, apply_e1, last); break;
+    case 19: launch_abp_v<SHAPE, ALIGN, SP, false, 19>(s, apply_e1, last); break;
+    case 20: launch_abp_v<SHAPE, ALIGN, SP, false, 20>(s, apply_e1, last); break;
     case 0: launch_abp_v<SHAPE, ALIGN, SP, false, 0>(s, apply_e1, last); break;
     case 1: launch_abp_v<SHAPE, ALIGN, SP, false, 1>(s, apply_e1, last); break;
     case 2: launch_abp_v<SHAPE, ALIGN, SP, false, 2>(s, apply_e1, last); break;
@@ -1266,7 +1272,7 @@ static constexpr int TUNE_REPS = 3;  // timed steps per candidate (after one unt
 static int step_hot(sg_system* s, int shape, bool apply_e1, bool last, bool energy) {
   const bool tuning = s->abp_on && !s->tuned && !energy;
   if (tuning) {
-    s->abp_variant = (s->tune_trial / (TUNE_REPS + 1)) % ABP_NVARIANT;
+    s->abp_variant = ABP_TUNED[(s->tune_trial / (TUNE_REPS + 1)) % ABP_NTUNED];
     CU(s, cudaEventRecord(s->ev_t0, s->stream));
   }
   if (s->abp_on && !energy && s->abp_variant == 8 && !s->tile_valid) {
@@ -1299,10 +1305,12 @@ static int step_hot(sg_system* s, int shape, bool apply_e1, bool last, bool ener
     const int v = s->abp_variant;
     if (s->tune_trial % (TUNE_REPS + 1) != 0) { s->tune_ms[v] += ms; s->tune_n[v]++; }
     s->tune_trial++;
-    if (s->tune_trial >= ABP_NVARIANT * (TUNE_REPS + 1)) {
-      int best = 0;
-      for (int c = 1; c < ABP_NVARIANT; c++)
+    if (s->tune_trial >= ABP_NTUNED * (TUNE_REPS + 1)) {
+      int best = ABP_TUNED[0];
+      for (int i = 1; i < ABP_NTUNED; i++) {
+        const int c = ABP_TUNED[i];
         if (s->tune_ms[c] / s->tune_n[c] < s->tune_ms[best] / s->tune_n[best]) best = c;
+      }
       s->abp_variant = best;
       s->tuned = true;
     }

@@ -265,7 +265,7 @@ VARIANT_CASES = {
 
 
 @pytest.mark.parametrize("case", sorted(VARIANT_CASES))
-@pytest.mark.parametrize("variant", list(range(15)))
+@pytest.mark.parametrize("variant", list(range(21)))
 def test_every_tuning_variant_gives_identical_bits(variant, case):
     c = VARIANT_CASES[case]
     n = c["n"]
