@@ -75,6 +75,8 @@ struct sg_system {
   int nact = 0;
   int *rebuild = nullptr, *status = nullptr, *maxnb = nullptr;
   int *bstatus = nullptr;   // list-build status (overflow), separate from the run's status word
+  void* xfer = nullptr;     // staging for host transfers in particle-id order (largest replica)
+  int* xerr = nullptr;      // set by the transfer kernels on an id outside the replica
   int *exec_cnt = nullptr;  // steps executed in a batch (batched stepping)
   int *fire_cnt = nullptr;  // per replica: blocks of k_fire_b done (the last one runs the FIRE control)
   int64_t since_rebuild = 0, last_gap = 8;  // batch length follows the steps between rebuilds
@@ -334,6 +336,69 @@ static int slot_map(sg_system* s, int replica, std::vector<int>& slot_of_id) {
   return SG_OK;
 }
 
+}  // extern "C"
+
+// Host arrays are in particle-id order, device slots in cell order: uploads
+// copy the array as it is into a staging buffer and gather it into slot order
+// on the device (slot k holds particle id[k]); downloads scatter slots into
+// id order on the device and copy the staging buffer back as it is.
+template <class T>
+__global__ void k_gather_ids(T* __restrict__ dst, const T* __restrict__ src, const int* __restrict__ id, int n,
+                             int* err) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int i = id[k];
+  if ((unsigned)i < (unsigned)n) dst[k] = src[i];
+  else atomicOr(err, 1);
+}
+
+template <class T>
+__global__ void k_scatter_ids(T* __restrict__ dst, const T* __restrict__ src, const int* __restrict__ id, int n,
+                              int* err) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int i = id[k];
+  if ((unsigned)i < (unsigned)n) dst[i] = src[k];
+  else atomicOr(err, 1);
+}
+
+static int xfer_ready(sg_system* s) {
+  if (s->xfer) return SG_OK;
+  int maxn = 0;
+  for (int v : s->n) maxn = std::max(maxn, v);
+  s->xfer = s->mem.alloc<double>(std::max(1, maxn));
+  s->xerr = s->mem.alloc<int>(1);
+  if (s->mem.err != cudaSuccess) { s->mem.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "transfer staging allocation failed"); }
+  return SG_OK;
+}
+
+// Copies n values of T between host (id order) and the replica's slots.
+template <class T>
+static int xfer_field(sg_system* s, int replica, T* dev, T* host, bool to_device) {
+  int rc = xfer_ready(s);
+  if (rc) return rc;
+  const int n = s->n[replica], off = s->off[replica];
+  if (n == 0) return SG_OK;
+  T* stage = (T*)s->xfer;
+  const int g = (n + 255) / 256;
+  CU(s, cudaMemsetAsync(s->xerr, 0, sizeof(int), s->stream));
+  if (to_device) {
+    CU(s, cudaMemcpyAsync(stage, host, sizeof(T) * n, cudaMemcpyHostToDevice, s->stream));
+    k_gather_ids<T><<<g, 256, 0, s->stream>>>(dev + off, stage, s->st.id + off, n, s->xerr);
+  } else {
+    k_scatter_ids<T><<<g, 256, 0, s->stream>>>(stage, dev + off, s->st.id + off, n, s->xerr);
+    CU(s, cudaMemcpyAsync(host, stage, sizeof(T) * n, cudaMemcpyDeviceToHost, s->stream));
+  }
+  CU(s, cudaGetLastError());
+  int bad = 0;
+  CU(s, cudaMemcpyAsync(&bad, s->xerr, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  if (bad) return fail(s, SG_ERR_STATE, "corrupt id map");
+  return SG_OK;
+}
+
+extern "C" {
+
 static int field_ptr(sg_system* s, const char* field, void** p, bool* is_int, int* nfield) {
   *nfield = -1;
   for (int i = 0; i < kNumDynDouble; i++)
@@ -356,29 +421,24 @@ int sg_upload(sg_system* s, int replica, const char* field, const void* host) {
   int rc = field_ptr(s, field, &dp, &is_int, &nf);
   if (rc) return rc;
   const int n = s->n[replica], off = s->off[replica];
-  std::vector<int> slot_of_id;
-  if ((rc = slot_map(s, replica, slot_of_id))) return rc;
   if (!dp) {  // surface normal: kept on the host, used where no constraint sets it
+    std::vector<int> slot_of_id;
+    if ((rc = slot_map(s, replica, slot_of_id))) return rc;
     int c = field[1] - 'x';
     const double* h = (const double*)host;
     for (int i = 0; i < n; i++) s->uploaded_N[c][off + i] = h[i];
     return SG_OK;
   }
   if (is_int) {
-    std::vector<int> buf(n);
     const int* h = (const int*)host;
-    for (int i = 0; i < n; i++) buf[slot_of_id[i]] = h[i];
     if (!std::strcmp(field, "type"))
       for (int i = 0; i < n; i++)
         if (h[i] < 1 || h[i] > s->ntypes) return fail(s, SG_ERR_ARG, "particle type outside 1..ntypes");
-    CU(s, cudaMemcpyAsync((int*)dp + off, buf.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s->stream));
+    rc = xfer_field<int>(s, replica, (int*)dp, (int*)host, true);
   } else {
-    std::vector<double> buf(n);
-    const double* h = (const double*)host;
-    for (int i = 0; i < n; i++) buf[slot_of_id[i]] = h[i];
-    CU(s, cudaMemcpyAsync((double*)dp + off, buf.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+    rc = xfer_field<double>(s, replica, (double*)dp, (double*)host, true);
   }
-  CU(s, cudaStreamSynchronize(s->stream));
+  if (rc) return rc;
   s->e1_applied = false;
   s->forces_fresh = false;
   return SG_OK;
@@ -390,9 +450,9 @@ int sg_download(sg_system* s, int replica, const char* field, void* host) {
   int rc = field_ptr(s, field, &dp, &is_int, &nf);
   if (rc) return rc;
   const int n = s->n[replica], off = s->off[replica];
-  std::vector<int> ids(n);
-  CU(s, cudaMemcpyAsync(ids.data(), s->st.id + off, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
   if (!dp) {
+    std::vector<int> ids(n);
+    CU(s, cudaMemcpyAsync(ids.data(), s->st.id + off, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
     // surface normal of the last constraint that sets one (plane: (0,0,1),
     // sphere: x/R as in constraint_sphere.hpp:76)
     const int comp = field[1] - 'x';
@@ -420,20 +480,8 @@ int sg_download(sg_system* s, int replica, const char* field, void* host) {
     }
     return SG_OK;
   }
-  if (is_int) {
-    std::vector<int> buf(n);
-    CU(s, cudaMemcpyAsync(buf.data(), (int*)dp + off, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
-    CU(s, cudaStreamSynchronize(s->stream));
-    int* h = (int*)host;
-    for (int k = 0; k < n; k++) h[ids[k]] = buf[k];
-  } else {
-    std::vector<double> buf(n);
-    CU(s, cudaMemcpyAsync(buf.data(), (double*)dp + off, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
-    CU(s, cudaStreamSynchronize(s->stream));
-    double* h = (double*)host;
-    for (int k = 0; k < n; k++) h[ids[k]] = buf[k];
-  }
-  return SG_OK;
+  if (is_int) return xfer_field<int>(s, replica, (int*)dp, (int*)host, false);
+  return xfer_field<double>(s, replica, (double*)dp, (double*)host, false);
 }
 
 // ---------------------------------------------------------------------------
