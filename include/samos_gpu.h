@@ -204,15 +204,21 @@ int  sg_set_profiling(sg_system* s, int on);
  * without the specialisation.  All give the same results; the switch exists
  * so tests can compare them.  No reference counterpart.                     */
 int  sg_set_path(sg_system* s, int path);
-/* Kernel variant of the specialised active-Brownian step (0..4: per-particle
- * neighbour sweep, neighbour records fetched ahead x resident blocks per SM;
- * 5: flattened warp-wide pair sweep); all variants compute the
- * same bits.  By default the engine's autotuner times every variant on the
+/* Kernel variant of the specialised active-Brownian step (0..20: per-particle
+ * neighbour sweeps that differ in how far ahead neighbour records are
+ * fetched, resident blocks per SM, lane order and where the Gaussian draws
+ * are taken; a flattened warp-wide sweep; shared-memory staged and tiled
+ * sweeps); all variants compute the same bits.  By default the engine's autotuner times every variant on the
  * first steps of a run and keeps the fastest; sg_set_variant pins one
  * (-1 re-enables tuning), sg_get_variant reports the choice (-1 = not yet
  * tuned).  No reference counterpart.                                        */
 int  sg_set_variant(sg_system* s, int variant);
 int  sg_get_variant(const sg_system* s);
+/* Neighbour-list build kernel: 0 = automatic (lanes of a team share one
+ * particle's 27-cell stencil when fewer than 2^20 particles are rebuilt,
+ * one thread per particle otherwise), 1 = always one thread per particle,
+ * 2 = always teams.  All build the same lists.  No reference counterpart.   */
+int  sg_set_build(sg_system* s, int mode);
 
 /* ---- device view (for kernels that work on the engine's state) -----------
  * No reference counterpart.  Device pointers into the handle's current

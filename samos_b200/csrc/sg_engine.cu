@@ -107,6 +107,7 @@ struct sg_system {
   int* tile_slot = nullptr;
   uint16_t* nbpos = nullptr;
   int nbpos_cap = 0;
+  int build_mode = 0;        // list build: 0 automatic, 1 one thread per particle, 2 teams of TEAM lanes
   bool tile_valid = false;
   // ordered variants: per-block lane order by neighbour count (k_lane_order)
   uint8_t* lane_order = nullptr;
@@ -530,6 +531,8 @@ static int prepare_blist(sg_system* s) {
 }
 static const int* blist_of(const sg_system* s) { return s->nblist == s->nblocks ? nullptr : s->blist; }
 
+static constexpr int64_t kTeamBelow = 1 << 20;  // particles: team list build below this many
+
 static int rebuild_flagged(sg_system* s, bool* sorted) {
   s->forces_fresh = false;
   bool any_sort = false;
@@ -558,6 +561,9 @@ static int rebuild_flagged(sg_system* s, bool* sorted) {
   }
   const int nseg = (int)s->segs_h.size();
   if (nseg == 0) return SG_OK;
+  int64_t nflag = 0;  // particles of the flagged replicas
+  for (int r = 0; r < s->nrep; r++)
+    if (s->rebuild_h[r]) nflag += s->n[r];
   CU(s, cudaMemcpyAsync(s->segs, s->segs_h.data(), sizeof(CellSeg) * nseg, cudaMemcpyHostToDevice, s->stream));
   for (int attempt = 0; attempt < 4; attempt++) {
     k_seg_zero<<<std::min((nvirt + 255) / 256, 148 * 16), 256, 0, s->stream>>>(s->segs, nseg, nvirt, s->cell_cnt,
@@ -587,8 +593,15 @@ static int rebuild_flagged(sg_system* s, bool* sorted) {
       k_rb_copyback<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->alt, s->cur, s->st_alt, s->st, bl);
       LAUNCH_CHECK(s);
     }
-    k_rb_build<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->st, s->nl, s->perm,
-                                           s->cell_start, s->cell_cnt, s->bstatus, s->maxnb, bl);
+    // a rebuild of few particles is latency bound: split each particle's
+    // stencil over a team of lanes; a large one is issue bound: one thread each
+    if (s->build_mode == 2 || (s->build_mode == 0 && nflag < kTeamBelow))
+      k_rb_build_team<<<ng * TEAM_SUB, TEAM * TEAM_PARTS, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur,
+                                                                          s->st, s->nl, s->perm, s->cell_start,
+                                                                          s->cell_cnt, s->bstatus, s->maxnb, bl);
+    else
+      k_rb_build<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->st, s->nl, s->perm,
+                                             s->cell_start, s->cell_cnt, s->bstatus, s->maxnb, bl);
     LAUNCH_CHECK(s);
     int st = 0, mx = 0;
     CU(s, cudaMemcpyAsync(&st, s->bstatus, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
@@ -597,12 +610,17 @@ static int rebuild_flagged(sg_system* s, bool* sorted) {
     if (!(st & ST_OVERFLOW)) {
       // tile data: re-derived for the rebuilt blocks (the others keep theirs);
       // a grown list capacity invalidates every block's positions
+      // (dropped once the tuner has settled on a variant that does not read
+      // them; taking such a variant later re-derives them in full)
       if (s->lane_order && s->order_valid) {
-        k_lane_order<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->nl, s->lane_order, bl);
-        LAUNCH_CHECK(s);
+        if (s->tuned && !abp_ordered(s->abp_variant)) s->order_valid = false;
+        else {
+          k_lane_order<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->nl, s->lane_order, bl);
+          LAUNCH_CHECK(s);
+        }
       }
       if (s->tile_n && s->tile_valid) {
-        if (s->nbpos_cap < s->nl.cap) s->tile_valid = false;
+        if (s->nbpos_cap < s->nl.cap || (s->tuned && s->abp_variant != 8)) s->tile_valid = false;
         else {
           k_tile_prep<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->nl, s->tile_n, s->tile_slot, s->nbpos, bl);
           LAUNCH_CHECK(s);
@@ -1677,6 +1695,12 @@ int sg_set_variant(sg_system* s, int variant) {
 }
 
 int sg_get_variant(const sg_system* s) { return s ? (s->tuned ? s->abp_variant : -1) : SG_ERR_ARG; }
+
+int sg_set_build(sg_system* s, int mode) {
+  if (!s || mode < 0 || mode > 2) return SG_ERR_ARG;
+  s->build_mode = mode;
+  return SG_OK;
+}
 
 int sg_set_path(sg_system* s, int path) {
   if (!s || path < 0 || path > 2) return SG_ERR_ARG;

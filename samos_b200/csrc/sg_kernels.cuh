@@ -1045,17 +1045,11 @@ __device__ __forceinline__ int build_stencil(const Replica& R, int a, int b, int
   return ncells;
 }
 
-__global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                           const int* __restrict__ rebuild, Dyn d, Stat st, NbList nl,
-                           const int* __restrict__ cslot, const int* __restrict__ cstart,
-                           const int* __restrict__ ccnt, int* __restrict__ status, int* __restrict__ maxnb, const int* __restrict__ blist = nullptr) {
-  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
-  const int r = blk_rep[bid_];
-  const int mode = rebuild[r];
-  if (!mode) return;
-  const Replica& R = reps[r];
-  const int k = bid_ * BLOCK + threadIdx.x;
-  if (k - R.off >= R.n) return;
+// The list of slot k, built by one thread (the reference algorithm as it stands).
+__device__ __forceinline__ void build_particle(const Replica& R, int mode, int k, Dyn d, Stat st, NbList nl,
+                                              const int* __restrict__ cslot, const int* __restrict__ cstart,
+                                              const int* __restrict__ ccnt, int* __restrict__ status,
+                                              int* __restrict__ maxnb) {
   const double x = d.x[k], y = d.y[k], z = d.z[k];
   const int myid = st.id[k];
   int a, b, c;
@@ -1133,6 +1127,123 @@ __global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restri
     nl.cnt[k] = total; nl.lo[k] = nlo;
   }
   nl.ox[k] = x; nl.oy[k] = y; nl.oz[k] = z;
+}
+
+__global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                           const int* __restrict__ rebuild, Dyn d, Stat st, NbList nl,
+                           const int* __restrict__ cslot, const int* __restrict__ cstart,
+                           const int* __restrict__ ccnt, int* __restrict__ status, int* __restrict__ maxnb, const int* __restrict__ blist = nullptr) {
+  const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
+  const int r = blk_rep[bid_];
+  const int mode = rebuild[r];
+  if (!mode) return;
+  const Replica& R = reps[r];
+  const int k = bid_ * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  build_particle(R, mode, k, d, st, nl, cslot, cstart, ccnt, status, maxnb);
+}
+
+// Cell m (0..26) of the 27-cell stencil of (a, b, c), in the visiting order
+// of build_stencil (x offset outermost, z innermost), with periodic wrap.
+__device__ __forceinline__ int stencil_cell(const Replica& R, int a, int b, int c, int m) {
+  int ia = a + m / 9 - 1, ib = b + (m / 3) % 3 - 1, ic = c + m % 3 - 1;
+  if (ia < 0) ia = R.cnx - 1; else if (ia == R.cnx) ia = 0;
+  if (ib < 0) ib = R.cny - 1; else if (ib == R.cny) ib = 0;
+  if (ic < 0) ic = R.cnz - 1; else if (ic == R.cnz) ic = 0;
+  return R.cny * R.cnz * ia + R.cnz * ib + ic;
+}
+
+// Team list build: TEAM lanes per particle, lane t sweeping its own run of
+// consecutive stencil cells, so a rebuild of a few small replicas is not
+// bound by one thread's chain of dependent loads.  Concatenated in lane order
+// the lanes' finds are in stencil visiting order; the lower-id ones are then
+// ranked by id (ties by position, i.e. a stable sort) and the higher-id ones
+// written in that order: the lists are those of k_rb_build.  The N^2 path and
+// a lane with more finds than it stages fall back to build_particle.
+constexpr int TEAM = 8;
+constexpr int TEAM_PARTS = 32;  // particles per block of TEAM * TEAM_PARTS threads
+constexpr int TEAM_SUB = BLOCK / TEAM_PARTS;  // blocks per packed block
+constexpr int NB_TEAM = 16;     // finds staged per lane and side
+
+__global__ void __launch_bounds__(TEAM * TEAM_PARTS)
+k_rb_build_team(const Replica* __restrict__ reps, const int* __restrict__ blk_rep, const int* __restrict__ rebuild,
+                Dyn d, Stat st, NbList nl, const int* __restrict__ cslot, const int* __restrict__ cstart,
+                const int* __restrict__ ccnt, int* __restrict__ status, int* __restrict__ maxnb,
+                const int* __restrict__ blist = nullptr) {
+  __shared__ unsigned long long lokeys[TEAM_PARTS][NB_LOCAL];
+  const int bid_ = blist ? blist[blockIdx.x / TEAM_SUB] : (int)(blockIdx.x / TEAM_SUB);
+  const int r = blk_rep[bid_];
+  const int mode = rebuild[r];
+  if (!mode) return;
+  const Replica& R = reps[r];
+  const int pl = threadIdx.x / TEAM, t = threadIdx.x % TEAM;
+  const int k = bid_ * BLOCK + (blockIdx.x % TEAM_SUB) * TEAM_PARTS + pl;
+  if (k - R.off >= R.n) return;  // the whole team leaves together
+  const unsigned tmask = 0xffu << ((threadIdx.x & 31) & ~(TEAM - 1));
+  if (!R.use_cell) {
+    if (t == 0) build_particle(R, mode, k, d, st, nl, cslot, cstart, ccnt, status, maxnb);
+    return;
+  }
+  const double x = d.x[k], y = d.y[k], z = d.z[k];
+  const int myid = st.id[k];
+  int a, b, c;
+  cell_of(R, x, y, z, a, b, c);
+  const int base0 = cstart[R.cell_off];
+  unsigned long long lo[NB_TEAM];  // (id << 32) | slot
+  int up[NB_TEAM];
+  int nlo = 0, nup = 0;
+  const int m1 = (t + 1) * 27 / TEAM;
+  for (int m = t * 27 / TEAM; m < m1; m++) {
+    const int cg = R.cell_off + stencil_cell(R, a, b, c, m);
+    const int s0 = R.off + cstart[cg] - base0, n = ccnt[cg];
+    for (int q = 0; q < n; q++) {
+      const int j = mode == 2 ? s0 + q : cslot[s0 + q];
+      const int jid = st.id[j];
+      if (jid == myid) continue;
+      double dx, dy, dz;
+      if (myid < jid) { dx = x - d.x[j]; dy = y - d.y[j]; dz = z - d.z[j]; }
+      else { dx = d.x[j] - x; dy = d.y[j] - y; dz = d.z[j] - z; }
+      apply_periodic(R, dx, dy, dz);
+      if (dx * dx + dy * dy + dz * dz < R.cut2) {
+        if (jid < myid) { if (nlo < NB_TEAM) lo[nlo] = ((unsigned long long)(unsigned)jid << 32) | (unsigned)j; nlo++; }
+        else { if (nup < NB_TEAM) up[nup] = j; nup++; }
+      }
+    }
+  }
+  if (__any_sync(tmask, nlo > NB_TEAM || nup > NB_TEAM)) {
+    if (t == 0) build_particle(R, mode, k, d, st, nl, cslot, cstart, ccnt, status, maxnb);
+    return;
+  }
+  int plo = nlo, pup = nup;  // inclusive scans over the team
+  for (int o = 1; o < TEAM; o <<= 1) {
+    const int u = __shfl_up_sync(tmask, plo, o, TEAM), v = __shfl_up_sync(tmask, pup, o, TEAM);
+    if (t >= o) { plo += u; pup += v; }
+  }
+  const int tot_lo = __shfl_sync(tmask, plo, TEAM - 1, TEAM), tot_up = __shfl_sync(tmask, pup, TEAM - 1, TEAM);
+  plo -= nlo; pup -= nup;
+  const int total = tot_lo + tot_up;
+  if (t == 0) {
+    atomicMax(maxnb, total);
+    nl.ox[k] = x; nl.oy[k] = y; nl.oz[k] = z;
+  }
+  if (tot_lo > NB_LOCAL || total > nl.cap) {  // the one-thread build's overflow rule
+    if (t == 0) { atomicOr(status, ST_OVERFLOW); nl.cnt[k] = 0; nl.lo[k] = 0; }
+    return;
+  }
+  for (int i = 0; i < nlo; i++) lokeys[pl][plo + i] = lo[i];
+  __syncwarp(tmask);
+  for (int i = t; i < tot_lo; i += TEAM) {
+    const unsigned long long v = lokeys[pl][i];
+    const unsigned vid = (unsigned)(v >> 32);
+    int rank = 0;
+    for (int m = 0; m < tot_lo; m++) {
+      const unsigned mid = (unsigned)(lokeys[pl][m] >> 32);
+      rank += (mid < vid || (mid == vid && m < i)) ? 1 : 0;
+    }
+    nl.nb[(size_t)rank * nl.stride + k] = (int)(unsigned)(v & 0xffffffffull);
+  }
+  for (int i = 0; i < nup; i++) nl.nb[(size_t)(tot_lo + pup + i) * nl.stride + k] = up[i];
+  if (t == 0) { nl.cnt[k] = total; nl.lo[k] = tot_lo; }
 }
 
 }  // namespace sg

@@ -101,6 +101,7 @@ def load() -> C.CDLL:
         "sg_positions_changed": (I, [P]),
         "sg_memcpy": (I, [P, P, I64]),
         "sg_set_variant": (I, [P, I]),
+        "sg_set_build": (I, [P, I]),
         "sg_get_variant": (I, [P]),
         "sg_compute_static": (I, [I, D, D, D, I, D, D] + [P] * 7 + [D, D, I, I, D, D] + [P] * 6 + [P]),
         "sg_compute_static_scratch_bytes": (I64, []),
@@ -309,8 +310,12 @@ class Engine:
         self._check(self.lib.sg_positions_changed(self.h))
 
     def set_variant(self, v: int) -> None:
-        """Pin a step-kernel variant (0..4) or re-enable autotuning (-1)."""
+        """Pin a step-kernel variant (0..20) or re-enable autotuning (-1)."""
         self._check(self.lib.sg_set_variant(self.h, int(v)))
+
+    def set_build(self, mode: int) -> None:
+        """Neighbour-list build kernel: 0 automatic, 1 one thread per particle, 2 teams."""
+        self._check(self.lib.sg_set_build(self.h, int(mode)))
 
     def variant(self) -> int:
         return int(self.lib.sg_get_variant(self.h))

@@ -64,6 +64,79 @@ def test_pairs_sphere_identical():
     np.testing.assert_array_equal(ej, oj)
 
 
+def full_lists(e):
+    """Every slot's whole neighbour list (lower-id part, then upper part) in
+    particle ids, keyed by the particle id, read through the device view."""
+    v = e.view()
+    n = v.slots
+    cnt = np.empty(n, np.int32)
+    ids = np.empty(n, np.int32)
+    e._check(e.lib.sg_memcpy(cnt.ctypes.data, v.nb_cnt, cnt.nbytes))
+    e._check(e.lib.sg_memcpy(ids.ctypes.data, v.id, ids.nbytes))
+    rows = int(cnt.max())
+    nb = np.empty((rows, v.nb_stride), np.int32)
+    for q in range(rows):
+        e._check(e.lib.sg_memcpy(nb[q].ctypes.data, v.nb + 4 * q * v.nb_stride, 4 * v.nb_stride))
+    out = {}
+    for k in range(n):
+        out[int(ids[k])] = [int(ids[nb[q, k]]) for q in range(cnt[k])]
+    return out
+
+
+def clustered_disks(per=24, grid=12, spacing=4.0, seed=9):
+    """Tight clumps of `per` disks on a square grid: every disk has all its
+    clump in its own cell, more finds than one lane of a team build stages."""
+    rng = np.random.default_rng(seed)
+    cx, cy = np.meshgrid(np.arange(grid) * spacing, np.arange(grid) * spacing)
+    L = grid * spacing
+    c = np.stack([cx.ravel(), cy.ravel()], 1) - L / 2 + spacing / 2
+    a = rng.uniform(0.0, 2.0 * np.pi, (len(c), per))
+    rr = 0.4 * np.sqrt(rng.uniform(0.0, 1.0, (len(c), per)))
+    x = (c[:, 0:1] + rr * np.cos(a)).ravel()
+    y = (c[:, 1:2] + rr * np.sin(a)).ravel()
+    n = len(x)
+    order = rng.permutation(n)
+    th = rng.uniform(0.0, 2.0 * np.pi, n)
+    parts = dict(x=x[order], y=y[order], z=np.zeros(n), vx=np.zeros(n), vy=np.zeros(n), vz=np.zeros(n),
+                 nx=np.cos(th), ny=np.sin(th), nz=np.zeros(n), radius=np.full(n, 0.1))
+    return parts, L
+
+
+BUILD_CASES = {
+    "plane_cells": lambda: (plane_disks(2000, 0.6, seed=1), 10.0, True, ("plane", {})),
+    "plane_two_cell_z": lambda: (plane_disks(800, 0.6, seed=3), 6.0, True, ("plane", {})),
+    "plane_nsq": lambda: (plane_disks(500, 0.6, seed=2), 4.0, True, ("plane", {})),
+    "plane_clumps": lambda: (clustered_disks(), 10.0, True, ("plane", {})),
+}
+
+
+@pytest.mark.parametrize("case", list(BUILD_CASES) + ["sphere"])
+def test_team_and_thread_list_builds_identical(case):
+    if case == "sphere":
+        parts, R = sphere_disks(3000, seed=4)
+        box, periodic, cons = (2 * R + 6.0,) * 3, False, ("sphere", {"r": repr(R)})
+    else:
+        (parts, L), lz, periodic, cons = BUILD_CASES[case]()
+        box = (L, L, lz)
+    n = len(parts["x"])
+    lists, pairs = [], []
+    for mode in (1, 2):
+        e = Engine(n)
+        e.set_build(mode)
+        drive(e, parts, box, periodic=periodic, nlist=(2.4, 0.3), constraint=cons)
+        lists.append(full_lists(e))
+        pairs.append(e.pairs())
+    o = OracleSystem(n)
+    drive(o, parts, box, periodic=periodic, nlist=(2.4, 0.3), constraint=cons)
+    assert lists[0] == lists[1]
+    oi, oj = o.pairs()
+    for ei, ej in pairs:
+        np.testing.assert_array_equal(ei, oi)
+        np.testing.assert_array_equal(ej, oj)
+    if case == "plane_clumps":  # some disks have more finds on one side than a lane stages (16)
+        assert max(max(sum(j < i for j in v), sum(j > i for j in v)) for i, v in lists[0].items()) > 16
+
+
 def compute_both(parts, box, pairs=(), aligns=(), externals=(), nlist=(2.4, 0.3), periodic=True,
                  constraint=("plane", {}), ntypes=1, pair_params=(), align_params=()):
     n = len(parts["x"])
