@@ -215,7 +215,7 @@ int  sg_set_path(sg_system* s, int path);
 int  sg_set_variant(sg_system* s, int variant);
 int  sg_get_variant(const sg_system* s);
 /* Neighbour-list build kernel: 0 = automatic (lanes of a team share one
- * particle's 27-cell stencil when fewer than 2^20 particles are rebuilt,
+ * particle's 27-cell stencil when fewer than 2^16 particles are rebuilt,
  * one thread per particle otherwise), 1 = always one thread per particle,
  * 2 = always teams.  All build the same lists.  No reference counterpart.   */
 int  sg_set_build(sg_system* s, int mode);

@@ -65,9 +65,15 @@ struct sg_system {
   int *pcell = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
   int *tmp = nullptr, *perm = nullptr, *scan_bsum = nullptr;
   CellSeg* segs = nullptr;            // cell ranges of the replicas being rebuilt
-  std::vector<CellSeg> segs_h;
   int* blist = nullptr;               // blocks of the replicas being rebuilt (null: every block)
-  std::vector<int> blist_h;
+  // pinned staging of the small per-rebuild uploads (block list, cell
+  // segments) and of the build's status readback; ev_pin marks the last copy
+  // out of the staging, which must have run before the staging is rewritten
+  int* pin_blist = nullptr;
+  CellSeg* pin_segs = nullptr;
+  int* pin_res = nullptr;
+  cudaEvent_t ev_pin = nullptr;
+  bool b_pending = false;  // ev_b0 / ev_b1 bracket a rebuild not yet added to the run's rebuild time
   int nblist = 0;
   // minimiser: blocks of the replicas that have not converged (null: every block)
   int* act = nullptr;
@@ -252,6 +258,16 @@ int sg_create(int n_replicas, const int32_t* n_particles, int ntypes, sg_system*
   s->perm = m.alloc<int>(s->slots);
   if (!ok || m.err != cudaSuccess) { m.free_all(); cudaStreamDestroy(s->stream); delete s; return SG_ERR_NOMEM; }
   cudaMallocHost((void**)&s->rebuild_h, sizeof(int) * n_replicas);
+  cudaMallocHost((void**)&s->pin_blist, sizeof(int) * std::max(1, s->nblocks));
+  cudaMallocHost((void**)&s->pin_segs, sizeof(CellSeg) * n_replicas);
+  cudaMallocHost((void**)&s->pin_res, sizeof(int) * 2);
+  cudaEventCreateWithFlags(&s->ev_pin, cudaEventDisableTiming);
+  if (!s->rebuild_h || !s->pin_blist || !s->pin_segs || !s->pin_res) {
+    for (void* h : {(void*)s->rebuild_h, (void*)s->pin_blist, (void*)s->pin_segs, (void*)s->pin_res})
+      if (h) cudaFreeHost(h);
+    if (s->ev_pin) cudaEventDestroy(s->ev_pin);
+    m.free_all(); cudaStreamDestroy(s->stream); delete s; return SG_ERR_NOMEM;
+  }
   cudaEventCreate(&s->ev_run0); cudaEventCreate(&s->ev_run1);
   cudaEventCreate(&s->ev_k0); cudaEventCreate(&s->ev_k1);
   cudaEventCreate(&s->ev_t0); cudaEventCreate(&s->ev_t1);
@@ -296,7 +312,9 @@ int sg_destroy(sg_system* s) {
   cudaStreamSynchronize(s->stream);
   s->mem.free_all();
   for (double* t : s->tables) cudaFree(t);
-  if (s->rebuild_h) cudaFreeHost(s->rebuild_h);
+  for (void* h : {(void*)s->rebuild_h, (void*)s->pin_blist, (void*)s->pin_segs, (void*)s->pin_res})
+    if (h) cudaFreeHost(h);
+  if (s->ev_pin) cudaEventDestroy(s->ev_pin);
   for (cudaEvent_t ev : {s->ev_run0, s->ev_run1, s->ev_k0, s->ev_k1, s->ev_t0, s->ev_t1, s->ev_b0, s->ev_b1})
     if (ev) cudaEventDestroy(ev);
   cudaStreamDestroy(s->stream);
@@ -514,26 +532,32 @@ static constexpr int kSortEvery = 8;
 // rebuild launch over these only.  When every replica is flagged the list is
 // left null and the passes cover the whole grid.
 static int prepare_blist(sg_system* s) {
-  s->blist_h.clear();
+  CU(s, cudaEventSynchronize(s->ev_pin));
+  int nb = 0;
   bool all = true;
   for (int r = 0; r < s->nrep; r++) {
     if (!s->rebuild_h[r]) { all = false; continue; }
-    for (int b = 0; b < s->rep_nblk_h[r]; b++) s->blist_h.push_back(s->rep_blk0_h[r] + b);
+    for (int b = 0; b < s->rep_nblk_h[r]; b++) s->pin_blist[nb++] = s->rep_blk0_h[r] + b;
   }
-  s->nblist = all ? s->nblocks : (int)s->blist_h.size();
+  s->nblist = all ? s->nblocks : nb;
   if (all || s->nblist == 0) return SG_OK;
   if (!s->blist) {
     s->blist = s->mem.alloc<int>(s->nblocks);
     if (!s->blist) { s->mem.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "block list"); }
   }
-  CU(s, cudaMemcpyAsync(s->blist, s->blist_h.data(), sizeof(int) * s->nblist, cudaMemcpyHostToDevice, s->stream));
+  CU(s, cudaMemcpyAsync(s->blist, s->pin_blist, sizeof(int) * s->nblist, cudaMemcpyHostToDevice, s->stream));
+  CU(s, cudaEventRecord(s->ev_pin, s->stream));
   return SG_OK;
 }
 static const int* blist_of(const sg_system* s) { return s->nblist == s->nblocks ? nullptr : s->blist; }
 
-static constexpr int64_t kTeamBelow = 1 << 20;  // particles: team list build below this many
+// Team list build below this many rebuilt particles: one thread per particle
+// leaves most of the GPU idle there (65,536-particle sphere: 8x the threads
+// in flight); from a few 10^5 particles on, the team's extra instructions
+// cost more than its shorter chains save (4,194,304 disks: 2.8 vs 1.3 ms).
+static constexpr int64_t kTeamBelow = 1 << 16;
 
-static int rebuild_flagged(sg_system* s, bool* sorted) {
+static int rebuild_flagged(sg_system* s, bool* sorted, bool blist_ready = false) {
   s->forces_fresh = false;
   bool any_sort = false;
   for (int r = 0; r < s->nrep; r++) {
@@ -544,27 +568,27 @@ static int rebuild_flagged(sg_system* s, bool* sorted) {
   }
   if (sorted) *sorted = any_sort;
   CU(s, cudaMemcpyAsync(s->rebuild, s->rebuild_h, sizeof(int) * s->nrep, cudaMemcpyHostToDevice, s->stream));
-  {
+  if (!blist_ready) {
     int rc = prepare_blist(s);
     if (rc) return rc;
   }
   const int* bl = blist_of(s);
   const int ng = s->nblist;
   // cell ranges of the flagged replicas (the cell passes touch only these)
-  s->segs_h.clear();
-  int nvirt = 0;
+  CU(s, cudaEventSynchronize(s->ev_pin));
+  int nvirt = 0, nseg = 0;
   for (int r = 0; r < s->nrep; r++) {
     if (!s->rebuild_h[r]) continue;
     const Replica& R = s->reps_h[r];
-    s->segs_h.push_back(CellSeg{R.cell_off, R.ncell, nvirt, 0});
+    s->pin_segs[nseg++] = CellSeg{R.cell_off, R.ncell, nvirt, 0};
     nvirt += R.ncell;
   }
-  const int nseg = (int)s->segs_h.size();
   if (nseg == 0) return SG_OK;
   int64_t nflag = 0;  // particles of the flagged replicas
   for (int r = 0; r < s->nrep; r++)
     if (s->rebuild_h[r]) nflag += s->n[r];
-  CU(s, cudaMemcpyAsync(s->segs, s->segs_h.data(), sizeof(CellSeg) * nseg, cudaMemcpyHostToDevice, s->stream));
+  CU(s, cudaMemcpyAsync(s->segs, s->pin_segs, sizeof(CellSeg) * nseg, cudaMemcpyHostToDevice, s->stream));
+  CU(s, cudaEventRecord(s->ev_pin, s->stream));
   for (int attempt = 0; attempt < 4; attempt++) {
     k_seg_zero<<<std::min((nvirt + 255) / 256, 148 * 16), 256, 0, s->stream>>>(s->segs, nseg, nvirt, s->cell_cnt,
                                                                                   s->cell_fill);
@@ -603,10 +627,10 @@ static int rebuild_flagged(sg_system* s, bool* sorted) {
       k_rb_build<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->st, s->nl, s->perm,
                                              s->cell_start, s->cell_cnt, s->bstatus, s->maxnb, bl);
     LAUNCH_CHECK(s);
-    int st = 0, mx = 0;
-    CU(s, cudaMemcpyAsync(&st, s->bstatus, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-    CU(s, cudaMemcpyAsync(&mx, s->maxnb, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CU(s, cudaMemcpyAsync(s->pin_res, s->bstatus, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CU(s, cudaMemcpyAsync(s->pin_res + 1, s->maxnb, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     CU(s, cudaStreamSynchronize(s->stream));
+    const int st = s->pin_res[0], mx = s->pin_res[1];
     if (!(st & ST_OVERFLOW)) {
       // tile data: re-derived for the rebuilt blocks (the others keep theirs);
       // a grown list capacity invalidates every block's positions
@@ -1387,6 +1411,18 @@ static int step_hot(sg_system* s, int shape, bool apply_e1, bool last, bool ener
 // Rebuild the lists of the replicas flagged in s->rebuild_h (already read
 // back), keeping the packed records in step (mid-run: unpack / re-pack the
 // rebuilt replicas around the build).
+// Adds the device time of the last rebuild to *rebuild_ms (its end event has
+// normally run by the time this is called, so no wait).
+static int flush_rebuild_time(sg_system* s, double* rebuild_ms) {
+  if (!s->b_pending) return SG_OK;
+  s->b_pending = false;
+  CU(s, cudaEventSynchronize(s->ev_b1));
+  float bms = 0.f;
+  CU(s, cudaEventElapsedTime(&bms, s->ev_b0, s->ev_b1));
+  *rebuild_ms += bms;
+  return SG_OK;
+}
+
 static int rebuild_pending(sg_system* s, int shape, bool last, double* rebuild_ms) {
   bool any = false;
   for (int r = 0; r < s->nrep; r++) any = any || s->rebuild_h[r];
@@ -1394,18 +1430,16 @@ static int rebuild_pending(sg_system* s, int shape, bool last, double* rebuild_m
   s->last_gap = std::max<int64_t>(1, s->since_rebuild);
   s->since_rebuild = 0;
   int rc;
+  if ((rc = flush_rebuild_time(s, rebuild_ms))) return rc;
   CU(s, cudaEventRecord(s->ev_b0, s->stream));
   if ((rc = prepare_blist(s))) return rc;
   if (shape != HOT_NONE && !last && (rc = hot_unpack(s, shape, true))) return rc;
   bool sorted = false;
-  if ((rc = rebuild_flagged(s, &sorted))) return rc;
+  if ((rc = rebuild_flagged(s, &sorted, true))) return rc;
   if (shape != HOT_NONE && !last && sorted && (rc = hot_pack(s, shape, true))) return rc;
   CU(s, cudaMemsetAsync(s->rebuild, 0, sizeof(int) * s->nrep, s->stream));
   CU(s, cudaEventRecord(s->ev_b1, s->stream));
-  CU(s, cudaEventSynchronize(s->ev_b1));
-  float bms = 0.f;
-  CU(s, cudaEventElapsedTime(&bms, s->ev_b0, s->ev_b1));
-  *rebuild_ms += bms;
+  s->b_pending = true;  // read once the stream has passed it (next rebuild or run end)
   return SG_OK;
 }
 
@@ -1521,6 +1555,7 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
   const int64_t launches0 = s->launches, builds0 = s->builds_run;
   double kernel_ms = 0.0, rebuild_ms = 0.0;
   int64_t kernels_timed = 0;
+  s->b_pending = false;
   CU(s, cudaEventRecord(s->ev_run0, s->stream));
   CU(s, cudaMemsetAsync(s->status, 0, sizeof(int), s->stream));
   // run-step counters restart with every `run` (samos.cpp:881); a
@@ -1607,6 +1642,7 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
   CU(s, cudaStreamSynchronize(s->stream));
   float run_ms = 0.f;
   CU(s, cudaEventElapsedTime(&run_ms, s->ev_run0, s->ev_run1));
+  if (int rcb = flush_rebuild_time(s, &rebuild_ms)) return rcb;
   int rc = pull_clk(s);
   if (rc) return rc;
   if (conv_out)
