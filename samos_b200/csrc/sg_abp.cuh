@@ -60,20 +60,54 @@ constexpr int ABP_NTUNED = (int)(sizeof(ABP_TUNED) / sizeof(ABP_TUNED[0]));
 // neighbour count, largest first (ties by slot), so each warp's 32 lanes have
 // similar list lengths and the warp's sweep is not set by one long list.
 // Padding slots go last.  Each particle's own arithmetic is unchanged.
+constexpr int LO_KEYS = 128;  // distinct sort keys the counting sort handles (list lengths 0..126 + padding)
+static_assert(BLOCK == LO_KEYS, "k_lane_order scans one key per thread");
+
 __global__ void __launch_bounds__(BLOCK)
 k_lane_order(const Replica* __restrict__ reps, const int* __restrict__ blk_rep, NbList nl,
              uint8_t* __restrict__ order, const int* __restrict__ blist = nullptr) {
+  constexpr int NW = BLOCK / 32;
+  __shared__ int hist[NW][LO_KEYS];  // per warp: lanes holding each key
+  __shared__ int wsum[NW];
   __shared__ int sc[BLOCK];
   const int b = blist ? blist[blockIdx.x] : (int)blockIdx.x, t = threadIdx.x, k = b * BLOCK + t;
   const Replica& R = reps[blk_rep[b]];
   const int c = (k - R.off < R.n) ? nl.cnt[k] : -1;
-  sc[t] = c;
-  __syncthreads();
-  int rank = 0;
-  for (int u = 0; u < BLOCK; u++) {
-    const int cu = sc[u];
-    rank += (cu > c || (cu == c && u < t)) ? 1 : 0;
+  if (nl.cap + 2 > LO_KEYS) {  // long lists (same branch for the whole grid): rank by comparison
+    sc[t] = c;
+    __syncthreads();
+    int rank = 0;
+    for (int u = 0; u < BLOCK; u++) {
+      const int cu = sc[u];
+      rank += (cu > c || (cu == c && u < t)) ? 1 : 0;
+    }
+    order[(size_t)b * BLOCK + rank] = (uint8_t)t;
+    return;
   }
+  // stable counting sort on key = count + 1 (padding 0), largest key first
+  const int key = c + 1, w = t >> 5, lane = t & 31;
+  for (int i = t; i < NW * LO_KEYS; i += BLOCK) (&hist[0][0])[i] = 0;
+  __syncthreads();
+  const unsigned same = __match_any_sync(0xffffffffu, key);
+  const int below = __popc(same & ((1u << lane) - 1u));  // same key, lower lane
+  if (below == 0) hist[w][key] = __popc(same);
+  __syncthreads();
+  // thread t holds key 127 - t: an inclusive scan over t sums the keys >= that key
+  const int rk = LO_KEYS - 1 - t;
+  int tot = 0;
+  for (int u = 0; u < NW; u++) tot += hist[u][rk];
+  int inc = tot;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += v;
+  }
+  if (lane == 31) wsum[w] = inc;
+  __syncthreads();
+  for (int u = 0; u < w; u++) inc += wsum[u];
+  sc[rk] = inc - tot;  // lanes with a larger key than rk
+  __syncthreads();
+  int rank = sc[key] + below;
+  for (int u = 0; u < w; u++) rank += hist[u][key];
   order[(size_t)b * BLOCK + rank] = (uint8_t)t;
 }
 
