@@ -37,23 +37,36 @@ struct AbpParams {
 // 0-4 per-particle sweep, 5 flattened, 6-7 staged (cp.async), 8 shared-memory
 // tile, 9-10 per-particle sweep with lanes assigned in neighbour-count order,
 // 11-14 ordered with the Gaussian draws taken before the sweep (fewer live
-// registers inside it), at rising occupancy; 15-16 the same with each
-// neighbour record fetched one iteration before it is used, at 6-12 blocks/SM
-constexpr int ABP_NVARIANT = 21;
-__host__ __device__ constexpr int abp_chunk(int v) {
+// registers inside it), at rising occupancy; 15-20 the same with each
+// neighbour record fetched one iteration before it is used, at 6-12 blocks/SM;
+// 21-27 twins of 18 / 17 / 19 / 11 / 3 / 12 / 13 that read the parameters of
+// a one-replica system from the kernel's own parameter space (constant-bank
+// operands of the FP64 instructions) instead of a shared-memory copy, whose
+// per-neighbour loads otherwise sit on the sweep's dependency chains.
+constexpr int ABP_NVARIANT = 28;
+__host__ __device__ constexpr bool abp_byval(int v) { return v >= 21; }
+// the shared-memory twin of a by-value variant (taken when several replicas
+// share the launch); every other property of a by-value variant is its twin's
+__host__ __device__ constexpr int abp_twin(int v) {
+  return v == 21 ? 18 : v == 22 ? 17 : v == 23 ? 19 : v == 24 ? 11 : v == 25 ? 3 : v == 26 ? 12 : v == 27 ? 13 : v;
+}
+__host__ __device__ constexpr int abp_chunk(int v0) {
+  const int v = abp_twin(v0);
   return v == 0 ? 4 : v == 1 ? 4 : v == 2 ? 2 : v == 3 ? 2 : v == 9 ? 2 : v == 10 ? 4 : v >= 15 ? 1 : v >= 11 ? 2 : 8;
 }
-__host__ __device__ constexpr int abp_minb(int v) {
+__host__ __device__ constexpr int abp_minb(int v0) {
+  const int v = abp_twin(v0);
   return v == 0 ? 5 : v == 1 ? 4 : v == 2 ? 6 : v == 3 ? 4 : v == 9 ? 6 : v == 10 ? 5 : v == 11 ? 6 : v == 12 ? 7
-       : v == 13 ? 8 : v == 14 ? 10 : v == 15 ? 7 : v == 16 ? 6 : v == 17 ? 8 : v == 18 ? 9 : v == 19 ? 10 : v == 20 ? 12 : 3;
+       : v == 13 ? 8 : v == 14 ? 10 : v == 15 ? 7 : v == 16 ? 6 : v == 17 ? 8 : v == 18 ? 9 : v == 19 ? 10 : v == 20 ? 12
+       : 3;
 }
-__host__ __device__ constexpr bool abp_ordered(int v) { return v >= 9; }
-__host__ __device__ constexpr bool abp_prenoise(int v) { return v >= 11; }
-__host__ __device__ constexpr bool abp_pipelined(int v) { return v >= 15; }
+__host__ __device__ constexpr bool abp_ordered(int v) { return abp_twin(v) >= 9; }
+__host__ __device__ constexpr bool abp_prenoise(int v) { return abp_twin(v) >= 11; }
+__host__ __device__ constexpr bool abp_pipelined(int v) { return abp_twin(v) >= 15; }
 
 // The variants the autotuner times (every one can still be pinned): those
 // that never won on the plane, sphere or replica workloads are left out.
-constexpr int ABP_TUNED[] = {0, 1, 2, 3, 8, 9, 10, 11, 12, 13, 15, 16, 17, 18};
+constexpr int ABP_TUNED[] = {0, 1, 2, 3, 8, 9, 10, 11, 12, 13, 15, 16, 17, 18, 21, 22, 23, 24, 25, 26, 27};
 constexpr int ABP_NTUNED = (int)(sizeof(ABP_TUNED) / sizeof(ABP_TUNED[0]));
 
 // Lane order of a block for the ordered variants: its particles sorted by
@@ -254,14 +267,21 @@ __device__ __forceinline__ void abp_finish(const AbpParams& S, int r, int k, dou
   }
 }
 
+template <bool BYVAL>
+__device__ __forceinline__ const AbpParams& abp_params(const AbpParams& pv, const AbpParams& staged) {
+  if constexpr (BYVAL) return pv;
+  else return staged;
+}
+
 template <int SHAPE, int ALIGN, bool SP, bool ENERGY, int VAR>
 __global__ void __launch_bounds__(BLOCK, abp_minb(VAR))
 k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, const Clock* __restrict__ clk,
            const D4* __restrict__ Gin, D4* __restrict__ Gout, const D4* __restrict__ Hin, D4* __restrict__ Hout,
            Dyn d, Stat st, NbList nl, int* __restrict__ rebuild, int* __restrict__ status, int apply_e1, int last,
-           double* epart, int nblocks, const uint8_t* __restrict__ lane_order = nullptr) {
+           double* epart, int nblocks, const uint8_t* __restrict__ lane_order,
+           const __grid_constant__ AbpParams pv) {
   constexpr bool PLANE = SHAPE == HOT_PLANE;
-  __shared__ AbpParams S;
+  __shared__ AbpParams S_sh;
   __shared__ uint64_t s_base;
   __shared__ int s_step;
   const int r = blk_rep[blockIdx.x];
@@ -270,12 +290,14 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
     constexpr int NW = (int)(sizeof(AbpParams) / 8);
     static_assert(sizeof(AbpParams) % 8 == 0, "AbpParams must be 8-byte granular");
     static_assert(NW <= BLOCK, "AbpParams too large for one-word-per-thread staging");
-    if (threadIdx.x < NW)
-      reinterpret_cast<unsigned long long*>(&S)[threadIdx.x] =
+    if (!abp_byval(VAR) && threadIdx.x < NW)
+      reinterpret_cast<unsigned long long*>(&S_sh)[threadIdx.x] =
           reinterpret_cast<const unsigned long long*>(prm + r)[threadIdx.x];
     if (threadIdx.x == 0) { s_base = clk[r].ctr[0]; s_step = clk[r].run_step; }
   }
   __syncthreads();
+  // by-value variants: the one replica's parameters, read from parameter space
+  const AbpParams& S = abp_params<abp_byval(VAR)>(pv, S_sh);
   static_assert(!(abp_ordered(VAR) && ENERGY), "the ordered variants change the block's energy summation order");
   static_assert(!abp_pipelined(VAR) || abp_prenoise(VAR), "the pipelined sweep takes the draws first");
   const int k = blockIdx.x * BLOCK +

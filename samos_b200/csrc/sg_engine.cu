@@ -105,6 +105,7 @@ struct sg_system {
   D4 *G[2] = {nullptr, nullptr}, *H[2] = {nullptr, nullptr};
   std::vector<std::vector<double>> pair_tab_h, align_tab_h, ext_tab_h;
   AbpParams* abp = nullptr;
+  AbpParams abp0_h{};  // replica 0's parameters, passed by value to the by-value variants
   bool abp_on = false;
   // shared-memory tile variant: per-block distinct neighbour slots and the
   // lists rewritten as positions in them (k_tile_prep), valid until the next
@@ -1238,6 +1239,7 @@ static int abp_upload(sg_system* s) {
   if (!s->abp) s->abp = s->mem.alloc<AbpParams>(s->nrep);
   if (!s->abp) { s->mem.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "abp params"); }
   CU(s, cudaMemcpyAsync(s->abp, h.data(), sizeof(AbpParams) * s->nrep, cudaMemcpyHostToDevice, s->stream));
+  s->abp0_h = h[0];
   return SG_OK;
 }
 
@@ -1248,7 +1250,7 @@ static void launch_abp_v(sg_system* s, bool apply_e1, bool last) {
   const int b = s->hot_buf;
   k_abp_step<SHAPE, ALIGN, SP, ENERGY, VAR><<<s->nblocks, BLOCK, 0, s->stream>>>(
       s->abp, s->blk_rep, s->clk, s->G[b], s->G[1 - b], s->H[b], s->H[1 - b], s->cur, s->st, s->nl, s->rebuild,
-      s->status, apply_e1 ? 1 : 0, last ? 1 : 0, s->epart, s->nblocks, s->lane_order);
+      s->status, apply_e1 ? 1 : 0, last ? 1 : 0, s->epart, s->nblocks, s->lane_order, s->abp0_h);
 }
 
 // cudaFuncSetAttribute is per device: remember, per kernel, the devices it
@@ -1317,7 +1319,8 @@ static void launch_abp_tile(sg_system* s, bool apply_e1, bool last) {
 template <int SHAPE, int ALIGN, bool SP>
 static void launch_abp3(sg_system* s, bool apply_e1, bool last, bool energy) {
   if (energy) { launch_abp_v<SHAPE, ALIGN, SP, true, 1>(s, apply_e1, last); return; }
-  switch (s->abp_variant) {
+  // by-value variants carry one replica's parameters: several replicas take the twin
+  switch (s->nrep > 1 ? abp_twin(s->abp_variant) : s->abp_variant) {
     case 5: launch_abp_flat<SHAPE, ALIGN, SP, false>(s, apply_e1, last); break;
     case 6: launch_abp_staged<SHAPE, ALIGN, SP, false, 4, 4>(s, apply_e1, last); break;
     case 7: launch_abp_staged<SHAPE, ALIGN, SP, false, 4, 5>(s, apply_e1, last); break;
@@ -1334,6 +1337,13 @@ static void launch_abp3(sg_system* s, bool apply_e1, bool last, bool energy) {
     case 18: launch_abp_v<SHAPE, ALIGN, SP, false, 18>(s, apply_e1, last); break;
     case 19: launch_abp_v<SHAPE, ALIGN, SP, false, 19>(s, apply_e1, last); break;
     case 20: launch_abp_v<SHAPE, ALIGN, SP, false, 20>(s, apply_e1, last); break;
+    case 21: launch_abp_v<SHAPE, ALIGN, SP, false, 21>(s, apply_e1, last); break;
+    case 22: launch_abp_v<SHAPE, ALIGN, SP, false, 22>(s, apply_e1, last); break;
+    case 23: launch_abp_v<SHAPE, ALIGN, SP, false, 23>(s, apply_e1, last); break;
+    case 24: launch_abp_v<SHAPE, ALIGN, SP, false, 24>(s, apply_e1, last); break;
+    case 25: launch_abp_v<SHAPE, ALIGN, SP, false, 25>(s, apply_e1, last); break;
+    case 26: launch_abp_v<SHAPE, ALIGN, SP, false, 26>(s, apply_e1, last); break;
+    case 27: launch_abp_v<SHAPE, ALIGN, SP, false, 27>(s, apply_e1, last); break;
     case 0: launch_abp_v<SHAPE, ALIGN, SP, false, 0>(s, apply_e1, last); break;
     case 1: launch_abp_v<SHAPE, ALIGN, SP, false, 1>(s, apply_e1, last); break;
     case 2: launch_abp_v<SHAPE, ALIGN, SP, false, 2>(s, apply_e1, last); break;
