@@ -85,6 +85,13 @@ int  sg_set_timestep(sg_system* s, double dt);
  * "ix","iy","iz".  Arrays are in particle-id order (length n_particles[r]). */
 int  sg_upload(sg_system* s, int replica, const char* field, const void* host);
 int  sg_download(sg_system* s, int replica, const char* field, void* host);
+/* Page-locked host memory for the arrays given to sg_upload / sg_download:
+ * copies from and to it run at the link's speed, where pageable arrays go
+ * through the driver's staging buffers (and a fresh pageable destination is
+ * faulted in page by page during the copy).  Plain cudaMallocHost /
+ * cudaFreeHost; no reference counterpart (host plumbing).                   */
+int  sg_host_alloc(int64_t bytes, void** ptr);
+int  sg_host_free(void* ptr);
 
 /* ---- neighbour list ------------------------------------------------------
  * NeighbourList(sys, msg, rcut, pad) (src/system/neighbour_list.hpp:124-217)

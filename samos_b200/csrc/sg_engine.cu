@@ -1715,6 +1715,23 @@ int sg_replica_slots(const sg_system* s, int replica, int32_t* offset, int32_t* 
   return SG_OK;
 }
 
+int sg_host_alloc(int64_t bytes, void** ptr) {
+  if (!ptr || bytes < 0) return SG_ERR_ARG;
+  *ptr = nullptr;
+  if (bytes == 0) return SG_OK;
+  if (cudaMallocHost(ptr, (size_t)bytes) != cudaSuccess) {
+    cudaGetLastError();
+    *ptr = nullptr;
+    return SG_ERR_NOMEM;
+  }
+  return SG_OK;
+}
+
+int sg_host_free(void* ptr) {
+  if (!ptr) return SG_OK;
+  return cudaFreeHost(ptr) == cudaSuccess ? SG_OK : SG_ERR_CUDA;
+}
+
 int sg_memcpy(void* dst, const void* src, int64_t bytes) {
   if (bytes < 0 || (!dst && bytes) || (!src && bytes)) return SG_ERR_ARG;
   return cudaMemcpy(dst, src, (size_t)bytes, cudaMemcpyDefault) == cudaSuccess ? SG_OK : SG_ERR_CUDA;

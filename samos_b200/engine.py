@@ -10,6 +10,8 @@ from __future__ import annotations
 import ctypes as C
 import os
 
+import weakref
+
 import numpy as np
 
 _LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsamos_gpu.so")
@@ -100,6 +102,8 @@ def load() -> C.CDLL:
         "sg_replica_slots": (I, [P, I, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
         "sg_positions_changed": (I, [P]),
         "sg_memcpy": (I, [P, P, I64]),
+        "sg_host_alloc": (I, [I64, C.POINTER(P)]),
+        "sg_host_free": (I, [P]),
         "sg_set_variant": (I, [P, I]),
         "sg_set_build": (I, [P, I]),
         "sg_get_variant": (I, [P]),
@@ -112,6 +116,31 @@ def load() -> C.CDLL:
         f.argtypes = args
     _lib = lib
     return lib
+
+
+def pinned_empty(n: int, dtype=np.float64) -> np.ndarray:
+    """A numpy array of n elements in page-locked host memory (sg_host_alloc),
+    freed when the array is garbage-collected.  Uploads from and downloads into
+    such arrays run at the link's speed."""
+    lib = load()
+    dt = np.dtype(dtype)
+    nbytes = max(1, int(n) * dt.itemsize)
+    p = C.c_void_p()
+    rc = lib.sg_host_alloc(nbytes, C.byref(p))
+    if rc != 0 or not p.value:
+        raise EngineError(rc or -3, "page-locked host allocation failed")
+    buf = (C.c_char * nbytes).from_address(p.value)
+    a = np.frombuffer(buf, dtype=dt, count=int(n))
+    weakref.finalize(buf, lib.sg_host_free, C.c_void_p(p.value))
+    return a
+
+
+def pinned_copy(values, dtype=np.float64) -> np.ndarray:
+    """Page-locked copy of an array (see pinned_empty)."""
+    v = np.ascontiguousarray(values, dtype=dtype)
+    a = pinned_empty(v.size, dtype)
+    a[:] = v.ravel()
+    return a
 
 
 def _arr(a):
@@ -174,9 +203,16 @@ class Engine:
             raise ValueError(f"{field}: expected {self.n[replica]} values, got {a.shape}")
         self._check(self.lib.sg_upload(self.h, replica, field.encode(), a.ctypes.data_as(C.c_void_p)))
 
-    def download(self, field: str, replica: int = 0) -> np.ndarray:
+    def download(self, field: str, replica: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        """The field in particle-id order; written into `out` when given
+        (contiguous, the field's dtype and length), e.g. a pinned_empty array."""
         dtype = np.int32 if field in INT_FIELDS else np.float64
-        a = np.empty(self.n[replica], dtype=dtype)
+        if out is None:
+            a = np.empty(self.n[replica], dtype=dtype)
+        else:
+            a = out
+            if a.dtype != dtype or a.shape != (self.n[replica],) or not a.flags.c_contiguous or not a.flags.writeable:
+                raise ValueError(f"{field}: out must be a writeable contiguous {dtype} array of {self.n[replica]}")
         self._check(self.lib.sg_download(self.h, replica, field.encode(), a.ctypes.data_as(C.c_void_p)))
         return a
 
