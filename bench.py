@@ -171,11 +171,10 @@ def sphere_parts(n, seed):
                 nz=t[:, 2].copy(), radius=np.ones(n)), R
 
 
-def batched_leg(n_rep=256, warm=80, steps=100, seed=7, device=0):
+def ensemble_replicas(n_rep=256, seed=7):
     """256 sphere systems, N log-uniform in [1024, 65536], R = sqrt(N/4), v0 ~ U[0.01,1],
     J ~ U[0,1], nu ~ logU[1e-3,1], own seeds; soft k=10 + polar, dt=1e-3."""
-    from samos_b200 import Engine
-    from samos_b200.ensemble import SphereReplica, sphere_ensemble
+    from samos_b200.ensemble import SphereReplica
     rng = np.random.default_rng(seed)
     reps = []
     for i in range(n_rep):
@@ -183,6 +182,32 @@ def batched_leg(n_rep=256, warm=80, steps=100, seed=7, device=0):
         parts, R = sphere_parts(n, seed * 1000 + i)
         reps.append(SphereReplica(parts=parts, R=R, v0=float(rng.uniform(0.01, 1.0)), J=float(rng.uniform(0.0, 1.0)),
                                   nu=float(np.exp(rng.uniform(np.log(1e-3), 0.0))), seed=int(rng.integers(1, 2**31 - 1))))
+    return reps
+
+
+def ensemble_only(variant=-1, warm=80, steps=100, device=0):
+    """The batched half of batched_leg alone (profiling runs): one engine over
+    the 256 replicas, `warm` untimed steps, then `steps` timed ones."""
+    from samos_b200 import Engine
+    from samos_b200.ensemble import sphere_ensemble
+    reps = ensemble_replicas()
+    eng = sphere_ensemble(reps, engine=Engine([len(r.parts["x"]) for r in reps], device=device))
+    if variant >= 0:
+        eng.set_variant(variant)
+    eng.run(warm - 1)
+    st = eng.run(steps - 1)
+    out = dict(workload="256-replica sphere ensemble", particles=sum(len(r.parts["x"]) for r in reps),
+               ms_per_step=st.device_ms / st.steps_done, nlist_builds=st.nlist_builds,
+               rebuild_ms_per_step=st.rebuild_ms / st.steps_done, kernel_variant=eng.variant())
+    eng.close()
+    return out
+
+
+def batched_leg(n_rep=256, warm=80, steps=100, seed=7, device=0):
+    """The replicas of ensemble_replicas stepped in one engine, then one at a time."""
+    from samos_b200 import Engine
+    from samos_b200.ensemble import sphere_ensemble
+    reps = ensemble_replicas(n_rep, seed)
     total = sum(len(r.parts["x"]) for r in reps)
     eng = sphere_ensemble(reps, engine=Engine([len(r.parts["x"]) for r in reps], device=device))
     eng.run(warm - 1)
@@ -326,6 +351,8 @@ def main():
                     help="pin the step-kernel variant instead of autotuning (profiling runs: ncu distorts the tuner's timings)")
     ap.add_argument("--particles", type=int, default=N_PART,
                     help="system size (profiling runs use a smaller system of the same density)")
+    ap.add_argument("--ensemble-only", action="store_true",
+                    help="run only the batched 256-replica ensemble (profiling runs) and print its timing")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if ws > 1:
@@ -337,6 +364,11 @@ def main():
             dist.destroy_process_group()
         return rc
     args.warmup = max(args.warmup, 3)
+    if args.ensemble_only:
+        out = ensemble_only(args.variant, device=local)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return 0
 
     from samos_b200 import Engine
     from samos_b200.plugins import Simulation
