@@ -38,6 +38,28 @@ def test_batched_equals_serial_bitwise():
         single.close()
 
 
+@pytest.mark.parametrize("byval,twin", [(22, 17), (24, 11)])
+def test_by_value_variant_pinned_on_an_ensemble_runs_its_twin(byval, twin):
+    # a variant that takes one replica's parameters by value cannot serve
+    # several replicas: the engine runs its shared-memory twin, same bits
+    reps = make_reps(4, 3)
+    runs = []
+    for v in (byval, twin):
+        e = sphere_ensemble(reps)
+        e.set_variant(v)
+        e.run(150)
+        runs.append(e)
+    for i in range(len(reps)):
+        for f in FIELDS:
+            np.testing.assert_array_equal(runs[0].download(f, replica=i), runs[1].download(f, replica=i),
+                                          err_msg=f"rep {i} {f}")
+    single = sphere_ensemble([reps[2]])
+    single.set_variant(byval)
+    single.run(150)
+    for f in FIELDS:
+        np.testing.assert_array_equal(single.download(f), runs[0].download(f, replica=2), err_msg=f)
+
+
 def test_batched_replica_matches_oracle():
     reps = make_reps(3, 2)
     batched = sphere_ensemble(reps)
