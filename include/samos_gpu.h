@@ -37,7 +37,8 @@ enum { SG_PAIR_SOFT = 0, SG_PAIR_LJ = 1, SG_PAIR_MORSE = 2, SG_PAIR_GAUSSIAN = 3
 enum { SG_ALIGN_POLAR = 0, SG_ALIGN_NEMATIC = 1, SG_ALIGN_VICSEK = 2 };
 enum { SG_EXT_SELF_PROPULSION = 0 };
 enum { SG_CONS_NONE = 0, SG_CONS_PLANE = 1, SG_CONS_SPHERE = 2, SG_CONS_CYLINDER = 3, SG_CONS_TORUS = 4,
-       SG_CONS_ELLIPSOID = 5 };
+       SG_CONS_ELLIPSOID = 5, SG_CONS_PEANUT = 6, SG_CONS_GYROID = 7, SG_CONS_HOURGLASS = 8,
+       SG_CONS_GAUSSIAN_BUMP = 9 };
 enum { SG_INT_BROWNIAN = 0, SG_INT_BROWNIAN_POS = 1, SG_INT_BROWNIAN_ALIGN = 2,
        SG_INT_LANGEVIN = 3, SG_INT_FIRE = 4, SG_INT_NVE = 5, SG_INT_VICSEK = 6 };
 enum { SG_VALUE_CONSTANT = 0, SG_VALUE_LINEAR = 1 };
@@ -124,11 +125,17 @@ int  sg_add_align(sg_system* s, int kind, double J, double rcut, const double* t
 int  sg_add_external(sg_system* s, int kind, double alpha, const double* type_alpha,
                      int has_params);
 /* Constraint (register_constraints.cpp:35-61): params =
- * {plane: zpos | sphere: r | cylinder: r | torus: c | ellipsoid: a,
+ * {plane: zpos | sphere: r | cylinder: r | torus: c | ellipsoid: a |
+ *  peanut: a | hourglass: R | gaussian_bump: A,
  *  plane: unlimited, maxiter, tol, rescale, rescale_steps, rescale_freq,
- *  torus: a | ellipsoid: b, ellipsoid: c} (9 values; torus and ellipsoid
- * project with Constraint::enforce's SHAKE iteration, constraint.cpp:40-87);
- * enforced on every particle at once like src/samos.cpp:518-522.           */
+ *  torus: a | ellipsoid: b | peanut: b | hourglass: A | gaussian_bump: a,
+ *  ellipsoid: c | hourglass: n | gaussian_bump: b} (9 values; gyroid takes
+ * none, its period is the box).  The implicit surfaces (torus and after)
+ * project with Constraint::enforce's SHAKE iteration, constraint.cpp:40-87.
+ * Peanut needs b > a (constraint_peanut.hpp:84-88; rejected here), an
+ * explicitly given hourglass A at most R (constraint_hourglass.hpp:85; the
+ * hosts check it).  Enforced on every particle at once like
+ * src/samos.cpp:518-522.                                                   */
 int  sg_add_constraint(sg_system* s, int kind, const double* params);
 /* As sg_add_constraint, with params[0] (plane zpos / sphere r) given per
  * replica in value0[n_replicas] before the immediate enforce, so each

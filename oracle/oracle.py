@@ -156,7 +156,8 @@ class OracleSystem:
     def add_constraint(self, kind, params):
         p = np.zeros(9)
         p[:len(params)] = params
-        self.lib.or_add_constraint(self.h, int(kind), _p(p))
+        if self.lib.or_add_constraint(self.h, int(kind), _p(p)) != 0:
+            raise ValueError("constraint parameters rejected (as the reference constructor rejects them)")
         self.lib.or_enforce_all(self.h)  # samos.cpp:518-522
 
     def add_integrator(self, kind, params, temperature=None):

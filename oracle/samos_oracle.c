@@ -21,6 +21,10 @@
 #include <stdlib.h>
 #include <string.h>
 
+#ifndef M_PI  /* strict C11 <math.h> does not define it */
+#define M_PI 3.14159265358979323846
+#endif
+
 /* ------------------------------------------------------------------------ */
 /* noise stream                                                              */
 /* ------------------------------------------------------------------------ */
@@ -209,8 +213,8 @@ typedef struct {
 typedef struct {
   int kind;
   double zpos; int unlimited;      /* plane */
-  double r;                        /* sphere; cylinder r; torus c; ellipsoid a */
-  double b2, b3;                   /* torus a; ellipsoid b, c */
+  double r;                        /* sphere; cylinder r; torus c; ellipsoid a; peanut a; hourglass R; bump A */
+  double b2, b3;                   /* torus a; ellipsoid b, c; peanut b; hourglass A, n; bump a, b */
   int max_iter; double tol;
   double rescale; int rescale_steps, rescale_freq; double scale;
 } or_cons;
@@ -881,13 +885,17 @@ static void ext_self_propulsion(or_system* s, or_ext* e)
 int or_add_constraint(or_system* s, int kind, const double* p)
 {
   if (s->ncons >= OR_MAX_COMP) return -1;
+  if (kind == OR_CONS_PEANUT) {  /* constraint_peanut.hpp:84-88, on the defaults too (a 10, b 8) */
+    const double a = p ? p[0] : 10.0, b = p ? p[7] : 8.0;
+    if (b <= a) return -1;
+  }
   or_cons* c = &s->cons[s->ncons++];
   memset(c, 0, sizeof(*c));
   c->kind = kind;
   c->zpos = p ? p[0] : 0.0; c->unlimited = p ? (int)p[1] : 0;
-  c->r = p ? p[0] : 1.0;
-  if (kind == OR_CONS_TORUS || kind == OR_CONS_ELLIPSOID) {  /* params[7], params[8] */
-    c->b2 = p ? p[7] : (kind == OR_CONS_TORUS ? 0.5 : 1.0);
+  c->r = p ? p[0] : (kind == OR_CONS_PEANUT || kind == OR_CONS_HOURGLASS ? 10.0 : 1.0);
+  if (kind >= OR_CONS_TORUS) {  /* params[7], params[8] */
+    c->b2 = p ? p[7] : (kind == OR_CONS_TORUS ? 0.5 : kind == OR_CONS_PEANUT ? 8.0 : 1.0);
     c->b3 = p ? p[8] : 1.0;
   }
   c->max_iter = p ? (int)p[2] : 100;
@@ -966,27 +974,72 @@ static void cylinder_enforce(or_system* s, const or_cons* c, int i)
   }
 }
 
-/* compute_gradient / constraint_value of the implicit surfaces:
-   ConstraintTorus (constraint_torus.cpp: (c - sqrt(x^2+y^2))^2 + z^2 - a^2)
-   and ConstraintEllipsoid (constraint_ellipsoid.cpp: x^2/a^2 + y^2/b^2 + z^2/c^2 - 1) */
-static void implicit_gradient(const or_cons* c, double x, double y, double z, double* gx, double* gy, double* gz)
+/* compute_gradient / constraint_value of the implicit surfaces, in the
+   reference's operation order: ConstraintTorus (constraint_torus.cpp:
+   (c - sqrt(x^2+y^2))^2 + z^2 - a^2), ConstraintEllipsoid
+   (constraint_ellipsoid.cpp: x^2/a^2 + y^2/b^2 + z^2/c^2 - 1),
+   ConstraintPeanut (constraint_peanut.cpp:47-66), ConstraintGyroid
+   (constraint_gyroid.cpp:61-80, periodic in the box), ConstraintHourglass
+   (constraint_hourglass.cpp:47-68) and ConstraintGaussianBump
+   (constraint_gaussian_bump.cpp:58-75) */
+static void implicit_gradient(const or_system* s, const or_cons* c, double x, double y, double z, double* gx,
+                              double* gy, double* gz)
 {
   if (c->kind == OR_CONS_TORUS) {
     double sqr_xy = sqrt(x * x + y * y);
     double fact = -2.0 * (c->r - sqr_xy) / sqr_xy;
     *gx = x * fact; *gy = y * fact; *gz = 2.0 * z;
-  } else {
+  } else if (c->kind == OR_CONS_ELLIPSOID) {
     *gx = 2.0 * x / c->r / c->r; *gy = 2.0 * y / c->b2 / c->b2; *gz = 2.0 * z / c->b3 / c->b3;
+  } else if (c->kind == OR_CONS_PEANUT) {
+    double fact_1 = 4.0 * c->r * c->r;
+    double fact_2 = 4.0 * (x * x + y * y + z * z);
+    *gx = (-fact_1 + fact_2) * x;
+    *gy = (fact_1 + fact_2) * y;
+    *gz = (fact_1 + fact_2) * z;
+  } else if (c->kind == OR_CONS_GYROID) {
+    double lx = s->Lx, ly = s->Ly, lz = s->Lz;
+    *gx = (2.0 * M_PI * (cos((2.0 * M_PI * x) / lx) * cos((2.0 * M_PI * z) / lz) -
+                         sin((2.0 * M_PI * x) / lx) * sin((2.0 * M_PI * y) / ly))) / lx;
+    *gy = (2.0 * M_PI * (cos((2.0 * M_PI * x) / lx) * cos((2.0 * M_PI * y) / ly) -
+                         sin((2.0 * M_PI * y) / ly) * sin((2.0 * M_PI * z) / lz))) / ly;
+    *gz = (2.0 * M_PI * (cos((2.0 * M_PI * y) / ly) * cos((2.0 * M_PI * z) / lz) -
+                         sin((2.0 * M_PI * x) / lx) * sin((2.0 * M_PI * z) / lz))) / lz;
+  } else if (c->kind == OR_CONS_HOURGLASS) {
+    double lz = s->Lz, A = c->b2, n = c->b3;
+    *gx = 2.0 * x;
+    *gy = 2.0 * y;
+    *gz = (-4.0 * A * n * M_PI * cos((2.0 * n * M_PI * z) / lz) * (c->r + A * sin((2.0 * n * M_PI * z) / lz))) / lz;
+  } else {
+    double fact = exp(-x * x / c->b2 - y * y / c->b3);
+    *gx = -2.0 * c->r * x * fact / c->b2;
+    *gy = -2.0 * c->r * y * fact / c->b3;
+    *gz = -1.0;
   }
 }
 
-static double implicit_value(const or_cons* c, double x, double y, double z)
+static double implicit_value(const or_system* s, const or_cons* c, double x, double y, double z)
 {
   if (c->kind == OR_CONS_TORUS) {
     double ft = c->r - sqrt(x * x + y * y);
     return ft * ft + z * z - c->b2 * c->b2;
   }
-  return x * x / c->r / c->r + y * y / c->b2 / c->b2 + z * z / c->b3 / c->b3 - 1.0;
+  if (c->kind == OR_CONS_ELLIPSOID) return x * x / c->r / c->r + y * y / c->b2 / c->b2 + z * z / c->b3 / c->b3 - 1.0;
+  if (c->kind == OR_CONS_PEANUT) {
+    double a = c->r, b = c->b2;
+    double tr = x * x + y * y + z * z;
+    return a * a * a * a - b * b * b * b - 2.0 * a * a * (x * x - y * y - z * z) + tr * tr;
+  }
+  if (c->kind == OR_CONS_GYROID) {
+    double lx = s->Lx, ly = s->Ly, lz = s->Lz;
+    return cos((2.0 * M_PI * z) / lz) * sin((2.0 * M_PI * x) / lx) + cos((2.0 * M_PI * x) / lx) * sin((2.0 * M_PI * y) / ly) +
+           cos((2.0 * M_PI * y) / ly) * sin((2.0 * M_PI * z) / lz);
+  }
+  if (c->kind == OR_CONS_HOURGLASS) {
+    double zfact = c->r + c->b2 * sin(2.0 * M_PI / s->Lz * c->b3 * z);
+    return x * x + y * y - zfact * zfact;
+  }
+  return c->r * exp(-x * x / c->b2 - y * y / c->b3) - z;
 }
 
 /* compute_normal of each non-plane surface (the gradient normalised for the
@@ -997,7 +1050,7 @@ static void surface_normal(or_system* s, const or_cons* c, int i, double* Nx, do
   if (c->kind == OR_CONS_SPHERE) { *Nx = s->x[i] / c->r; *Ny = s->y[i] / c->r; *Nz = s->z[i] / c->r; }
   else if (c->kind == OR_CONS_CYLINDER) { *Nx = s->x[i] / c->r; *Ny = s->y[i] / c->r; *Nz = 0.0; }
   else {
-    implicit_gradient(c, s->x[i], s->y[i], s->z[i], Nx, Ny, Nz);
+    implicit_gradient(s, c, s->x[i], s->y[i], s->z[i], Nx, Ny, Nz);
     double len_N = sqrt(*Nx * *Nx + *Ny * *Ny + *Nz * *Nz);
     *Nx /= len_N; *Ny /= len_N; *Nz /= len_N;
   }
@@ -1010,13 +1063,13 @@ static void surface_normal(or_system* s, const or_cons* c, int i, double* Nx, do
 static void implicit_enforce(or_system* s, const or_cons* c, int i)
 {
   double ref_gx, ref_gy, ref_gz;
-  implicit_gradient(c, s->x[i], s->y[i], s->z[i], &ref_gx, &ref_gy, &ref_gz);
+  implicit_gradient(s, c, s->x[i], s->y[i], s->z[i], &ref_gx, &ref_gy, &ref_gz);
   int iter = 0;
   while (iter++ < c->max_iter) {
     double gx, gy, gz;
-    implicit_gradient(c, s->x[i], s->y[i], s->z[i], &gx, &gy, &gz);
+    implicit_gradient(s, c, s->x[i], s->y[i], s->z[i], &gx, &gy, &gz);
     double sv = gx * ref_gx + gy * ref_gy + gz * ref_gz;
-    double g = implicit_value(c, s->x[i], s->y[i], s->z[i]);
+    double g = implicit_value(s, c, s->x[i], s->y[i], s->z[i]);
     double lambda = g / sv;
     if (!(fabs(g) > c->tol)) break;
     s->x[i] -= lambda * ref_gx;
@@ -1041,7 +1094,7 @@ static void enforce_one(or_system* s, int i)
     if (c->kind == OR_CONS_PLANE) plane_enforce(s, c, i);
     else if (c->kind == OR_CONS_SPHERE) sphere_enforce(s, c, i);
     else if (c->kind == OR_CONS_CYLINDER) cylinder_enforce(s, c, i);
-    else if (c->kind == OR_CONS_TORUS || c->kind == OR_CONS_ELLIPSOID) implicit_enforce(s, c, i);
+    else if (c->kind >= OR_CONS_TORUS) implicit_enforce(s, c, i);
     else if (s->periodic) enforce_periodic(s, i);
   }
 }

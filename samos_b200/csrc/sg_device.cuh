@@ -25,7 +25,11 @@ constexpr int BLOCK = 128;          // particle slots per block; replicas are pa
 
 enum { PAIR_SOFT = 0, PAIR_LJ = 1, PAIR_MORSE = 2, PAIR_GAUSSIAN = 3 };
 enum { ALIGN_POLAR = 0, ALIGN_NEMATIC = 1, ALIGN_VICSEK = 2 };
-enum { CONS_NONE = 0, CONS_PLANE = 1, CONS_SPHERE = 2, CONS_CYLINDER = 3, CONS_TORUS = 4, CONS_ELLIPSOID = 5 };
+enum { CONS_NONE = 0, CONS_PLANE = 1, CONS_SPHERE = 2, CONS_CYLINDER = 3, CONS_TORUS = 4, CONS_ELLIPSOID = 5,
+       CONS_PEANUT = 6, CONS_GYROID = 7, CONS_HOURGLASS = 8, CONS_GAUSSIAN_BUMP = 9 };
+// surfaces given by an implicit function g = 0 and projected by the base
+// class's SHAKE iteration (no enforce of their own in the reference)
+__host__ __device__ __forceinline__ bool cons_implicit(int kind) { return kind >= CONS_TORUS; }
 enum { INT_BROWNIAN = 0, INT_BROWNIAN_POS = 1, INT_BROWNIAN_ALIGN = 2, INT_LANGEVIN = 3, INT_FIRE = 4, INT_NVE = 5, INT_VICSEK = 6 };
 enum { LANGEVIN_BAOAB = 0, LANGEVIN_SPV = 1, LANGEVIN_BBK = 2 };
 
@@ -316,35 +320,82 @@ __device__ __forceinline__ void cylinder_enforce(const Replica& R, double rc, Pa
   }
 }
 
-// implicit surfaces: ConstraintTorus ((c - sqrt(x^2+y^2))^2 + z^2 - a^2,
-// constraint_torus.cpp) and ConstraintEllipsoid (x^2/a^2 + y^2/b^2 + z^2/c^2 - 1,
-// constraint_ellipsoid.cpp): gradient and value
-__host__ __device__ __forceinline__ void implicit_gradient(const ConsComp& C, double a0, double x, double y, double z,
-                                                  double& gx, double& gy, double& gz) {
+// implicit surfaces, gradient and value in the reference's operation order:
+// ConstraintTorus ((c - sqrt(x^2+y^2))^2 + z^2 - a^2, constraint_torus.cpp),
+// ConstraintEllipsoid (x^2/a^2 + y^2/b^2 + z^2/c^2 - 1, constraint_ellipsoid.cpp),
+// ConstraintPeanut (a^4 - b^4 - 2a^2 (x^2 - y^2 - z^2) + (x^2+y^2+z^2)^2,
+// constraint_peanut.cpp:47-66), ConstraintGyroid (periodic in the box,
+// constraint_gyroid.cpp:61-80), ConstraintHourglass (x^2 + y^2 - (R + A
+// sin(2 pi n z / lz))^2, constraint_hourglass.cpp:47-68) and
+// ConstraintGaussianBump (A exp(-x^2/a - y^2/b) - z, constraint_gaussian_bump.cpp:58-75).
+// a0 is the replica's first shape parameter (torus c, ellipsoid a, peanut a,
+// hourglass R, bump A), C.b2 / C.b3 the second and third.
+__host__ __device__ __forceinline__ void implicit_gradient(const ConsComp& C, const Replica& R, double a0, double x,
+                                                           double y, double z, double& gx, double& gy, double& gz) {
   if (C.kind == CONS_TORUS) {
     double sqr_xy = sqrt(x * x + y * y);
     double fact = -2.0 * (a0 - sqr_xy) / sqr_xy;
     gx = x * fact; gy = y * fact; gz = 2.0 * z;
-  } else {
+  } else if (C.kind == CONS_ELLIPSOID) {
     gx = 2.0 * x / a0 / a0; gy = 2.0 * y / C.b2 / C.b2; gz = 2.0 * z / C.b3 / C.b3;
+  } else if (C.kind == CONS_PEANUT) {
+    double fact_1 = 4.0 * a0 * a0;
+    double fact_2 = 4.0 * (x * x + y * y + z * z);
+    gx = (-fact_1 + fact_2) * x;
+    gy = (fact_1 + fact_2) * y;
+    gz = (fact_1 + fact_2) * z;
+  } else if (C.kind == CONS_GYROID) {
+    const double lx = R.Lx, ly = R.Ly, lz = R.Lz;
+    gx = (2.0 * M_PI * (cos((2.0 * M_PI * x) / lx) * cos((2.0 * M_PI * z) / lz) -
+                        sin((2.0 * M_PI * x) / lx) * sin((2.0 * M_PI * y) / ly))) / lx;
+    gy = (2.0 * M_PI * (cos((2.0 * M_PI * x) / lx) * cos((2.0 * M_PI * y) / ly) -
+                        sin((2.0 * M_PI * y) / ly) * sin((2.0 * M_PI * z) / lz))) / ly;
+    gz = (2.0 * M_PI * (cos((2.0 * M_PI * y) / ly) * cos((2.0 * M_PI * z) / lz) -
+                        sin((2.0 * M_PI * x) / lx) * sin((2.0 * M_PI * z) / lz))) / lz;
+  } else if (C.kind == CONS_HOURGLASS) {
+    const double lz = R.Lz, A = C.b2, n = C.b3;
+    gx = 2.0 * x;
+    gy = 2.0 * y;
+    gz = (-4.0 * A * n * M_PI * cos((2.0 * n * M_PI * z) / lz) * (a0 + A * sin((2.0 * n * M_PI * z) / lz))) / lz;
+  } else {  // gaussian bump
+    double fact = exp(-x * x / C.b2 - y * y / C.b3);
+    gx = -2.0 * a0 * x * fact / C.b2;
+    gy = -2.0 * a0 * y * fact / C.b3;
+    gz = -1.0;
   }
 }
-__device__ __forceinline__ double implicit_value(const ConsComp& C, double a0, double x, double y, double z) {
+__host__ __device__ __forceinline__ double implicit_value(const ConsComp& C, const Replica& R, double a0, double x,
+                                                          double y, double z) {
   if (C.kind == CONS_TORUS) {
     double ft = a0 - sqrt(x * x + y * y);
     return ft * ft + z * z - C.b2 * C.b2;
   }
-  return x * x / a0 / a0 + y * y / C.b2 / C.b2 + z * z / C.b3 / C.b3 - 1.0;
+  if (C.kind == CONS_ELLIPSOID) return x * x / a0 / a0 + y * y / C.b2 / C.b2 + z * z / C.b3 / C.b3 - 1.0;
+  if (C.kind == CONS_PEANUT) {
+    const double b = C.b2;
+    double tr = x * x + y * y + z * z;
+    return a0 * a0 * a0 * a0 - b * b * b * b - 2.0 * a0 * a0 * (x * x - y * y - z * z) + tr * tr;
+  }
+  if (C.kind == CONS_GYROID) {
+    const double lx = R.Lx, ly = R.Ly, lz = R.Lz;
+    return cos((2.0 * M_PI * z) / lz) * sin((2.0 * M_PI * x) / lx) + cos((2.0 * M_PI * x) / lx) * sin((2.0 * M_PI * y) / ly) +
+           cos((2.0 * M_PI * y) / ly) * sin((2.0 * M_PI * z) / lz);
+  }
+  if (C.kind == CONS_HOURGLASS) {
+    double zfact = a0 + C.b2 * sin(2.0 * M_PI / R.Lz * C.b3 * z);
+    return x * x + y * y - zfact * zfact;
+  }
+  return a0 * exp(-x * x / C.b2 - y * y / C.b3) - z;
 }
 
 // compute_normal of the curved surfaces (sphere x/R; cylinder x/r, y/r, 0,
 // constraint_cylinder.hpp:76-80; implicit: the normalised gradient)
-__host__ __device__ __forceinline__ void surface_normal(const ConsComp& C, double a0, const Part& p, double& Nx, double& Ny,
-                                               double& Nz) {
+__host__ __device__ __forceinline__ void surface_normal(const ConsComp& C, const Replica& R, double a0, const Part& p,
+                                                        double& Nx, double& Ny, double& Nz) {
   if (C.kind == CONS_SPHERE) { Nx = p.x / a0; Ny = p.y / a0; Nz = p.z / a0; }
   else if (C.kind == CONS_CYLINDER) { Nx = p.x / a0; Ny = p.y / a0; Nz = 0.0; }
   else {
-    implicit_gradient(C, a0, p.x, p.y, p.z, Nx, Ny, Nz);
+    implicit_gradient(C, R, a0, p.x, p.y, p.z, Nx, Ny, Nz);
     double len_N = sqrt(Nx * Nx + Ny * Ny + Nz * Nz);
     Nx /= len_N; Ny /= len_N; Nz /= len_N;
   }
@@ -354,13 +405,13 @@ __host__ __device__ __forceinline__ void surface_normal(const ConsComp& C, doubl
 // gradient at the start point, then the tangent projections)
 __device__ __forceinline__ void implicit_enforce(const ConsComp& C, const Replica& R, double a0, Part& p) {
   double ref_gx, ref_gy, ref_gz;
-  implicit_gradient(C, a0, p.x, p.y, p.z, ref_gx, ref_gy, ref_gz);
+  implicit_gradient(C, R, a0, p.x, p.y, p.z, ref_gx, ref_gy, ref_gz);
   int iter = 0;
   while (iter++ < C.max_iter) {
     double gx, gy, gz;
-    implicit_gradient(C, a0, p.x, p.y, p.z, gx, gy, gz);
+    implicit_gradient(C, R, a0, p.x, p.y, p.z, gx, gy, gz);
     double sv = gx * ref_gx + gy * ref_gy + gz * ref_gz;
-    double g = implicit_value(C, a0, p.x, p.y, p.z);
+    double g = implicit_value(C, R, a0, p.x, p.y, p.z);
     double lambda = g / sv;
     if (!(fabs(g) > C.tol)) break;
     p.x -= lambda * ref_gx;
@@ -368,7 +419,7 @@ __device__ __forceinline__ void implicit_enforce(const ConsComp& C, const Replic
     p.z -= lambda * ref_gz;
   }
   double Nx, Ny, Nz;
-  surface_normal(C, a0, p, Nx, Ny, Nz);
+  surface_normal(C, R, a0, p, Nx, Ny, Nz);
   double v_dot_N = p.vx * Nx + p.vy * Ny + p.vz * Nz;
   double n_dot_N = p.nx * Nx + p.ny * Ny + p.nz * Nz;
   p.vx -= v_dot_N * Nx; p.vy -= v_dot_N * Ny; p.vz -= v_dot_N * Nz;
@@ -386,7 +437,7 @@ __device__ __forceinline__ void enforce_all(const Program& P, const Replica& R, 
     if (kind == CONS_PLANE) plane_enforce(R, R.cons_p[c], P.cons[c].unlimited, p);
     else if (kind == CONS_SPHERE) sphere_enforce(R.cons_p[c], p);
     else if (kind == CONS_CYLINDER) cylinder_enforce(R, R.cons_p[c], p);
-    else if (kind == CONS_TORUS || kind == CONS_ELLIPSOID) implicit_enforce(P.cons[c], R, R.cons_p[c], p);
+    else if (cons_implicit(kind)) implicit_enforce(P.cons[c], R, R.cons_p[c], p);
     else enforce_periodic(R, p);
   }
 }
@@ -402,7 +453,7 @@ __device__ __forceinline__ double project_torque(const Program& P, const Replica
     if (kind == CONS_PLANE) val += p.tz;
     else if (kind != CONS_NONE) {
       double Nx, Ny, Nz;
-      surface_normal(P.cons[c], R.cons_p[c], p, Nx, Ny, Nz);
+      surface_normal(P.cons[c], R, R.cons_p[c], p, Nx, Ny, Nz);
       val += p.tx * Nx + p.ty * Ny + p.tz * Nz;
     } else val += 0.0;
   }
@@ -423,7 +474,7 @@ __device__ __forceinline__ void rotate_director(const Program& P, const Replica&
       p.nx = nx / len; p.ny = ny / len;
     } else if (kind != CONS_NONE) {
       double U, V, W;
-      surface_normal(P.cons[c], R.cons_p[c], p, U, V, W);
+      surface_normal(P.cons[c], R, R.cons_p[c], p, U, V, W);
       double cs = cos(phi), sn = sin(phi);
       double dot = U * p.nx + V * p.ny + W * p.nz;
       double nx = U * dot * (1.0 - cs) + p.nx * cs + (-W * p.ny + V * p.nz) * sn;
@@ -448,7 +499,7 @@ __device__ __forceinline__ void rotate_velocity(const Program& P, const Replica&
       p.vx = vx; p.vy = vy;
     } else if (kind != CONS_NONE) {
       double U, V, W;
-      surface_normal(P.cons[c], R.cons_p[c], p, U, V, W);
+      surface_normal(P.cons[c], R, R.cons_p[c], p, U, V, W);
       double cs = cos(phi), sn = sin(phi);
       double dot = U * p.vx + V * p.vy + W * p.vz;
       double vx = U * dot * (1.0 - cs) + p.vx * cs + (-W * p.vy + V * p.vz) * sn;

@@ -493,7 +493,7 @@ int sg_download(sg_system* s, int replica, const char* field, void* host) {
           Part q;
           q.x = X[k]; q.y = Y[k]; q.z = Z[k];
           double N[3];
-          surface_normal(C, a0, q, N[0], N[1], N[2]);
+          surface_normal(C, s->reps_h[replica], a0, q, N[0], N[1], N[2]);
           h[ids[k]] = N[comp];
         }
       }
@@ -819,24 +819,50 @@ int sg_add_external(sg_system* s, int kind, double alpha, const double* type_alp
 }
 
 // Program-level part of a constraint: kind, plane flag, the second and third
-// shape parameters (torus a; ellipsoid b, c: params[7], params[8]) and the
-// SHAKE settings of the implicit surfaces (maxiter params[2], tol params[3]).
+// shape parameters (params[7], params[8]: torus a; ellipsoid b, c; peanut b;
+// hourglass A, n; gaussian bump a, b) and the SHAKE settings of the implicit
+// surfaces (maxiter params[2], tol params[3]).  Without params the
+// reference's defaults (peanut: a 10, b 8, which its b > a check rejects).
 static void set_cons(ConsComp& C, int kind, const double* params) {
   C.kind = kind;
   C.unlimited = (kind == CONS_PLANE && params) ? (int)params[1] : 0;
   C.max_iter = params ? (int)params[2] : 100;
   C.tol = params ? params[3] : 1e-6;
-  C.b2 = (kind == CONS_TORUS || kind == CONS_ELLIPSOID) ? (params ? params[7] : (kind == CONS_TORUS ? 0.5 : 1.0)) : 0.0;
-  C.b3 = kind == CONS_ELLIPSOID ? (params ? params[8] : 1.0) : 0.0;
+  double d2 = 0.0, d3 = 0.0;
+  if (kind == CONS_TORUS) d2 = 0.5;
+  else if (kind == CONS_ELLIPSOID) { d2 = 1.0; d3 = 1.0; }
+  else if (kind == CONS_PEANUT) d2 = 8.0;
+  else if (kind == CONS_HOURGLASS) { d2 = 1.0; d3 = 1.0; }
+  else if (kind == CONS_GAUSSIAN_BUMP) { d2 = 1.0; d3 = 1.0; }
+  C.b2 = params ? params[7] : d2;
+  C.b3 = params ? params[8] : d3;
+}
+
+static double cons_first_default(int kind) {
+  return kind == CONS_PLANE || kind == CONS_NONE || kind == CONS_GYROID ? 0.0
+       : kind == CONS_PEANUT || kind == CONS_HOURGLASS ? 10.0 : 1.0;
+}
+
+// the peanut constructor's check (constraint_peanut.hpp:84-88); the
+// hourglass one applies only to an amplitude given explicitly, so the hosts
+// make it where they parse the parameters
+static int check_cons(sg_system* s, const ConsComp& C, double first) {
+  if (C.kind == CONS_PEANUT && C.b2 <= first)
+    return fail(s, SG_ERR_ARG, "Parameter b has to be larger than parameter a. Otherwise the surface will be disconnected.");
+  return SG_OK;
 }
 
 int sg_add_constraint_per_replica(sg_system* s, int kind, const double* params, const double* value0) {
-  if (!s || !value0 || kind < SG_CONS_NONE || kind > SG_CONS_ELLIPSOID) return fail(s, SG_ERR_ARG, "bad constraint");
+  if (!s || !value0 || kind < SG_CONS_NONE || kind > SG_CONS_GAUSSIAN_BUMP) return fail(s, SG_ERR_ARG, "bad constraint");
   Program& P = s->prog;
   if (P.ncons >= MAX_CONS) return fail(s, SG_ERR_ARG, "too many constraints");
   if (params && params[4] != 0.0 && params[4] != 1.0)
     return fail(s, SG_ERR_UNSUPPORTED, "constraint rescale is not supported by the GPU path");
   set_cons(P.cons[P.ncons], kind, params);
+  for (int r = 0; r < s->nrep; r++) {
+    int rc = check_cons(s, P.cons[P.ncons], value0[r]);
+    if (rc) return rc;
+  }
   for (int r = 0; r < s->nrep; r++) s->reps_h[r].cons_p[P.ncons] = value0[r];
   P.ncons++;
   int rc = push_reps(s);
@@ -845,14 +871,15 @@ int sg_add_constraint_per_replica(sg_system* s, int kind, const double* params, 
 }
 
 int sg_add_constraint(sg_system* s, int kind, const double* params) {
-  if (!s || kind < SG_CONS_NONE || kind > SG_CONS_ELLIPSOID) return fail(s, SG_ERR_ARG, "sg_add_constraint: bad kind");
+  if (!s || kind < SG_CONS_NONE || kind > SG_CONS_GAUSSIAN_BUMP) return fail(s, SG_ERR_ARG, "sg_add_constraint: bad kind");
   Program& P = s->prog;
   if (P.ncons >= MAX_CONS) return fail(s, SG_ERR_ARG, "too many constraints");
   if (params && params[4] != 0.0 && params[4] != 1.0)
     return fail(s, SG_ERR_UNSUPPORTED, "constraint rescale is not supported by the GPU path");
   set_cons(P.cons[P.ncons], kind, params);
-  for (int r = 0; r < s->nrep; r++)
-    s->reps_h[r].cons_p[P.ncons] = params ? params[0] : (kind == CONS_PLANE || kind == CONS_NONE ? 0.0 : 1.0);
+  const double first = params ? params[0] : cons_first_default(kind);
+  if (int rc = check_cons(s, P.cons[P.ncons], first)) return rc;
+  for (int r = 0; r < s->nrep; r++) s->reps_h[r].cons_p[P.ncons] = first;
   P.ncons++;
   int rc = push_reps(s);
   if (rc) return rc;

@@ -185,6 +185,10 @@ ConstraintSpec resolve_constraint(const std::string& name, const Params& p) {
   else if (name == "cylinder") s.kind = SG_CONS_CYLINDER;
   else if (name == "torus") s.kind = SG_CONS_TORUS;
   else if (name == "ellipsoid") s.kind = SG_CONS_ELLIPSOID;
+  else if (name == "peanut") s.kind = SG_CONS_PEANUT;
+  else if (name == "gyroid") s.kind = SG_CONS_GYROID;
+  else if (name == "hourglass") s.kind = SG_CONS_HOURGLASS;
+  else if (name == "gaussian_bump") s.kind = SG_CONS_GAUSSIAN_BUMP;
   else throw HostError("Constraint " + name + " is not part of the GPU path.");
   if (has(p, "group") && p.at("group") != "all") throw HostError("Constraint groups other than 'all' are not part of the GPU path.");
   // Constraint base (constraint.hpp:56-120); tol is parsed as an int there (82)
@@ -195,6 +199,16 @@ ConstraintSpec resolve_constraint(const std::string& name, const Params& p) {
   else if (name == "sphere" || name == "cylinder") first = get(p, "r", 1.0);
   else if (name == "torus") { first = get(p, "c", 1.0); second = get(p, "a", 0.5); }  // constraint_torus.hpp
   else if (name == "ellipsoid") { first = get(p, "a", 1.0); second = get(p, "b", 1.0); third = get(p, "c", 1.0); }
+  else if (name == "peanut") {  // constraint_peanut.hpp:62-88
+    first = get(p, "a", 10.0); second = get(p, "b", 8.0);
+    if (second <= first)
+      throw HostError("Parameter b has to be larger than parameter a. Otherwise the surface will be disconnected.");
+  } else if (name == "hourglass") {  // constraint_hourglass.hpp:64-102 (A checked only when given)
+    first = get(p, "R", 10.0); second = get(p, "A", 1.0); third = get(p, "n", 1.0);
+    if (has(p, "A") && second > first) throw HostError("Hourglass constraint. Amplitude has to be smaller than the radius.");
+  } else if (name == "gaussian_bump") {  // constraint_gaussian_bump.hpp
+    first = get(p, "A", 1.0); second = get(p, "a", 1.0); third = get(p, "b", 1.0);
+  }
   const double v[9] = {first, unlimited, maxiter, tol, get(p, "rescale", 1.0), get(p, "rescale_steps", 1000.0),
                        get(p, "rescale_freq", 10.0), second, third};
   for (int i = 0; i < 9; i++) s.params[i] = v[i];

@@ -194,8 +194,10 @@ def resolve_external(name: str, params: dict, ntypes: int) -> ExternalSpec:
 def resolve_constraint(name: str, params: dict) -> tuple[int, list[float]]:
     """constraint <name> {...} (constraint.hpp:56-120, constraint_plane.hpp,
     constraint_sphere.hpp, constraint_cylinder.hpp, constraint_torus.hpp,
-    constraint_ellipsoid.hpp): returns (kind, [zpos|r|c|a, unlimited, maxiter,
-    tol, rescale, rescale_steps, rescale_freq, torus a|ellipsoid b, ellipsoid c])."""
+    constraint_ellipsoid.hpp, constraint_peanut.hpp, constraint_gyroid.hpp,
+    constraint_hourglass.hpp, constraint_gaussian_bump.hpp): returns (kind,
+    [zpos|r|c|a|R|A, unlimited, maxiter, tol, rescale, rescale_steps,
+    rescale_freq, second shape parameter, third shape parameter])."""
     if name not in E.CONSTRAINT:
         raise PluginError(f"Constraint {name} is not part of the GPU path.")
     if "group" in params and params["group"] != "all":
@@ -216,6 +218,17 @@ def resolve_constraint(name: str, params: dict) -> tuple[int, list[float]]:
         first, second, unlimited = _f(params, "c", 1.0), _f(params, "a", 0.5), 0.0
     elif name == "ellipsoid":  # constraint_ellipsoid.hpp: a, b, c (1)
         first, second, third, unlimited = _f(params, "a", 1.0), _f(params, "b", 1.0), _f(params, "c", 1.0), 0.0
+    elif name == "peanut":  # constraint_peanut.hpp:62-88: a (10), b (8), b > a required
+        first, second, unlimited = _f(params, "a", 10.0), _f(params, "b", 8.0), 0.0
+        if second <= first:
+            raise PluginError("Parameter b has to be larger than parameter a. Otherwise the surface will be "
+                              "disconnected.")
+    elif name == "hourglass":  # constraint_hourglass.hpp:64-102: R (10), A (1; if given, at most R), n (1)
+        first, second, third, unlimited = _f(params, "R", 10.0), _f(params, "A", 1.0), _f(params, "n", 1.0), 0.0
+        if "A" in params and second > first:
+            raise PluginError("Hourglass constraint. Amplitude has to be smaller than the radius.")
+    elif name == "gaussian_bump":  # constraint_gaussian_bump.hpp: A, a, b (1)
+        first, second, third, unlimited = _f(params, "A", 1.0), _f(params, "a", 1.0), _f(params, "b", 1.0), 0.0
     else:
         first, unlimited = 0.0, 0.0
     return E.CONSTRAINT[name], [first, unlimited, maxiter, tol, rescale, rescale_steps, rescale_freq, second, third]

@@ -71,12 +71,57 @@ def drive(backend, parts, box, periodic=True, nlist=(2.4, 0.3), constraint=("pla
     return sim
 
 
+def gyroid_value(x, y, z, box):
+    lx, ly, lz = box
+    return (np.cos(2 * np.pi * z / lz) * np.sin(2 * np.pi * x / lx) + np.cos(2 * np.pi * x / lx) * np.sin(2 * np.pi * y / ly)
+            + np.cos(2 * np.pi * y / ly) * np.sin(2 * np.pi * z / lz))
+
+
+def gyroid_gradient(x, y, z, box):
+    lx, ly, lz = box
+    X, Y, Z = 2 * np.pi * x / lx, 2 * np.pi * y / ly, 2 * np.pi * z / lz
+    return np.stack([2 * np.pi * (np.cos(X) * np.cos(Z) - np.sin(X) * np.sin(Y)) / lx,
+                     2 * np.pi * (np.cos(X) * np.cos(Y) - np.sin(Y) * np.sin(Z)) / ly,
+                     2 * np.pi * (np.cos(Y) * np.cos(Z) - np.sin(X) * np.sin(Z)) / lz], -1)
+
+
 def surface_disks(kind, n, seed=1, **shape):
-    """n particles scattered near a cylinder (r), torus (c, a) or ellipsoid
-    (a, b, c) around the origin, with random directors; the constraint
-    projects them on the surface when it is added."""
+    """n particles scattered near a cylinder (r), torus (c, a), ellipsoid
+    (a, b, c), peanut (a, b), hourglass (R, A, n_nodes, Lz), Gaussian bump
+    (A, a, b, L) or gyroid (box) around the origin, with random directors; the
+    constraint projects them on the surface when it is added."""
     rng = np.random.default_rng(seed)
     u, v = rng.uniform(0.0, 2.0 * np.pi, n), rng.uniform(0.0, 2.0 * np.pi, n)
+    if kind == "peanut":  # rays from the origin to the surface (b > a: one root in r^2)
+        a, b = shape["a"], shape["b"]
+        w = rng.normal(size=(3, n))
+        w /= np.linalg.norm(w, axis=0)
+        c = w[0] ** 2 - w[1] ** 2 - w[2] ** 2
+        r = np.sqrt(a * a * c + np.sqrt(a ** 4 * c * c - a ** 4 + b ** 4))
+        x, y, z = r * w[0], r * w[1], r * w[2]
+    elif kind == "hourglass":
+        R, A, nn, Lz = shape["R"], shape["A"], shape["n_nodes"], shape["Lz"]
+        z = rng.uniform(-0.45 * Lz, 0.45 * Lz, n)
+        rho = R + A * np.sin(2 * np.pi * nn * z / Lz)
+        x, y = rho * np.cos(u), rho * np.sin(u)
+    elif kind == "gaussian_bump":
+        A, a, b, L = shape["A"], shape["a"], shape["b"], shape["L"]
+        x, y = rng.uniform(-0.45 * L, 0.45 * L, n), rng.uniform(-0.45 * L, 0.45 * L, n)
+        z = A * np.exp(-x * x / a - y * y / b)
+    elif kind == "gyroid":  # random points pulled onto the surface by Newton steps along the gradient
+        box = shape["box"]
+        p = np.stack([rng.uniform(-h / 2, h / 2, n) for h in box], -1)
+        for _ in range(30):
+            g = gyroid_value(p[:, 0], p[:, 1], p[:, 2], box)
+            G = gyroid_gradient(p[:, 0], p[:, 1], p[:, 2], box)
+            p -= (g / np.maximum(np.sum(G * G, -1), 1e-12))[:, None] * G
+        x, y, z = p[:, 0], p[:, 1], p[:, 2]
+    if kind in ("peanut", "hourglass", "gaussian_bump", "gyroid"):
+        jitter = rng.normal(0.0, 0.02, (3, n))
+        d = rng.normal(size=(3, n))
+        d /= np.linalg.norm(d, axis=0)
+        return dict(x=x + jitter[0], y=y + jitter[1], z=z + jitter[2], vx=np.zeros(n), vy=np.zeros(n),
+                    vz=np.zeros(n), nx=d[0], ny=d[1], nz=d[2], radius=np.full(n, 1.0))
     if kind == "cylinder":
         r, Lz = shape["r"], shape["Lz"]
         x, y, z = r * np.cos(u), r * np.sin(u), rng.uniform(-Lz / 2, Lz / 2, n)

@@ -386,6 +386,25 @@ def test_trajectory_curved_constraints(kind, shape, box, n):
     assert_traj(e, o)
 
 
+@pytest.mark.parametrize("kind,shape,conf,box,periodic,n", [
+    ("peanut", {"a": 8.0, "b": 10.0}, {"a": "8.0", "b": "10.0"}, (60.0, 60.0, 60.0), False, 400),
+    ("hourglass", {"R": 10.0, "A": 2.0, "n_nodes": 2.0, "Lz": 40.0}, {"R": "10.0", "A": "2.0", "n": "2.0"},
+     (40.0, 40.0, 40.0), False, 700),
+    ("gaussian_bump", {"A": 4.0, "a": 30.0, "b": 20.0, "L": 40.0}, {"A": "4.0", "a": "30.0", "b": "20.0"},
+     (40.0, 40.0, 20.0), False, 400),
+    ("gyroid", {"box": (30.0, 30.0, 30.0)}, {}, (30.0, 30.0, 30.0), True, 800),
+])
+def test_trajectory_implicit_surfaces(kind, shape, conf, box, periodic, n):
+    # active Brownian particles on a peanut / hourglass / Gaussian bump /
+    # gyroid (SHAKE projection of the implicit surface, the generic fused
+    # kernel), 300 steps against the oracle with the shared noise stream
+    parts = surface_disks(kind, n, seed=18, **shape)
+    e, o = run_both(n, parts, box, 299, periodic=periodic, nlist=(2.4, 0.3), constraint=(kind, conf),
+                    pairs=[("soft", {"k": "10"})], aligns=[("polar", {"J": "0.2"})], dt=1e-3,
+                    integrators=[("brownian", {"v0": "1.0", "nu": "0.1", "seed": "4"})])
+    assert_traj(e, o)
+
+
 def test_trajectory_vicsek_model():
     # the Vicsek integrator with the Vicsek aligner (and a soft repulsion
     # through the mobility), on the generic fused kernel

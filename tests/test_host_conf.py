@@ -128,6 +128,28 @@ def test_command_order_rules(tmp_path):
     assert r.returncode == 1 and "non-existent integrator" in r.stderr
 
 
+@pytest.mark.parametrize("line,kind", [
+    ("constraint peanut { a = 8; b = 10 }", 6),
+    ("constraint gyroid { }", 7),
+    ("constraint hourglass { R = 10; A = 2; n = 2 }", 8),
+    ("constraint gaussian_bump { A = 2; a = 3; b = 4 }", 9),
+])
+def test_implicit_surface_constraints_parse(tmp_path, line, kind):
+    r = check(tmp_path, CONF.replace("constraint plane { }", line))
+    assert r.returncode == 0, r.stderr
+    assert parse_describe(r.stdout)["constraint"][0][0] == str(kind)
+
+
+@pytest.mark.parametrize("line,msg", [
+    ("constraint peanut { }", "Parameter b has to be larger than parameter a"),
+    ("constraint peanut { a = 5; b = 5 }", "Parameter b has to be larger than parameter a"),
+    ("constraint hourglass { R = 3; A = 4 }", "Amplitude has to be smaller than the radius"),
+])
+def test_implicit_surface_parameter_errors(tmp_path, line, msg):
+    r = check(tmp_path, CONF.replace("constraint plane { }", line))
+    assert r.returncode == 1 and msg in r.stderr, r.stderr
+
+
 def test_vicsek_and_nve_integrators_parse(tmp_path):
     conf = CONF.replace("integrator brownian_pos { seed = 7; mu = 1.0 }\nintegrator brownian_align { seed = 8; nu = 0.1, mur = 1.0 }\n",
                         "integrator vicsek { v0 = 0.5; eta = 0.3; seed = 2 }\n")

@@ -9,7 +9,7 @@ import pytest
 
 from oracle.oracle import OracleSystem, noise_gauss, noise_log, noise_uniform
 from samos_b200 import engine as E
-from scenarios import drive, plane_disks, sphere_disks, surface_disks
+from scenarios import drive, gyroid_gradient, gyroid_value, plane_disks, sphere_disks, surface_disks
 
 
 def two(x2, y2=0.0, r=(1.0, 1.0), box=20.0, n1=(1.0, 0.0, 0.0), n2=(0.0, 1.0, 0.0)):
@@ -246,3 +246,73 @@ def test_curved_constraints_project_onto_their_surface(kind, shape, box):
         N /= np.linalg.norm(N, axis=1)[:, None]
     assert np.allclose(np.linalg.norm(n, axis=1), 1.0, atol=1e-14)
     assert np.abs(np.sum(n * N, 1)).max() <= 1e-6
+
+
+IMPLICIT_CASES = [
+    ("peanut", {"a": 8.0, "b": 10.0}, {"a": 8.0, "b": 10.0}, (60.0, 60.0, 60.0), False),
+    ("hourglass", {"R": 10.0, "A": 2.0, "n_nodes": 2.0, "Lz": 40.0}, {"R": 10.0, "A": 2.0, "n": 2.0},
+     (40.0, 40.0, 40.0), False),
+    ("gaussian_bump", {"A": 4.0, "a": 30.0, "b": 20.0, "L": 40.0}, {"A": 4.0, "a": 30.0, "b": 20.0},
+     (40.0, 40.0, 20.0), False),
+    ("gyroid", {"box": (30.0, 30.0, 30.0)}, {}, (30.0, 30.0, 30.0), True),
+]
+
+
+def implicit_np(kind, conf, box, x, y, z):
+    """g and its normalised gradient in numpy, from the formulas in the
+    reference's constraint_<kind>.cpp."""
+    if kind == "peanut":
+        a, b = conf["a"], conf["b"]
+        tr = x * x + y * y + z * z
+        g = a ** 4 - b ** 4 - 2 * a * a * (x * x - y * y - z * z) + tr * tr
+        G = np.stack([(-4 * a * a + 4 * tr) * x, (4 * a * a + 4 * tr) * y, (4 * a * a + 4 * tr) * z], 1)
+    elif kind == "hourglass":
+        R, A, nn, lz = conf["R"], conf["A"], conf["n"], box[2]
+        zf = R + A * np.sin(2 * np.pi * nn * z / lz)
+        g = x * x + y * y - zf * zf
+        G = np.stack([2 * x, 2 * y, -4 * A * nn * np.pi * np.cos(2 * nn * np.pi * z / lz) * zf / lz], 1)
+    elif kind == "gaussian_bump":
+        A, a, b = conf["A"], conf["a"], conf["b"]
+        f = np.exp(-x * x / a - y * y / b)
+        g = A * f - z
+        G = np.stack([-2 * A * x * f / a, -2 * A * y * f / b, -np.ones_like(z)], 1)
+    else:
+        g = gyroid_value(x, y, z, box)
+        G = gyroid_gradient(x, y, z, box)
+    return g, G / np.linalg.norm(G, axis=1)[:, None]
+
+
+@pytest.mark.parametrize("kind,shape,conf,box,periodic", IMPLICIT_CASES)
+def test_implicit_surfaces_project_onto_their_surface(kind, shape, conf, box, periodic):
+    # peanut, hourglass, Gaussian bump and gyroid have no enforce of their own:
+    # Constraint::enforce's SHAKE projection (constraint.cpp:40-87) along their
+    # gradients brings every particle to g = 0 within tol; directors unit and
+    # tangent to the normalised gradient, which is also the stored normal
+    parts = surface_disks(kind, 300, seed=6, **shape)
+    o = OracleSystem(300)
+    drive(o, parts, box, periodic=periodic, constraint=(kind, {k: repr(v) for k, v in conf.items()}))
+    x, y, z = o.download("x"), o.download("y"), o.download("z")
+    n = np.stack([o.download("nx"), o.download("ny"), o.download("nz")], 1)
+    g, N = implicit_np(kind, conf, box, x, y, z)
+    assert np.abs(g).max() <= 1e-6
+    assert np.allclose(np.linalg.norm(n, axis=1), 1.0, atol=1e-14)
+    assert np.abs(np.sum(n * N, 1)).max() <= 1e-6
+    NN = np.stack([o.download("Nx"), o.download("Ny"), o.download("Nz")], 1)
+    np.testing.assert_allclose(NN, N, atol=1e-12)
+
+
+def test_implicit_surface_parameters_checked_like_the_reference():
+    from samos_b200.plugins import PluginError, resolve_constraint
+    with pytest.raises(PluginError):
+        resolve_constraint("peanut", {})  # defaults a 10, b 8 (constraint_peanut.hpp:62-88)
+    with pytest.raises(PluginError):
+        resolve_constraint("peanut", {"a": "5", "b": "5"})
+    with pytest.raises(PluginError):
+        resolve_constraint("hourglass", {"R": "3", "A": "4"})
+    kind, p = resolve_constraint("hourglass", {"R": "0.5"})  # A defaults to 1, unchecked
+    assert p[0] == 0.5 and p[7] == 1.0 and p[8] == 1.0
+    kind, p = resolve_constraint("gaussian_bump", {"A": "2", "a": "3", "b": "4"})
+    assert (p[0], p[7], p[8]) == (2.0, 3.0, 4.0)
+    o = OracleSystem(4)
+    with pytest.raises(ValueError):
+        o.add_constraint(E.CONSTRAINT["peanut"], [5.0, 0, 100, 1e-6, 1, 1000, 10, 4.0, 0.0])
