@@ -893,7 +893,8 @@ int or_add_constraint(or_system* s, int kind, const double* p)
   memset(c, 0, sizeof(*c));
   c->kind = kind;
   c->zpos = p ? p[0] : 0.0; c->unlimited = p ? (int)p[1] : 0;
-  c->r = p ? p[0] : (kind == OR_CONS_PEANUT || kind == OR_CONS_HOURGLASS ? 10.0 : 1.0);
+  c->r = p ? p[0] : (kind == OR_CONS_PEANUT || kind == OR_CONS_HOURGLASS ? 10.0 : kind == OR_CONS_SLAB ? 0.0 : 1.0);
+  if (kind == OR_CONS_PLANE_WALLS && c->r > s->xhi) c->r = s->xhi;  /* constraint_plane_walls.hpp:64-71 */
   if (kind >= OR_CONS_TORUS) {  /* params[7], params[8] */
     c->b2 = p ? p[7] : (kind == OR_CONS_TORUS ? 0.5 : kind == OR_CONS_PEANUT ? 8.0 : 1.0);
     c->b3 = p ? p[8] : 1.0;
@@ -1087,6 +1088,33 @@ static void implicit_enforce(or_system* s, const or_cons* c, int i)
   if (s->periodic) enforce_periodic(s, i);
 }
 
+/* ConstraintSlab::enforce (constraint_slab.cpp:35-61): reflect z into
+   [z_lo, z_hi] (vz and nz reversed), then the periodic wrap; its normal is
+   zero (constraint_slab.hpp:94) */
+static void slab_enforce(or_system* s, const or_cons* c, int i)
+{
+  if (s->z[i] < c->r) { s->z[i] = c->r; s->vz[i] = -s->vz[i]; s->nz[i] = -s->nz[i]; }
+  if (s->z[i] > c->b2) { s->z[i] = c->b2; s->vz[i] = -s->vz[i]; s->nz[i] = -s->nz[i]; }
+  s->Nx[i] = 0.0; s->Ny[i] = 0.0; s->Nz[i] = 0.0;
+  if (s->periodic) enforce_periodic(s, i);
+}
+
+/* ConstraintPlaneWalls::enforce (constraint_plane_walls.cpp:38-70): z = 0,
+   vz = fz = 0, y wrapped without image flag, walls at x = +-l; normal
+   (0, 0, 1) (constraint_plane_walls.hpp:90) */
+static void plane_walls_enforce(or_system* s, const or_cons* c, int i)
+{
+  double ylo = s->ylo, yhi = s->yhi, ly = yhi - ylo;
+  s->z[i] = 0.0; s->vz[i] = 0.0; s->fz[i] = 0.0;
+  s->Nx[i] = 0.0; s->Ny[i] = 0.0; s->Nz[i] = 1.0;
+  if (s->periodic) {
+    if (s->y[i] <= ylo) s->y[i] += ly;
+    else if (s->y[i] >= yhi) s->y[i] -= ly;
+  }
+  if (s->x[i] >= c->r) { s->x[i] = c->r; s->vx[i] = -s->vx[i]; }
+  else if (s->x[i] <= -c->r) { s->x[i] = -c->r; s->vx[i] = -s->vx[i]; }
+}
+
 static void enforce_one(or_system* s, int i)
 {
   for (int k = 0; k < s->ncons; k++) {
@@ -1094,7 +1122,9 @@ static void enforce_one(or_system* s, int i)
     if (c->kind == OR_CONS_PLANE) plane_enforce(s, c, i);
     else if (c->kind == OR_CONS_SPHERE) sphere_enforce(s, c, i);
     else if (c->kind == OR_CONS_CYLINDER) cylinder_enforce(s, c, i);
-    else if (c->kind >= OR_CONS_TORUS) implicit_enforce(s, c, i);
+    else if (c->kind >= OR_CONS_TORUS && c->kind <= OR_CONS_GAUSSIAN_BUMP) implicit_enforce(s, c, i);
+    else if (c->kind == OR_CONS_SLAB) slab_enforce(s, c, i);
+    else if (c->kind == OR_CONS_PLANE_WALLS) plane_walls_enforce(s, c, i);
     else if (s->periodic) enforce_periodic(s, i);
   }
 }
@@ -1113,7 +1143,8 @@ static double project_torque(or_system* s, int i)
   double val = 0.0;
   for (int k = 0; k < s->ncons; k++) {
     const or_cons* c = &s->cons[k];
-    if (c->kind == OR_CONS_PLANE) val += s->tz[i];
+    if (c->kind == OR_CONS_PLANE || c->kind == OR_CONS_PLANE_WALLS) val += s->tz[i];
+    else if (c->kind == OR_CONS_SLAB) val += 0.0;  /* constraint_slab.hpp:91 */
     else if (c->kind != OR_CONS_NONE) {
       double Nx, Ny, Nz;
       surface_normal(s, c, i, &Nx, &Ny, &Nz);
@@ -1130,14 +1161,14 @@ static void rotate_director(or_system* s, int i, double phi)
 {
   for (int k = 0; k < s->ncons; k++) {
     const or_cons* c = &s->cons[k];
-    if (c->kind == OR_CONS_PLANE) {
+    if (c->kind == OR_CONS_PLANE || c->kind == OR_CONS_PLANE_WALLS) {
       double cs = cos(phi), sn = sin(phi);
       double Rxx = cs, Rxy = -sn, Ryx = sn, Ryy = cs;
       double nx = Rxx * s->nx[i] + Rxy * s->ny[i];
       double ny = Ryx * s->nx[i] + Ryy * s->ny[i];
       double len = sqrt(nx * nx + ny * ny);
       s->nx[i] = nx / len; s->ny[i] = ny / len;
-    } else if (c->kind != OR_CONS_NONE) {
+    } else if (c->kind != OR_CONS_NONE && c->kind != OR_CONS_SLAB) {  /* the slab does not rotate */
       double U, V, W;
       surface_normal(s, c, i, &U, &V, &W);
       double cs = cos(phi), sn = sin(phi);
@@ -1157,13 +1188,13 @@ static void rotate_velocity(or_system* s, int i, double phi)
 {
   for (int k = 0; k < s->ncons; k++) {
     const or_cons* c = &s->cons[k];
-    if (c->kind == OR_CONS_PLANE) {
+    if (c->kind == OR_CONS_PLANE || c->kind == OR_CONS_PLANE_WALLS) {
       double cs = cos(phi), sn = sin(phi);
       double Rxx = cs, Rxy = -sn, Ryx = sn, Ryy = cs;
       double vx = Rxx * s->vx[i] + Rxy * s->vy[i];
       double vy = Ryx * s->vx[i] + Ryy * s->vy[i];
       s->vx[i] = vx; s->vy[i] = vy;
-    } else if (c->kind != OR_CONS_NONE) {
+    } else if (c->kind != OR_CONS_NONE && c->kind != OR_CONS_SLAB) {  /* the slab does not rotate */
       double U, V, W;
       surface_normal(s, c, i, &U, &V, &W);
       double cs = cos(phi), sn = sin(phi);

@@ -26,10 +26,13 @@ constexpr int BLOCK = 128;          // particle slots per block; replicas are pa
 enum { PAIR_SOFT = 0, PAIR_LJ = 1, PAIR_MORSE = 2, PAIR_GAUSSIAN = 3 };
 enum { ALIGN_POLAR = 0, ALIGN_NEMATIC = 1, ALIGN_VICSEK = 2 };
 enum { CONS_NONE = 0, CONS_PLANE = 1, CONS_SPHERE = 2, CONS_CYLINDER = 3, CONS_TORUS = 4, CONS_ELLIPSOID = 5,
-       CONS_PEANUT = 6, CONS_GYROID = 7, CONS_HOURGLASS = 8, CONS_GAUSSIAN_BUMP = 9 };
+       CONS_PEANUT = 6, CONS_GYROID = 7, CONS_HOURGLASS = 8, CONS_GAUSSIAN_BUMP = 9, CONS_SLAB = 10,
+       CONS_PLANE_WALLS = 11 };
 // surfaces given by an implicit function g = 0 and projected by the base
 // class's SHAKE iteration (no enforce of their own in the reference)
-__host__ __device__ __forceinline__ bool cons_implicit(int kind) { return kind >= CONS_TORUS; }
+__host__ __device__ __forceinline__ bool cons_implicit(int kind) {
+  return kind >= CONS_TORUS && kind <= CONS_GAUSSIAN_BUMP;
+}
 enum { INT_BROWNIAN = 0, INT_BROWNIAN_POS = 1, INT_BROWNIAN_ALIGN = 2, INT_LANGEVIN = 3, INT_FIRE = 4, INT_NVE = 5, INT_VICSEK = 6 };
 enum { LANGEVIN_BAOAB = 0, LANGEVIN_SPV = 1, LANGEVIN_BBK = 2 };
 
@@ -401,6 +404,27 @@ __host__ __device__ __forceinline__ void surface_normal(const ConsComp& C, const
   }
 }
 
+// ConstraintSlab::enforce (constraint_slab.cpp:35-61): z kept in [z_lo, z_hi]
+// by reflection (vz, nz reversed), then the system's periodic wrap
+__device__ __forceinline__ void slab_enforce(const Replica& R, double z_lo, double z_hi, Part& p) {
+  if (p.z < z_lo) { p.z = z_lo; p.vz = -p.vz; p.nz = -p.nz; }
+  if (p.z > z_hi) { p.z = z_hi; p.vz = -p.vz; p.nz = -p.nz; }
+  enforce_periodic(R, p);
+}
+
+// ConstraintPlaneWalls::enforce (constraint_plane_walls.cpp:38-70): z = 0,
+// vz = fz = 0, y wrapped when periodic (no image flag), walls at x = +-l that
+// stop the particle and reverse vx
+__device__ __forceinline__ void plane_walls_enforce(const Replica& R, double l, Part& p) {
+  p.z = 0.0; p.vz = 0.0; p.fz = 0.0;
+  if (R.periodic) {
+    if (p.y <= R.ylo) p.y += R.Ly;
+    else if (p.y >= R.yhi) p.y -= R.Ly;
+  }
+  if (p.x >= l) { p.x = l; p.vx = -p.vx; }
+  else if (p.x <= -l) { p.x = -l; p.vx = -p.vx; }
+}
+
 // Constraint::enforce, constraints/constraint.cpp:40-87 (SHAKE along the
 // gradient at the start point, then the tangent projections)
 __device__ __forceinline__ void implicit_enforce(const ConsComp& C, const Replica& R, double a0, Part& p) {
@@ -438,6 +462,8 @@ __device__ __forceinline__ void enforce_all(const Program& P, const Replica& R, 
     else if (kind == CONS_SPHERE) sphere_enforce(R.cons_p[c], p);
     else if (kind == CONS_CYLINDER) cylinder_enforce(R, R.cons_p[c], p);
     else if (cons_implicit(kind)) implicit_enforce(P.cons[c], R, R.cons_p[c], p);
+    else if (kind == CONS_SLAB) slab_enforce(R, R.cons_p[c], P.cons[c].b2, p);
+    else if (kind == CONS_PLANE_WALLS) plane_walls_enforce(R, R.cons_p[c], p);
     else enforce_periodic(R, p);
   }
 }
@@ -450,7 +476,8 @@ __device__ __forceinline__ double project_torque(const Program& P, const Replica
   double val = 0.0;
   for (int c = 0; c < P.ncons; c++) {
     int kind = P.cons[c].kind;
-    if (kind == CONS_PLANE) val += p.tz;
+    if (kind == CONS_PLANE || kind == CONS_PLANE_WALLS) val += p.tz;
+    else if (kind == CONS_SLAB) val += 0.0;  // constraint_slab.hpp:91
     else if (kind != CONS_NONE) {
       double Nx, Ny, Nz;
       surface_normal(P.cons[c], R, R.cons_p[c], p, Nx, Ny, Nz);
@@ -465,14 +492,14 @@ __device__ __forceinline__ double project_torque(const Program& P, const Replica
 __device__ __forceinline__ void rotate_director(const Program& P, const Replica& R, Part& p, double phi) {
   for (int c = 0; c < P.ncons; c++) {
     int kind = P.cons[c].kind;
-    if (kind == CONS_PLANE) {
+    if (kind == CONS_PLANE || kind == CONS_PLANE_WALLS) {
       double cs = cos(phi), sn = sin(phi);
       double Rxx = cs, Rxy = -sn, Ryx = sn, Ryy = cs;
       double nx = Rxx * p.nx + Rxy * p.ny;
       double ny = Ryx * p.nx + Ryy * p.ny;
       double len = sqrt(nx * nx + ny * ny);
       p.nx = nx / len; p.ny = ny / len;
-    } else if (kind != CONS_NONE) {
+    } else if (kind != CONS_NONE && kind != CONS_SLAB) {  // the slab does not rotate (constraint_slab.hpp:85-88)
       double U, V, W;
       surface_normal(P.cons[c], R, R.cons_p[c], p, U, V, W);
       double cs = cos(phi), sn = sin(phi);
@@ -491,13 +518,13 @@ __device__ __forceinline__ void rotate_director(const Program& P, const Replica&
 __device__ __forceinline__ void rotate_velocity(const Program& P, const Replica& R, Part& p, double phi) {
   for (int c = 0; c < P.ncons; c++) {
     int kind = P.cons[c].kind;
-    if (kind == CONS_PLANE) {
+    if (kind == CONS_PLANE || kind == CONS_PLANE_WALLS) {
       double cs = cos(phi), sn = sin(phi);
       double Rxx = cs, Rxy = -sn, Ryx = sn, Ryy = cs;
       double vx = Rxx * p.vx + Rxy * p.vy;
       double vy = Ryx * p.vx + Ryy * p.vy;
       p.vx = vx; p.vy = vy;
-    } else if (kind != CONS_NONE) {
+    } else if (kind != CONS_NONE && kind != CONS_SLAB) {  // the slab does not rotate (constraint_slab.hpp:85-88)
       double U, V, W;
       surface_normal(P.cons[c], R, R.cons_p[c], p, U, V, W);
       double cs = cos(phi), sn = sin(phi);

@@ -484,9 +484,12 @@ int sg_download(sg_system* s, int replica, const char* field, void* host) {
     double* h = (double*)host;
     for (int i = 0; i < n; i++) h[i] = s->uploaded_N[comp][off + i];
     for (int c = 0; c < s->prog.ncons; c++) {
-      if (s->prog.cons[c].kind == CONS_PLANE)
+      const int kind = s->prog.cons[c].kind;
+      if (kind == CONS_PLANE || kind == CONS_PLANE_WALLS)
         for (int i = 0; i < n; i++) h[i] = comp == 2 ? 1.0 : 0.0;
-      else if (s->prog.cons[c].kind != CONS_NONE) {  // compute_normal of the curved surfaces
+      else if (kind == CONS_SLAB)  // constraint_slab.hpp:94
+        for (int i = 0; i < n; i++) h[i] = 0.0;
+      else if (kind != CONS_NONE) {  // compute_normal of the curved surfaces
         const ConsComp& C = s->prog.cons[c];
         const double a0 = s->reps_h[replica].cons_p[c];
         for (int k = 0; k < n; k++) {
@@ -834,13 +837,20 @@ static void set_cons(ConsComp& C, int kind, const double* params) {
   else if (kind == CONS_PEANUT) d2 = 8.0;
   else if (kind == CONS_HOURGLASS) { d2 = 1.0; d3 = 1.0; }
   else if (kind == CONS_GAUSSIAN_BUMP) { d2 = 1.0; d3 = 1.0; }
+  else if (kind == CONS_SLAB) d2 = 1.0;  // z_hi (constraint_slab.hpp:68-78)
   C.b2 = params ? params[7] : d2;
   C.b3 = params ? params[8] : d3;
 }
 
 static double cons_first_default(int kind) {
-  return kind == CONS_PLANE || kind == CONS_NONE || kind == CONS_GYROID ? 0.0
+  return kind == CONS_PLANE || kind == CONS_NONE || kind == CONS_GYROID || kind == CONS_SLAB ? 0.0
        : kind == CONS_PEANUT || kind == CONS_HOURGLASS ? 10.0 : 1.0;
+}
+
+// a wall position beyond the box is moved to its edge
+// (constraint_plane_walls.hpp:64-71)
+static double cons_first_of(const sg_system* s, int kind, double first, int r) {
+  return kind == CONS_PLANE_WALLS && first > s->reps_h[r].xhi ? s->reps_h[r].xhi : first;
 }
 
 // the peanut constructor's check (constraint_peanut.hpp:84-88); the
@@ -853,7 +863,7 @@ static int check_cons(sg_system* s, const ConsComp& C, double first) {
 }
 
 int sg_add_constraint_per_replica(sg_system* s, int kind, const double* params, const double* value0) {
-  if (!s || !value0 || kind < SG_CONS_NONE || kind > SG_CONS_GAUSSIAN_BUMP) return fail(s, SG_ERR_ARG, "bad constraint");
+  if (!s || !value0 || kind < SG_CONS_NONE || kind > SG_CONS_PLANE_WALLS) return fail(s, SG_ERR_ARG, "bad constraint");
   Program& P = s->prog;
   if (P.ncons >= MAX_CONS) return fail(s, SG_ERR_ARG, "too many constraints");
   if (params && params[4] != 0.0 && params[4] != 1.0)
@@ -863,7 +873,7 @@ int sg_add_constraint_per_replica(sg_system* s, int kind, const double* params, 
     int rc = check_cons(s, P.cons[P.ncons], value0[r]);
     if (rc) return rc;
   }
-  for (int r = 0; r < s->nrep; r++) s->reps_h[r].cons_p[P.ncons] = value0[r];
+  for (int r = 0; r < s->nrep; r++) s->reps_h[r].cons_p[P.ncons] = cons_first_of(s, kind, value0[r], r);
   P.ncons++;
   int rc = push_reps(s);
   if (rc) return rc;
@@ -871,7 +881,7 @@ int sg_add_constraint_per_replica(sg_system* s, int kind, const double* params, 
 }
 
 int sg_add_constraint(sg_system* s, int kind, const double* params) {
-  if (!s || kind < SG_CONS_NONE || kind > SG_CONS_GAUSSIAN_BUMP) return fail(s, SG_ERR_ARG, "sg_add_constraint: bad kind");
+  if (!s || kind < SG_CONS_NONE || kind > SG_CONS_PLANE_WALLS) return fail(s, SG_ERR_ARG, "sg_add_constraint: bad kind");
   Program& P = s->prog;
   if (P.ncons >= MAX_CONS) return fail(s, SG_ERR_ARG, "too many constraints");
   if (params && params[4] != 0.0 && params[4] != 1.0)
@@ -879,7 +889,7 @@ int sg_add_constraint(sg_system* s, int kind, const double* params) {
   set_cons(P.cons[P.ncons], kind, params);
   const double first = params ? params[0] : cons_first_default(kind);
   if (int rc = check_cons(s, P.cons[P.ncons], first)) return rc;
-  for (int r = 0; r < s->nrep; r++) s->reps_h[r].cons_p[P.ncons] = first;
+  for (int r = 0; r < s->nrep; r++) s->reps_h[r].cons_p[P.ncons] = cons_first_of(s, kind, first, r);
   P.ncons++;
   int rc = push_reps(s);
   if (rc) return rc;

@@ -189,6 +189,8 @@ ConstraintSpec resolve_constraint(const std::string& name, const Params& p) {
   else if (name == "gyroid") s.kind = SG_CONS_GYROID;
   else if (name == "hourglass") s.kind = SG_CONS_HOURGLASS;
   else if (name == "gaussian_bump") s.kind = SG_CONS_GAUSSIAN_BUMP;
+  else if (name == "slab") s.kind = SG_CONS_SLAB;
+  else if (name == "walls") s.kind = SG_CONS_PLANE_WALLS;
   else throw HostError("Constraint " + name + " is not part of the GPU path.");
   if (has(p, "group") && p.at("group") != "all") throw HostError("Constraint groups other than 'all' are not part of the GPU path.");
   // Constraint base (constraint.hpp:56-120); tol is parsed as an int there (82)
@@ -208,6 +210,10 @@ ConstraintSpec resolve_constraint(const std::string& name, const Params& p) {
     if (has(p, "A") && second > first) throw HostError("Hourglass constraint. Amplitude has to be smaller than the radius.");
   } else if (name == "gaussian_bump") {  // constraint_gaussian_bump.hpp
     first = get(p, "A", 1.0); second = get(p, "a", 1.0); third = get(p, "b", 1.0);
+  } else if (name == "slab") {  // constraint_slab.hpp:56-78
+    first = get(p, "z_lo", 0.0); second = get(p, "z_hi", 1.0);
+  } else if (name == "walls") {  // constraint_plane_walls.hpp:56-74 (the engine moves l to the box edge)
+    first = get(p, "l", 1.0);
   }
   const double v[9] = {first, unlimited, maxiter, tol, get(p, "rescale", 1.0), get(p, "rescale_steps", 1000.0),
                        get(p, "rescale_freq", 10.0), second, third};

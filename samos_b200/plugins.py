@@ -195,7 +195,8 @@ def resolve_constraint(name: str, params: dict) -> tuple[int, list[float]]:
     """constraint <name> {...} (constraint.hpp:56-120, constraint_plane.hpp,
     constraint_sphere.hpp, constraint_cylinder.hpp, constraint_torus.hpp,
     constraint_ellipsoid.hpp, constraint_peanut.hpp, constraint_gyroid.hpp,
-    constraint_hourglass.hpp, constraint_gaussian_bump.hpp): returns (kind,
+    constraint_hourglass.hpp, constraint_gaussian_bump.hpp, constraint_slab.hpp,
+    constraint_plane_walls.hpp): returns (kind,
     [zpos|r|c|a|R|A, unlimited, maxiter, tol, rescale, rescale_steps,
     rescale_freq, second shape parameter, third shape parameter])."""
     if name not in E.CONSTRAINT:
@@ -229,6 +230,10 @@ def resolve_constraint(name: str, params: dict) -> tuple[int, list[float]]:
             raise PluginError("Hourglass constraint. Amplitude has to be smaller than the radius.")
     elif name == "gaussian_bump":  # constraint_gaussian_bump.hpp: A, a, b (1)
         first, second, third, unlimited = _f(params, "A", 1.0), _f(params, "a", 1.0), _f(params, "b", 1.0), 0.0
+    elif name == "slab":  # constraint_slab.hpp:56-78: z_lo (0), z_hi (1)
+        first, second, unlimited = _f(params, "z_lo", 0.0), _f(params, "z_hi", 1.0), 0.0
+    elif name == "walls":  # constraint_plane_walls.hpp:56-74: l (1; beyond the box: the box edge)
+        first, unlimited = _f(params, "l", 1.0), 0.0
     else:
         first, unlimited = 0.0, 0.0
     return E.CONSTRAINT[name], [first, unlimited, maxiter, tol, rescale, rescale_steps, rescale_freq, second, third]

@@ -405,6 +405,31 @@ def test_trajectory_implicit_surfaces(kind, shape, conf, box, periodic, n):
     assert_traj(e, o)
 
 
+def test_trajectory_slab_and_walls():
+    # 3-D active particles between the slab's planes (reflections, no
+    # rotation: constraint_slab.hpp:85-91) and 2-D ones between walls at
+    # x = +-l (constraint_plane_walls.cpp), 300 steps against the oracle
+    rng = np.random.default_rng(31)
+    n, L = 1200, 40.0
+    d = rng.normal(size=(3, n))
+    d /= np.linalg.norm(d, axis=0)
+    parts = dict(x=rng.uniform(-L / 2, L / 2, n), y=rng.uniform(-L / 2, L / 2, n), z=rng.uniform(-2.5, 2.5, n),
+                 vx=np.zeros(n), vy=np.zeros(n), vz=np.zeros(n), nx=d[0], ny=d[1], nz=d[2], radius=np.full(n, 1.0))
+    e, o = run_both(n, parts, (L, L, 20.0), 299, periodic=True, nlist=(2.4, 0.3),
+                    constraint=("slab", {"z_lo": "-2.0", "z_hi": "2.0"}), pairs=[("soft", {"k": "10"})],
+                    aligns=[("polar", {"J": "0.2"})], dt=1e-3,
+                    integrators=[("brownian", {"v0": "3.0", "nu": "0.1", "seed": "5"})])
+    assert_traj(e, o)
+    assert np.all(np.abs(e.download("z")) <= 2.0)
+    parts, L = plane_disks(1500, 0.5, seed=32)
+    e, o = run_both(1500, parts, (L, L, 10.0), 299, periodic=True, nlist=(2.4, 0.3),
+                    constraint=("walls", {"l": repr(0.4 * L)}), pairs=[("soft", {"k": "10", "use_particle_radii": ""})],
+                    aligns=[("polar", {"J": "0.2"})], dt=1e-3,
+                    integrators=[("brownian", {"v0": "3.0", "nu": "0.1", "seed": "6"})])
+    assert_traj(e, o)
+    assert np.all(np.abs(e.download("x")) <= 0.4 * L)
+
+
 def test_trajectory_vicsek_model():
     # the Vicsek integrator with the Vicsek aligner (and a soft repulsion
     # through the mobility), on the generic fused kernel

@@ -316,3 +316,27 @@ def test_implicit_surface_parameters_checked_like_the_reference():
     o = OracleSystem(4)
     with pytest.raises(ValueError):
         o.add_constraint(E.CONSTRAINT["peanut"], [5.0, 0, 100, 1e-6, 1, 1000, 10, 4.0, 0.0])
+
+
+def test_slab_and_walls_reflect_like_the_reference():
+    # ConstraintSlab::enforce (constraint_slab.cpp:35-61): z clamped into
+    # [z_lo, z_hi] with vz and nz reversed; ConstraintPlaneWalls::enforce
+    # (constraint_plane_walls.cpp:38-70): z = 0, walls at x = +-l reverse vx,
+    # and l beyond the box is moved to the box edge (constraint_plane_walls.hpp:64-71)
+    parts = dict(x=np.array([0.0, 1.0, 2.0]), y=np.zeros(3), z=np.array([-3.0, 0.5, 4.0]),
+                 vx=np.array([1.0, 2.0, 3.0]), vy=np.zeros(3), vz=np.array([0.5, 0.5, 0.5]),
+                 nx=np.array([0.6, 0.6, 0.6]), ny=np.zeros(3), nz=np.array([0.8, 0.8, 0.8]), radius=np.ones(3))
+    o = OracleSystem(3)
+    drive(o, parts, (20.0, 20.0, 20.0), periodic=False, constraint=("slab", {"z_lo": "-1.0", "z_hi": "2.0"}))
+    np.testing.assert_array_equal(o.download("z"), [-1.0, 0.5, 2.0])
+    np.testing.assert_array_equal(o.download("vz"), [-0.5, 0.5, -0.5])
+    np.testing.assert_array_equal(o.download("nz"), [-0.8, 0.8, -0.8])
+    parts2 = dict(parts, x=np.array([-9.0, 1.0, 9.5]))
+    o = OracleSystem(3)
+    drive(o, parts2, (20.0, 20.0, 20.0), periodic=False, constraint=("walls", {"l": "8.0"}))
+    np.testing.assert_array_equal(o.download("x"), [-8.0, 1.0, 8.0])
+    np.testing.assert_array_equal(o.download("vx"), [-1.0, 2.0, -3.0])
+    np.testing.assert_array_equal(o.download("z"), [0.0, 0.0, 0.0])
+    o = OracleSystem(3)
+    drive(o, parts2, (16.0, 16.0, 20.0), periodic=False, constraint=("walls", {"l": "12.0"}))
+    np.testing.assert_array_equal(o.download("x"), [-8.0, 1.0, 8.0])  # l = xhi = 8
