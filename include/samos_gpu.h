@@ -38,7 +38,7 @@ enum { SG_ALIGN_POLAR = 0, SG_ALIGN_NEMATIC = 1, SG_ALIGN_VICSEK = 2 };
 enum { SG_EXT_SELF_PROPULSION = 0 };
 enum { SG_CONS_NONE = 0, SG_CONS_PLANE = 1, SG_CONS_SPHERE = 2, SG_CONS_CYLINDER = 3, SG_CONS_TORUS = 4,
        SG_CONS_ELLIPSOID = 5, SG_CONS_PEANUT = 6, SG_CONS_GYROID = 7, SG_CONS_HOURGLASS = 8,
-       SG_CONS_GAUSSIAN_BUMP = 9, SG_CONS_SLAB = 10, SG_CONS_PLANE_WALLS = 11 };
+       SG_CONS_GAUSSIAN_BUMP = 9, SG_CONS_SLAB = 10, SG_CONS_PLANE_WALLS = 11, SG_CONS_TETRAHEDRON = 12 };
 enum { SG_INT_BROWNIAN = 0, SG_INT_BROWNIAN_POS = 1, SG_INT_BROWNIAN_ALIGN = 2,
        SG_INT_LANGEVIN = 3, SG_INT_FIRE = 4, SG_INT_NVE = 5, SG_INT_VICSEK = 6 };
 enum { SG_VALUE_CONSTANT = 0, SG_VALUE_LINEAR = 1 };
@@ -126,10 +126,12 @@ int  sg_add_external(sg_system* s, int kind, double alpha, const double* type_al
                      int has_params);
 /* Constraint (register_constraints.cpp:35-61): params =
  * {plane: zpos | sphere: r | cylinder: r | torus: c | ellipsoid: a |
- *  peanut: a | hourglass: R | gaussian_bump: A | slab: z_lo | walls: l,
+ *  peanut: a | hourglass: R | gaussian_bump: A | slab: z_lo | walls: l |
+ *  tetrahedron: scale,
  *  plane: unlimited, maxiter, tol, rescale, rescale_steps, rescale_freq,
  *  torus: a | ellipsoid: b | peanut: b | hourglass: A | gaussian_bump: a |
- *  slab: z_hi, ellipsoid: c | hourglass: n | gaussian_bump: b} (9 values;
+ *  slab: z_hi | tetrahedron: value, ellipsoid: c | hourglass: n |
+ *  gaussian_bump: b} (9 values;
  * gyroid takes none, its period is the box; a walls l beyond the box
  * is moved to its edge, constraint_plane_walls.hpp:64-71).  The implicit surfaces (torus and after)
  * project with Constraint::enforce's SHAKE iteration, constraint.cpp:40-87.

@@ -893,7 +893,9 @@ int or_add_constraint(or_system* s, int kind, const double* p)
   memset(c, 0, sizeof(*c));
   c->kind = kind;
   c->zpos = p ? p[0] : 0.0; c->unlimited = p ? (int)p[1] : 0;
-  c->r = p ? p[0] : (kind == OR_CONS_PEANUT || kind == OR_CONS_HOURGLASS ? 10.0 : kind == OR_CONS_SLAB ? 0.0 : 1.0);
+  c->r = p ? p[0]
+           : (kind == OR_CONS_PEANUT || kind == OR_CONS_HOURGLASS || kind == OR_CONS_TETRAHEDRON ? 10.0
+              : kind == OR_CONS_SLAB ? 0.0 : 1.0);
   if (kind == OR_CONS_PLANE_WALLS && c->r > s->xhi) c->r = s->xhi;  /* constraint_plane_walls.hpp:64-71 */
   if (kind >= OR_CONS_TORUS) {  /* params[7], params[8] */
     c->b2 = p ? p[7] : (kind == OR_CONS_TORUS ? 0.5 : kind == OR_CONS_PEANUT ? 8.0 : 1.0);
@@ -975,6 +977,12 @@ static void cylinder_enforce(or_system* s, const or_cons* c, int i)
   }
 }
 
+/* ConstraintTetrahedron's unit charges (constraint_tetrahedron.hpp:42-45),
+   scaled by the constraint's scale; the surface is an equipotential of
+   sum 1/|r - a_i| (constraint_tetrahedron.cpp:47-80) */
+static const double TETRA[4][3] = {{1.0, 0.0, -0.7071067811865475}, {-1.0, 0.0, -0.7071067811865475},
+                                   {0.0, 1.0, 0.7071067811865475}, {0.0, -1.0, 0.7071067811865475}};
+
 /* compute_gradient / constraint_value of the implicit surfaces, in the
    reference's operation order: ConstraintTorus (constraint_torus.cpp:
    (c - sqrt(x^2+y^2))^2 + z^2 - a^2), ConstraintEllipsoid
@@ -1006,6 +1014,15 @@ static void implicit_gradient(const or_system* s, const or_cons* c, double x, do
                          sin((2.0 * M_PI * y) / ly) * sin((2.0 * M_PI * z) / lz))) / ly;
     *gz = (2.0 * M_PI * (cos((2.0 * M_PI * y) / ly) * cos((2.0 * M_PI * z) / lz) -
                          sin((2.0 * M_PI * x) / lx) * sin((2.0 * M_PI * z) / lz))) / lz;
+  } else if (c->kind == OR_CONS_TETRAHEDRON) {
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int k = 0; k < 4; k++) {
+      double px = x - c->r * TETRA[k][0], py = y - c->r * TETRA[k][1], pz = z - c->r * TETRA[k][2];
+      double l = sqrt(px * px + py * py + pz * pz);
+      double l3 = l * l * l;
+      sx += px / l3; sy += py / l3; sz += pz / l3;
+    }
+    *gx = -sx; *gy = -sy; *gz = -sz;
   } else if (c->kind == OR_CONS_HOURGLASS) {
     double lz = s->Lz, A = c->b2, n = c->b3;
     *gx = 2.0 * x;
@@ -1035,6 +1052,14 @@ static double implicit_value(const or_system* s, const or_cons* c, double x, dou
     double lx = s->Lx, ly = s->Ly, lz = s->Lz;
     return cos((2.0 * M_PI * z) / lz) * sin((2.0 * M_PI * x) / lx) + cos((2.0 * M_PI * x) / lx) * sin((2.0 * M_PI * y) / ly) +
            cos((2.0 * M_PI * y) / ly) * sin((2.0 * M_PI * z) / lz);
+  }
+  if (c->kind == OR_CONS_TETRAHEDRON) {
+    double g = 0.0;
+    for (int k = 0; k < 4; k++) {
+      double px = x - c->r * TETRA[k][0], py = y - c->r * TETRA[k][1], pz = z - c->r * TETRA[k][2];
+      g += 1.0 / sqrt(px * px + py * py + pz * pz);
+    }
+    return g - c->b2;
   }
   if (c->kind == OR_CONS_HOURGLASS) {
     double zfact = c->r + c->b2 * sin(2.0 * M_PI / s->Lz * c->b3 * z);
@@ -1122,7 +1147,8 @@ static void enforce_one(or_system* s, int i)
     if (c->kind == OR_CONS_PLANE) plane_enforce(s, c, i);
     else if (c->kind == OR_CONS_SPHERE) sphere_enforce(s, c, i);
     else if (c->kind == OR_CONS_CYLINDER) cylinder_enforce(s, c, i);
-    else if (c->kind >= OR_CONS_TORUS && c->kind <= OR_CONS_GAUSSIAN_BUMP) implicit_enforce(s, c, i);
+    else if ((c->kind >= OR_CONS_TORUS && c->kind <= OR_CONS_GAUSSIAN_BUMP) || c->kind == OR_CONS_TETRAHEDRON)
+      implicit_enforce(s, c, i);
     else if (c->kind == OR_CONS_SLAB) slab_enforce(s, c, i);
     else if (c->kind == OR_CONS_PLANE_WALLS) plane_walls_enforce(s, c, i);
     else if (s->periodic) enforce_periodic(s, i);

@@ -36,7 +36,7 @@ enum { OR_ALIGN_POLAR = 0, OR_ALIGN_NEMATIC = 1, OR_ALIGN_VICSEK = 2 };
 enum { OR_EXT_SELF_PROPULSION = 0 };
 enum { OR_CONS_NONE = 0, OR_CONS_PLANE = 1, OR_CONS_SPHERE = 2, OR_CONS_CYLINDER = 3, OR_CONS_TORUS = 4,
        OR_CONS_ELLIPSOID = 5, OR_CONS_PEANUT = 6, OR_CONS_GYROID = 7, OR_CONS_HOURGLASS = 8,
-       OR_CONS_GAUSSIAN_BUMP = 9, OR_CONS_SLAB = 10, OR_CONS_PLANE_WALLS = 11 };
+       OR_CONS_GAUSSIAN_BUMP = 9, OR_CONS_SLAB = 10, OR_CONS_PLANE_WALLS = 11, OR_CONS_TETRAHEDRON = 12 };
 enum { OR_INT_BROWNIAN = 0, OR_INT_BROWNIAN_POS = 1, OR_INT_BROWNIAN_ALIGN = 2,
        OR_INT_LANGEVIN = 3, OR_INT_FIRE = 4, OR_INT_NVE = 5, OR_INT_VICSEK = 6 };
 enum { OR_VALUE_CONSTANT = 0, OR_VALUE_LINEAR = 1 };
@@ -86,7 +86,8 @@ int    or_add_external(or_system* s, int kind, double alpha,
    in [7]}, ellipsoid {a, -, .., b in [7], c in [8]}, peanut {a, .., b in [7]},
    gyroid {} (the box is its period), hourglass {R, .., A in [7], n in [8]},
    gaussian_bump {A, .., a in [7], b in [8]}, slab {z_lo, .., z_hi in [7]},
-   plane_walls {l, moved to the box edge if beyond it}; base {maxiter, tol, rescale,
+   plane_walls {l, moved to the box edge if beyond it}, tetrahedron {scale, ..,
+   value in [7]}; base {maxiter, tol, rescale,
    rescale_steps, rescale_freq} in params[2..6].  Returns -1 for parameters
    the reference constructor rejects (peanut b <= a). */
 int    or_add_constraint(or_system* s, int kind, const double* params);

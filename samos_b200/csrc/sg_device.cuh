@@ -27,11 +27,22 @@ enum { PAIR_SOFT = 0, PAIR_LJ = 1, PAIR_MORSE = 2, PAIR_GAUSSIAN = 3 };
 enum { ALIGN_POLAR = 0, ALIGN_NEMATIC = 1, ALIGN_VICSEK = 2 };
 enum { CONS_NONE = 0, CONS_PLANE = 1, CONS_SPHERE = 2, CONS_CYLINDER = 3, CONS_TORUS = 4, CONS_ELLIPSOID = 5,
        CONS_PEANUT = 6, CONS_GYROID = 7, CONS_HOURGLASS = 8, CONS_GAUSSIAN_BUMP = 9, CONS_SLAB = 10,
-       CONS_PLANE_WALLS = 11 };
+       CONS_PLANE_WALLS = 11, CONS_TETRAHEDRON = 12 };
 // surfaces given by an implicit function g = 0 and projected by the base
 // class's SHAKE iteration (no enforce of their own in the reference)
 __host__ __device__ __forceinline__ bool cons_implicit(int kind) {
-  return kind >= CONS_TORUS && kind <= CONS_GAUSSIAN_BUMP;
+  return (kind >= CONS_TORUS && kind <= CONS_GAUSSIAN_BUMP) || kind == CONS_TETRAHEDRON;
+}
+
+// ConstraintTetrahedron's four unit charges (constraint_tetrahedron.hpp:42-45),
+// scaled by the constraint's scale; the surface is an equipotential of
+// sum 1/|r - a_i| (constraint_tetrahedron.cpp:47-80)
+__host__ __device__ __forceinline__ void tetra_charge(int i, double s, double& ax, double& ay, double& az) {
+  const double h = 0.7071067811865475;
+  const double cx = i == 0 ? 1.0 : i == 1 ? -1.0 : 0.0;
+  const double cy = i == 2 ? 1.0 : i == 3 ? -1.0 : 0.0;
+  const double cz = i < 2 ? -h : h;
+  ax = s * cx; ay = s * cy; az = s * cz;
 }
 enum { INT_BROWNIAN = 0, INT_BROWNIAN_POS = 1, INT_BROWNIAN_ALIGN = 2, INT_LANGEVIN = 3, INT_FIRE = 4, INT_NVE = 5, INT_VICSEK = 6 };
 enum { LANGEVIN_BAOAB = 0, LANGEVIN_SPV = 1, LANGEVIN_BBK = 2 };
@@ -355,6 +366,17 @@ __host__ __device__ __forceinline__ void implicit_gradient(const ConsComp& C, co
                         sin((2.0 * M_PI * y) / ly) * sin((2.0 * M_PI * z) / lz))) / ly;
     gz = (2.0 * M_PI * (cos((2.0 * M_PI * y) / ly) * cos((2.0 * M_PI * z) / lz) -
                         sin((2.0 * M_PI * x) / lx) * sin((2.0 * M_PI * z) / lz))) / lz;
+  } else if (C.kind == CONS_TETRAHEDRON) {
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int i = 0; i < 4; i++) {
+      double ax, ay, az;
+      tetra_charge(i, a0, ax, ay, az);
+      const double px = x - ax, py = y - ay, pz = z - az;
+      const double l = sqrt(px * px + py * py + pz * pz);
+      const double l3 = l * l * l;
+      sx += px / l3; sy += py / l3; sz += pz / l3;
+    }
+    gx = -sx; gy = -sy; gz = -sz;
   } else if (C.kind == CONS_HOURGLASS) {
     const double lz = R.Lz, A = C.b2, n = C.b3;
     gx = 2.0 * x;
@@ -383,6 +405,16 @@ __host__ __device__ __forceinline__ double implicit_value(const ConsComp& C, con
     const double lx = R.Lx, ly = R.Ly, lz = R.Lz;
     return cos((2.0 * M_PI * z) / lz) * sin((2.0 * M_PI * x) / lx) + cos((2.0 * M_PI * x) / lx) * sin((2.0 * M_PI * y) / ly) +
            cos((2.0 * M_PI * y) / ly) * sin((2.0 * M_PI * z) / lz);
+  }
+  if (C.kind == CONS_TETRAHEDRON) {
+    double g = 0.0;
+    for (int i = 0; i < 4; i++) {
+      double ax, ay, az;
+      tetra_charge(i, a0, ax, ay, az);
+      const double px = x - ax, py = y - ay, pz = z - az;
+      g += 1.0 / sqrt(px * px + py * py + pz * pz);
+    }
+    return g - C.b2;
   }
   if (C.kind == CONS_HOURGLASS) {
     double zfact = a0 + C.b2 * sin(2.0 * M_PI / R.Lz * C.b3 * z);

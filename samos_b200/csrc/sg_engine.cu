@@ -838,13 +838,14 @@ static void set_cons(ConsComp& C, int kind, const double* params) {
   else if (kind == CONS_HOURGLASS) { d2 = 1.0; d3 = 1.0; }
   else if (kind == CONS_GAUSSIAN_BUMP) { d2 = 1.0; d3 = 1.0; }
   else if (kind == CONS_SLAB) d2 = 1.0;  // z_hi (constraint_slab.hpp:68-78)
+  else if (kind == CONS_TETRAHEDRON) d2 = 1.0;  // value (constraint_tetrahedron.hpp:78-88)
   C.b2 = params ? params[7] : d2;
   C.b3 = params ? params[8] : d3;
 }
 
 static double cons_first_default(int kind) {
   return kind == CONS_PLANE || kind == CONS_NONE || kind == CONS_GYROID || kind == CONS_SLAB ? 0.0
-       : kind == CONS_PEANUT || kind == CONS_HOURGLASS ? 10.0 : 1.0;
+       : kind == CONS_PEANUT || kind == CONS_HOURGLASS || kind == CONS_TETRAHEDRON ? 10.0 : 1.0;
 }
 
 // a wall position beyond the box is moved to its edge
@@ -863,7 +864,7 @@ static int check_cons(sg_system* s, const ConsComp& C, double first) {
 }
 
 int sg_add_constraint_per_replica(sg_system* s, int kind, const double* params, const double* value0) {
-  if (!s || !value0 || kind < SG_CONS_NONE || kind > SG_CONS_PLANE_WALLS) return fail(s, SG_ERR_ARG, "bad constraint");
+  if (!s || !value0 || kind < SG_CONS_NONE || kind > SG_CONS_TETRAHEDRON) return fail(s, SG_ERR_ARG, "bad constraint");
   Program& P = s->prog;
   if (P.ncons >= MAX_CONS) return fail(s, SG_ERR_ARG, "too many constraints");
   if (params && params[4] != 0.0 && params[4] != 1.0)
@@ -881,7 +882,7 @@ int sg_add_constraint_per_replica(sg_system* s, int kind, const double* params, 
 }
 
 int sg_add_constraint(sg_system* s, int kind, const double* params) {
-  if (!s || kind < SG_CONS_NONE || kind > SG_CONS_PLANE_WALLS) return fail(s, SG_ERR_ARG, "sg_add_constraint: bad kind");
+  if (!s || kind < SG_CONS_NONE || kind > SG_CONS_TETRAHEDRON) return fail(s, SG_ERR_ARG, "sg_add_constraint: bad kind");
   Program& P = s->prog;
   if (P.ncons >= MAX_CONS) return fail(s, SG_ERR_ARG, "too many constraints");
   if (params && params[4] != 0.0 && params[4] != 1.0)

@@ -21,7 +21,8 @@ PAIR = {"soft": 0, "lj": 1, "morse": 2, "gaussian": 3}
 ALIGN = {"polar": 0, "nematic": 1, "vicsek": 2}
 EXTERNAL = {"self_propulsion": 0}
 CONSTRAINT = {"none": 0, "plane": 1, "sphere": 2, "cylinder": 3, "torus": 4, "ellipsoid": 5, "peanut": 6,
-              "gyroid": 7, "hourglass": 8, "gaussian_bump": 9, "slab": 10, "walls": 11}
+              "gyroid": 7, "hourglass": 8, "gaussian_bump": 9, "slab": 10, "walls": 11,
+              "tetrahedron": 12}
 INTEGRATOR = {"brownian": 0, "brownian_pos": 1, "brownian_align": 2, "langevin": 3, "fire": 4, "nve": 5, "vicsek": 6}
 PAIR_NPARAM = 8
 INT_NPARAM = 16

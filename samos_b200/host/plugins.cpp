@@ -191,6 +191,7 @@ ConstraintSpec resolve_constraint(const std::string& name, const Params& p) {
   else if (name == "gaussian_bump") s.kind = SG_CONS_GAUSSIAN_BUMP;
   else if (name == "slab") s.kind = SG_CONS_SLAB;
   else if (name == "walls") s.kind = SG_CONS_PLANE_WALLS;
+  else if (name == "tetrahedron") s.kind = SG_CONS_TETRAHEDRON;
   else throw HostError("Constraint " + name + " is not part of the GPU path.");
   if (has(p, "group") && p.at("group") != "all") throw HostError("Constraint groups other than 'all' are not part of the GPU path.");
   // Constraint base (constraint.hpp:56-120); tol is parsed as an int there (82)
@@ -214,6 +215,8 @@ ConstraintSpec resolve_constraint(const std::string& name, const Params& p) {
     first = get(p, "z_lo", 0.0); second = get(p, "z_hi", 1.0);
   } else if (name == "walls") {  // constraint_plane_walls.hpp:56-74 (the engine moves l to the box edge)
     first = get(p, "l", 1.0);
+  } else if (name == "tetrahedron") {  // constraint_tetrahedron.hpp:62-88
+    first = get(p, "scale", 10.0); second = get(p, "value", 1.0);
   }
   const double v[9] = {first, unlimited, maxiter, tol, get(p, "rescale", 1.0), get(p, "rescale_steps", 1000.0),
                        get(p, "rescale_freq", 10.0), second, third};

@@ -234,6 +234,8 @@ def resolve_constraint(name: str, params: dict) -> tuple[int, list[float]]:
         first, second, unlimited = _f(params, "z_lo", 0.0), _f(params, "z_hi", 1.0), 0.0
     elif name == "walls":  # constraint_plane_walls.hpp:56-74: l (1; beyond the box: the box edge)
         first, unlimited = _f(params, "l", 1.0), 0.0
+    elif name == "tetrahedron":  # constraint_tetrahedron.hpp:62-88: scale (10), value (1)
+        first, second, unlimited = _f(params, "scale", 10.0), _f(params, "value", 1.0), 0.0
     else:
         first, unlimited = 0.0, 0.0
     return E.CONSTRAINT[name], [first, unlimited, maxiter, tol, rescale, rescale_steps, rescale_freq, second, third]

@@ -85,6 +85,23 @@ def gyroid_gradient(x, y, z, box):
                      2 * np.pi * (np.cos(Y) * np.cos(Z) - np.sin(X) * np.sin(Z)) / lz], -1)
 
 
+TETRA = np.array([[1.0, 0.0, -0.7071067811865475], [-1.0, 0.0, -0.7071067811865475],
+                  [0.0, 1.0, 0.7071067811865475], [0.0, -1.0, 0.7071067811865475]])
+
+
+def tetra_value(p, scale, value):
+    """sum over the four scaled charges of 1/|r - a_i|, minus the level."""
+    return sum(1.0 / np.linalg.norm(p - scale * a, axis=-1) for a in TETRA) - value
+
+
+def tetra_gradient(p, scale):
+    g = 0.0
+    for a in TETRA:
+        d = p - scale * a
+        g = g + d / np.linalg.norm(d, axis=-1)[..., None] ** 3
+    return -g
+
+
 def surface_disks(kind, n, seed=1, **shape):
     """n particles scattered near a cylinder (r), torus (c, a), ellipsoid
     (a, b, c), peanut (a, b), hourglass (R, A, n_nodes, Lz), Gaussian bump
@@ -108,6 +125,16 @@ def surface_disks(kind, n, seed=1, **shape):
         A, a, b, L = shape["A"], shape["a"], shape["b"], shape["L"]
         x, y = rng.uniform(-0.45 * L, 0.45 * L, n), rng.uniform(-0.45 * L, 0.45 * L, n)
         z = A * np.exp(-x * x / a - y * y / b)
+    elif kind == "tetrahedron":  # rays from the origin, bisected to the level (inside it above, outside below)
+        s, val = shape["scale"], shape["value"]
+        w = rng.normal(size=(n, 3))
+        w /= np.linalg.norm(w, axis=1)[:, None]
+        lo, hi = np.zeros(n), np.full(n, 20.0 * s)
+        for _ in range(80):
+            mid = 0.5 * (lo + hi)
+            inside = tetra_value(mid[:, None] * w, s, val) > 0.0
+            lo, hi = np.where(inside, mid, lo), np.where(inside, hi, mid)
+        x, y, z = (hi[:, None] * w).T
     elif kind == "gyroid":  # random points pulled onto the surface by Newton steps along the gradient
         box = shape["box"]
         p = np.stack([rng.uniform(-h / 2, h / 2, n) for h in box], -1)
@@ -116,7 +143,7 @@ def surface_disks(kind, n, seed=1, **shape):
             G = gyroid_gradient(p[:, 0], p[:, 1], p[:, 2], box)
             p -= (g / np.maximum(np.sum(G * G, -1), 1e-12))[:, None] * G
         x, y, z = p[:, 0], p[:, 1], p[:, 2]
-    if kind in ("peanut", "hourglass", "gaussian_bump", "gyroid"):
+    if kind in ("peanut", "hourglass", "gaussian_bump", "gyroid", "tetrahedron"):
         jitter = rng.normal(0.0, 0.02, (3, n))
         d = rng.normal(size=(3, n))
         d /= np.linalg.norm(d, axis=0)

@@ -393,10 +393,11 @@ def test_trajectory_curved_constraints(kind, shape, box, n):
     ("gaussian_bump", {"A": 4.0, "a": 30.0, "b": 20.0, "L": 40.0}, {"A": "4.0", "a": "30.0", "b": "20.0"},
      (40.0, 40.0, 20.0), False, 400),
     ("gyroid", {"box": (30.0, 30.0, 30.0)}, {}, (30.0, 30.0, 30.0), True, 800),
+    ("tetrahedron", {"scale": 10.0, "value": 0.3}, {"scale": "10.0", "value": "0.3"}, (80.0, 80.0, 80.0), False, 600),
 ])
 def test_trajectory_implicit_surfaces(kind, shape, conf, box, periodic, n):
     # active Brownian particles on a peanut / hourglass / Gaussian bump /
-    # gyroid (SHAKE projection of the implicit surface, the generic fused
+    # gyroid / tetrahedral equipotential (SHAKE projection of the implicit surface, the generic fused
     # kernel), 300 steps against the oracle with the shared noise stream
     parts = surface_disks(kind, n, seed=18, **shape)
     e, o = run_both(n, parts, box, 299, periodic=periodic, nlist=(2.4, 0.3), constraint=(kind, conf),

@@ -133,6 +133,9 @@ def test_command_order_rules(tmp_path):
     ("constraint gyroid { }", 7),
     ("constraint hourglass { R = 10; A = 2; n = 2 }", 8),
     ("constraint gaussian_bump { A = 2; a = 3; b = 4 }", 9),
+    ("constraint slab { z_lo = -1; z_hi = 1 }", 10),
+    ("constraint walls { l = 15 }", 11),
+    ("constraint tetrahedron { scale = 10; value = 0.3 }", 12),
 ])
 def test_implicit_surface_constraints_parse(tmp_path, line, kind):
     r = check(tmp_path, CONF.replace("constraint plane { }", line))

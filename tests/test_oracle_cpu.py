@@ -9,7 +9,8 @@ import pytest
 
 from oracle.oracle import OracleSystem, noise_gauss, noise_log, noise_uniform
 from samos_b200 import engine as E
-from scenarios import drive, gyroid_gradient, gyroid_value, plane_disks, sphere_disks, surface_disks
+from scenarios import (drive, gyroid_gradient, gyroid_value, plane_disks, sphere_disks, surface_disks, tetra_gradient,
+                       tetra_value)
 
 
 def two(x2, y2=0.0, r=(1.0, 1.0), box=20.0, n1=(1.0, 0.0, 0.0), n2=(0.0, 1.0, 0.0)):
@@ -255,6 +256,7 @@ IMPLICIT_CASES = [
     ("gaussian_bump", {"A": 4.0, "a": 30.0, "b": 20.0, "L": 40.0}, {"A": 4.0, "a": 30.0, "b": 20.0},
      (40.0, 40.0, 20.0), False),
     ("gyroid", {"box": (30.0, 30.0, 30.0)}, {}, (30.0, 30.0, 30.0), True),
+    ("tetrahedron", {"scale": 10.0, "value": 0.3}, {"scale": 10.0, "value": 0.3}, (80.0, 80.0, 80.0), False),
 ]
 
 
@@ -276,6 +278,10 @@ def implicit_np(kind, conf, box, x, y, z):
         f = np.exp(-x * x / a - y * y / b)
         g = A * f - z
         G = np.stack([-2 * A * x * f / a, -2 * A * y * f / b, -np.ones_like(z)], 1)
+    elif kind == "tetrahedron":
+        p = np.stack([x, y, z], 1)
+        g = tetra_value(p, conf["scale"], conf["value"])
+        G = tetra_gradient(p, conf["scale"])
     else:
         g = gyroid_value(x, y, z, box)
         G = gyroid_gradient(x, y, z, box)
