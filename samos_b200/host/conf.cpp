@@ -81,10 +81,11 @@ void split_command(const std::string& line, std::string& cmd, std::string& rest)
   rest = trim(t.substr(i));
 }
 
-bool split_type_params(const std::string& rest, std::string& type, std::string& params) {
+bool split_type_params(const std::string& rest, std::string& type, std::string& params, bool file_name) {
   const std::string t = trim(rest);
   size_t i = 0;
-  while (i < t.size() && (std::isalnum((unsigned char)t[i]) || t[i] == '_')) i++;
+  // log / dump names are file names: letters, digits, '_' and '.' (parse_log_dump.hpp:63)
+  while (i < t.size() && (std::isalnum((unsigned char)t[i]) || t[i] == '_' || (file_name && t[i] == '.'))) i++;
   type = t.substr(0, i);
   params = trim(t.substr(i));
   if (params.empty()) params = "{}";

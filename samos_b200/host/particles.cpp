@@ -124,6 +124,7 @@ Particles read_particles(const std::string& path) {
     P.ix.push_back(has_keys ? (int)dbl("ix", -1, 0.0) : 0);
     P.iy.push_back(has_keys ? (int)dbl("iy", -1, 0.0) : 0);
     P.iz.push_back(has_keys ? (int)dbl("iz", -1, 0.0) : 0);
+    P.molecule.push_back(has_keys ? (int)dbl("molecule", -1, 0.0) : 0);
   }
   if (P.x.empty()) throw HostError("No particles read from " + path);
   P.ntypes = (int)types.size();
@@ -133,15 +134,5 @@ Particles read_particles(const std::string& path) {
   return P;
 }
 
-void write_input_dump(const std::string& path, const Particles& p) {
-  FILE* f = std::fopen(path.c_str(), "w");
-  if (!f) throw HostError("Cannot open dump file " + path);
-  std::fprintf(f, "keys: id type radius x y z vx vy vz nx ny nz omega ix iy iz\n");
-  for (size_t i = 0; i < p.size(); i++)
-    std::fprintf(f, "%d %d %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %d %d %d\n", p.id[i],
-                 p.type[i], p.radius[i], p.x[i], p.y[i], p.z[i], p.vx[i], p.vy[i], p.vz[i], p.nx[i], p.ny[i], p.nz[i],
-                 p.omega[i], p.ix[i], p.iy[i], p.iz[i]);
-  std::fclose(f);
-}
 
 }  // namespace samos_host

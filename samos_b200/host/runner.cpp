@@ -10,18 +10,19 @@
 // map order; integrators are inserted at their map position when created
 // and removed by `disable`, so their noise streams persist across runs as the
 // reference's RNG objects do.
+#include <cctype>
 #include <climits>
 #include <cmath>
 #include <cstdio>
+#include <ctime>
 #include <fstream>
 #include <iostream>
+#include <set>
 #include <sstream>
 
 #include "samos_host.hpp"
 
 namespace samos_host {
-
-namespace {
 
 int64_t to_i64(const std::string& s, const char* what) {
   char* end = nullptr;
@@ -35,8 +36,6 @@ double to_dbl(const std::string& s, const char* what) {
   if (s.empty() || *end != '\0') throw HostError(std::string("Could not parse ") + what + " command.");
   return v;
 }
-
-}  // namespace
 
 Samos::~Samos() {
   if (h_) sg_destroy(h_);
@@ -101,6 +100,9 @@ void Samos::execute_line(const std::string& raw, int line_no) {
 
   if (cmd == "messages") {
     return;  // host messages go to stderr here
+  } else if (cmd == "config") {  // the JSON record of parameters (samos.cpp, Messenger): not written here
+    if (!opt_.quiet) std::fprintf(stderr, "config: the parameter record is not written by the GPU host.\n");
+    return;
   } else if (cmd == "box") {  // samos.cpp:186-230
     typed("box");
     if (type == "periodic") periodic_ = true;
@@ -281,45 +283,49 @@ void Samos::cmd_run(int64_t steps) {
 
 void Samos::cmd_dump(const std::string& rest) {
   std::string name, ptext;
-  if (!split_type_params(rest, name, ptext)) throw HostError("Error parsing dump command.");
+  if (!split_type_params(rest, name, ptext, true)) throw HostError("Error parsing dump command.");
   Params p;
   if (!parse_params(ptext, p)) throw HostError("Error parsing dump parameters.");
-  Dump d;
-  d.name = name;
-  d.type = p.count("type") ? p["type"] : "input";
-  if (d.type != "input" && d.type != "full") throw HostError("Dump type " + d.type + " is not part of the GPU path.");
-  d.start = p.count("start") ? to_i64(p["start"], "dump") : 0;
-  d.freq = p.count("freq") ? to_i64(p["freq"], "dump") : 1;
-  d.multi = p.count("multi") != 0;
-  if (d.freq <= 0) throw HostError("Dump frequency has to be positive.");
-  dumps_.push_back(d);
+  dumps_.push_back(make_dump(name, p, (int32_t)parts_.size()));
 }
 
+// Logger ctor (logger.cpp:40-124): `step` always first, then every
+// parameter key other than freq (std::map order) naming a quantity; freq
+// defaults to 100; the header names the file, the time and the columns.
 void Samos::cmd_log(const std::string& rest) {
   std::string name, ptext;
-  if (!split_type_params(rest, name, ptext)) throw HostError("Error parsing log command.");
+  if (!split_type_params(rest, name, ptext, true)) throw HostError("Error parsing log command.");
   Params p;
   if (!parse_params(ptext, p)) throw HostError("Error parsing log parameters.");
   Log l;
   l.name = name;
-  l.freq = p.count("freq") ? to_i64(p["freq"], "log") : 1;
+  l.freq = p.count("freq") ? to_i64(p["freq"], "log") : 100;
   if (l.freq <= 0) throw HostError("Log frequency has to be positive.");
-  std::string what = p.count("what") ? p["what"] : "";
-  // logger columns the engine reduces (logger.cpp:49-77); '+'-separated here
-  std::stringstream ss(what);
-  std::string c;
-  while (std::getline(ss, c, '+'))
-    if (!c.empty()) {
-      if (c != "soft_energy" && c != "lj_energy" && c != "morse_energy" && c != "gaussian_energy" &&
-          c != "polar_align" && c != "nematic_align" && c != "velocity")
-        throw HostError("Log column " + c + " is not part of the GPU path.");
-      l.cols.push_back(c);
-    }
+  static const std::set<std::string> here = {"step", "velocity", "vec_velocity", "kinetic_energy", "size",
+                                             "soft_energy", "lj_energy", "morse_energy", "gaussian_energy",
+                                             "polar_align", "nematic_align"};
+  static const std::set<std::string> elsewhere = {
+      "soft_attractive_energy", "rod_energy", "ljrod_energy", "vp_energy", "line_tension_energy",
+      "boundary_bending_energy", "boundary_attraction_energy", "coulomb_energy", "bare_coulomb_energy",
+      "coulomb3_energy", "yukawa_energy", "harmonic_bond_energy", "harmonic_angle_energy", "cosine_angle_energy",
+      "external_gravity_energy", "external_harmonic_energy", "area", "avg_perim"};
+  l.cols.push_back("step");
+  for (const auto& kv : p) {
+    std::string q = kv.first;
+    for (auto& ch : q) ch = (char)std::tolower((unsigned char)ch);
+    if (q == "freq") continue;
+    if (here.count(q)) l.cols.push_back(q);
+    else if (elsewhere.count(q)) throw HostError("Log quantity " + q + " is not part of the GPU path.");
+    else throw HostError("Unknown log quantity : " + q + ".");
+  }
   logs_.push_back(l);
   std::FILE* f = std::fopen(l.name.c_str(), "w");
   if (!f) throw HostError("Cannot open log file " + l.name);
-  std::fprintf(f, "# step");
-  for (const auto& col : l.cols) std::fprintf(f, " %s", col.c_str());
+  char when[64];
+  std::time_t now = std::time(nullptr);
+  std::strftime(when, sizeof when, "%Y-%b-%d %H:%M:%S", std::localtime(&now));
+  std::fprintf(f, "# Log file : %s\n# Generated on : %s\n# ", l.name.c_str(), when);
+  for (size_t i = 0; i < l.cols.size(); i++) std::fprintf(f, "(%zu) %s ", i + 1, l.cols[i].c_str());
   std::fprintf(f, "\n");
   std::fclose(f);
 }
@@ -329,7 +335,9 @@ void Samos::report(int64_t step) {
   bool energies = false;
   for (const auto& l : logs_)
     if (step % l.freq == 0)
-      for (const auto& c : l.cols) energies = energies || c != "velocity";
+      for (const auto& c : l.cols)
+        energies = energies || c == "soft_energy" || c == "lj_energy" || c == "morse_energy" || c == "gaussian_energy" ||
+                   c == "polar_align" || c == "nematic_align";
   if (energies) check(sg_compute(h_, dt_), "sg_compute");
   auto down = [&](const char* f, void* p) { check(sg_download(h_, 0, f, p), "sg_download"); };
   down("x", parts_.x.data()); down("y", parts_.y.data()); down("z", parts_.z.data());
@@ -337,26 +345,50 @@ void Samos::report(int64_t step) {
   down("nx", parts_.nx.data()); down("ny", parts_.ny.data()); down("nz", parts_.nz.data());
   down("omega", parts_.omega.data());
   down("ix", parts_.ix.data()); down("iy", parts_.iy.data()); down("iz", parts_.iz.data());
+  DumpState ds;
+  ds.parts = &parts_;
+  ds.lx = lx_; ds.ly = ly_; ds.lz = lz_;
+  std::vector<double> F[3], N[3];
   for (const auto& d : dumps_) {
-    if (step < d.start || step % d.freq) continue;  // Dump::dump, dump.cpp:351-360
-    char num[32];
-    std::snprintf(num, sizeof num, "_%010lld", (long long)step);
-    write_input_dump(d.multi ? d.name + num + ".dat" : d.name + ".dat", parts_);
+    if (!dump_due(d, step)) continue;
+    if (d.type == "full" && d.p.count("force") && F[0].empty()) {
+      const char* names[3] = {"fx", "fy", "fz"};
+      for (int c = 0; c < 3; c++) { F[c].resize(parts_.size()); down(names[c], F[c].data()); }
+    }
+    if (d.type == "full" && d.p.count("normal") && N[0].empty()) {
+      const char* names[3] = {"Nx", "Ny", "Nz"};
+      for (int c = 0; c < 3; c++) { N[c].resize(parts_.size()); down(names[c], N[c].data()); }
+    }
+    ds.fx = &F[0]; ds.fy = &F[1]; ds.fz = &F[2];
+    ds.Nx = &N[0]; ds.Ny = &N[1]; ds.Nz = &N[2];
+    write_dump(d, step, ds);
   }
-  for (const auto& l : logs_) {
+  for (const auto& l : logs_) {  // Logger::log (logger.cpp:128-139): each column then a space
     if (step % l.freq) continue;
     std::FILE* f = std::fopen(l.name.c_str(), "a");
     if (!f) throw HostError("Cannot open log file " + l.name);
-    std::fprintf(f, "%lld", (long long)step);
+    const double N = (double)parts_.size();
     for (const auto& c : l.cols) {
+      if (c == "step") { std::fprintf(f, "%8lld  ", (long long)step); continue; }       // log_step.hpp:55
+      if (c == "size") { std::fprintf(f, "%6lld  ", (long long)parts_.size()); continue; }  // log_size.hpp:55
       double v = 0.0;
       if (c == "velocity") {  // log_velocity.hpp:56-65: mean speed
         for (size_t i = 0; i < parts_.size(); i++)
           v += std::sqrt(parts_.vx[i] * parts_.vx[i] + parts_.vy[i] * parts_.vy[i] + parts_.vz[i] * parts_.vz[i]);
-        v /= (double)parts_.size();
-      } else {
+        v /= N;
+      } else if (c == "vec_velocity") {  // log_vec_velocity.hpp:56-68: |sum v| / N
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (size_t i = 0; i < parts_.size(); i++) { sx += parts_.vx[i]; sy += parts_.vy[i]; sz += parts_.vz[i]; }
+        v = std::sqrt(sx * sx + sy * sy + sz * sz) / N;
+      } else if (c == "kinetic_energy") {  // log_kinetic_eng.hpp:56-66: sum v^2 / (2 m), / N
+        for (size_t i = 0; i < parts_.size(); i++) {
+          const double v2 = parts_.vx[i] * parts_.vx[i] + parts_.vy[i] * parts_.vy[i] + parts_.vz[i] * parts_.vz[i];
+          v += 0.5 * v2 / parts_.mass[i];
+        }
+        v /= N;
+      } else {  // the term's total energy from the last force evaluation (log_pair_eng.hpp, log_pair_align.hpp)
         const bool align = c == "polar_align" || c == "nematic_align";
-        const std::string want = align ? c.substr(0, c.find('_')) : c.substr(0, c.find('_'));
+        const std::string want = c.substr(0, c.find('_'));
         int comp = 0;
         bool found = false;
         if (align) {
@@ -364,11 +396,11 @@ void Samos::report(int64_t step) {
         } else {
           for (const auto& kv : pairs_) { if (kv.first == want) { found = true; break; } comp++; }
         }
-        if (!found) throw HostError("Log column " + c + " names a term that is not defined.");
+        if (!found)
+          throw HostError(std::string(align ? "Pair alignment" : "Pair potential") + " of type " + want + " not defined.");
         check(sg_energy(h_, 0, align ? 1 : 0, comp, &v), "sg_energy");
-        v /= (double)parts_.size();  // per particle, as the reference's loggers report
       }
-      std::fprintf(f, " %.12g", v);
+      std::fprintf(f, "%12.6e  ", v);
     }
     std::fprintf(f, "\n");
     std::fclose(f);

@@ -30,11 +30,12 @@ bool parse_params(const std::string& text, Params& out);
 // "cmd rest" -> (cmd, rest)
 void split_command(const std::string& line, std::string& cmd, std::string& rest);
 // "name { ... }" -> (name, "{ ... }"); the brace part may be absent ("{}").
-bool split_type_params(const std::string& rest, std::string& type, std::string& params);
+bool split_type_params(const std::string& rest, std::string& type, std::string& params,
+                       bool file_name = false);
 
 // ---- particles (particles.cpp) -------------------------------------------------------
 struct Particles {
-  std::vector<int32_t> id, type, ix, iy, iz;
+  std::vector<int32_t> id, type, ix, iy, iz, molecule;
   std::vector<double> radius, x, y, z, vx, vy, vz, nx, ny, nz, omega, mass;
   int ntypes = 0;  // distinct types (System::System, system.cpp:445)
   size_t size() const { return x.size(); }
@@ -42,8 +43,30 @@ struct Particles {
 // System::System input reader (src/system/system.cpp:76-450): `keys:` header,
 // the deprecated `# id type radius ...` header, or the old positional format.
 Particles read_particles(const std::string& path);
-// `dump <name> {type=input}`: a `keys:` file the reader above reads back.
-void write_input_dump(const std::string& path, const Particles& p);
+// numbers of a command's parameters; a malformed one stops with "Could not parse <what> command."
+int64_t to_i64(const std::string& s, const char* what);
+double to_dbl(const std::string& s, const char* what);
+
+// ---- dumps (dump.cpp) -----------------------------------------------------------------
+struct DumpSpec {
+  std::string name, type, ext, dir, path;  // path: the single file when not `multi`
+  int64_t start = 0, freq = 100, offset = 0;
+  bool multi = false, header = false, keys = false;
+  double scale = 1.0;
+  Params p;
+};
+// What a dump reads: the particles (refreshed from the device), the box, and
+// forces and surface normals when a dump asks for them.
+struct DumpState {
+  const Particles* parts = nullptr;
+  double lx = 0.0, ly = 0.0, lz = 0.0;
+  const std::vector<double> *fx = nullptr, *fy = nullptr, *fz = nullptr, *Nx = nullptr, *Ny = nullptr, *Nz = nullptr;
+};
+// Dump ctor (src/dump/dump.cpp:45-340): validates, opens the single file
+// (and writes the DCD header) as the reference does at construction.
+DumpSpec make_dump(const std::string& name, const Params& p, int32_t n_particles);
+bool dump_due(const DumpSpec& d, int64_t step);  // Dump::dump, dump.cpp:353-356
+void write_dump(const DumpSpec& d, int64_t step, const DumpState& s);
 
 // ---- plugins (plugins.cpp) -------------------------------------------------------------
 struct PairSpec {
@@ -130,8 +153,7 @@ class Samos {
   std::map<std::string, ExternalSpec> externals_;
   std::map<std::string, IntegratorSpec> integrators_;  // key type_group, as samos.cpp
   std::vector<std::string> committed_integ_;           // device order (map order)
-  struct Dump { std::string name, type; int64_t start = 0, freq = 1; bool multi = false; };
-  std::vector<Dump> dumps_;
+  std::vector<DumpSpec> dumps_;
   struct Log { std::string name; int64_t freq = 1; std::vector<std::string> cols; };
   std::vector<Log> logs_;
   int64_t steps_run_ = 0;  // the reference's time_step

@@ -38,7 +38,9 @@ def plane_parts(n=400, L=40.0, seed=3):
 
 
 def run_host(conf_path, *flags):
-    return subprocess.run([BIN, *flags, conf_path], capture_output=True, text=True, timeout=600)
+    # from the conf file's directory, where its dumps and logs land
+    return subprocess.run([BIN, *flags, conf_path], capture_output=True, text=True, timeout=600,
+                          cwd=os.path.dirname(os.path.abspath(conf_path)))
 
 
 def check(tmp_path, conf_text, parts=None, style="keys"):
@@ -153,6 +155,37 @@ def test_implicit_surface_parameter_errors(tmp_path, line, msg):
     assert r.returncode == 1 and msg in r.stderr, r.stderr
 
 
+@pytest.mark.parametrize("line,msg", [
+    ("dump a { start = 0 }", "No dump type specified."),
+    ("dump a { type = mol2 }", "Dump type mol2 is not part of the GPU path."),
+    ("dump a { type = foo }", "Unsupported dump type foo."),
+    ("dump a { type = dcd; multi }", "DCD files cannot be split."),
+    ("log a.log { area }", "Log quantity area is not part of the GPU path."),
+    ("log a.log { foo }", "Unknown log quantity : foo."),
+])
+def test_dump_and_log_errors_follow_the_reference(tmp_path, line, msg):
+    r = check(tmp_path, CONF.replace("run 10\n", line + "\nrun 10\n"))
+    assert r.returncode == 1 and msg in r.stderr, r.stderr
+
+
+def test_dump_files_and_log_header_at_construction(tmp_path):
+    # the reference opens a dump's single file (writing the DCD header) and a
+    # log's file (writing its header) when the command is read
+    extra = ("dump traj { type = dcd; freq = 5 }\ndump pos { type = xyz; freq = 5 }\n"
+             "dump frames { type = full; multi; coordinate }\nlog run.log { freq = 5; velocity; soft_energy }\n"
+             "config c { type = json }\n")
+    r = check(tmp_path, CONF.replace("run 10\n", extra + "run 10\n"))
+    assert r.returncode == 0, r.stderr
+    head = (tmp_path / "traj.dcd").read_bytes()
+    assert len(head) == 4 + 84 + 4 + 4 + 164 + 4 + 4 + 4 + 4 and head[4:8] == b"CORD"
+    assert np.frombuffer(head[-8:-4], np.int32)[0] == 400  # particles
+    assert (tmp_path / "pos.xyz").read_text() == ""
+    assert not list(tmp_path.glob("frames*"))  # multi: one file per dump, none yet
+    log = (tmp_path / "run.log").read_text().splitlines()
+    assert log[0] == "# Log file : run.log" and log[1].startswith("# Generated on : ")
+    assert log[2].split() == ["#", "(1)", "step", "(2)", "soft_energy", "(3)", "velocity"]
+
+
 def test_vicsek_and_nve_integrators_parse(tmp_path):
     conf = CONF.replace("integrator brownian_pos { seed = 7; mu = 1.0 }\nintegrator brownian_align { seed = 8; nu = 0.1, mur = 1.0 }\n",
                         "integrator vicsek { v0 = 0.5; eta = 0.3; seed = 2 }\n")
@@ -203,9 +236,21 @@ def python_run(parts, L, segments):
     return {f: e.download(f) for f in ("x", "y", "nx", "ny")}
 
 
-def read_dump(path):
-    rows = np.loadtxt(path, skiprows=1)
-    return {"x": rows[:, 3], "y": rows[:, 4], "nx": rows[:, 9], "ny": rows[:, 10]}
+def read_dump(path, n):
+    """Last frame of a `type=full; coordinate; director` dump (one file, frames
+    appended, as the reference writes it without `multi`)."""
+    rows = np.array([[float(v) for v in line.split()] for line in open(path)
+                     if line.strip() and not line.startswith(("#", "keys"))])
+    rows = rows[-n:]
+    return {"x": rows[:, 0], "y": rows[:, 1], "nx": rows[:, 3], "ny": rows[:, 4]}
+
+
+def assert_dump_matches(got, want):
+    # x, y printed with %16.10e, directors with %10.6f (dump.cpp:616-625)
+    for f in ("x", "y"):
+        np.testing.assert_allclose(got[f], want[f], rtol=0, atol=1e-8, err_msg=f)
+    for f in ("nx", "ny"):
+        np.testing.assert_allclose(got[f], want[f], rtol=0, atol=1e-6, err_msg=f)
 
 
 @pytest.mark.gpu
@@ -217,17 +262,16 @@ def test_host_run_matches_python_binding(tmp_path, dump_freq, last_dump):
     # there (sg_run, then sg_run_continue).
     parts, L = plane_parts(900, 50.0, seed=9)
     write_particles(tmp_path / "p.dat", parts)
-    dump = f"dump out {{ type=input; start=0; freq={dump_freq} }}\n"
+    dump = f"dump out {{ type=full; start=0; freq={dump_freq}; coordinate; director }}\n"
     conf = CONF.replace("lx = 40.0;  ly = 40.0", "lx = 50.0;  ly = 50.0").replace("run 10\n", dump + "run 480\n")
     (tmp_path / "c.conf").write_text(conf)
     r = subprocess.run([BIN, "--quiet", str(tmp_path / "c.conf")], capture_output=True, text=True, timeout=600,
                        cwd=tmp_path)
     assert r.returncode == 0, r.stderr
-    got = read_dump(tmp_path / "out.dat")
+    got = read_dump(tmp_path / "out.dat", len(parts["x"]))
     want = python_run(parts, L, ([("brownian_pos", {"seed": "7", "mu": "1.0"}),
                                   ("brownian_align", {"seed": "8", "nu": "0.1", "mur": "1.0"})], last_dump - 1))
-    for f in ("x", "y", "nx", "ny"):
-        np.testing.assert_array_equal(got[f], want[f], err_msg=f)
+    assert_dump_matches(got, want)
 
 
 @pytest.mark.gpu
@@ -244,12 +288,12 @@ def test_host_disable_and_new_integrator_between_runs(tmp_path):
             "external self_propulsion { alpha = 1.0 }\ntimestep 0.01\n"
             "integrator brownian_pos { seed = 1;  mu = 1.0; group = all }\n"
             "integrator brownian_align { seed = 1;  mur = 1.0; nu = 0.1; group = all }\n"
-            "dump out { type=input; start=0; freq=50 }\nrun 249\n")
+            "dump out { type=full; start=0; freq=50; coordinate; director }\nrun 249\n")
     (tmp_path / "c.conf").write_text(conf)
     r = subprocess.run([BIN, "--quiet", str(tmp_path / "c.conf")], capture_output=True, text=True, timeout=600,
                        cwd=tmp_path)
     assert r.returncode == 0, r.stderr
-    got = read_dump(tmp_path / "out.dat")  # written at global step 400 (top of the run's iteration 200)
+    got = read_dump(tmp_path / "out.dat", len(parts["x"]))  # last frame: global step 400 (top of iteration 200)
 
     e = Engine(len(parts["x"]))
     e.set_box(45.0, 45.0, 10.0, True)
@@ -279,5 +323,91 @@ def test_host_disable_and_new_integrator_between_runs(tmp_path):
     e.insert_integrator(0, k, p, t)  # "brownian_align_all" < "brownian_pos_all"
     e.run(199)                       # global steps 200..399
     e.begin_step()                   # the dump at global step 400 sees the next step's enforce
-    for f in ("x", "y", "nx", "ny"):
-        np.testing.assert_array_equal(got[f], e.download(f), err_msg=f)
+    assert_dump_matches(got, {f: e.download(f) for f in ("x", "y", "nx", "ny")})
+
+
+@pytest.mark.gpu
+def test_host_dump_types_and_log_columns(tmp_path):
+    # every dump type and log column of the GPU path, from one host run,
+    # against the Python binding's state at the last dump step (at the
+    # precision each format prints, dump.cpp / log_*.hpp)
+    from samos_b200 import Engine
+    from scenarios import drive
+    parts, L = plane_parts(900, 50.0, seed=9)
+    write_particles(tmp_path / "p.dat", parts)
+    extra = ("dump pos { type = xyz; freq = 50 }\n"
+             "dump vel { type = velocity; freq = 50; header; scale = 0.5 }\n"
+             "dump dirs { type = director; freq = 50 }\n"
+             "dump arrows { type = xyzv; freq = 50; velocity; scale = 2 }\n"
+             "dump inp { type = input; freq = 50 }\n"
+             "dump traj { type = dcd; freq = 50 }\n"
+             "dump pic { type = vtp; freq = 50 }\n"
+             "dump frames { type = full; freq = 50; multi; keys; id; tp; radius; coordinate; velocity; force; "
+             "director; image_flags; normal }\n"
+             "log run.log { freq = 50; velocity; vec_velocity; kinetic_energy; soft_energy; polar_align }\n")
+    conf = CONF.replace("lx = 40.0;  ly = 40.0", "lx = 50.0;  ly = 50.0").replace("run 10\n", extra + "run 100\n")
+    (tmp_path / "c.conf").write_text(conf)
+    r = subprocess.run([BIN, "--quiet", str(tmp_path / "c.conf")], capture_output=True, text=True, timeout=600,
+                       cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    n = len(parts["x"])
+    e = Engine(n)
+    drive(e, parts, (L, L, 10.0), nlist=(2.4, 0.3), constraint=("plane", {}),
+          pairs=[("soft", {"k": "10.0", "use_particle_radii": ""})], aligns=[("polar", {"J": "0.1"})], dt=1e-3,
+          integrators=[("brownian_pos", {"seed": "7", "mu": "1.0"}),
+                       ("brownian_align", {"seed": "8", "nu": "0.1", "mur": "1.0"})]).run(99)
+    e.begin_step()  # the dumps at step 100 see that step's enforce
+    e.compute(1e-3)
+    S = {f: e.download(f) for f in ("x", "y", "z", "vx", "vy", "vz", "nx", "ny", "nz", "fx", "fy", "fz", "omega",
+                                     "ix", "iy", "iz", "Nx", "Ny", "Nz", "radius")}
+
+    def last(path, width, skip=()):
+        rows = [line for line in open(path) if line.strip() and not line.startswith(skip)]
+        return rows[-n:] if width is None else [line.split("\t") for line in rows[-n:]]
+
+    xyz = np.array([[float(v) for v in row] for row in last(tmp_path / "pos.xyz", 0, skip=("Generated",))])[:, 1:]
+    np.testing.assert_allclose(xyz[:, 0], S["x"], atol=1e-6)
+    np.testing.assert_allclose(xyz[:, 1], S["y"], atol=1e-6)
+    assert open(tmp_path / "pos.xyz").read().count("Generated by SAMoS code.") == 3  # steps 0, 50, 100
+    vel = np.array([[float(v) for v in row] for row in last(tmp_path / "vel.vel", 0, skip=("#",))])
+    np.testing.assert_allclose(vel[:, 3], 0.5 * S["vx"], rtol=1e-7, atol=1e-12)
+    np.testing.assert_allclose(vel[:, 0], S["x"] - 0.25 * S["vx"], rtol=1e-7, atol=1e-12)
+    assert open(tmp_path / "vel.vel").readline() == "# scale a = 0.5\n"
+    dirs = np.array([[float(v) for v in row] for row in last(tmp_path / "dirs.dir", 0)])
+    np.testing.assert_allclose(dirs[:, 3], S["nx"], rtol=1e-7, atol=1e-12)
+    arrows = last(tmp_path / "arrows.xyzv", 0, skip=("Generated",))
+    assert {row[0] for row in arrows} == {"A"}
+    np.testing.assert_allclose([float(row[4]) for row in arrows], 2 * S["vx"], rtol=1e-7, atol=1e-12)
+    inp = np.array([[float(v) for v in row.split()] for row in last(tmp_path / "inp.inp", None, skip=("keys",))])
+    np.testing.assert_allclose(inp[:, 4], S["x"], atol=1e-6)
+    np.testing.assert_allclose(inp[:, 10], S["nx"], atol=1e-6)
+    np.testing.assert_allclose(inp[:, 13], S["omega"], atol=1e-6)  # the `length` column carries omega
+    raw = (tmp_path / "traj.dcd").read_bytes()
+    frame = 4 + 48 + 4 + 3 * (4 + 4 * n + 4)
+    assert (len(raw) - 276) == 3 * frame
+    zc = np.frombuffer(raw[-(4 + 4 * n):-4], np.float32)
+    xc = np.frombuffer(raw[-(3 * (4 + 4 * n + 4)) + 4:-(3 * (4 + 4 * n + 4)) + 4 + 4 * n], np.float32)
+    np.testing.assert_allclose(xc, S["x"].astype(np.float32))
+    np.testing.assert_array_equal(zc, S["z"].astype(np.float32))
+    assert not (tmp_path / "pic.vtp").exists() or (tmp_path / "pic.vtp").stat().st_size == 0
+    full = np.loadtxt(tmp_path / "frames_0000000100.dat", skiprows=1)
+    keys = open(tmp_path / "frames_0000000100.dat").readline().split()[1:]
+    # (omega left out: its "%8.5f " runs into the director column when negative, as in the reference)
+    assert keys == ["id", "type", "radius", "x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "nx", "ny", "nz",
+                    "ix", "iy", "iz", "nvx", "nvy", "nvz"]
+    col = {k: full[:, i] for i, k in enumerate(keys)}
+    np.testing.assert_array_equal(col["id"], np.arange(n))
+    for k, f, tol in (("x", "x", 1e-8), ("vx", "vx", 1e-6), ("fx", "fx", 1e-6), ("ny", "ny", 1e-6),
+                      ("nvz", "Nz", 1e-6)):
+        np.testing.assert_allclose(col[k], S[f], rtol=1e-7, atol=tol, err_msg=k)
+    np.testing.assert_array_equal(col["ix"], S["ix"])
+    log = [line.split() for line in open(tmp_path / "run.log") if not line.startswith("#")]
+    assert [int(r[0]) for r in log] == [0, 50, 100]
+    step, kin, polar, soft, vec, speed = (float(v) for v in log[-1])  # step, then std::map key order
+    v2 = S["vx"] ** 2 + S["vy"] ** 2 + S["vz"] ** 2
+    assert speed == pytest.approx(np.mean(np.sqrt(v2)), rel=1e-6)
+    vs = np.array([S["vx"].sum(), S["vy"].sum(), S["vz"].sum()])
+    assert vec == pytest.approx(np.linalg.norm(vs) / n, rel=1e-6, abs=1e-12)
+    assert kin == pytest.approx(np.mean(0.5 * v2), rel=1e-6)
+    assert soft == pytest.approx(e.energy(0, 0), rel=1e-6)
+    assert polar == pytest.approx(e.energy(1, 0), rel=1e-6)
