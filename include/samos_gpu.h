@@ -258,6 +258,10 @@ typedef struct {
 int  sg_get_view(sg_system* s, sg_view* out);
 int  sg_replica_slots(const sg_system* s, int replica, int32_t* offset, int32_t* n);
 int  sg_positions_changed(sg_system* s);
+/* Particle::coordination after the last list build (neighbour_list.cpp:
+ * 185-206, 229-268): the listed neighbours within the sum of the radii at
+ * the build positions, per particle id (n_particles[replica] values).     */
+int  sg_coordination(sg_system* s, int replica, int32_t* out);
 /* cudaMemcpy with direction inferred from the pointers (helper for callers
  * that hold device pointers from a view).                                   */
 int  sg_memcpy(void* dst, const void* src, int64_t bytes);

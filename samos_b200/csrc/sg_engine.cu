@@ -721,6 +721,45 @@ int sg_build_nlist(sg_system* s) {
   return SG_OK;
 }
 
+// Particle::coordination as NeighbourList::build_cell / build_nsq leave it
+// (neighbour_list.cpp:185-206, 229-268): for every listed pair, both
+// particles count it when their distance at the build, minimum image, is
+// below the sum of their radii.  Output indexed by particle id.
+int sg_coordination(sg_system* s, int replica, int32_t* out) {
+  if (!s || !out || replica < 0 || replica >= s->nrep) return fail(s, SG_ERR_ARG, "sg_coordination: bad argument");
+  if (!s->has_nlist) return fail(s, SG_ERR_STATE, "no neighbour list");
+  const int n = s->n[replica], off = s->off[replica], C = s->nl.cap;
+  const Replica& R = s->reps_h[replica];
+  std::vector<int> cnt(n), lo(n), ids(n), nb((size_t)C * n);
+  std::vector<double> X(n), Y(n), Z(n), rad(n);
+  CU(s, cudaMemcpyAsync(cnt.data(), s->nl.cnt + off, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaMemcpyAsync(lo.data(), s->nl.lo + off, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaMemcpyAsync(ids.data(), s->st.id + off, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaMemcpyAsync(X.data(), s->nl.ox + off, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaMemcpyAsync(Y.data(), s->nl.oy + off, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaMemcpyAsync(Z.data(), s->nl.oz + off, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaMemcpyAsync(rad.data(), s->st.r + off, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+  for (int q = 0; q < C; q++)
+    CU(s, cudaMemcpyAsync(nb.data() + (size_t)q * n, s->nl.nb + (size_t)q * s->nl.stride + off, sizeof(int) * n,
+                          cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  for (int i = 0; i < n; i++) out[i] = 0;
+  for (int k = 0; k < n; k++)
+    for (int q = lo[k]; q < cnt[k]; q++) {  // each pair once: from its lower-id end
+      const int m = nb[(size_t)q * n + k] - off;
+      double dx = X[k] - X[m], dy = Y[k] - Y[m], dz = Z[k] - Z[m];
+      if (R.periodic) {  // System::apply_periodic, system.cpp:1083-1094
+        if (dx > R.xhi) dx -= R.Lx; else if (dx < R.xlo) dx += R.Lx;
+        if (dy > R.yhi) dy -= R.Ly; else if (dy < R.ylo) dy += R.Ly;
+        if (dz > R.zhi) dz -= R.Lz; else if (dz < R.zlo) dz += R.Lz;
+      }
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      const double r = rad[k] + rad[m];
+      if (d2 < r * r) { out[ids[k]]++; out[ids[m]]++; }
+    }
+  return SG_OK;
+}
+
 int sg_get_pairs(sg_system* s, int replica, int32_t* out_i, int32_t* out_j, int64_t cap, int64_t* n_pairs) {
   if (!s || replica < 0 || replica >= s->nrep || !n_pairs) return fail(s, SG_ERR_ARG, "sg_get_pairs: bad argument");
   if (!s->has_nlist) return fail(s, SG_ERR_STATE, "no neighbour list");

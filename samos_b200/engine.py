@@ -105,6 +105,7 @@ def load() -> C.CDLL:
         "sg_positions_changed": (I, [P]),
         "sg_memcpy": (I, [P, P, I64]),
         "sg_host_alloc": (I, [I64, C.POINTER(P)]),
+        "sg_coordination": (I, [P, I, C.POINTER(C.c_int32)]),
         "sg_host_free": (I, [P]),
         "sg_set_variant": (I, [P, I]),
         "sg_set_build": (I, [P, I]),
@@ -217,6 +218,12 @@ class Engine:
                 raise ValueError(f"{field}: out must be a writeable contiguous {dtype} array of {self.n[replica]}")
         self._check(self.lib.sg_download(self.h, replica, field.encode(), a.ctypes.data_as(C.c_void_p)))
         return a
+
+    def coordination(self, replica: int = 0) -> np.ndarray:
+        """Contacts per particle at the last list build (Particle::coordination)."""
+        out = np.empty(self.n[replica], np.int32)
+        self._check(self.lib.sg_coordination(self.h, replica, out.ctypes.data_as(C.POINTER(C.c_int32))))
+        return out
 
     def set_nlist(self, rcut, pad):
         self._check(self.lib.sg_set_nlist(self.h, float(rcut), float(pad)))

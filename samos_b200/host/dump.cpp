@@ -1,7 +1,8 @@
 // Dumps of the conf-file host, following Dump (src/dump/dump.cpp): types
-// input, full, xyz, velocity, director, xyzv and dcd with the reference's
-// extensions, file naming, headers and number formats; vtp is accepted and
-// writes nothing, as a reference built without VTK does (dump.cpp:404-407).
+// input, full, xyz, velocity, director, xyzv, dcd and vtp with the
+// reference's extensions, file naming, headers and number formats; vtp as a
+// VTK XML PolyData file (ASCII) with the point arrays Dump::dump_vtp adds for
+// particles without mesh or bonds (dump.cpp:1109-1230).
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -93,7 +94,7 @@ DumpSpec make_dump(const std::string& name, const Params& p, int32_t n) {
       if (p.count(q)) throw HostError(std::string("Dump quantity ") + q + " is not part of the GPU path.");
   if (d.type == "dcd" && d.multi) throw HostError("DCD files cannot be split. mulifile flag is not permitted.");
   d.scale = p.count("scale") ? to_dbl(p.at("scale"), "dump") : 1.0;
-  if (!d.multi && d.type != "vtp") {  // one file for the whole run, opened now (dump.cpp:160-170)
+  if (!d.multi) {  // one file for the whole run, opened now (dump.cpp:160-170; a vtp one stays empty)
     d.path = d.dir + "/" + d.name + "." + d.ext;
     std::FILE* f = std::fopen(d.path.c_str(), d.type == "dcd" ? "wb" : "w");
     if (!f) throw HostError("Cannot open dump file " + d.path);
@@ -105,8 +106,57 @@ DumpSpec make_dump(const std::string& name, const Params& p, int32_t n) {
 
 bool dump_due(const DumpSpec& d, int64_t step) { return step >= d.start && step % d.freq == 0; }
 
+namespace {
+
+// Dump::dump_vtp (dump.cpp:1109-1230): one file per dump, <name>_<step>.vtp;
+// Pressure is the trace of the particle stress, which none of the GPU path's
+// potentials sets (zero, as in the reference); NumNeigh is the coordination.
+void write_vtp(const DumpSpec& d, int64_t step, const DumpState& s) {
+  char num[32];
+  std::snprintf(num, sizeof num, "%010lld", (long long)step);
+  const std::string path = d.dir + "/" + d.name + "_" + num + "." + d.ext;
+  std::FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) throw HostError("Cannot open dump file " + path);
+  const Particles& P = *s.parts;
+  const size_t N = P.size();
+  std::fprintf(f, "<?xml version=\"1.0\"?>\n<VTKFile type=\"PolyData\" version=\"0.1\" byte_order=\"LittleEndian\">\n"
+                  "  <PolyData>\n    <Piece NumberOfPoints=\"%zu\" NumberOfVerts=\"0\" NumberOfLines=\"0\" "
+                  "NumberOfStrips=\"0\" NumberOfPolys=\"0\">\n      <PointData>\n", N);
+  auto ints = [&](const char* name, auto get) {
+    std::fprintf(f, "        <DataArray type=\"Int32\" Name=\"%s\" format=\"ascii\">\n", name);
+    for (size_t i = 0; i < N; i++) std::fprintf(f, "%d\n", (int)get(i));
+    std::fprintf(f, "        </DataArray>\n");
+  };
+  auto reals = [&](const char* name, int comps, auto get) {
+    std::fprintf(f, "        <DataArray type=\"Float64\" Name=\"%s\" NumberOfComponents=\"%d\" format=\"ascii\">\n",
+                 name, comps);
+    for (size_t i = 0; i < N; i++) {
+      for (int c = 0; c < comps; c++) std::fprintf(f, c ? " %.17g" : "%.17g", get(i, c));
+      std::fputs("\n", f);
+    }
+    std::fprintf(f, "        </DataArray>\n");
+  };
+  ints("Id", [&](size_t i) { return P.id[i]; });
+  ints("Type", [&](size_t i) { return P.type[i]; });
+  reals("Radius", 1, [&](size_t i, int) { return P.radius[i]; });
+  reals("NativeArea", 1, [&](size_t i, int) { return 3.14159265359 * P.radius[i] * P.radius[i]; });  // particle.hpp:81
+  reals("Pressure", 1, [&](size_t, int) { return 0.0; });
+  reals("Velocity", 3, [&](size_t i, int c) { return c == 0 ? P.vx[i] : c == 1 ? P.vy[i] : P.vz[i]; });
+  reals("Force", 3, [&](size_t i, int c) { return c == 0 ? (*s.fx)[i] : c == 1 ? (*s.fy)[i] : (*s.fz)[i]; });
+  reals("Director", 3, [&](size_t i, int c) { return c == 0 ? P.nx[i] : c == 1 ? P.ny[i] : P.nz[i]; });
+  reals("NDirector", 3, [&](size_t i, int c) { return c == 0 ? -P.nx[i] : c == 1 ? -P.ny[i] : -P.nz[i]; });
+  reals("NumNeigh", 1, [&](size_t i, int) { return (double)(*s.coordination)[i]; });
+  std::fprintf(f, "      </PointData>\n      <Points>\n"
+                  "        <DataArray type=\"Float64\" NumberOfComponents=\"3\" format=\"ascii\">\n");
+  for (size_t i = 0; i < N; i++) std::fprintf(f, "%.17g %.17g %.17g\n", P.x[i], P.y[i], P.z[i]);
+  std::fprintf(f, "        </DataArray>\n      </Points>\n    </Piece>\n  </PolyData>\n</VTKFile>\n");
+  std::fclose(f);
+}
+
+}  // namespace
+
 void write_dump(const DumpSpec& d, int64_t step, const DumpState& s) {
-  if (d.type == "vtp") return;
+  if (d.type == "vtp") { write_vtp(d, step, s); return; }
   std::string path = d.path;
   const char* mode = d.type == "dcd" ? "ab" : "a";
   if (d.multi) {

@@ -349,9 +349,14 @@ void Samos::report(int64_t step) {
   ds.parts = &parts_;
   ds.lx = lx_; ds.ly = ly_; ds.lz = lz_;
   std::vector<double> F[3], N[3];
+  std::vector<int32_t> coord;
   for (const auto& d : dumps_) {
     if (!dump_due(d, step)) continue;
-    if (d.type == "full" && d.p.count("force") && F[0].empty()) {
+    if (d.type == "vtp" && coord.empty()) {
+      coord.resize(parts_.size());
+      check(sg_coordination(h_, 0, coord.data()), "sg_coordination");
+    }
+    if (((d.type == "full" && d.p.count("force")) || d.type == "vtp") && F[0].empty()) {
       const char* names[3] = {"fx", "fy", "fz"};
       for (int c = 0; c < 3; c++) { F[c].resize(parts_.size()); down(names[c], F[c].data()); }
     }
@@ -361,6 +366,7 @@ void Samos::report(int64_t step) {
     }
     ds.fx = &F[0]; ds.fy = &F[1]; ds.fz = &F[2];
     ds.Nx = &N[0]; ds.Ny = &N[1]; ds.Nz = &N[2];
+    ds.coordination = &coord;
     write_dump(d, step, ds);
   }
   for (const auto& l : logs_) {  // Logger::log (logger.cpp:128-139): each column then a space

@@ -61,6 +61,7 @@ struct DumpState {
   const Particles* parts = nullptr;
   double lx = 0.0, ly = 0.0, lz = 0.0;
   const std::vector<double> *fx = nullptr, *fy = nullptr, *fz = nullptr, *Nx = nullptr, *Ny = nullptr, *Nz = nullptr;
+  const std::vector<int32_t>* coordination = nullptr;
 };
 // Dump ctor (src/dump/dump.cpp:45-340): validates, opens the single file
 // (and writes the DCD header) as the reference does at construction.

@@ -454,3 +454,21 @@ def test_trajectory_vicsek_generic_fused_path():
                     pairs=[("soft", {"k": "10", "use_particle_radii": ""})], aligns=[("vicsek", {"rcut": "2.0"})],
                     dt=1e-3, integrators=[("brownian", {"v0": "0.5", "nu": "0.1", "seed": "3"})])
     assert_traj(e, o)
+
+
+def test_coordination_counts_contacts_at_the_build():
+    # Particle::coordination (neighbour_list.cpp:185-206, 229-268): every
+    # listed pair within the sum of the radii at the build counts for both
+    parts, L = plane_disks(3000, 0.7, seed=41)
+    e = Engine(3000)
+    drive(e, parts, (L, L, 10.0), nlist=(2.4, 0.3))
+    e.build_nlist()
+    i, j = e.pairs()
+    x, y, r = e.download("x"), e.download("y"), e.download("radius")
+    dx, dy = x[i] - x[j], y[i] - y[j]
+    dx -= L * np.round(dx / L)
+    dy -= L * np.round(dy / L)
+    touch = dx * dx + dy * dy < (r[i] + r[j]) ** 2
+    want = np.bincount(i[touch], minlength=3000) + np.bincount(j[touch], minlength=3000)
+    np.testing.assert_array_equal(e.coordination(), want)
+    assert want.sum() > 3000

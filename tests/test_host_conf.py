@@ -389,7 +389,23 @@ def test_host_dump_types_and_log_columns(tmp_path):
     xc = np.frombuffer(raw[-(3 * (4 + 4 * n + 4)) + 4:-(3 * (4 + 4 * n + 4)) + 4 + 4 * n], np.float32)
     np.testing.assert_allclose(xc, S["x"].astype(np.float32))
     np.testing.assert_array_equal(zc, S["z"].astype(np.float32))
-    assert not (tmp_path / "pic.vtp").exists() or (tmp_path / "pic.vtp").stat().st_size == 0
+    assert (tmp_path / "pic.vtp").stat().st_size == 0  # opened at construction, frames go to pic_<step>.vtp
+    import re
+    xml = (tmp_path / "pic_0000000100.vtp").read_text()
+
+    def arr(name, comps=1):
+        body = re.search(r'Name="%s"[^>]*>(.*?)</DataArray>' % name, xml, re.S).group(1)
+        return np.array(body.split(), float).reshape(-1, comps)
+
+    np.testing.assert_array_equal(arr("Id")[:, 0], np.arange(n))
+    np.testing.assert_allclose(arr("Velocity", 3)[:, 0], S["vx"], rtol=1e-15, atol=0)
+    np.testing.assert_allclose(arr("Force", 3)[:, 1], S["fy"], rtol=1e-15, atol=0)
+    np.testing.assert_array_equal(arr("NDirector", 3), -arr("Director", 3))
+    np.testing.assert_allclose(arr("NativeArea")[:, 0], 3.14159265359 * S["radius"] ** 2, rtol=1e-15)
+    assert not arr("Pressure").any()
+    np.testing.assert_array_equal(arr("NumNeigh")[:, 0], e.coordination())
+    pts = re.search(r"<Points>\s*<DataArray[^>]*>(.*?)</DataArray>", xml, re.S).group(1)
+    np.testing.assert_array_equal(np.array(pts.split(), float).reshape(-1, 3)[:, 0], S["x"])
     full = np.loadtxt(tmp_path / "frames_0000000100.dat", skiprows=1)
     keys = open(tmp_path / "frames_0000000100.dat").readline().split()[1:]
     # (omega left out: its "%8.5f " runs into the director column when negative, as in the reference)
