@@ -172,6 +172,16 @@ int  sg_add_integrator(sg_system* s, int kind, const double* params,
  *   order before a run.                                                   */
 int  sg_insert_integrator(sg_system* s, int pos, int kind, const double* params, const double* temperature_value);
 int  sg_disable_integrator(sg_system* s, int index);
+/* `group <name> {...}` (samos.cpp:1108-1140, System::make_group,
+ * system.cpp:462-572): group index 1..7 of replica r gets the particles with
+ * member[id] != 0 (the host evaluates type / not_type / r_* / x_*... on its
+ * particles); their order in the group is their index order.               */
+int  sg_define_group(sg_system* s, int replica, int group, const uint8_t* member);
+/* An integrator's `group = <name>` (integrator.hpp:67-109): the integrator at
+ * map position `index` moves only the members of `group` (0 = all), drawing
+ * its noise in group order.  brownian, brownian_pos, brownian_align and
+ * vicsek take groups here; the others act on "all".                         */
+int  sg_set_integrator_group(sg_system* s, int index, int group);
 int  sg_clear_forces(sg_system* s);
 
 /* Per-replica override of one numeric parameter (batched ensembles):

@@ -46,6 +46,8 @@ def load() -> C.CDLL:
         "or_add_align": (I, [P, I, D, D, dp, I]),
         "or_add_external": (I, [P, I, D, dp, I]),
         "or_add_constraint": (I, [P, I, dp]),
+        "or_define_group": (I, [P, I, C.c_void_p]),
+        "or_set_integrator_group": (I, [P, I, I]),
         "or_add_integrator": (I, [P, I, dp, dp]),
         "or_integrator_state": (I, [P, I, dp]),
         "or_compute": (None, [P, D]), "or_enforce_all": (None, [P]),
@@ -165,6 +167,15 @@ class OracleSystem:
         p[:len(params)] = params
         t = _d(temperature)
         self.lib.or_add_integrator(self.h, int(kind), _p(p), _p(t))
+
+    def define_group(self, group, member, replica=0):
+        m = np.ascontiguousarray(member, dtype=np.uint8)
+        if self.lib.or_define_group(self.h, int(group), m.ctypes.data) != 0:
+            raise ValueError("bad group index")
+
+    def set_integrator_group(self, index, group):
+        if self.lib.or_set_integrator_group(self.h, int(index), int(group)) != 0:
+            raise ValueError("bad integrator or group index")
 
     def compute(self, dt):
         self.lib.or_compute(self.h, float(dt))

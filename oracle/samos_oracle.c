@@ -229,6 +229,7 @@ typedef struct {
   double alpha, alpha_init, old_energy; int last_neg, converged;
   /* BBK noise vectors */
   double *Rx, *Ry, *Rz;
+  int group;  /* 0 = all, else a group defined by or_define_group */
 } or_integ;
 
 #define OR_MAX_COMP 8
@@ -251,6 +252,7 @@ struct or_system {
   or_ext exts[OR_MAX_COMP]; int nexts;
   or_cons cons[OR_MAX_COMP]; int ncons;
   or_integ integ[OR_MAX_COMP]; int ninteg;
+  int* glist[OR_MAX_GROUPS]; int gsize[OR_MAX_GROUPS];  /* group members in particle-index order */
 };
 
 #define NFIELDS 22
@@ -290,6 +292,7 @@ void or_destroy(or_system* s)
   for (int k = 0; k < s->naligns; k++) free(s->aligns[k].table);
   for (int k = 0; k < s->nexts; k++) free(s->exts[k].type_alpha);
   for (int k = 0; k < s->ninteg; k++) { free(s->integ[k].Rx); free(s->integ[k].Ry); free(s->integ[k].Rz); }
+  for (int k = 0; k < OR_MAX_GROUPS; k++) free(s->glist[k]);
   free(s);
 }
 
@@ -1377,6 +1380,28 @@ int or_add_integrator(or_system* s, int kind, const double* p, const double* tem
   return s->ninteg - 1;
 }
 
+/* System::make_group (system.cpp:462-572): members in particle-index order */
+int or_define_group(or_system* s, int group, const unsigned char* member)
+{
+  if (group < 1 || group >= OR_MAX_GROUPS) return -1;
+  free(s->glist[group]);
+  s->glist[group] = (int*)malloc(sizeof(int) * (size_t)(s->N > 0 ? s->N : 1));
+  int n = 0;
+  for (int i = 0; i < s->N; i++)
+    if (member[i]) s->glist[group][n++] = i;
+  s->gsize[group] = n;
+  return 0;
+}
+
+/* an integrator's `group` parameter (integrator.hpp:67-109) */
+int or_set_integrator_group(or_system* s, int idx, int group)
+{
+  if (idx < 0 || idx >= s->ninteg || group < 0 || group >= OR_MAX_GROUPS) return -1;
+  if (group && !s->glist[group]) return -1;
+  s->integ[idx].group = group;
+  return 0;
+}
+
 int or_integrator_state(or_system* s, int idx, double* out)
 {
   or_integ* g = &s->integ[idx];
@@ -1396,13 +1421,17 @@ static void integ_brownian(or_system* s, or_integ* g)
   double T = value_get(&g->temp, s->run_step);
   double B = sqrt(2.0 * mu * T);
   double sqrt_dt = sqrt(dt);
+  const int M = g->group ? s->gsize[g->group] : N;  /* the integrator's group, in index order */
   if (nematic)
-    for (int i = 0; i < N; i++)
+    for (int q = 0; q < M; q++) {
+      const int i = g->group ? s->glist[g->group][q] : q;
       if (rng_drnd(&g->rng) < flip) {
         s->nx[i] = -s->nx[i]; s->ny[i] = -s->ny[i]; s->nz[i] = -s->nz[i];
         if (velocity) { s->vx[i] = -s->vx[i]; s->vy[i] = -s->vy[i]; s->vz[i] = -s->vz[i]; }
       }
-  for (int i = 0; i < N; i++) {
+    }
+  for (int q = 0; q < M; q++) {
+    const int i = g->group ? s->glist[g->group][q] : q;
     double fd_x = v0 * s->nx[i] + mu * s->fx[i];
     double fd_y = v0 * s->ny[i] + mu * s->fy[i];
     double fd_z = v0 * s->nz[i] + mu * s->fz[i];
@@ -1432,7 +1461,9 @@ static void integ_brownian_pos(or_system* s, or_integ* g)
   double T = value_get(&g->temp, s->run_step);
   double B = sqrt(2.0 * mu * T);
   double sqrt_dt = sqrt(dt);
-  for (int i = 0; i < N; i++) {
+  const int M = g->group ? s->gsize[g->group] : N;
+  for (int q = 0; q < M; q++) {
+    const int i = g->group ? s->glist[g->group][q] : q;
     s->vx[i] = mu * s->fx[i]; s->vy[i] = mu * s->fy[i]; s->vz[i] = mu * s->fz[i];
     s->x[i] += dt * s->vx[i]; s->y[i] += dt * s->vy[i]; s->z[i] += dt * s->vz[i];
     if (T > 0.0) {
@@ -1455,10 +1486,14 @@ static void integ_brownian_align(or_system* s, or_integ* g)
   int nematic = (int)g->p[6];
   double flip = nematic ? dt / g->p[7] : 0.0;
   double stoch_coeff = sqrt(nu * dt);
+  const int M = g->group ? s->gsize[g->group] : N;
   if (nematic)
-    for (int i = 0; i < N; i++)
+    for (int q = 0; q < M; q++) {
+      const int i = g->group ? s->glist[g->group][q] : q;
       if (rng_drnd(&g->rng) < flip) { s->nx[i] = -s->nx[i]; s->ny[i] = -s->ny[i]; s->nz[i] = -s->nz[i]; }
-  for (int i = 0; i < N; i++) {
+    }
+  for (int q = 0; q < M; q++) {
+    const int i = g->group ? s->glist[g->group][q] : q;
     s->omega[i] = mur * project_torque(s, i);
     double dtheta = dt * s->omega[i] + stoch_coeff * rng_gauss(&g->rng, 1.0);
     rotate_director(s, i, dtheta);
@@ -1701,7 +1736,9 @@ static void integ_vicsek(or_system* s, or_integ* g)
   int N = s->N;
   double dt = g->dt, v0 = g->p[1], eta = g->p[2], mu = g->p[3];
   double noise = eta * sqrt(dt);
-  for (int i = 0; i < N; i++) {
+  const int M = g->group ? s->gsize[g->group] : N;
+  for (int q = 0; q < M; q++) {
+    const int i = g->group ? s->glist[g->group][q] : q;
     s->vx[i] = v0 * s->tx[i] + mu * s->fx[i];
     s->vy[i] = v0 * s->ty[i] + mu * s->fy[i];
     s->vz[i] = v0 * s->tz[i] + mu * s->fz[i];

@@ -94,6 +94,11 @@ int    or_add_constraint(or_system* s, int kind, const double* params);
 int    or_add_integrator(or_system* s, int kind, const double* params,
                          const double* temperature_value);
 int    or_integrator_state(or_system* s, int idx, double* out /* 8 */);
+/* particle groups: group 1..OR_MAX_GROUPS-1 gets the particles with
+   member[i] != 0 (index order); an integrator then moves only its group */
+#define OR_MAX_GROUPS 8
+int    or_define_group(or_system* s, int group, const unsigned char* member);
+int    or_set_integrator_group(or_system* s, int idx, int group);
 
 /* one force + torque evaluation (reset, potentials, aligners) */
 void   or_compute(or_system* s, double dt);

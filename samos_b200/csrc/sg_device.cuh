@@ -65,7 +65,10 @@ struct ExtComp { int kind, has_params; const double* type_alpha; };
 // b2, b3: torus tube radius a; ellipsoid b, c (the first shape parameter is
 // per replica, Replica::cons_p); max_iter, tol: the SHAKE projection
 struct ConsComp { int kind, unlimited, max_iter, pad; double b2, b3, tol; };
-struct IntegComp { int kind, method, nematic, velocity; Value temp; };
+// group: 0 = "all", else the index of a particle group (System::make_group)
+// whose members alone the integrator moves, in group order
+struct IntegComp { int kind, method, nematic, velocity, group, pad_g; Value temp; };
+constexpr int MAX_GROUPS = 8;  // "all" and up to seven defined groups
 
 // The configured component program, passed by value to every kernel.
 struct Program {
@@ -93,6 +96,7 @@ struct Replica {
   double cons_p[MAX_CONS];     // plane: zpos; sphere: r
   double integ_p[MAX_INTEG][INT_NPARAM];
   uint32_t seed[MAX_INTEG];
+  int gsize[MAX_GROUPS];       // members of each defined group
 };
 
 // Per-replica evolving scalars (device array, updated by the tail kernels).

@@ -114,6 +114,12 @@ struct sg_system {
   int* tile_slot = nullptr;
   uint16_t* nbpos = nullptr;
   int nbpos_cap = 0;
+  // particle groups (System::make_group): per slot-of-id a bit per group, and
+  // each member's position in its group (ids are fixed, so both are indexed
+  // by replica offset + particle id and never move with the slots)
+  uint8_t* gmask = nullptr;
+  int* grank = nullptr;
+  std::vector<uint8_t> gmask_h;
   int build_mode = 0;        // list build: 0 automatic, 1 one thread per particle, 2 teams of TEAM lanes
   bool tile_valid = false;
   // ordered variants: per-block lane order by neighbour count (k_lane_order)
@@ -946,6 +952,7 @@ int sg_add_integrator(sg_system* s, int kind, const double* params, const double
   C.method = kind == INT_LANGEVIN ? (int)params[10] : 0;
   C.nematic = (kind == INT_BROWNIAN || kind == INT_BROWNIAN_ALIGN) ? (params[6] != 0.0) : 0;
   C.velocity = kind == INT_BROWNIAN ? (params[8] != 0.0) : 0;
+  C.group = 0;
   C.temp = make_value(temp);
   const int c = P.ninteg;
   for (int r = 0; r < s->nrep; r++) {
@@ -1007,6 +1014,45 @@ int sg_insert_integrator(sg_system* s, int pos, int kind, const double* params, 
   move_integrator(s, s->prog.ninteg - 1, pos);
   if ((rc = push_reps(s))) return rc;
   return push_clk(s);
+}
+
+int sg_define_group(sg_system* s, int replica, int group, const uint8_t* member) {
+  if (!s || !member || replica < 0 || replica >= s->nrep || group < 1 || group >= MAX_GROUPS)
+    return fail(s, SG_ERR_ARG, "sg_define_group: bad replica, group index or member array");
+  CU(s, cudaStreamSynchronize(s->stream));
+  if (!s->gmask) {
+    s->gmask = s->mem.alloc<uint8_t>(s->slots);
+    s->grank = s->mem.alloc<int>((size_t)MAX_GROUPS * s->slots);
+    if (!s->gmask || !s->grank) { s->mem.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "group tables"); }
+    s->gmask_h.assign(s->slots, 0);
+    CU(s, cudaMemsetAsync(s->gmask, 0, s->slots, s->stream));
+  }
+  const int n = s->n[replica], off = s->off[replica];
+  std::vector<int> rank(n, -1);
+  int size = 0;
+  for (int i = 0; i < n; i++) {  // members in particle-index order (System::make_group, system.cpp:558-567)
+    const uint8_t bit = (uint8_t)(1u << group);
+    if (member[i]) { rank[i] = size++; s->gmask_h[off + i] |= bit; }
+    else s->gmask_h[off + i] &= (uint8_t)~bit;
+  }
+  s->reps_h[replica].gsize[group] = size;
+  CU(s, cudaMemcpyAsync(s->gmask + off, s->gmask_h.data() + off, n, cudaMemcpyHostToDevice, s->stream));
+  CU(s, cudaMemcpyAsync(s->grank + (size_t)group * s->slots + off, rank.data(), sizeof(int) * n,
+                        cudaMemcpyHostToDevice, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  return push_reps(s);
+}
+
+int sg_set_integrator_group(sg_system* s, int index, int group) {
+  if (!s || index < 0 || index >= s->prog.ninteg || group < 0 || group >= MAX_GROUPS)
+    return fail(s, SG_ERR_ARG, "sg_set_integrator_group: bad integrator or group index");
+  const int kind = s->prog.integ[index].kind;
+  if (group && kind != INT_BROWNIAN && kind != INT_BROWNIAN_POS && kind != INT_BROWNIAN_ALIGN && kind != INT_VICSEK)
+    return fail(s, SG_ERR_UNSUPPORTED, "integrator groups other than 'all' are supported for brownian, brownian_pos, "
+                                       "brownian_align and vicsek");
+  if (group && !s->gmask) return fail(s, SG_ERR_STATE, "sg_set_integrator_group: group not defined");
+  s->prog.integ[index].group = group;
+  return SG_OK;
 }
 
 int sg_disable_integrator(sg_system* s, int index) {
@@ -1188,11 +1234,11 @@ static int step_fused(sg_system* s, bool apply_e1, bool energy) {
   if (energy)
     k_step_brownian<true><<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alt, s->st, s->nl,
                                                        s->rebuild, s->status, s->dt_global, apply_e1 ? 1 : 0,
-                                                       s->epart, nb);
+                                                       s->epart, nb, s->gmask, s->grank, s->slots);
   else
     k_step_brownian<false><<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alt, s->st, s->nl,
                                                         s->rebuild, s->status, s->dt_global, apply_e1 ? 1 : 0,
-                                                        s->epart, nb);
+                                                        s->epart, nb, s->gmask, s->grank, s->slots);
   LAUNCH_CHECK(s);
   if (s->profile) CU(s, cudaEventRecord(s->ev_k1, s->stream));
   std::swap(s->cur, s->alt);
@@ -1205,6 +1251,8 @@ static int step_fused(sg_system* s, bool apply_e1, bool energy) {
 static int hot_shape(const sg_system* s) {
   const Program& P = s->prog;
   if (s->force_generic == 1 || !fused_program(P) || P.ncons != 1) return HOT_NONE;
+  for (int c = 0; c < P.ninteg; c++)
+    if (P.integ[c].group) return HOT_NONE;  // grouped integrators: the generic fused kernel
   for (int c = 0; c < P.nalign; c++)
     if (P.align[c].kind == ALIGN_VICSEK) return HOT_NONE;
   for (int c = 0; c < P.ninteg; c++)

@@ -163,9 +163,8 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out,
 // IntegratorBrownian::integrate, integrators/integrator_brownian.cpp:42-124
 __device__ __forceinline__ void integ_brownian(const Program& P, const Replica& R, const IntegComp& ic,
                                                const double* ip, uint32_t seed, uint64_t base,
-                                               int run_step, int n, Part& p) {
+                                               int run_step, int n, uint64_t g, Part& p) {
   const double dt = ip[0], v0 = ip[1], nu = ip[2], mu = ip[3], mur = ip[4];
-  const uint64_t g = (uint64_t)p.id;
   if (ic.nematic) {
     double flip = dt / ip[7];
     if (noise_uniform(seed, base + g) < flip) {
@@ -203,13 +202,13 @@ __device__ __forceinline__ void integ_brownian(const Program& P, const Replica& 
 // IntegratorBrownianPos::integrate, integrators/integrator_brownian_pos.cpp:37-84
 __device__ __forceinline__ void integ_brownian_pos(const Program& P, const Replica& R, const IntegComp& ic,
                                                    const double* ip, uint32_t seed, uint64_t base,
-                                                   int run_step, Part& p) {
+                                                   int run_step, uint64_t g, Part& p) {
   const double dt = ip[0], mu = ip[3];
   const double T = value_get(ic.temp, run_step);
   p.vx = mu * p.fx; p.vy = mu * p.fy; p.vz = mu * p.fz;
   p.x += dt * p.vx; p.y += dt * p.vy; p.z += dt * p.vz;
   if (T > 0.0) {
-    const uint64_t c0 = base + (uint64_t)p.id * 3u;
+    const uint64_t c0 = base + g * 3u;
     const double B = sqrt(2.0 * mu * T);
     const double sqrt_dt = sqrt(dt);
     double fr_x = B * noise_gauss(seed, c0 + 0);
@@ -225,9 +224,8 @@ __device__ __forceinline__ void integ_brownian_pos(const Program& P, const Repli
 // IntegratorBrownianAlign::integrate, integrators/integrator_brownian_align.cpp:41-76
 __device__ __forceinline__ void integ_brownian_align(const Program& P, const Replica& R, const IntegComp& ic,
                                                      const double* ip, uint32_t seed, uint64_t base,
-                                                     int n, Part& p) {
+                                                     int n, uint64_t g, Part& p) {
   const double dt = ip[0], nu = ip[2], mur = ip[4];
-  const uint64_t g = (uint64_t)p.id;
   if (ic.nematic) {
     double flip = dt / ip[7];
     if (noise_uniform(seed, base + g) < flip) { p.nx = -p.nx; p.ny = -p.ny; p.nz = -p.nz; }
@@ -244,14 +242,14 @@ __device__ __forceinline__ void integ_brownian_align(const Program& P, const Rep
 // is turned by a uniform angle of width eta sqrt(dt); one uniform draw per
 // particle.
 __device__ __forceinline__ void integ_vicsek(const Program& P, const Replica& R, const double* ip, uint32_t seed,
-                                             uint64_t base, Part& p) {
+                                             uint64_t base, uint64_t g, Part& p) {
   const double dt = ip[0], v0 = ip[1], eta = ip[2], mu = ip[3];
   const double noise = eta * sqrt(dt);
   p.vx = v0 * p.tx + mu * p.fx;
   p.vy = v0 * p.ty + mu * p.fy;
   p.vz = v0 * p.tz + mu * p.fz;
   enforce_all(P, R, p);
-  const double theta = 2.0 * noise * 3.14159265358979323846 * (noise_uniform(seed, base + (uint64_t)p.id) - 0.5);
+  const double theta = 2.0 * noise * 3.14159265358979323846 * (noise_uniform(seed, base + g) - 0.5);
   rotate_velocity(P, R, p, theta);
   p.x += dt * p.vx; p.y += dt * p.vy; p.z += dt * p.vz;
   enforce_all(P, R, p);
@@ -346,7 +344,8 @@ __global__ void __launch_bounds__(BLOCK)
 k_step_brownian(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                 const Clock* __restrict__ clk, Dyn cur, Dyn nxt, Stat st, NbList nl,
                 int* __restrict__ rebuild, int* __restrict__ status, double dt_global, int apply_e1,
-                double* epart, int nblocks) {
+                double* epart, int nblocks, const uint8_t* __restrict__ gmask, const int* __restrict__ grank,
+                int slots) {
   const int r = my_replica(blk_rep);
   const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
@@ -362,14 +361,23 @@ k_step_brownian(Program P, const Replica* __restrict__ reps, const int* __restri
     for (int c = 0; c < P.ninteg; c++) {
       const IntegComp ic = P.integ[c];
       const uint64_t base = clk[r].ctr[c];
+      // a grouped integrator moves its members only, drawing in group order
+      // (IntegratorBrownian::integrate loops over the group's particles)
+      uint64_t g = (uint64_t)p.id;
+      int n = R.n;
+      if (ic.group) {
+        if (!((gmask[R.off + p.id] >> ic.group) & 1u)) continue;
+        g = (uint64_t)grank[(size_t)ic.group * slots + R.off + p.id];
+        n = R.gsize[ic.group];
+      }
       if (ic.kind == INT_BROWNIAN)
-        integ_brownian(P, R, ic, R.integ_p[c], R.seed[c], base, run_step, R.n, p);
+        integ_brownian(P, R, ic, R.integ_p[c], R.seed[c], base, run_step, n, g, p);
       else if (ic.kind == INT_BROWNIAN_POS)
-        integ_brownian_pos(P, R, ic, R.integ_p[c], R.seed[c], base, run_step, p);
+        integ_brownian_pos(P, R, ic, R.integ_p[c], R.seed[c], base, run_step, g, p);
       else if (ic.kind == INT_BROWNIAN_ALIGN)
-        integ_brownian_align(P, R, ic, R.integ_p[c], R.seed[c], base, R.n, p);
+        integ_brownian_align(P, R, ic, R.integ_p[c], R.seed[c], base, n, g, p);
       else if (ic.kind == INT_VICSEK)
-        integ_vicsek(P, R, R.integ_p[c], R.seed[c], base, p);
+        integ_vicsek(P, R, R.integ_p[c], R.seed[c], base, g, p);
     }
     if (need_update(R, nl, k, p)) {
       if (rebuild[r] == 0) atomicOr(&rebuild[r], 1);
@@ -412,7 +420,7 @@ __device__ __forceinline__ void tail_one(const Program& P, const Replica& R, Clo
   for (int c = 0; c < P.ninteg; c++) {
     const IntegComp& ic = P.integ[c];
     if (ic.kind == INT_LANGEVIN) C.ctr[c] += langevin_draws(ic, R.integ_p[c], C.run_step, R.n);
-    else C.ctr[c] += draws_per_call(ic, C.run_step, R.n);
+    else C.ctr[c] += draws_per_call(ic, C.run_step, ic.group ? R.gsize[ic.group] : R.n);
   }
   C.run_step++;
   C.time_step++;

@@ -106,6 +106,8 @@ def load() -> C.CDLL:
         "sg_memcpy": (I, [P, P, I64]),
         "sg_host_alloc": (I, [I64, C.POINTER(P)]),
         "sg_coordination": (I, [P, I, C.POINTER(C.c_int32)]),
+        "sg_define_group": (I, [P, I, I, P]),
+        "sg_set_integrator_group": (I, [P, I, I]),
         "sg_host_free": (I, [P]),
         "sg_set_variant": (I, [P, I]),
         "sg_set_build": (I, [P, I]),
@@ -218,6 +220,17 @@ class Engine:
                 raise ValueError(f"{field}: out must be a writeable contiguous {dtype} array of {self.n[replica]}")
         self._check(self.lib.sg_download(self.h, replica, field.encode(), a.ctypes.data_as(C.c_void_p)))
         return a
+
+    def define_group(self, group: int, member, replica: int = 0) -> None:
+        """Group `group` (1..7) of a replica: the particles with member[id] != 0."""
+        m = np.ascontiguousarray(member, dtype=np.uint8)
+        if m.shape != (self.n[replica],):
+            raise ValueError("one membership flag per particle expected")
+        self._check(self.lib.sg_define_group(self.h, replica, int(group), m.ctypes.data_as(C.c_void_p)))
+
+    def set_integrator_group(self, index: int, group: int) -> None:
+        """The integrator at map position `index` moves only group `group` (0 = all)."""
+        self._check(self.lib.sg_set_integrator_group(self.h, int(index), int(group)))
 
     def coordination(self, replica: int = 0) -> np.ndarray:
         """Contacts per particle at the last list build (Particle::coordination)."""

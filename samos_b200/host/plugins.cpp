@@ -230,7 +230,7 @@ IntegratorSpec resolve_integrator(const std::string& name, const Params& p, doub
   double* q = s.params;
   const double dt = get(p, "dt", dt_global);
   if (!(dt > 0.0)) throw HostError("Integrator step has not been set.");
-  if (has(p, "group") && p.at("group") != "all") throw HostError("Integrator groups other than 'all' are not part of the GPU path.");
+  s.group = has(p, "group") ? p.at("group") : std::string("all");
   q[0] = dt;
   auto seed = [&]() { return has(p, "seed") ? (double)to_int("seed", p.at("seed")) : 0.0; };
   if (name == "brownian") {  // integrator_brownian.hpp:55-160

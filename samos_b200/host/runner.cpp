@@ -181,6 +181,12 @@ void Samos::execute_line(const std::string& raw, int line_no) {
       throw HostError("Integrator of type " + type + " (for group " + key.substr(type.size() + 1) +
                       ") already exists. You need to disable the old one first.");
     IntegratorSpec s = resolve_integrator(type, p, dt_);
+    int group = 0;
+    if (s.group != "all") {
+      auto g = groups_.find(s.group);
+      if (g == groups_.end()) throw HostError("Group " + s.group + " is not defined.");
+      group = g->second;
+    }
     integrators_[key] = s;
     int pos = 0;
     for (const auto& kv : integrators_) {
@@ -189,6 +195,7 @@ void Samos::execute_line(const std::string& raw, int line_no) {
     }
     committed_integ_.insert(committed_integ_.begin() + pos, key);
     if (h_) check(sg_insert_integrator(h_, pos, s.kind, s.params, s.temperature), "sg_insert_integrator");
+    if (h_ && group) check(sg_set_integrator_group(h_, pos, group), "sg_set_integrator_group");
   } else if (cmd == "disable") {  // samos.cpp:1143-1180
     if (integrators_.empty()) throw HostError("Integrator not defined.");
     typed("disable");
@@ -214,8 +221,10 @@ void Samos::execute_line(const std::string& raw, int line_no) {
   } else if (cmd == "log") {
     need_system("adding logs");
     cmd_log(rest);
-  } else if (cmd == "group") {
-    throw HostError("Particle groups other than 'all' are not part of the GPU path.");
+  } else if (cmd == "group") {  // samos.cpp:1108-1140, System::make_group (system.cpp:462-572)
+    need_system("adding any particle groups");
+    typed("group");
+    cmd_group(type, p);
   } else {
     throw HostError("Command " + cmd + " (line " + std::to_string(line_no) + ") is not part of the GPU path.");
   }
@@ -279,6 +288,47 @@ void Samos::cmd_run(int64_t steps) {
   if (!opt_.quiet)
     std::fprintf(stderr, "Run of %lld steps done: %lld neighbour-list builds, %.3f ms on the device.\n",
                  (long long)total, (long long)builds, ms);
+}
+
+// Members: the particles meeting every given criterion on the state at this
+// command, in index order.
+void Samos::cmd_group(const std::string& name, const Params& p) {
+  if (name == "boundary" || name == "tissue")
+    throw HostError("Groups \"tissue\" and \"boundary\" are reserved and cannot be used.");
+  if (groups_.count(name))
+    throw HostError("Group " + name + " is already defined (adding to a group is not part of the GPU path).");
+  if (groups_.size() >= 7) throw HostError("More than 7 particle groups are not part of the GPU path.");
+  static const std::set<std::string> crit = {"type", "not_type", "r_eq", "r_le", "r_ge", "x_le",
+                                             "x_ge", "y_le", "y_ge", "z_le", "z_ge"};
+  bool positions = false;
+  for (const auto& kv : p) {
+    if (!crit.count(kv.first)) throw HostError("Group criterion " + kv.first + " is not part of the GPU path.");
+    positions = positions || kv.first[0] == 'x' || kv.first[0] == 'y' || kv.first[0] == 'z';
+  }
+  if (positions && h_) {  // the current positions, not the input's
+    check(sg_download(h_, 0, "x", parts_.x.data()), "sg_download");
+    check(sg_download(h_, 0, "y", parts_.y.data()), "sg_download");
+    check(sg_download(h_, 0, "z", parts_.z.data()), "sg_download");
+  }
+  std::vector<uint8_t> member(parts_.size(), 1);
+  for (const auto& kv : p) {
+    const std::string& k = kv.first;
+    for (size_t i = 0; i < parts_.size(); i++) {
+      bool ok = true;
+      if (k == "type") ok = parts_.type[i] == (int)to_i64(kv.second, "group");
+      else if (k == "not_type") ok = parts_.type[i] != (int)to_i64(kv.second, "group");
+      else {
+        const double v = to_dbl(kv.second, "group");
+        const double q = k[0] == 'r' ? parts_.radius[i] : k[0] == 'x' ? parts_.x[i] : k[0] == 'y' ? parts_.y[i] : parts_.z[i];
+        const std::string op = k.substr(2);
+        ok = op == "eq" ? q == v : op == "le" ? q <= v : q >= v;
+      }
+      member[i] = member[i] && ok;
+    }
+  }
+  const int idx = (int)groups_.size() + 1;
+  groups_[name] = idx;
+  if (h_) check(sg_define_group(h_, 0, idx, member.data()), "sg_define_group");
 }
 
 void Samos::cmd_dump(const std::string& rest) {

@@ -101,6 +101,7 @@ struct IntegratorSpec {
   int kind = 0;
   double params[SG_INT_NPARAM] = {0};
   double temperature[4] = {0.0, 0.0, 1.0, 1000.0};
+  std::string group = "all";  // integrator.hpp:67-109
 };
 
 PairSpec resolve_pair(const std::string& name, const Params& p, int ntypes, double nlist_rcut);
@@ -136,6 +137,7 @@ class Samos {
   void cmd_run(int64_t steps);
   void cmd_dump(const std::string& rest);
   void cmd_log(const std::string& rest);
+  void cmd_group(const std::string& name, const Params& p);
   void report(int64_t step);  // dumps and logs at the top of global step `step`
   void check(int rc, const char* what) const;
 
@@ -153,6 +155,7 @@ class Samos {
   std::map<std::string, AlignSpec> aligns_;
   std::map<std::string, ExternalSpec> externals_;
   std::map<std::string, IntegratorSpec> integrators_;  // key type_group, as samos.cpp
+  std::map<std::string, int> groups_;                   // `group` commands: name -> engine group index
   std::vector<std::string> committed_integ_;           // device order (map order)
   std::vector<DumpSpec> dumps_;
   struct Log { std::string name; int64_t freq = 1; std::vector<std::string> cols; };

@@ -250,8 +250,6 @@ def resolve_integrator(name: str, params: dict, dt_global: float) -> tuple[int, 
     dt = _f(params, "dt", dt_global)
     if not dt > 0.0:
         raise PluginError("Integrator step has not been set.")
-    if "group" in params and params["group"] != "all":
-        raise PluginError("Integrator groups other than 'all' are not part of the GPU path.")
     p[0] = dt
     if name == "brownian":  # integrator_brownian.hpp:55-160
         _known(params, _INT_BASE + ["v0", "nu", "mu", "mur", "seed", "nematic", "tau", "velocity_align"],
@@ -320,7 +318,42 @@ class Simulation:
         self.integrators: dict[str, tuple] = {}
         self.committed = False
         self.has_constraint = False
+        self.groups: dict[str, int] = {}
 
+    GROUP_CRITERIA = ("type", "not_type", "r_eq", "r_le", "r_ge", "x_le", "x_ge", "y_le", "y_ge", "z_le", "z_ge")
+
+    def group(self, name, params=None):
+        """group <name> {...} (samos.cpp:1108-1140, System::make_group,
+        system.cpp:462-572): the particles meeting every given criterion, on
+        the state at this command, in index order."""
+        params = params or {}
+        if name in ("boundary", "tissue"):
+            raise PluginError('Groups "tissue" and "boundary" are reserved and cannot be used.')
+        if name in self.groups:
+            raise PluginError(f"Group {name} is already defined (adding to a group is not part of the GPU path).")
+        if len(self.groups) >= 7:
+            raise PluginError("More than 7 particle groups are not part of the GPU path.")
+        unknown = [k for k in params if k not in self.GROUP_CRITERIA]
+        if unknown:
+            raise PluginError(f"Group criterion {unknown[0]} is not part of the GPU path.")
+        tp = self.b.download("type")
+        r = self.b.download("radius")
+        xyz = {c: self.b.download(c) for c in "xyz"}
+        add = np.ones(len(tp), bool)
+        for k, v in params.items():
+            if k == "type":
+                add &= tp == int(v)
+            elif k == "not_type":
+                add &= tp != int(v)
+            elif k.startswith("r_"):
+                val = float(v)
+                add &= {"eq": r == val, "le": r <= val, "ge": r >= val}[k[2:]]
+            else:
+                val, c = float(v), xyz[k[0]]
+                add &= c <= val if k.endswith("_le") else c >= val
+        idx = len(self.groups) + 1
+        self.b.define_group(idx, add.astype(np.uint8))
+        self.groups[name] = idx
     def box(self, lx, ly, lz, periodic=True):
         self.b.set_box(lx, ly, lz, periodic)
 
@@ -362,10 +395,13 @@ class Simulation:
 
     def integrator(self, name, params=None):
         params = params or {}
-        key = name + "_" + params.get("group", "all")
+        group = params.get("group", "all")
+        if group != "all" and group not in self.groups:
+            raise PluginError(f"Group {group} is not defined.")
+        key = name + "_" + group
         if key in self.integrators:
-            raise PluginError(f"Integrator of type {name} (for group all) already exists.")
-        self.integrators[key] = resolve_integrator(name, params, self.dt)
+            raise PluginError(f"Integrator of type {name} (for group {group}) already exists.")
+        self.integrators[key] = resolve_integrator(name, params, self.dt) + (self.groups.get(group, 0),)
 
     def commit(self):
         if self.committed:
@@ -380,9 +416,11 @@ class Simulation:
         for name in sorted(self.externals):
             s = self.externals[name]
             self.b.add_external(s.kind, s.alpha, s.type_alpha, s.has_params)
-        for key in sorted(self.integrators):
-            kind, p, temp = self.integrators[key]
+        for pos, key in enumerate(sorted(self.integrators)):
+            kind, p, temp, group = self.integrators[key]
             self.b.add_integrator(kind, p, temp)
+            if group:
+                self.b.set_integrator_group(pos, group)
         self.committed = True
 
     def run(self, steps):

@@ -472,3 +472,29 @@ def test_coordination_counts_contacts_at_the_build():
     want = np.bincount(i[touch], minlength=3000) + np.bincount(j[touch], minlength=3000)
     np.testing.assert_array_equal(e.coordination(), want)
     assert want.sum() > 3000
+
+
+@pytest.mark.parametrize("integrators", [
+    # the two-component example: one brownian integrator per group, the passive one at T > 0
+    [("brownian", {"group": "active", "v0": "0.5", "nu": "0.01", "seed": "1"}),
+     ("brownian", {"group": "passive", "v0": "0.0", "nu": "0.0", "seed": "4", "temperature_control": "constant",
+                   "min_val": "0.3"})],
+    # positions of one group, rotations of all (nematic flips), map order across groups
+    [("brownian_pos", {"group": "passive", "seed": "2", "min_val": "0.1"}),
+     ("brownian_align", {"seed": "5", "nu": "0.2", "nematic": "", "tau": "0.5"})],
+])
+def test_trajectory_grouped_integrators(integrators):
+    n = 1800
+    parts, L = plane_disks(n, 0.6, seed=45)
+    parts["type"] = np.where(np.arange(n) % 3 == 0, 2, 1)
+    runs = []
+    for b in (Engine(n, 2), OracleSystem(n, 2)):
+        sim = drive(b, parts, (L, L, 10.0), nlist=(2.4, 0.3), pairs=[("soft", {"k": "10", "use_particle_radii": ""})],
+                    aligns=[("polar", {"J": "0.2"})], dt=1e-3, ntypes=2)
+        sim.group("passive", {"type": "1"})
+        sim.group("active", {"type": "2"})
+        for name, p in integrators:
+            sim.integrator(name, dict(p))
+        sim.run(299)
+        runs.append(b)
+    assert_traj(*runs)

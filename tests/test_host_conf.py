@@ -104,7 +104,9 @@ def test_check_mode_resolves_like_the_python_plugins(tmp_path):
     ("integrator nosuch { }", "not part of the GPU path"),
     ("box cubic { lx = 4 }", "Unknown box type"),
     ("pair_potential soft { k = 10.0; ", "Error parsing"),
-    ("group g { type = 1 }", "not part of the GPU path"),
+    ("group g { molecule = 1 }", "Group criterion molecule is not part of the GPU path."),
+    ("group tissue { type = 1 }", 'Groups "tissue" and "boundary" are reserved'),
+    ("integrator brownian { group = nosuch }", "Group nosuch is not defined."),
 ])
 def test_errors_follow_the_reference(tmp_path, bad, msg):
     lines = CONF.splitlines()
@@ -184,6 +186,20 @@ def test_dump_files_and_log_header_at_construction(tmp_path):
     log = (tmp_path / "run.log").read_text().splitlines()
     assert log[0] == "# Log file : run.log" and log[1].startswith("# Generated on : ")
     assert log[2].split() == ["#", "(1)", "step", "(2)", "soft_energy", "(3)", "velocity"]
+
+
+def test_groups_and_grouped_integrators_parse(tmp_path):
+    # the two-component example's pattern: groups by type, one integrator per group
+    parts, _ = plane_parts()
+    parts["type"] = np.where(np.arange(len(parts["x"])) % 3 == 0, 2, 1)
+    conf = CONF.replace("integrator brownian_pos { seed = 7; mu = 1.0 }\nintegrator brownian_align { seed = 8; nu = 0.1, mur = 1.0 }\n",
+                        "group passive { type = 1 }\ngroup active { type = 2 }\n"
+                        "integrator brownian { group = active; seed = 1; v0 = 0.5 }\n"
+                        "integrator brownian { group = passive; seed = 4; v0 = 0.0; temperature_control = constant; "
+                        "min_val = 0.3 }\n")
+    r = check(tmp_path, conf, parts=parts)
+    assert r.returncode == 0, r.stderr
+    assert [x[0] for x in parse_describe(r.stdout)["integrator"]] == ["brownian_active", "brownian_passive"]
 
 
 def test_vicsek_and_nve_integrators_parse(tmp_path):

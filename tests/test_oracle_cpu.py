@@ -346,3 +346,21 @@ def test_slab_and_walls_reflect_like_the_reference():
     o = OracleSystem(3)
     drive(o, parts2, (16.0, 16.0, 20.0), periodic=False, constraint=("walls", {"l": "12.0"}))
     np.testing.assert_array_equal(o.download("x"), [-8.0, 1.0, 8.0])  # l = xhi = 8
+
+
+def test_grouped_integrator_moves_its_group_only():
+    # IntegratorBrownian over its group (integrator_brownian.cpp:50-121): the
+    # other particles keep their positions when nothing else integrates them
+    n = 600
+    parts, L = plane_disks(n, 0.5, seed=44)
+    parts["type"] = np.where(np.arange(n) % 3 == 0, 2, 1)
+    o = OracleSystem(n, 2)
+    sim = drive(o, parts, (L, L, 10.0), nlist=(2.4, 0.3), pairs=[("soft", {"k": "10"})], dt=1e-3, ntypes=2)
+    sim.group("active", {"type": "2"})
+    sim.integrator("brownian", {"group": "active", "v0": "1.0", "nu": "0.1", "seed": "3"})
+    x0, y0 = o.download("x").copy(), o.download("y").copy()
+    sim.run(50)
+    moved = (o.download("x") != x0) | (o.download("y") != y0)
+    assert np.array_equal(moved, parts["type"] == 2)
+    with pytest.raises(Exception):
+        sim.group("active", {"type": "1"})
