@@ -138,7 +138,14 @@ int  sg_add_external(sg_system* s, int kind, double alpha, const double* type_al
  * Peanut needs b > a (constraint_peanut.hpp:84-88; rejected here), an
  * explicitly given hourglass A at most R (constraint_hourglass.hpp:85; the
  * hosts check it).  Enforced on every particle at once like
- * src/samos.cpp:518-522.                                                   */
+ * src/samos.cpp:518-522.  rescale / rescale_steps / rescale_freq scale the
+ * sphere and cylinder radius and the tetrahedron scale by
+ * rescale^(freq/steps) every freq global steps (constraint_sphere.cpp:87-104,
+ * constraint_cylinder.cpp:79-96, constraint_tetrahedron.cpp:88-109), at the
+ * top of the step, then rebuild the lists (samos.cpp:882-886); a run with a
+ * rescaling constraint allows no second constraint.  The plane's box
+ * rescale is refused (SG_ERR_UNSUPPORTED); the other kinds ignore the
+ * parameters, as the base class's rescale does (constraint.hpp:144).        */
 int  sg_add_constraint(sg_system* s, int kind, const double* params);
 /* As sg_add_constraint, with params[0] (plane zpos / sphere r) given per
  * replica in value0[n_replicas] before the immediate enforce, so each

@@ -1236,9 +1236,14 @@ static void rotate_velocity(or_system* s, int i, double phi)
   }
 }
 
-/* ConstraintSphere::rescale (constraint_sphere.cpp:87-104) and
-   ConstraintPlane::rescale (constraint_plane.cpp:168-188), OR-ed by
-   Constrainer::rescale (constrainer.hpp:117-123) */
+/* Constraint::rescale per kind, OR-ed by Constrainer::rescale
+   (constrainer.hpp:117-123): ConstraintSphere::rescale
+   (constraint_sphere.cpp:87-104) and ConstraintTetrahedron::rescale
+   (constraint_tetrahedron.cpp:88-109) scale r / s on steps below
+   rescale_steps, ConstraintCylinder::rescale (constraint_cylinder.cpp:79-96)
+   up to and including it, ConstraintPlane::rescale
+   (constraint_plane.cpp:168-188) scales the box and every position; the
+   other constraints keep the base class's no-op (constraint.hpp:144) */
 static int constraints_rescale(or_system* s)
 {
   int res = 0;
@@ -1246,21 +1251,27 @@ static int constraints_rescale(or_system* s)
     or_cons* c = &s->cons[k];
     int r = 0;
     if (res) continue; /* `res || rescale()` short-circuits */
-    if (c->rescale != 1.0 && c->kind != OR_CONS_NONE) {
+    if (c->rescale != 1.0) {
       int step = s->time_step;
-      if ((step % c->rescale_freq == 0) && (step < c->rescale_steps)) {
-        if (c->kind == OR_CONS_SPHERE) {
-          c->r *= c->scale;
-          for (int i = 0; i < s->N; i++) sphere_enforce(s, c, i);
-        } else {
-          double a = c->scale;
-          s->Lx *= a; s->Ly *= a; s->Lz *= a;
-          s->xlo *= a; s->ylo *= a; s->zlo *= a;
-          s->xhi *= a; s->yhi *= a; s->zhi *= a;
-          for (int i = 0; i < s->N; i++) {
-            s->x[i] *= a; s->y[i] *= a; s->z[i] *= a;
-            plane_enforce(s, c, i);
-          }
+      int due = step % c->rescale_freq == 0 &&
+                (c->kind == OR_CONS_CYLINDER ? step <= c->rescale_steps : step < c->rescale_steps);
+      if (!due) {
+      } else if (c->kind == OR_CONS_SPHERE || c->kind == OR_CONS_CYLINDER || c->kind == OR_CONS_TETRAHEDRON) {
+        c->r *= c->scale;
+        for (int i = 0; i < s->N; i++) {
+          if (c->kind == OR_CONS_SPHERE) sphere_enforce(s, c, i);
+          else if (c->kind == OR_CONS_CYLINDER) cylinder_enforce(s, c, i);
+          else implicit_enforce(s, c, i);
+        }
+        r = 1;
+      } else if (c->kind == OR_CONS_PLANE) {
+        double a = c->scale;
+        s->Lx *= a; s->Ly *= a; s->Lz *= a;
+        s->xlo *= a; s->ylo *= a; s->zlo *= a;
+        s->xhi *= a; s->yhi *= a; s->zhi *= a;
+        for (int i = 0; i < s->N; i++) {
+          s->x[i] *= a; s->y[i] *= a; s->z[i] *= a;
+          plane_enforce(s, c, i);
         }
         r = 1;
       }

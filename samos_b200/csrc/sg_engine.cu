@@ -120,6 +120,11 @@ struct sg_system {
   uint8_t* gmask = nullptr;
   int* grank = nullptr;
   std::vector<uint8_t> gmask_h;
+  // ConstraintSphere::rescale settings per constraint (rescale, rescale_steps,
+  // rescale_freq, and the per-event factor rescale^(freq/steps), constraint.hpp:97-104)
+  struct Rescale { double rescale = 1.0, scale = 1.0; int steps = 1000, freq = 10; };
+  std::vector<Rescale> cons_rescale;
+  int64_t rescaled_at = -1;  // global step whose rescale sg_begin_step already applied
   int build_mode = 0;        // list build: 0 automatic, 1 one thread per particle, 2 teams of TEAM lanes
   bool tile_valid = false;
   // ordered variants: per-block lane order by neighbour count (k_lane_order)
@@ -888,6 +893,50 @@ static void set_cons(ConsComp& C, int kind, const double* params) {
   C.b3 = params ? params[8] : d3;
 }
 
+static bool rescales(int kind) { return kind == CONS_SPHERE || kind == CONS_CYLINDER || kind == CONS_TETRAHEDRON; }
+
+static void set_rescale(sg_system* s, int c, const double* params) {
+  if ((int)s->cons_rescale.size() <= c) s->cons_rescale.resize(c + 1);
+  sg_system::Rescale& q = s->cons_rescale[c];
+  q = sg_system::Rescale();
+  // the other constraints take the parameters and keep the base class's
+  // no-op rescale (constraint.hpp:144)
+  if (!params || params[4] == 0.0 || !rescales(s->prog.cons[c].kind)) return;
+  q.rescale = params[4];
+  q.steps = (int)params[5];
+  q.freq = (int)params[6];
+  q.scale = std::pow(q.rescale, (double)q.freq / (double)q.steps);
+}
+
+static bool rescaling(const sg_system* s) {
+  for (int c = 0; c < s->prog.ncons && c < (int)s->cons_rescale.size(); c++)
+    if (s->cons_rescale[c].rescale != 1.0) return true;
+  return false;
+}
+
+// Constrainer::rescale (constrainer.hpp:117-123) at global step `step`: the
+// first constraint due scales its size (every replica) and projects every
+// particle onto the new surface; true when one did (the caller then rebuilds
+// the lists).  Sphere radius (constraint_sphere.cpp:87-104) and tetrahedron
+// scale (constraint_tetrahedron.cpp:88-109) on steps below rescale_steps,
+// cylinder radius (constraint_cylinder.cpp:79-96) up to and including it.
+static int apply_rescale(sg_system* s, int64_t step, bool* done) {
+  *done = false;
+  for (int c = 0; c < s->prog.ncons && c < (int)s->cons_rescale.size(); c++) {
+    const sg_system::Rescale& q = s->cons_rescale[c];
+    const bool in_range = s->prog.cons[c].kind == CONS_CYLINDER ? step <= q.steps : step < q.steps;
+    if (q.rescale == 1.0 || step % q.freq != 0 || !in_range) continue;
+    for (int r = 0; r < s->nrep; r++) s->reps_h[r].cons_p[c] *= q.scale;
+    int rc = push_reps(s);
+    if (rc) return rc;
+    k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, nullptr);
+    LAUNCH_CHECK(s);
+    *done = true;
+    return SG_OK;
+  }
+  return SG_OK;
+}
+
 static double cons_first_default(int kind) {
   return kind == CONS_PLANE || kind == CONS_NONE || kind == CONS_GYROID || kind == CONS_SLAB ? 0.0
        : kind == CONS_PEANUT || kind == CONS_HOURGLASS || kind == CONS_TETRAHEDRON ? 10.0 : 1.0;
@@ -912,13 +961,14 @@ int sg_add_constraint_per_replica(sg_system* s, int kind, const double* params, 
   if (!s || !value0 || kind < SG_CONS_NONE || kind > SG_CONS_TETRAHEDRON) return fail(s, SG_ERR_ARG, "bad constraint");
   Program& P = s->prog;
   if (P.ncons >= MAX_CONS) return fail(s, SG_ERR_ARG, "too many constraints");
-  if (params && params[4] != 0.0 && params[4] != 1.0)
-    return fail(s, SG_ERR_UNSUPPORTED, "constraint rescale is not supported by the GPU path");
+  if (params && params[4] != 0.0 && params[4] != 1.0 && kind == CONS_PLANE)
+    return fail(s, SG_ERR_UNSUPPORTED, "constraint rescale of the plane's box is not part of the GPU path");
   set_cons(P.cons[P.ncons], kind, params);
   for (int r = 0; r < s->nrep; r++) {
     int rc = check_cons(s, P.cons[P.ncons], value0[r]);
     if (rc) return rc;
   }
+  set_rescale(s, P.ncons, params);
   for (int r = 0; r < s->nrep; r++) s->reps_h[r].cons_p[P.ncons] = cons_first_of(s, kind, value0[r], r);
   P.ncons++;
   int rc = push_reps(s);
@@ -930,11 +980,12 @@ int sg_add_constraint(sg_system* s, int kind, const double* params) {
   if (!s || kind < SG_CONS_NONE || kind > SG_CONS_TETRAHEDRON) return fail(s, SG_ERR_ARG, "sg_add_constraint: bad kind");
   Program& P = s->prog;
   if (P.ncons >= MAX_CONS) return fail(s, SG_ERR_ARG, "too many constraints");
-  if (params && params[4] != 0.0 && params[4] != 1.0)
-    return fail(s, SG_ERR_UNSUPPORTED, "constraint rescale is not supported by the GPU path");
+  if (params && params[4] != 0.0 && params[4] != 1.0 && kind == CONS_PLANE)
+    return fail(s, SG_ERR_UNSUPPORTED, "constraint rescale of the plane's box is not part of the GPU path");
   set_cons(P.cons[P.ncons], kind, params);
   const double first = params ? params[0] : cons_first_default(kind);
   if (int rc = check_cons(s, P.cons[P.ncons], first)) return rc;
+  set_rescale(s, P.ncons, params);
   for (int r = 0; r < s->nrep; r++) s->reps_h[r].cons_p[P.ncons] = cons_first_of(s, kind, first, r);
   P.ncons++;
   int rc = push_reps(s);
@@ -1104,8 +1155,24 @@ int sg_set_replica_param(sg_system* s, int replica, int cls, int comp, int slot,
 // ---------------------------------------------------------------------------
 // execution
 // ---------------------------------------------------------------------------
+static int rebuild_pending(sg_system* s, int shape, bool last, double* rebuild_ms);
+
 int sg_begin_step(sg_system* s) {
   if (!s) return SG_ERR_ARG;
+  if (!s->e1_applied && rescaling(s) && s->rescaled_at < 0) {
+    // a rescale due at this step comes before its enforce (samos.cpp:882-888)
+    int rc = pull_clk(s);
+    if (rc) return rc;
+    const int64_t step = s->clk_h[0].time_step;
+    bool scaled = false;
+    if ((rc = apply_rescale(s, step, &scaled))) return rc;
+    s->rescaled_at = step;  // the run continuing from here skips it
+    if (scaled && s->has_nlist) {
+      for (int r = 0; r < s->nrep; r++) s->rebuild_h[r] = 1;
+      double ms = 0.0;
+      if ((rc = rebuild_pending(s, HOT_NONE, false, &ms))) return rc;
+    }
+  }
   if (!s->e1_applied) {
     k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, nullptr);
     LAUNCH_CHECK(s);
@@ -1253,6 +1320,7 @@ static int hot_shape(const sg_system* s) {
   if (s->force_generic == 1 || !fused_program(P) || P.ncons != 1) return HOT_NONE;
   for (int c = 0; c < P.ninteg; c++)
     if (P.integ[c].group) return HOT_NONE;  // grouped integrators: the generic fused kernel
+  if (rescaling(s)) return HOT_NONE;        // the rescale acts between steps, before their enforce
   for (int c = 0; c < P.nalign; c++)
     if (P.align[c].kind == ALIGN_VICSEK) return HOT_NONE;
   for (int c = 0; c < P.ninteg; c++)
@@ -1701,14 +1769,35 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
     for (int r = 0; r < s->nrep; r++) { s->clk_h[r].run_step = 0; s->clk_h[r].halt = 0; }
     if ((rc = push_clk(s))) return rc;
   }
+  // constraint rescaling acts at the top of a step, before its enforce
+  // (samos.cpp:882-888): such runs go one step at a time, e1 never pre-applied
+  const bool resc = rescaling(s);
+  if (resc && s->prog.ncons != 1)
+    return fail(s, SG_ERR_UNSUPPORTED, "constraint rescale needs a single constraint on the GPU path");
+  int64_t step0 = 0;
+  if (resc) {
+    int rcp = pull_clk(s);
+    if (rcp) return rcp;
+    step0 = s->clk_h[0].time_step;
+  }
   int64_t done = 0;
   for (int64_t t = 0; t <= steps; t++) {
     const bool last = (t == steps);
     int rc;
+    if (resc && s->rescaled_at == step0 + t) {
+      s->rescaled_at = -1;  // applied by sg_begin_step before this segment
+    } else if (resc) {
+      bool scaled = false;
+      if ((rc = apply_rescale(s, step0 + t, &scaled))) return rc;
+      if (scaled && needs_nl) {  // nlist->build() after a rescale
+        for (int r = 0; r < s->nrep; r++) s->rebuild_h[r] = 1;
+        if ((rc = rebuild_pending(s, shape, false, &rebuild_ms))) return rc;
+      }
+    }
     // batched stepping: steps enqueued kBatch at a time with no host round
     // trip, the first step that flags a rebuild halting the rest (same bits)
     const int64_t K = std::min<int64_t>(needs_nl ? std::min<int64_t>(kBatch, s->last_gap / 2) : kBatch, steps - t);
-    if (driver && t > 0 && !last && K > 1 && !s->profile) {
+    if (driver && t > 0 && !last && K > 1 && !s->profile && !resc) {
       int64_t ex = 0;
       bool all = false;
       if ((rc = run_fire_batch(s, std::min<int64_t>(K, 16), needs_nl, &ex, &rebuild_ms, &all))) return rc;
@@ -1739,8 +1828,8 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
         k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, nullptr);
         LAUNCH_CHECK(s);
       }
-      rc = step_fused(s, !last, last);
-      s->e1_applied = !last;
+      rc = step_fused(s, !last && !resc, last);
+      s->e1_applied = !last && !resc;
     } else {
       rc = step_unfused(s, last, driver);
       s->e1_applied = false;

@@ -12,7 +12,7 @@ import pytest
 
 from oracle.oracle import OracleSystem
 from samos_b200 import Engine
-from scenarios import drive, plane_disks, sphere_disks, surface_disks
+from scenarios import drive, plane_disks, sphere_disks, surface_disks, tetra_value
 
 pytestmark = pytest.mark.gpu
 
@@ -498,3 +498,69 @@ def test_trajectory_grouped_integrators(integrators):
         sim.run(299)
         runs.append(b)
     assert_traj(*runs)
+
+
+def test_trajectory_sphere_rescale():
+    # ConstraintSphere::rescale (constraint_sphere.cpp:87-104): every
+    # rescale_freq steps below rescale_steps the radius grows by
+    # rescale^(freq/steps), every particle is projected onto the new sphere and
+    # the lists are rebuilt (samos.cpp:882-886)
+    parts, R = sphere_disks(1500, seed=46)
+    conf = {"r": repr(R), "rescale": "1.5", "rescale_steps": "1000", "rescale_freq": "10"}
+    box = (4 * R + 10.0,) * 3
+    e, o = run_both(1500, parts, box, 299, periodic=False, nlist=(2.4, 0.3), constraint=("sphere", conf),
+                    pairs=[("soft", {"k": "10"})], aligns=[("polar", {"J": "0.2"})], dt=1e-3,
+                    integrators=[("brownian", {"v0": "1.0", "nu": "0.1", "seed": "4"})])
+    assert_traj(e, o)
+    r_end = np.sqrt(e.download("x") ** 2 + e.download("y") ** 2 + e.download("z") ** 2)
+    np.testing.assert_allclose(r_end, R * (1.5 ** (10 / 1000)) ** 30, rtol=1e-12)
+
+
+def test_sphere_rescale_across_runs_and_begin_step():
+    # two `run` commands continue the global step the rescale is keyed on
+    # (ConstraintSphere::rescale reads System::get_step); sg_begin_step (the
+    # dump/log point at the top of a step) applies a due rescale once
+    parts, R = sphere_disks(1200, seed=47)
+    conf = {"r": repr(R), "rescale": "0.8", "rescale_steps": "300", "rescale_freq": "7"}
+    kw = dict(periodic=False, nlist=(2.4, 0.3), constraint=("sphere", conf), pairs=[("soft", {"k": "10"})],
+              aligns=[("nematic", {"J": "0.3"})], dt=1e-3,
+              integrators=[("brownian", {"v0": "0.8", "nu": "0.1", "seed": "5"})])
+    box = (4 * R + 10.0,) * 3
+    e, o = Engine(1200), OracleSystem(1200)
+    se, so = drive(e, parts, box, **kw), drive(o, parts, box, **kw)
+    se.run(139)
+    so.run(139)
+    e.begin_step()  # step 140 is a rescale step (140 % 7 == 0)
+    e.begin_step()
+    se.run(200)
+    so.run(200)
+    assert_traj(e, o)
+    events = len(range(0, 300, 7))
+    r_end = np.sqrt(e.download("x") ** 2 + e.download("y") ** 2 + e.download("z") ** 2)
+    np.testing.assert_allclose(r_end, R * (0.8 ** (7 / 300)) ** events, rtol=1e-12)
+
+
+@pytest.mark.parametrize("kind,shape,conf,box,periodic,n,a", [
+    ("cylinder", {"r": 10.0, "Lz": 60.0}, {"r": "10.0"}, (40.0, 40.0, 60.0), True, 700, 1.3),
+    ("tetrahedron", {"scale": 10.0, "value": 0.3}, {"scale": "10.0", "value": "0.3"}, (90.0, 90.0, 90.0), False, 600,
+     0.8),
+])
+def test_trajectory_rescaled_cylinder_and_tetrahedron(kind, shape, conf, box, periodic, n, a):
+    # ConstraintCylinder::rescale (constraint_cylinder.cpp:79-96: steps up to
+    # and including rescale_steps) and ConstraintTetrahedron::rescale
+    # (constraint_tetrahedron.cpp:88-109: below it, charges move with the
+    # scale).  The tetrahedron shrinks: growing its charges apart at a fixed
+    # level pinches the surface into lobes, where the SHAKE projection (and the
+    # reference's, constraint.cpp:40-87) divides by a vanishing gradient product
+    parts = surface_disks(kind, n, seed=19, **shape)
+    conf = dict(conf, rescale=repr(a), rescale_steps="200", rescale_freq="10")
+    e, o = run_both(n, parts, box, 299, periodic=periodic, nlist=(2.4, 0.3), constraint=(kind, conf),
+                    pairs=[("soft", {"k": "10"})], aligns=[("polar", {"J": "0.2"})], dt=1e-3,
+                    integrators=[("brownian", {"v0": "1.0", "nu": "0.1", "seed": "4"})])
+    assert_traj(e, o)
+    f = a ** (10 / 200)
+    x, y, z = e.download("x"), e.download("y"), e.download("z")
+    if kind == "cylinder":
+        np.testing.assert_allclose(np.hypot(x, y), 10.0 * f ** 21, rtol=1e-12)
+    else:
+        assert np.max(np.abs(tetra_value(np.stack([x, y, z], 1), 10.0 * f ** 20, 0.3))) < 2e-6

@@ -364,3 +364,49 @@ def test_grouped_integrator_moves_its_group_only():
     assert np.array_equal(moved, parts["type"] == 2)
     with pytest.raises(Exception):
         sim.group("active", {"type": "1"})
+
+
+@pytest.mark.parametrize("kind,shape,box,events", [
+    # rescale_steps 40, freq 10, run(40) = steps 0..40: the sphere rescales at
+    # 0, 10, 20, 30 (step < 40, constraint_sphere.cpp:92), the cylinder at 40
+    # as well (step <= 40, constraint_cylinder.cpp:84), the torus never
+    # (Constraint::rescale is a no-op, constraint.hpp:144)
+    ("sphere", None, None, 4),
+    ("cylinder", {"r": 10.0, "Lz": 40.0}, (40.0, 40.0, 40.0), 5),
+    ("torus", {"c": 12.0, "a": 5.0}, (50.0, 50.0, 50.0), 0),
+])
+def test_constraint_rescale_steps_per_kind(kind, shape, box, events):
+    if kind == "sphere":
+        parts, R = sphere_disks(200, seed=9)
+        conf, box, size = {"r": repr(R)}, (2 * R + 20,) * 3, R
+    else:
+        parts = surface_disks(kind, 200, seed=9, **shape)
+        conf = {k: repr(v) for k, v in shape.items() if k != "Lz"}
+        size = shape.get("r", shape.get("a"))
+    conf.update(rescale="1.2", rescale_steps="40", rescale_freq="10")
+    o = OracleSystem(200)
+    sim = drive(o, parts, box, periodic=(kind == "cylinder"), constraint=(kind, conf),
+                integrators=[("brownian", {"v0": "0", "nu": "0", "seed": "1"})], dt=1e-3)
+    sim.run(40)
+    x, y, z = o.download("x"), o.download("y"), o.download("z")
+    f = 1.2 ** (10 / 40)
+    if kind == "sphere":
+        np.testing.assert_allclose(np.sqrt(x * x + y * y + z * z), size * f ** events, rtol=1e-13)
+    elif kind == "cylinder":
+        np.testing.assert_allclose(np.hypot(x, y), size * f ** events, rtol=1e-13)
+    else:
+        g = (shape["c"] - np.hypot(x, y)) ** 2 + z ** 2 - shape["a"] ** 2
+        assert np.abs(g).max() <= 1e-6
+
+
+def test_plane_rescale_scales_the_box_and_positions():
+    # ConstraintPlane::rescale (constraint_plane.cpp:168-188) with Box::rescale
+    # (box.hpp:72-77): at step 0 the box and every coordinate scale together
+    parts, L = plane_disks(100, 0.3, seed=4)
+    o = OracleSystem(100)
+    sim = drive(o, parts, (L, L, 10.0), constraint=("plane", {"rescale": "2.0", "rescale_steps": "10",
+                                                              "rescale_freq": "10"}),
+                integrators=[("brownian", {"v0": "0", "nu": "0", "seed": "1"})], dt=1e-3)
+    x0 = o.download("x").copy()
+    sim.run(0)
+    np.testing.assert_allclose(o.download("x"), 2.0 * x0, rtol=1e-15)
