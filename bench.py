@@ -254,6 +254,142 @@ def ml_leg(count=48, seed=4242, device=0):
     return rep
 
 
+# ---------------------------------------------------------------------------
+# per-component rows: every potential, aligner, integrator and constraint
+# family of the hot path timed on the GPU beside the oracle on one core
+# ---------------------------------------------------------------------------
+def plane_mono(n, phi, seed):
+    """n radius-1 disks on a square lattice of spacing sqrt(pi/phi) (> 2 below
+    phi = 0.78: no overlaps, so the steep potentials start finite), jittered
+    by up to 0.1, in a periodic square box."""
+    rng = np.random.default_rng(seed)
+    m = int(np.ceil(np.sqrt(n)))
+    a = float(np.sqrt(np.pi / phi))
+    L = m * a
+    k = np.arange(n)
+    th = rng.uniform(0.0, 2.0 * np.pi, n)
+    z = np.zeros(n)
+    x = -L / 2 + (k % m + 0.5) * a + rng.uniform(-0.1, 0.1, n)
+    y = -L / 2 + (k // m + 0.5) * a + rng.uniform(-0.1, 0.1, n)
+    return dict(x=x, y=y, z=z, vx=z, vy=z, vz=z, nx=np.cos(th), ny=np.sin(th), nz=z, radius=np.ones(n)), L
+
+
+def torus_parts(n, seed):
+    """n radius-1 particles on a torus of tube radius a = c/3 at packing fraction 0.5."""
+    rng = np.random.default_rng(seed)
+    c = float(np.sqrt(3.0 * n / (2.0 * np.pi)))
+    a = c / 3.0
+    u, v = rng.uniform(0.0, 2.0 * np.pi, n), rng.uniform(0.0, 2.0 * np.pi, n)
+    x, y, z = (c + a * np.cos(v)) * np.cos(u), (c + a * np.cos(v)) * np.sin(u), a * np.sin(v)
+    t = np.stack([-np.sin(u), np.cos(u), np.zeros(n)])
+    zero = np.zeros(n)
+    return dict(x=x, y=y, z=z, vx=zero, vy=zero, vz=zero, nx=t[0], ny=t[1], nz=t[2], radius=np.ones(n)), c, a
+
+
+BROWNIAN_ROW = ("brownian", {"v0": "0.5", "nu": "0.1", "mu": "1", "mur": "1", "seed": "3"})
+ROWS = (
+    # name, geometry, pair, aligner, integrator, dt, state bytes per particle-step
+    ("brownian, soft (particle radii) + nematic, plane", "bidisperse",
+     ("soft", {"k": "10", "use_particle_radii": ""}), ("nematic", {"J": "0.5"}), BROWNIAN_ROW, 5e-4, 88),
+    ("brownian, lj (shifted) + polar, plane", "mono",
+     ("lj", {"epsilon": "1", "sigma": "1", "rcut": "2.5", "shifted": ""}), ("polar", {"J": "0.2"}), BROWNIAN_ROW,
+     1e-4, 88),
+    ("brownian, morse (shifted) + polar, plane", "mono",
+     ("morse", {"D": "1", "a": "2", "re": "2", "rcut": "2.5", "shifted": ""}), ("polar", {"J": "0.2"}),
+     BROWNIAN_ROW, 1e-3, 88),
+    ("brownian, gaussian + polar, plane", "mono",
+     ("gaussian", {"A": "2", "B": "-1", "alpha": "1", "beta": "3", "rA": "0", "rB": "1.5", "rcut": "2.5"}),
+     ("polar", {"J": "0.2"}), BROWNIAN_ROW, 1e-3, 88),
+    ("vicsek integrator, soft + vicsek aligner, plane", "mono", ("soft", {"k": "10"}), ("vicsek", {"rcut": "2.0"}),
+     ("vicsek", {"v0": "0.5", "eta": "0.3", "mu": "0.1", "seed": "5"}), 1e-2, 88),
+    ("langevin baoab, lj (shifted), plane", "mono",
+     ("lj", {"epsilon": "1", "sigma": "1", "rcut": "2.5", "shifted": ""}), None,
+     ("langevin", {"gamma": "1", "seed": "7", "method": "baoab", "min_val": "0.5"}), 1e-4, 88),
+    ("nve (limit 1e-4), soft + polar, plane", "mono", ("soft", {"k": "1"}), ("polar", {"J": "1"}),
+     ("nve", {"limit": "0.0001"}), 1e-3, 88),
+    ("fire, soft (particle radii), plane", "bidisperse", ("soft", {"k": "1", "use_particle_radii": ""}), None,
+     ("fire", {"dt_max": "0.1", "fmax_tolerance": "1e-10"}), 1e-2, 88),
+    ("brownian, soft + polar, sphere", "sphere", ("soft", {"k": "10"}), ("polar", {"J": "0.2"}),
+     ("brownian", {"v0": "1.0", "nu": "0.05", "mu": "1", "mur": "1", "seed": "3"}), 1e-3, 128),
+    ("brownian, soft + polar, torus (SHAKE projection)", "torus", ("soft", {"k": "10"}), ("polar", {"J": "0.2"}),
+     ("brownian", {"v0": "1.0", "nu": "0.05", "mu": "1", "mur": "1", "seed": "3"}), 1e-3, 128),
+)
+
+
+def row_system(backend, row, n, seed):
+    from samos_b200.plugins import Simulation
+    name, geom, pair, align, integ, dt, _ = row
+    sim = Simulation(backend)
+    if geom == "sphere":
+        parts, R = sphere_parts(n, seed)
+        zero = np.zeros(n)
+        parts.update(vx=zero, vy=zero, vz=zero)
+        sim.box(2 * R + 20, 2 * R + 20, 2 * R + 20, False)
+        cons, rc = ("sphere", {"r": repr(R)}), (2.4, 0.3)
+    elif geom == "torus":
+        parts, c, a = torus_parts(n, seed)
+        sim.box(2 * (c + a) + 20, 2 * (c + a) + 20, 2 * a + 20, False)
+        cons, rc = ("torus", {"c": repr(c), "a": repr(a)}), (2.4, 0.3)
+    else:
+        if geom == "bidisperse":
+            parts, L = make_particles(n, seed)
+            rc = (2.8, 0.3)
+        else:
+            parts, L = plane_mono(n, 0.6, seed)
+            rc = (2.8, 0.3)
+        sim.box(L, L, 10.0, True)
+        cons = ("plane", {})
+    sim.input(**parts)
+    sim.nlist(*rc)
+    sim.constraint(*cons)
+    sim.pair_potential(*pair)
+    if align:
+        sim.pair_align(*align)
+    sim.timestep(dt)
+    sim.integrator(*integ)
+    sim.commit()
+    return sim
+
+
+def rows_leg(n=1_048_576, warm=50, steps=200, cpu_n=16_384, cpu_warm=5, cpu_steps=20, device=0, only=None):
+    """Each row of ROWS: `warm` untimed then `steps` device-timed steps (CUDA
+    events on the engine stream, rebuilds included) at n particles, and the
+    oracle on one core at cpu_n particles of the same density.  `state_gbs` is
+    the row's state bytes per particle-step (plane: read x, y, nx, ny, r, write
+    x, y, nx, ny, vx, vy; 3-D: the same with z components) over the whole step
+    time, a floor on the traffic a step must move."""
+    from oracle.oracle import OracleSystem
+    from samos_b200 import Engine
+    peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0)) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    out = []
+    for i, row in enumerate(ROWS):
+        if only is not None and i != only:
+            continue
+        eng = Engine(n, device=device)
+        sim = row_system(eng, row, n, 100 + i)
+        sim.run(warm - 1)
+        extra = 0  # the autotuner of the specialised kernels finishes untimed
+        while eng.variant() < 0 and extra < 100:
+            eng.run(19)
+            extra += 20
+        st = eng.run(steps - 1)
+        ms = st.device_ms / st.steps_done
+        eng.close()
+        o = OracleSystem(cpu_n)
+        row_system(o, row, cpu_n, 100 + i).run(cpu_warm - 1)
+        t0 = time.perf_counter()
+        o.run(cpu_steps - 1)
+        cpu = cpu_n * cpu_steps / (time.perf_counter() - t0)
+        gbs = n * row[6] / (ms * 1e-3) / 1e9
+        out.append(dict(row=row[0], particles=n, steps=int(st.steps_done), ms_per_step=ms,
+                        particle_steps_per_s=n / (ms * 1e-3), nlist_builds=int(st.nlist_builds),
+                        state_bytes_per_particle_step=row[6], state_gbs=gbs, frac_of_hbm=gbs / peak,
+                        cpu_particles=cpu_n, cpu_particle_steps_per_s=cpu,
+                        gpu_over_cpu=n / (ms * 1e-3) / cpu))
+    return out
+
+
 def step_kernel_name(variant):
     """The fused step kernel the autotuner kept for the headline program
     (soft + nematic + brownian on a periodic plane)."""
@@ -353,6 +489,10 @@ def main():
                     help="system size (profiling runs use a smaller system of the same density)")
     ap.add_argument("--ensemble-only", action="store_true",
                     help="run only the batched 256-replica ensemble (profiling runs) and print its timing")
+    ap.add_argument("--rows", action="store_true",
+                    help="time every potential / aligner / integrator / constraint family at 1,048,576 particles "
+                         "beside the oracle on one core, print one JSON line per family")
+    ap.add_argument("--row", type=int, default=None, help="with --rows: time only this row (index into ROWS)")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if ws > 1:
@@ -368,6 +508,11 @@ def main():
         out = ensemble_only(args.variant, device=local)
         if rank == 0:
             print(json.dumps(out), flush=True)
+        return 0
+    if args.rows:
+        if rank == 0:
+            for r in rows_leg(device=local, only=args.row):
+                print(json.dumps(r), flush=True)
         return 0
 
     from samos_b200 import Engine

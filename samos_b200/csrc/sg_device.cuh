@@ -132,6 +132,19 @@ __device__ __forceinline__ void load_dyn(const Dyn& d, int k, Part& p) {
   p.omega = d.omega[k]; p.age = d.age[k];
   p.ix = d.ix[k]; p.iy = d.iy[k]; p.iz = d.iz[k];
 }
+// store of a per-particle pass that leaves the torques as they were (the
+// constraint enforce and the Langevin / NVE halves), omega and age only when
+// the pass writes them: the loads the pass never uses then drop out too
+template <bool OMEGA, bool AGE>
+__device__ __forceinline__ void store_dyn_moved(const Dyn& d, int k, const Part& p) {
+  d.x[k] = p.x; d.y[k] = p.y; d.z[k] = p.z;
+  d.vx[k] = p.vx; d.vy[k] = p.vy; d.vz[k] = p.vz;
+  d.nx[k] = p.nx; d.ny[k] = p.ny; d.nz[k] = p.nz;
+  d.fx[k] = p.fx; d.fy[k] = p.fy; d.fz[k] = p.fz;
+  if (OMEGA) d.omega[k] = p.omega;
+  if (AGE) d.age[k] = p.age;
+  d.ix[k] = p.ix; d.iy[k] = p.iy; d.iz[k] = p.iz;
+}
 __device__ __forceinline__ void store_dyn(const Dyn& d, int k, const Part& p) {
   d.x[k] = p.x; d.y[k] = p.y; d.z[k] = p.z;
   d.vx[k] = p.vx; d.vy[k] = p.vy; d.vz[k] = p.vz;

@@ -1236,6 +1236,26 @@ static bool fire_forces_reusable(const sg_system* s) {
   return true;
 }
 
+// The same for one Langevin (BAOAB or BBK: no position change after their
+// force pass, integrator_langevin.cpp:100-116, 228-252) or NVE integrator
+// (after its pass only velocities, omega and ages change, integrator_nve.cpp:
+// 104-140): periodic plane with zpos in the box, no external potentials, no
+// phase-in (ages advance after the pass).  Their start-of-step torques are
+// never read (Langevin ignores torques; NVE recomputes them in its own pass
+// before project_torque), so aligners do not stop the reuse; a step that
+// reports energies recomputes everything.
+static bool integ_forces_reusable(const sg_system* s) {
+  const Program& P = s->prog;
+  if (P.next || P.ncons != 1 || P.cons[0].kind != CONS_PLANE || P.ninteg != 1) return false;
+  const IntegComp& ic = P.integ[0];
+  if (!(ic.kind == INT_NVE || (ic.kind == INT_LANGEVIN && ic.method != LANGEVIN_SPV))) return false;
+  for (int c = 0; c < P.npair; c++)
+    if (P.pair[c].phase_in) return false;
+  for (const Replica& R : s->reps_h)
+    if (!R.periodic || !(R.cons_p[0] > R.zlo && R.cons_p[0] <= R.zhi)) return false;
+  return true;
+}
+
 static int step_unfused(sg_system* s, bool energy, bool driver) {
   const int nb = s->nblocks;
   // the minimiser launches the per-particle passes over the blocks of the
@@ -1243,10 +1263,16 @@ static int step_unfused(sg_system* s, bool energy, bool driver) {
   // only return)
   const int* al = driver && s->nact < nb ? s->act : nullptr;
   const int na = driver ? s->nact : nb;
-  const bool reuse_forces = s->forces_fresh && fire_forces_reusable(s);
+  const bool reuse_forces =
+      s->forces_fresh && (fire_forces_reusable(s) || (!energy && integ_forces_reusable(s)));
   // FIRE alone with reused forces: the start-of-step enforce runs inside the
   // first FIRE pass
-  const bool fuse_enforce = !s->e1_applied && reuse_forces && s->prog.ninteg == 1 && s->prog.integ[0].kind == INT_FIRE;
+  // (and the first half of a Langevin / NVE step likewise)
+  const bool fuse_enforce = !s->e1_applied && reuse_forces && s->prog.ninteg == 1 &&
+                            (s->prog.integ[0].kind == INT_FIRE || s->prog.integ[0].kind == INT_LANGEVIN ||
+                             s->prog.integ[0].kind == INT_NVE);
+  // the skin test runs inside the last pass of a step that has one integrator
+  const int skin_in = s->has_nlist && s->prog.ninteg == 1 ? 1 : 0;
   if (!s->e1_applied && !fuse_enforce) {  // samos.cpp:887-888 (already applied by sg_begin_step)
     k_enforce<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, driver ? s->clk : nullptr, al);
     LAUNCH_CHECK(s);
@@ -1259,17 +1285,24 @@ static int step_unfused(sg_system* s, bool energy, bool driver) {
   for (int c = 0; c < s->prog.ninteg; c++) {
     const IntegComp& ic = s->prog.integ[c];
     if (ic.kind == INT_LANGEVIN) {
-      k_langevin_a<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, c, s->Rn);
+      k_langevin_a<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, c, s->Rn,
+                                                fuse_enforce ? 1 : 0);
       LAUNCH_CHECK(s);
-      if ((rc = launch_force(s, s->reps_h[0].integ_p[c][0], false, true, false, true))) return rc;
-      k_langevin_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, c, s->Rn);
+      if ((rc = launch_force(s, s->reps_h[0].integ_p[c][0], false, true, false, energy))) return rc;
+      k_langevin_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, c, s->Rn, s->nl,
+                                                s->rebuild, s->status, skin_in);
       LAUNCH_CHECK(s);
+      s->forces_fresh = true;
+      skin_done = skin_in != 0;
     } else if (ic.kind == INT_NVE) {
-      k_nve_a<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, c);
+      k_nve_a<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, c, fuse_enforce ? 1 : 0);
       LAUNCH_CHECK(s);
-      if ((rc = launch_force(s, s->reps_h[0].integ_p[c][0], false, true, true, true))) return rc;
-      k_nve_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, c);
+      if ((rc = launch_force(s, s->reps_h[0].integ_p[c][0], false, true, true, energy))) return rc;
+      k_nve_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, c, s->nl, s->rebuild,
+                                           s->status, skin_in);
       LAUNCH_CHECK(s);
+      s->forces_fresh = true;
+      skin_done = skin_in != 0;
     } else if (ic.kind == INT_FIRE) {
       k_fire_a<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, fuse_enforce ? 1 : 0,
                                             al);

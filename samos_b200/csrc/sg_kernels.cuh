@@ -302,7 +302,7 @@ __global__ void k_enforce(Program P, const Replica* __restrict__ reps, const int
   load_dyn(d, k, p);
   p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
   enforce_all(P, R, p);
-  store_dyn(d, k, p);
+  store_dyn_moved<false, false>(d, k, p);  // the enforce writes no torque, omega or age
 }
 
 // reset + Potential::compute + Aligner::compute, storing F, tau and the
@@ -462,8 +462,10 @@ __global__ void k_set_halt(Clock* clk, int nrep, int v) {
 // Langevin (integrators/integrator_langevin.cpp): phase A before and phase B
 // after the integrator's own force evaluation.
 // ---------------------------------------------------------------------------
+// pre_enforce: the start-of-step enforce (samos.cpp:887-888) folded in, when
+// no force pass comes between it and this half (forces reused)
 __global__ void k_langevin_a(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                             const Clock* __restrict__ clk, Dyn d, Stat st, int c, const double* Rn) {
+                             const Clock* __restrict__ clk, Dyn d, Stat st, int c, const double* Rn, int pre_enforce) {
   const int r = my_replica(blk_rep);
   const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
@@ -471,6 +473,7 @@ __global__ void k_langevin_a(Program P, const Replica* __restrict__ reps, const 
   Part p;
   load_dyn(d, k, p);
   p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
+  if (pre_enforce) enforce_all(P, R, p);
   const IntegComp ic = P.integ[c];
   const double* ip = R.integ_p[c];
   const double dt = ip[0], gamma = ip[9];
@@ -515,11 +518,14 @@ __global__ void k_langevin_a(Program P, const Replica* __restrict__ reps, const 
     p.x += dt2 * p.vx; p.y += dt2 * p.vy; p.z += dt2 * p.vz;
     enforce_all(P, R, p);
   }
-  store_dyn(d, k, p);
+  store_dyn_moved<false, false>(d, k, p);
 }
 
+// skin: the step's skin test (neighbour_list.cpp:278-302) on the final
+// positions, folded in
 __global__ void k_langevin_b(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
-                             const Clock* __restrict__ clk, Dyn d, Stat st, int c, double* Rn) {
+                             const Clock* __restrict__ clk, Dyn d, Stat st, int c, double* Rn, NbList nl,
+                             int* __restrict__ rebuild, int* __restrict__ status, int skin) {
   const int r = my_replica(blk_rep);
   const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
@@ -573,7 +579,11 @@ __global__ void k_langevin_b(Program P, const Replica* __restrict__ reps, const 
     p.vx += fact * p.fx; p.vy += fact * p.fy; p.vz += fact * p.fz;
     p.age += dt;
   }
-  store_dyn(d, k, p);
+  store_dyn_moved<false, true>(d, k, p);
+  if (skin) {
+    if (need_update(R, nl, k, p) && rebuild[r] == 0) atomicOr(&rebuild[r], 1);
+    if (!finite3(p.x, p.y, p.z)) atomicOr(status, ST_NONFINITE);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -587,7 +597,7 @@ __global__ void k_langevin_b(Program P, const Replica* __restrict__ reps, const 
 __device__ __forceinline__ double sign_of(double x) { return x >= 0.0 ? 1.0 : -1.0; }  // integrator_nve.hpp:38
 
 __global__ void k_nve_a(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep, Dyn d, Stat st,
-                        int c) {
+                        int c, int pre_enforce) {
   const int r = my_replica(blk_rep);
   const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
@@ -595,6 +605,7 @@ __global__ void k_nve_a(Program P, const Replica* __restrict__ reps, const int* 
   Part p;
   load_dyn(d, k, p);
   p.id = st.id[k]; p.type = st.type[k]; p.r = st.r[k]; p.mass = st.mass[k];
+  if (pre_enforce) enforce_all(P, R, p);  // as in k_langevin_a
   const double* ip = R.integ_p[c];
   const double dt = ip[0], dt_2 = 0.5 * dt;
   const bool has_limit = ip[12] != 0.0, has_theta = ip[14] != 0.0;
@@ -612,11 +623,11 @@ __global__ void k_nve_a(Program P, const Replica* __restrict__ reps, const int* 
   double dtheta = dt * p.omega;  // nve.cpp:78-86
   if (has_theta && fabs(dtheta) > theta_limit) dtheta = sign_of(dtheta) * theta_limit;
   rotate_director(P, R, p, dtheta);
-  store_dyn(d, k, p);
+  store_dyn_moved<true, false>(d, k, p);
 }
 
 __global__ void k_nve_b(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep, Dyn d, Stat st,
-                        int c) {
+                        int c, NbList nl, int* __restrict__ rebuild, int* __restrict__ status, int skin) {
   const int r = my_replica(blk_rep);
   const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
@@ -641,7 +652,11 @@ __global__ void k_nve_b(Program P, const Replica* __restrict__ reps, const int* 
   p.omega += dt_2 * project_torque(P, R, p);
   if (has_limit && has_theta && fabs(p.omega) * dt > theta_limit) p.omega = sign_of(p.omega) * theta_limit / dt;
   p.age += dt;
-  store_dyn(d, k, p);
+  store_dyn_moved<true, true>(d, k, p);
+  if (skin) {  // as in k_langevin_b
+    if (need_update(R, nl, k, p) && rebuild[r] == 0) atomicOr(&rebuild[r], 1);
+    if (!finite3(p.x, p.y, p.z)) atomicOr(status, ST_NONFINITE);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -281,6 +281,29 @@ def test_trajectory_nve(limits):
     assert_traj(e, o, ("x", "y", "vx", "vy", "nx", "ny", "omega"))
 
 
+@pytest.mark.parametrize("integ", [
+    ("langevin", {"gamma": "1", "seed": "7", "method": "baoab", "min_val": "0.5"}),
+    ("langevin", {"gamma": "1", "seed": "7", "method": "bbk", "min_val": "0.5"}),
+    ("nve", {"limit": "0.0001"}),
+])
+def test_reused_start_of_step_forces_are_the_recomputed_ones(integ):
+    # within a run, Langevin (BAOAB, BBK) and NVE on a periodic plane take the
+    # start-of-step forces from the previous step's own force pass; every run
+    # starts by recomputing them, so 120 one-step runs recompute every time:
+    # both must give the same bits
+    n = 1000
+    parts, L = plane_disks(n, 0.6, seed=12)
+    kw = dict(nlist=(2.5, 0.3), pairs=[("soft", {"k": "1.0"})], aligns=[("polar", {"J": "1.0"})], dt=1e-3,
+              integrators=[integ])
+    a, b = Engine(n), Engine(n)
+    sa, sb = drive(a, parts, (L, L, 10.0), **kw), drive(b, parts, (L, L, 10.0), **kw)
+    sa.run(119)
+    for _ in range(120):
+        sb.run(0)
+    for f in ("x", "y", "vx", "vy", "nx", "ny", "omega", "fx", "fy"):
+        np.testing.assert_array_equal(a.download(f), b.download(f), err_msg=f)
+
+
 def test_fire_matches_oracle():
     n = 600
     parts, L = plane_disks(n, 0.86, seed=11, bidisperse=(1.0, 1.4))
