@@ -686,26 +686,46 @@ __global__ void k_fire_a(Program P, const Replica* __restrict__ reps, const int*
   p.omega += dt_2 * project_torque(P, R, p);
   double dtheta = dt * p.omega;
   rotate_director(P, R, p, dtheta);
-  store_dyn(d, k, p);
+  store_dyn_moved<true, false>(d, k, p);
 }
 
-// per replica: fixed-order sums over its blocks, convergence test and the
-// dt / alpha control (96-147).  alpha_mix[r] keeps the alpha the mixing step
-// must use (the value before this update).
-__device__ void fire_control(const Program& P, const Replica& R, Clock& C, int r, int c, const double* part,
-                             const double* epart, int nblocks, int b0, int nb, int driver, double* alpha_mix) {
-  if (C.fire_conv_step >= 0 || C.halt) return;
-  const double* ip = R.integ_p[c];
+// The per-replica sums of the block partials, taken by all threads of the
+// replica's last block: thread t sums blocks b0 + t, b0 + t + BLOCK, ... in
+// order, then a fixed tree over the threads (the same bits for a replica run
+// alone or inside an ensemble).  Returns P, |F|^2, |v|^2, max |F_i|^2, E on
+// thread 0.
+__device__ void fire_sums(const Program& P, const double* part, const double* epart, int nblocks, int b0, int nb,
+                          double out[5]) {
+  __shared__ double red[5][BLOCK];
+  const int t = threadIdx.x;
   double Ps = 0.0, Fn = 0.0, Vn = 0.0, Fm = 0.0, E = 0.0;
-  for (int b = b0; b < b0 + nb; b++) {  // fixed order; other blocks' partials, so past L1
+  for (int b = b0 + t; b < b0 + nb; b += BLOCK) {  // other blocks' partials, so past L1
     Ps += __ldcg(part + b); Fn += __ldcg(part + (size_t)nblocks + b); Vn += __ldcg(part + (size_t)2 * nblocks + b);
     Fm = fmax(Fm, __ldcg(part + (size_t)3 * nblocks + b));
   }
-  for (int pc = 0; pc < P.npair; pc++) {
-    double s = 0.0;
-    for (int b = b0; b < b0 + nb; b++) s += __ldcg(epart + (size_t)pc * nblocks + b);
-    E += s;
+  for (int pc = 0; pc < P.npair; pc++)
+    for (int b = b0 + t; b < b0 + nb; b += BLOCK) E += __ldcg(epart + (size_t)pc * nblocks + b);
+  red[0][t] = Ps; red[1][t] = Fn; red[2][t] = Vn; red[3][t] = Fm; red[4][t] = E;
+  __syncthreads();
+  for (int h = BLOCK / 2; h > 0; h >>= 1) {
+    if (t < h) {
+      red[0][t] += red[0][t + h]; red[1][t] += red[1][t + h]; red[2][t] += red[2][t + h];
+      red[3][t] = fmax(red[3][t], red[3][t + h]); red[4][t] += red[4][t + h];
+    }
+    __syncthreads();
   }
+  if (t == 0)
+    for (int i = 0; i < 5; i++) out[i] = red[i][0];
+}
+
+// FIRE's convergence test and dt / alpha control on the replica's sums
+// (integrator_fire.cpp:96-147).  alpha_mix[r] keeps the alpha the mixing step
+// must use (the value before this update).
+__device__ void fire_control(const Replica& R, Clock& C, int r, int c, const double sums[5], int driver,
+                             double* alpha_mix) {
+  if (C.fire_conv_step >= 0 || C.halt) return;
+  const double* ip = R.integ_p[c];
+  double Ps = sums[0], Fn = sums[1], Vn = sums[2], Fm = sums[3], E = sums[4];
   Fn = sqrt(Fn);
   Vn = sqrt(Vn);
   C.fire_P = Ps; C.fire_F = Fn; C.fire_V = Vn; C.fire_E = E; C.fire_Fmax2 = Fm;
@@ -765,7 +785,7 @@ __global__ void k_fire_b(Program P, const Replica* __restrict__ reps, const int*
     v[2] = p.vx * p.vx + p.vy * p.vy + p.vz * p.vz;
     enforce_all(P, R, p);
     p.omega += dt_2 * project_torque(P, R, p);
-    store_dyn(d, k, p);
+    store_dyn_moved<true, false>(d, k, p);
   }
   block_reduce_store<3>(v, part, nblocks, bid_);
   // max reduction (exact in any order)
@@ -784,10 +804,14 @@ __global__ void k_fire_b(Program P, const Replica* __restrict__ reps, const int*
   __syncthreads();
   if (threadIdx.x == 0) amlast = atomicAdd(&fire_cnt[r], 1) == rep_nblk[r] - 1;
   __syncthreads();
-  if (amlast && threadIdx.x == 0) {
+  if (amlast) {  // block-uniform
     __threadfence();
-    fire_control(P, R, clk[r], r, c, part, epart, nblocks, rep_blk0[r], rep_nblk[r], driver, alpha_mix);
-    fire_cnt[r] = 0;
+    double sums[5];
+    fire_sums(P, part, epart, nblocks, rep_blk0[r], rep_nblk[r], sums);
+    if (threadIdx.x == 0) {
+      fire_control(R, clk[r], r, c, sums, driver, alpha_mix);
+      fire_cnt[r] = 0;
+    }
   }
 }
 
