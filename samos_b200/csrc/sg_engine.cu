@@ -1717,6 +1717,42 @@ static int run_batch(sg_system* s, int shape, int64_t K, bool needs_nl, int64_t*
   return rebuild_pending(s, shape, false, rebuild_ms);
 }
 
+// The generic fused step (k_step_brownian), K steps enqueued without a host
+// round trip like run_batch: the halted steps' kernels return at once and
+// write nothing, so the buffer holding the state is the one after the
+// executed steps' swaps; the host swapped once per enqueued step and undoes
+// the swaps of the halted ones.
+static int run_batch_generic(sg_system* s, int64_t K, bool needs_nl, int64_t* executed, double* rebuild_ms) {
+  CU(s, cudaMemsetAsync(s->exec_cnt, 0, sizeof(int), s->stream));
+  if (!s->e1_applied) {  // the first step's start-of-step enforce (samos.cpp:887-888)
+    k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, nullptr);
+    LAUNCH_CHECK(s);
+  }
+  for (int64_t i = 0; i < K; i++) {
+    int rc = step_fused(s, true, false);
+    if (rc) return rc;
+    k_tail_batch<<<1, 256, 0, s->stream>>>(s->prog, s->reps, s->clk, s->nrep, s->rebuild, s->exec_cnt);
+    LAUNCH_CHECK(s);
+  }
+  int ex = 0;
+  CU(s, cudaMemcpyAsync(&ex, s->exec_cnt, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  if (needs_nl)
+    CU(s, cudaMemcpyAsync(s->rebuild_h, s->rebuild, sizeof(int) * s->nrep, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  if (ex < 1 || ex > K) return fail(s, SG_ERR_CUDA, "batched stepping: inconsistent step count");
+  if ((K - ex) & 1) std::swap(s->cur, s->alt);
+  s->e1_applied = true;
+  *executed = ex;
+  s->since_rebuild += ex;
+  if (!needs_nl) return SG_OK;
+  bool any = false;
+  for (int r = 0; r < s->nrep; r++) any = any || s->rebuild_h[r];
+  if (!any) return SG_OK;
+  k_set_halt<<<(s->nrep + 127) / 128, 128, 0, s->stream>>>(s->clk, s->nrep, 0);
+  LAUNCH_CHECK(s);
+  return rebuild_pending(s, HOT_NONE, false, rebuild_ms);
+}
+
 // Blocks of the replicas whose minimiser has not converged (from clk_h).
 static int refresh_active(sg_system* s) {
   s->act_h.clear();
@@ -1842,6 +1878,13 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
     if (shape != HOT_NONE && t > 0 && !last && K > 1 && !driver && !s->profile && (!s->abp_on || s->tuned)) {
       int64_t ex = 0;
       if ((rc = run_batch(s, shape, K, needs_nl, &ex, &rebuild_ms))) return rc;
+      done += ex;
+      t += ex - 1;
+      continue;
+    }
+    if (shape == HOT_NONE && fused && !resc && t > 0 && !last && K > 1 && !s->profile) {
+      int64_t ex = 0;
+      if ((rc = run_batch_generic(s, K, needs_nl, &ex, &rebuild_ms))) return rc;
       done += ex;
       t += ex - 1;
       continue;

@@ -347,6 +347,7 @@ k_step_brownian(Program P, const Replica* __restrict__ reps, const int* __restri
                 double* epart, int nblocks, const uint8_t* __restrict__ gmask, const int* __restrict__ grank,
                 int slots) {
   const int r = my_replica(blk_rep);
+  if (clk[r].halt) return;  // batched stepping: a rebuild is pending, this step does not run
   const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
   double e[MAX_PAIR + MAX_ALIGN];

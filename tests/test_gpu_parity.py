@@ -587,3 +587,34 @@ def test_trajectory_rescaled_cylinder_and_tetrahedron(kind, shape, conf, box, pe
         np.testing.assert_allclose(np.hypot(x, y), 10.0 * f ** 21, rtol=1e-12)
     else:
         assert np.max(np.abs(tetra_value(np.stack([x, y, z], 1), 10.0 * f ** 20, 0.3))) < 2e-6
+
+
+@pytest.mark.parametrize("kind", ["torus", "vicsek"])
+def test_generic_batched_stepping_gives_the_stepwise_bits(kind):
+    # the generic fused kernel enqueues up to 32 steps per host round trip,
+    # a step that flags a rebuild halting the rest; profiling mode steps one
+    # at a time: both must give the same bits, through rebuilds
+    if kind == "torus":
+        shape = {"c": 20.0, "a": 8.0}
+        n, box = 1500, (70.0, 70.0, 30.0)
+        parts = surface_disks("torus", n, seed=27, **shape)
+        kw = dict(periodic=False, nlist=(2.4, 0.3), constraint=("torus", {k: repr(v) for k, v in shape.items()}),
+                  pairs=[("soft", {"k": "10"})], aligns=[("polar", {"J": "0.2"})], dt=1e-3,
+                  integrators=[("brownian", {"v0": "2.0", "nu": "0.1", "seed": "4"})])
+    else:
+        n = 2000
+        parts, L = plane_disks(n, 0.5, seed=28)
+        box = (L, L, 10.0)
+        kw = dict(nlist=(2.4, 0.3), pairs=[("soft", {"k": "10", "use_particle_radii": ""})],
+                  aligns=[("vicsek", {"rcut": "2.0"})], dt=1e-2,
+                  integrators=[("vicsek", {"v0": "0.5", "eta": "0.3", "mu": "0.1", "seed": "5"})])
+    out = []
+    for prof in (False, True):
+        e = Engine(n)
+        e.set_profiling(prof)
+        sim = drive(e, parts, box, **kw)
+        st = sim.run(400)
+        out.append((e, st))
+    assert out[0][1].nlist_builds > 2  # rebuilds inside the batches
+    for f in ("x", "y", "z", "nx", "ny", "nz", "vx", "vy", "vz", "fx", "fy", "age", "ix", "iy"):
+        np.testing.assert_array_equal(out[0][0].download(f), out[1][0].download(f), err_msg=f)
