@@ -1295,10 +1295,10 @@ static int step_unfused(sg_system* s, bool energy, bool driver) {
       s->forces_fresh = true;
       skin_done = skin_in != 0;
     } else if (ic.kind == INT_NVE) {
-      k_nve_a<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, c, fuse_enforce ? 1 : 0);
+      k_nve_a<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, c, fuse_enforce ? 1 : 0);
       LAUNCH_CHECK(s);
       if ((rc = launch_force(s, s->reps_h[0].integ_p[c][0], false, true, true, energy))) return rc;
-      k_nve_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, c, s->nl, s->rebuild,
+      k_nve_b<<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, c, s->nl, s->rebuild,
                                            s->status, skin_in);
       LAUNCH_CHECK(s);
       s->forces_fresh = true;
@@ -1753,6 +1753,37 @@ static int run_batch_generic(sg_system* s, int64_t K, bool needs_nl, int64_t* ex
   return rebuild_pending(s, HOT_NONE, false, rebuild_ms);
 }
 
+// Langevin / NVE steps with reusable forces, K enqueued without a host round
+// trip like run_batch: after the first step (which may recompute the forces
+// and enforce on its own, and is never halted) a step is the two integrator
+// halves around one force pass, each returning at once while a rebuild is
+// pending; the steps run in place, so nothing is left to fix afterwards.
+static int run_batch_unfused(sg_system* s, int64_t K, bool needs_nl, int64_t* executed, double* rebuild_ms) {
+  CU(s, cudaMemsetAsync(s->exec_cnt, 0, sizeof(int), s->stream));
+  for (int64_t i = 0; i < K; i++) {
+    int rc = step_unfused(s, false, false);
+    if (rc) return rc;
+    k_tail_batch<<<1, 256, 0, s->stream>>>(s->prog, s->reps, s->clk, s->nrep, s->rebuild, s->exec_cnt);
+    LAUNCH_CHECK(s);
+  }
+  int ex = 0;
+  CU(s, cudaMemcpyAsync(&ex, s->exec_cnt, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  if (needs_nl)
+    CU(s, cudaMemcpyAsync(s->rebuild_h, s->rebuild, sizeof(int) * s->nrep, cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  if (ex < 1 || ex > K) return fail(s, SG_ERR_CUDA, "batched stepping: inconsistent step count");
+  s->e1_applied = false;
+  *executed = ex;
+  s->since_rebuild += ex;
+  if (!needs_nl) return SG_OK;
+  bool any = false;
+  for (int r = 0; r < s->nrep; r++) any = any || s->rebuild_h[r];
+  if (!any) return SG_OK;
+  k_set_halt<<<(s->nrep + 127) / 128, 128, 0, s->stream>>>(s->clk, s->nrep, 0);
+  LAUNCH_CHECK(s);
+  return rebuild_pending(s, HOT_NONE, false, rebuild_ms);
+}
+
 // Blocks of the replicas whose minimiser has not converged (from clk_h).
 static int refresh_active(sg_system* s) {
   s->act_h.clear();
@@ -1878,6 +1909,13 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
     if (shape != HOT_NONE && t > 0 && !last && K > 1 && !driver && !s->profile && (!s->abp_on || s->tuned)) {
       int64_t ex = 0;
       if ((rc = run_batch(s, shape, K, needs_nl, &ex, &rebuild_ms))) return rc;
+      done += ex;
+      t += ex - 1;
+      continue;
+    }
+    if (!fused && !driver && !resc && t > 0 && !last && K > 1 && !s->profile && integ_forces_reusable(s)) {
+      int64_t ex = 0;
+      if ((rc = run_batch_unfused(s, K, needs_nl, &ex, &rebuild_ms))) return rc;
       done += ex;
       t += ex - 1;
       continue;

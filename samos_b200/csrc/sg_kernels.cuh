@@ -468,6 +468,7 @@ __global__ void k_set_halt(Clock* clk, int nrep, int v) {
 __global__ void k_langevin_a(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                              const Clock* __restrict__ clk, Dyn d, Stat st, int c, const double* Rn, int pre_enforce) {
   const int r = my_replica(blk_rep);
+  if (clk[r].halt) return;  // batched stepping: a rebuild is pending
   const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
@@ -528,6 +529,7 @@ __global__ void k_langevin_b(Program P, const Replica* __restrict__ reps, const 
                              const Clock* __restrict__ clk, Dyn d, Stat st, int c, double* Rn, NbList nl,
                              int* __restrict__ rebuild, int* __restrict__ status, int skin) {
   const int r = my_replica(blk_rep);
+  if (clk[r].halt) return;  // batched stepping: a rebuild is pending
   const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
@@ -597,9 +599,10 @@ __global__ void k_langevin_b(Program P, const Replica* __restrict__ reps, const 
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double sign_of(double x) { return x >= 0.0 ? 1.0 : -1.0; }  // integrator_nve.hpp:38
 
-__global__ void k_nve_a(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep, Dyn d, Stat st,
-                        int c, int pre_enforce) {
+__global__ void k_nve_a(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                        const Clock* __restrict__ clk, Dyn d, Stat st, int c, int pre_enforce) {
   const int r = my_replica(blk_rep);
+  if (clk[r].halt) return;  // batched stepping: a rebuild is pending
   const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
@@ -627,9 +630,11 @@ __global__ void k_nve_a(Program P, const Replica* __restrict__ reps, const int* 
   store_dyn_moved<true, false>(d, k, p);
 }
 
-__global__ void k_nve_b(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep, Dyn d, Stat st,
-                        int c, NbList nl, int* __restrict__ rebuild, int* __restrict__ status, int skin) {
+__global__ void k_nve_b(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
+                        const Clock* __restrict__ clk, Dyn d, Stat st, int c, NbList nl, int* __restrict__ rebuild,
+                        int* __restrict__ status, int skin) {
   const int r = my_replica(blk_rep);
+  if (clk[r].halt) return;  // batched stepping: a rebuild is pending
   const Replica& R = reps[r];
   const int k = blockIdx.x * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;

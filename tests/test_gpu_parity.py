@@ -618,3 +618,28 @@ def test_generic_batched_stepping_gives_the_stepwise_bits(kind):
     assert out[0][1].nlist_builds > 2  # rebuilds inside the batches
     for f in ("x", "y", "z", "nx", "ny", "nz", "vx", "vy", "vz", "fx", "fy", "age", "ix", "iy"):
         np.testing.assert_array_equal(out[0][0].download(f), out[1][0].download(f), err_msg=f)
+
+
+@pytest.mark.parametrize("integ", [
+    ("langevin", {"gamma": "1", "seed": "7", "method": "baoab", "min_val": "1.0"}),
+    ("langevin", {"gamma": "1", "seed": "7", "method": "bbk", "min_val": "1.0"}),
+    ("nve", {}),
+])
+def test_unfused_batched_stepping_gives_the_stepwise_bits(integ):
+    # Langevin / NVE steps with reused forces are enqueued up to 32 per host
+    # round trip (halted after a step that flags a rebuild); profiling mode
+    # steps one at a time: the same bits, through rebuilds
+    n = 1500
+    parts, L = plane_disks(n, 0.6, seed=29)
+    kw = dict(nlist=(2.5, 0.3), pairs=[("soft", {"k": "1.0"})], aligns=[("polar", {"J": "1.0"})], dt=2e-3,
+              integrators=[integ])
+    out = []
+    for prof in (False, True):
+        e = Engine(n)
+        e.set_profiling(prof)
+        sim = drive(e, parts, (L, L, 10.0), **kw)
+        st = sim.run(400)
+        out.append((e, st))
+    assert out[0][1].nlist_builds >= 1
+    for f in ("x", "y", "vx", "vy", "nx", "ny", "omega", "fx", "fy", "age", "ix", "iy"):
+        np.testing.assert_array_equal(out[0][0].download(f), out[1][0].download(f), err_msg=f)
