@@ -340,7 +340,7 @@ __global__ void k_force(Program P, const Replica* __restrict__ reps, const int* 
 // map order, skin test, then (apply_e1) the next step's start-of-step
 // Constrainer::enforce; result into the next buffer.
 template <bool ENERGY>
-__global__ void __launch_bounds__(BLOCK, 6)
+__global__ void __launch_bounds__(BLOCK, 8)
 k_step_brownian(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                 const Clock* __restrict__ clk, Dyn cur, Dyn nxt, Stat st, NbList nl,
                 int* __restrict__ rebuild, int* __restrict__ status, double dt_global, int apply_e1,
