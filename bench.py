@@ -123,34 +123,69 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle on a bounded sample of the same workload
+# CPU baseline: the reference's own hot-path sources (oracle/_ref, built from
+# the SAMoS tree with its Release flags) on a bounded sample of the same
+# workload; the C oracle when that build is absent
 # ---------------------------------------------------------------------------
+class _Quiet:
+    """Sends this process's stdout (fd 1) to /dev/null: the reference's
+    particle reader prints one line per input column."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(null, 1)
+        os.close(null)
+        return self
+
+    def __exit__(self, *a):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
 def _cpu_sample(args):
-    n, warm, steps, seed = args
-    from oracle.oracle import OracleSystem
+    n, warm, steps, seed, kind = args
     from samos_b200.plugins import Simulation
     parts, L = make_particles(n, seed)
-    o = OracleSystem(n)
-    sim = Simulation(o)
-    configure(sim, parts, L)
-    sim.run(warm - 1)
-    t0 = time.perf_counter()
-    o.run(steps - 1)
-    dt = time.perf_counter() - t0
+    if kind == "reference":
+        from oracle.refsrc import RefSimulation
+        with _Quiet():
+            sim = RefSimulation(fast=True)
+            configure(sim, parts, L)
+            sim.run(warm - 1)
+            t0 = time.perf_counter()
+            sim.run(steps - 1)
+            dt = time.perf_counter() - t0
+    else:
+        from oracle.oracle import OracleSystem
+        o = OracleSystem(n)
+        sim = Simulation(o)
+        configure(sim, parts, L)
+        sim.run(warm - 1)
+        t0 = time.perf_counter()
+        o.run(steps - 1)
+        dt = time.perf_counter() - t0
     return n * steps / dt
 
 
 def cpu_baseline(n=131_072, warm=100, steps=60, procs=1):
     import multiprocessing as mp
+    from oracle import refsrc
+    kind = "reference" if refsrc.available(fast=True) else "port"
     if procs == 1:
-        v = _cpu_sample((n, warm, steps, 11))
+        v = _cpu_sample((n, warm, steps, 11, kind))
     else:
         ctx = mp.get_context("spawn")
         with ctx.Pool(procs) as pool:
-            v = sum(pool.map(_cpu_sample, [(n, warm, steps, 11 + i) for i in range(procs)]))
-    return dict(value=v, unit=UNIT, cores=procs, kind="port",
+            v = sum(pool.map(_cpu_sample, [(n, warm, steps, 11 + i, kind) for i in range(procs)]))
+    what = ("SAMoS's own hot-path sources built with its Release flags (-O3 -funroll-loops -ffast-math, "
+            "x86-64-v3), driven through their classes" if kind == "reference" else
+            "the C oracle (a restatement of the reference's loops, -O2 strict IEEE)")
+    return dict(value=v, unit=UNIT, cores=procs, kind=kind,
                 sample=f"{n} particles of the same density/composition (box scaled), {warm} untimed + "
-                       f"{steps} timed steps per process, {procs} single-threaded process(es)")
+                       f"{steps} timed steps per process, {procs} single-threaded process(es); {what}")
 
 
 # ---------------------------------------------------------------------------

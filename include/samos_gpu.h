@@ -129,9 +129,10 @@ int  sg_add_external(sg_system* s, int kind, double alpha, const double* type_al
  *  peanut: a | hourglass: R | gaussian_bump: A | slab: z_lo | walls: l |
  *  tetrahedron: scale,
  *  plane: unlimited, maxiter, tol, rescale, rescale_steps, rescale_freq,
- *  torus: a | ellipsoid: b | peanut: b | hourglass: A | gaussian_bump: a |
+ *  torus: a | ellipsoid: b | peanut: b | hourglass: A | gaussian_bump: a^2 |
  *  slab: z_hi | tetrahedron: value, ellipsoid: c | hourglass: n |
- *  gaussian_bump: b} (9 values;
+ *  gaussian_bump: b^2} (9 values; the bump's widths squared, as its
+ *  constructor stores them, constraint_gaussian_bump.hpp;
  * gyroid takes none, its period is the box; a walls l beyond the box
  * is moved to its edge, constraint_plane_walls.hpp:64-71).  The implicit surfaces (torus and after)
  * project with Constraint::enforce's SHAKE iteration, constraint.cpp:40-87.
@@ -318,12 +319,14 @@ int  sg_mlp_apply(const sg_view* v, const double* box, const float* disp, int32_
  * (about 4 MB) that every GPU loading this library holds until exit.  Limits:
  * n <= SG_STATIC_MAX_PARTICLES and int(lx/(rcut+pad))*int(ly/(rcut+pad))*
  * int(lz/(rcut+pad)) <= SG_STATIC_MAX_CELLS, else SG_ERR_ARG.  A particle
- * with more than 64 neighbours on one side of its id gets NaN outputs.  The
- * call is asynchronous on `stream` (NULL = default stream).  The first call
- * on a device looks up the scratch address for that device
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls share the one scratch array: calls whose work overlaps on the
- * GPU (different streams or host threads) race and must be serialised.     */
+ * with more than 64 neighbours on one side of its id gets NaN outputs, and
+ * the call counts it: sg_compute_static_overflow reports the count of the
+ * last call.  The call is asynchronous on `stream` (NULL = default stream).
+ * The first call on a device (and in each further CUDA context a host makes
+ * on it) looks up the scratch address there (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  All calls share the one scratch
+ * array, which keeps the last call's contents: calls whose work overlaps on
+ * the GPU (different streams or host threads) race and must be serialised. */
 #define SG_STATIC_MAX_PARTICLES 65536
 #define SG_STATIC_MAX_CELLS 262144
 int  sg_compute_static(int n, double lx, double ly, double lz, int periodic, double rcut, double pad,
@@ -334,6 +337,11 @@ int  sg_compute_static(int n, double lx, double ly, double lz, int periodic, dou
                        double* fx_device, double* fy_device, double* fz_device,
                        double* tau_x_device, double* tau_y_device, double* tau_z_device, void* stream);
 int64_t sg_compute_static_scratch_bytes(void);
+/* Companion of sg_compute_static (no counterpart in the reference either):
+ * writes to *count (host memory) how many particles of the last
+ * sg_compute_static call on this device had too many neighbours (and NaN
+ * outputs); waits for `stream`.  Allocates nothing.                        */
+int  sg_compute_static_overflow(int* count, void* stream);
 
 #ifdef __cplusplus
 }

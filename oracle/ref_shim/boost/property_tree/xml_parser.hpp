@@ -1,0 +1,3 @@
+// Stand-in: the writers live in ptree.hpp (oracle build test infrastructure).
+#pragma once
+#include "ptree.hpp"

@@ -214,7 +214,7 @@ typedef struct {
   int kind;
   double zpos; int unlimited;      /* plane */
   double r;                        /* sphere; cylinder r; torus c; ellipsoid a; peanut a; hourglass R; bump A */
-  double b2, b3;                   /* torus a; ellipsoid b, c; peanut b; hourglass A, n; bump a, b */
+  double b2, b3;                   /* torus a; ellipsoid b, c; peanut b; hourglass A, n; bump a^2, b^2 */
   int max_iter; double tol;
   double rescale; int rescale_steps, rescale_freq; double scale;
 } or_cons;

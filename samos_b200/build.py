@@ -20,9 +20,14 @@ ENGINE_SO = os.path.join(PKG, "libsamos_gpu.so")
 
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-# -fmad=false: no a*b+c contraction, so device arithmetic follows the
-# reference's evaluation order term by term.
-NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-shared"]
+NVCC_COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC"]
+# The FP64 particle path (engine, allocation-free entry point) is compiled
+# with -fmad=false: no a*b+c contraction, so device arithmetic follows the
+# reference's evaluation order term by term.  The FP32/BF16 network kernels of
+# the learned warm start have no bit-parity requirement and keep FMA.
+PARITY_UNITS = ("sg_engine.cu", "sg_static.cu")
+FREE_UNITS = ("sg_ml.cu",)
+OBJ_DIR = os.path.join(PKG, "_build")
 
 
 def _run(cmd: list[str]) -> None:
@@ -44,9 +49,19 @@ def _sources(d: str, exts: tuple[str, ...]) -> list[str]:
 def build_engine(force: bool = False) -> str:
     srcs = _sources(CSRC, (".cu", ".cuh")) + [os.path.join(INCLUDE, "samos_gpu.h")]
     if force or _stale(ENGINE_SO, srcs):
-        _run([NVCC, *NVCC_FLAGS, *ARCH, f"-I{INCLUDE}", "-o", ENGINE_SO,
-              os.path.join(CSRC, "sg_engine.cu"), os.path.join(CSRC, "sg_static.cu"),
-              os.path.join(CSRC, "sg_ml.cu")])
+        os.makedirs(OBJ_DIR, exist_ok=True)
+        objs, procs = [], []
+        for unit in PARITY_UNITS + FREE_UNITS:  # independent units, compiled side by side
+            obj = os.path.join(OBJ_DIR, unit.replace(".cu", ".o"))
+            fmad = ["-fmad=false"] if unit in PARITY_UNITS else []
+            cmd = [NVCC, *NVCC_COMMON, *fmad, *ARCH, f"-I{INCLUDE}", "-c", os.path.join(CSRC, unit), "-o", obj]
+            print("+", " ".join(cmd), file=sys.stderr)
+            procs.append((cmd, subprocess.Popen(cmd)))
+            objs.append(obj)
+        for cmd, p in procs:
+            if p.wait() != 0:
+                raise subprocess.CalledProcessError(p.returncode, cmd)
+        _run([NVCC, "-shared", *ARCH, "-o", ENGINE_SO, *objs])
     return ENGINE_SO
 
 

@@ -17,9 +17,12 @@
 // so results match sg_compute bit for bit.
 #include "samos_gpu.h"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+
+#include <mutex>
 
 namespace {
 
@@ -27,16 +30,28 @@ constexpr int kMaxParticles = SG_STATIC_MAX_PARTICLES;
 constexpr int kMaxCells = SG_STATIC_MAX_CELLS;
 constexpr int kScanTile = 1024;
 constexpr int kMaxBlocks = (kMaxCells + kScanTile - 1) / kScanTile;
-// int32 slots: pcell, tmp, slots (per particle); cnt, start, fill (per cell); block sums
-constexpr size_t kScratchInts = (size_t)3 * kMaxParticles + (size_t)3 * kMaxCells + kMaxBlocks;
+// int32 slots: pcell, tmp, slots (per particle); cnt, start, fill (per cell); block sums;
+// one word counting the particles of the last call that had too many neighbours
+constexpr size_t kScratchInts = (size_t)3 * kMaxParticles + (size_t)3 * kMaxCells + kMaxBlocks + 1;
 constexpr size_t kScratchBytes = kScratchInts * sizeof(int);
 
 // The scratch.  Host code must not use its name as an address: the address
-// is obtained per device with cudaGetSymbolAddress (see scratch_on_device).
+// is obtained per device and context with cudaGetSymbolAddress (see
+// scratch_on_device).
 static __device__ __align__(256) int g_scratch[kScratchInts];
 
-constexpr int kMaxDevices = 64;
-int* g_scratch_ptr[kMaxDevices] = {nullptr};
+// Scratch addresses already looked up, keyed by device and CUDA context: an
+// address is valid only in the context it was looked up in, and a host that
+// creates its own driver-API context, or resets the device, gets a new one.
+constexpr int kMaxCached = 64;
+struct CachedAddress {
+  int device;
+  CUcontext context;
+  int* address;
+};
+CachedAddress g_cache[kMaxCached];
+int g_cached = 0;
+std::mutex g_cache_mutex;
 
 struct Geo {
   int n, cnx, cny, cnz, use_cell, periodic;
@@ -141,7 +156,8 @@ __global__ void k_st_forces(Geo G, const double* __restrict__ x, const double* _
                             const double* __restrict__ rad, const int* __restrict__ start,
                             const int* __restrict__ cnt, const int* __restrict__ slots, double k_soft,
                             double a_soft, int use_radii, int align_kind, double Jeff, double rc,
-                            double* fx, double* fy, double* fz, double* tx, double* ty, double* tz) {
+                            double* fx, double* fy, double* fz, double* tx, double* ty, double* tz,
+                            int* overflow) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= G.n) return;
   const double xi = x[i], yi = y[i], zi = z[i];
@@ -184,6 +200,7 @@ __global__ void k_st_forces(Geo G, const double* __restrict__ x, const double* _
   if (over) {  // more than kLocal neighbours on one side: flag this particle
     const double bad = nan("");
     fx[i] = bad; fy[i] = bad; fz[i] = bad; tx[i] = bad; ty[i] = bad; tz[i] = bad;
+    atomicAdd(overflow, 1);
     return;
   }
   for (int p = 1; p < nlo; p++) {  // stable insertion sort by id
@@ -228,18 +245,49 @@ __global__ void k_st_forces(Geo G, const double* __restrict__ x, const double* _
   tx[i] = Tx; ty[i] = Ty; tz[i] = Tz;
 }
 
-// Set-up once per device, with that device current: the host-side name of
-// g_scratch is a stand-in, not a device address, so the address is looked up
-// and cached here.
+// The CUDA context current on this host thread (driver entry point fetched
+// through the runtime, so the library does not link the driver library).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+
+CUcontext current_context() {
+  static CtxGetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(f);
+  }();
+  CUcontext c = nullptr;
+  if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+  return c;
+}
+
+// Set-up once per device and context, with that device current: the
+// host-side name of g_scratch is a stand-in, not a device address, so the
+// address is looked up here (cudaGetSymbolAddress) and cached.  Without a
+// context handle to key on, the address is looked up on every call.
 int scratch_on_device(int** out) {
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SG_ERR_CUDA;
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || p == nullptr) return SG_ERR_CUDA;
-    g_scratch_ptr[dev] = static_cast<int*>(p);
+  if (cudaGetDevice(&dev) != cudaSuccess) return SG_ERR_CUDA;
+  // null until the runtime has made a context current on this thread (the
+  // lookup below does): such a call looks the address up without caching it
+  const CUcontext ctx = current_context();
+  std::lock_guard<std::mutex> lock(g_cache_mutex);
+  if (ctx)
+    for (int k = 0; k < g_cached; k++)
+      if (g_cache[k].device == dev && g_cache[k].context == ctx) {
+        *out = g_cache[k].address;
+        return SG_OK;
+      }
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || p == nullptr) return SG_ERR_CUDA;
+  if (ctx) {
+    // a full table starts over: addresses of earlier contexts are then looked up again
+    if (g_cached == kMaxCached) g_cached = 0;
+    g_cache[g_cached++] = CachedAddress{dev, ctx, static_cast<int*>(p)};
   }
-  *out = g_scratch_ptr[dev];
+  *out = static_cast<int*>(p);
   return SG_OK;
 }
 
@@ -258,6 +306,10 @@ extern "C" int sg_compute_static(int n, double lx, double ly, double lz, int per
   if (!x || !y || !z || !nx || !ny || !nz || !radius || !fx || !fy || !fz || !tau_x || !tau_y || !tau_z)
     return SG_ERR_ARG;
   const double cut = rcut + pad;
+  // the cell counts are cast to int below: reject any side too long for the
+  // scratch's cells first (this also rejects infinite and NaN sizes)
+  if (!(lx / cut <= (double)kMaxCells && ly / cut <= (double)kMaxCells && lz / cut <= (double)kMaxCells))
+    return SG_ERR_ARG;
   Geo G;
   G.n = n;
   G.periodic = periodic ? 1 : 0;
@@ -282,11 +334,13 @@ extern "C" int sg_compute_static(int n, double lx, double ly, double lz, int per
   int* start = cnt + kMaxCells;
   int* fill = start + kMaxCells;
   int* bsum = fill + kMaxCells;
+  int* overflow = bsum + kMaxBlocks;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int m = (int)ncell;
   // every call reuses the same scratch: clear what has to start at zero
   if (cudaMemsetAsync(cnt, 0, sizeof(int) * m, st) != cudaSuccess) return SG_ERR_CUDA;
   if (cudaMemsetAsync(fill, 0, sizeof(int) * m, st) != cudaSuccess) return SG_ERR_CUDA;
+  if (cudaMemsetAsync(overflow, 0, sizeof(int), st) != cudaSuccess) return SG_ERR_CUDA;
   const int tb = 128, nbk = (n + tb - 1) / tb, nsc = (m + kScanTile - 1) / kScanTile;
   k_st_bin<<<nbk, tb, 0, st>>>(G, x, y, z, pcell, cnt);
   k_st_scan_blocks<<<nsc, kScanTile, 0, st>>>(cnt, m, bsum);
@@ -296,8 +350,19 @@ extern "C" int sg_compute_static(int n, double lx, double ly, double lz, int per
   const double Jeff = align_kind == SG_ALIGN_NEMATIC ? 2.0 * J : J;  // pair_nematic_aligner.cpp:37
   k_st_forces<<<nbk, tb, 0, st>>>(G, x, y, z, nx, ny, nz, radius, start, cnt, slots, k_soft, a_soft,
                                   use_particle_radii, align_kind, Jeff, align_rcut, fx, fy, fz, tau_x, tau_y,
-                                  tau_z);
+                                  tau_z, overflow);
   return cudaGetLastError() == cudaSuccess ? SG_OK : SG_ERR_CUDA;
 }
 
 extern "C" int64_t sg_compute_static_scratch_bytes(void) { return (int64_t)kScratchBytes; }
+
+extern "C" int sg_compute_static_overflow(int* count, void* stream) {
+  if (!count) return SG_ERR_ARG;
+  int* base = nullptr;
+  int rc = scratch_on_device(&base);
+  if (rc != SG_OK) return rc;
+  const int* overflow = base + (kScratchInts - 1);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemcpyAsync(count, overflow, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return SG_ERR_CUDA;
+  return cudaStreamSynchronize(st) == cudaSuccess ? SG_OK : SG_ERR_CUDA;
+}

@@ -114,6 +114,7 @@ def load() -> C.CDLL:
         "sg_get_variant": (I, [P]),
         "sg_compute_static": (I, [I, D, D, D, I, D, D] + [P] * 7 + [D, D, I, I, D, D] + [P] * 6 + [P]),
         "sg_compute_static_scratch_bytes": (I64, []),
+        "sg_compute_static_overflow": (I, [C.POINTER(C.c_int), P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -209,8 +209,10 @@ ConstraintSpec resolve_constraint(const std::string& name, const Params& p) {
   } else if (name == "hourglass") {  // constraint_hourglass.hpp:64-102 (A checked only when given)
     first = get(p, "R", 10.0); second = get(p, "A", 1.0); third = get(p, "n", 1.0);
     if (has(p, "A") && second > first) throw HostError("Hourglass constraint. Amplitude has to be smaller than the radius.");
-  } else if (name == "gaussian_bump") {  // constraint_gaussian_bump.hpp
+  } else if (name == "gaussian_bump") {  // constraint_gaussian_bump.hpp: the widths a, b are stored squared
     first = get(p, "A", 1.0); second = get(p, "a", 1.0); third = get(p, "b", 1.0);
+    second *= second;
+    third *= third;
   } else if (name == "slab") {  // constraint_slab.hpp:56-78
     first = get(p, "z_lo", 0.0); second = get(p, "z_hi", 1.0);
   } else if (name == "walls") {  // constraint_plane_walls.hpp:56-74 (the engine moves l to the box edge)

@@ -228,8 +228,9 @@ def resolve_constraint(name: str, params: dict) -> tuple[int, list[float]]:
         first, second, third, unlimited = _f(params, "R", 10.0), _f(params, "A", 1.0), _f(params, "n", 1.0), 0.0
         if "A" in params and second > first:
             raise PluginError("Hourglass constraint. Amplitude has to be smaller than the radius.")
-    elif name == "gaussian_bump":  # constraint_gaussian_bump.hpp: A, a, b (1)
+    elif name == "gaussian_bump":  # constraint_gaussian_bump.hpp: A (1); widths a, b stored squared (1 if absent)
         first, second, third, unlimited = _f(params, "A", 1.0), _f(params, "a", 1.0), _f(params, "b", 1.0), 0.0
+        second, third = second * second, third * third
     elif name == "slab":  # constraint_slab.hpp:56-78: z_lo (0), z_hi (1)
         first, second, unlimited = _f(params, "z_lo", 0.0), _f(params, "z_hi", 1.0), 0.0
     elif name == "walls":  # constraint_plane_walls.hpp:56-74: l (1; beyond the box: the box edge)

@@ -124,7 +124,7 @@ def surface_disks(kind, n, seed=1, **shape):
     elif kind == "gaussian_bump":
         A, a, b, L = shape["A"], shape["a"], shape["b"], shape["L"]
         x, y = rng.uniform(-0.45 * L, 0.45 * L, n), rng.uniform(-0.45 * L, 0.45 * L, n)
-        z = A * np.exp(-x * x / a - y * y / b)
+        z = A * np.exp(-x * x / (a * a) - y * y / (b * b))
     elif kind == "tetrahedron":  # rays from the origin, bisected to the level (inside it above, outside below)
         s, val = shape["scale"], shape["value"]
         w = rng.normal(size=(n, 3))

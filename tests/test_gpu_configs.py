@@ -2,10 +2,12 @@
 the benchmark and the parity requirements name:
 
 * the 65,536-particle sphere (polar, v0 = 1, nu = 0.05, dt = 1e-3), compared
-  step by step for the first steps and then at intervals (shared noise);
+  step by step for the first steps and then at intervals (shared noise), and
+  after its 1,000th step;
 * the 4,194,304-disk headline system (soft + nematic on the particle radii,
   nlist 2.8 + 0.3): neighbour pairs and the first force/torque evaluation
-  compared in full, bit for bit;
+  compared in full, bit for bit, and a 64-step trajectory through list
+  rebuilds with the step-kernel variant the benchmark's autotuner settles on;
 * the 2,000-disk small case (soft + polar, v0 = 0.5, nu = 0.1, dt = 1e-3) run
   for its full 10,001 steps, with the drift between the two codes recorded
   against the 1000-step bar.
@@ -47,6 +49,51 @@ def test_sphere_65536_step_by_step():
             assert err <= 1e-9, f"step {c}: {f} differs by {err}"
     r = np.sqrt(e.download("x") ** 2 + e.download("y") ** 2 + e.download("z") ** 2)
     assert np.allclose(r, R, rtol=1e-13)
+
+
+def test_sphere_65536_after_1000_steps():
+    n = 65536
+    parts, R = sphere_disks(n, seed=23)
+    e, o = Engine(n), OracleSystem(n)
+    se, so = sphere_program(e, parts, R), sphere_program(o, parts, R)
+    st = se.run(999)
+    so.run(999)
+    for f in ("x", "y", "z", "nx", "ny", "nz"):
+        err = float(np.max(np.abs(e.download(f) - o.download(f))))
+        assert err <= 1e-9, f"step 1000: {f} differs by {err}"
+    # the oracle counts the build at `nlist` too; the engine's run statistics
+    # count the builds made inside the run (the first one included when the
+    # list is first built there)
+    assert st.nlist_builds in (o.nlist_builds() - 1, o.nlist_builds())
+
+
+def headline_program(b, parts, L):
+    return drive(b, parts, (L, L, 10.0), nlist=(2.8, 0.3), pairs=[("soft", {"k": "10", "use_particle_radii": ""})],
+                 aligns=[("nematic", {"J": "0.5"})], dt=5e-4,
+                 integrators=[("brownian", {"v0": "0.3", "nu": "0.1", "mu": "1", "mur": "1", "seed": "5"})])
+
+
+@pytest.mark.parametrize("variant", [22, -1])
+def test_headline_4M_trajectory_through_rebuilds(variant):
+    # the benchmark's system and step kernel (variant 22, the by-value
+    # pipelined kernel its autotuner settles on; -1 lets the autotuner time
+    # and pick), 64 steps through the first list rebuilds, against the oracle
+    n = 4194304
+    parts, L = plane_disks(n, 0.8, seed=1, bidisperse=(1.0, 1.4))
+    e, o = Engine(n), OracleSystem(n)
+    e.set_variant(variant)
+    se, so = headline_program(e, parts, L), headline_program(o, parts, L)
+    st = se.run(63)
+    so.run(63)
+    assert o.nlist_builds() >= 2  # the build at `nlist` plus at least one rebuild
+    assert st.nlist_builds in (o.nlist_builds() - 1, o.nlist_builds())
+    if variant == 22:
+        assert e.variant() == 22
+    for f in ("x", "y", "nx", "ny", "vx", "vy"):
+        err = float(np.max(np.abs(e.download(f) - o.download(f))))
+        assert err <= 1e-9, f"{f} differs by {err}"
+    for f in ("ix", "iy"):
+        np.testing.assert_array_equal(e.download(f), o.download(f), err_msg=f)
 
 
 def test_headline_4M_pairs_and_forces_bitexact():

@@ -274,7 +274,8 @@ def implicit_np(kind, conf, box, x, y, z):
         g = x * x + y * y - zf * zf
         G = np.stack([2 * x, 2 * y, -4 * A * nn * np.pi * np.cos(2 * nn * np.pi * z / lz) * zf / lz], 1)
     elif kind == "gaussian_bump":
-        A, a, b = conf["A"], conf["a"], conf["b"]
+        # the constructor stores the widths squared (constraint_gaussian_bump.hpp)
+        A, a, b = conf["A"], conf["a"] ** 2, conf["b"] ** 2
         f = np.exp(-x * x / a - y * y / b)
         g = A * f - z
         G = np.stack([-2 * A * x * f / a, -2 * A * y * f / b, -np.ones_like(z)], 1)
@@ -318,7 +319,7 @@ def test_implicit_surface_parameters_checked_like_the_reference():
     kind, p = resolve_constraint("hourglass", {"R": "0.5"})  # A defaults to 1, unchecked
     assert p[0] == 0.5 and p[7] == 1.0 and p[8] == 1.0
     kind, p = resolve_constraint("gaussian_bump", {"A": "2", "a": "3", "b": "4"})
-    assert (p[0], p[7], p[8]) == (2.0, 3.0, 4.0)
+    assert (p[0], p[7], p[8]) == (2.0, 9.0, 16.0)  # widths squared (constraint_gaussian_bump.hpp)
     o = OracleSystem(4)
     with pytest.raises(ValueError):
         o.add_constraint(E.CONSTRAINT["peanut"], [5.0, 0, 100, 1e-6, 1, 1000, 10, 4.0, 0.0])
