@@ -585,6 +585,7 @@ def main():
     pst = eng.run(min(args.steps, 200) - 1)
     eng.set_profiling(False)
     k_ms = pst.step_kernel_ms / max(1, pst.step_kernels)
+    rebuild_ms = pst.rebuild_ms / pst.nlist_builds if pst.nlist_builds else None
     achieved = n_part * BYTES_PER_PARTICLE_STEP / (k_ms * 1e-3) / 1e9
     peaks = {}
     try:
@@ -643,6 +644,7 @@ def main():
             roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
                           traffic=traffic, kernel=kernel, kernel_ms=k_ms,
                           algorithmic_bytes_per_particle_step=BYTES_PER_PARTICLE_STEP,
+                          list_build_ms=rebuild_ms, list_builds_profiled=int(pst.nlist_builds),
                           peak_source="MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"),
             e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
                      steps=e2e_steps, finite=bool(finite)),

@@ -252,10 +252,24 @@ int  sg_set_path(sg_system* s, int path);
 int  sg_set_variant(sg_system* s, int variant);
 int  sg_get_variant(const sg_system* s);
 /* Neighbour-list build kernel: 0 = automatic (lanes of a team share one
- * particle's 27-cell stencil when fewer than 2^16 particles are rebuilt,
- * one thread per particle otherwise), 1 = always one thread per particle,
- * 2 = always teams.  All build the same lists.  No reference counterpart.   */
+ * particle's 27-cell stencil when fewer than 2^16 particles are rebuilt;
+ * from 2^16 on, cell tiles staged in shared memory when every rebuilt
+ * replica is quasi-2-D -- cell path, at least 3 cells along x and y, exactly
+ * 3 along z -- else one thread per particle), 1 = always one thread per
+ * particle, 2 = always teams, 3 = cell tiles wherever eligible (one thread
+ * per particle elsewhere).  All build the same lists.  No reference
+ * counterpart.                                                              */
 int  sg_set_build(sg_system* s, int mode);
+/* Order of FIRE's sums P = sum v.F, |F|^2 and |v|^2 (integrator_fire.cpp:
+ * 79-94), whose values steer dt, alpha and the velocity mixing:
+ * 0 (default, throughput) = a fixed tree over blocks, deterministic and the
+ * same for a replica alone or in an ensemble, but not the reference's order,
+ * so iteration counts can differ from the reference's by a few percent;
+ * 1 (parity) = one particle at a time in particle-id order, the reference's
+ * order, so with fmax_tolerance set FIRE takes the reference's iterations
+ * bit for bit (the energy in the reference's own convergence test stays a
+ * tree sum).  Costs a sequential pass over each replica per iteration.      */
+int  sg_set_fire_order(sg_system* s, int ordered);
 
 /* ---- device view (for kernels that work on the engine's state) -----------
  * No reference counterpart.  Device pointers into the handle's current

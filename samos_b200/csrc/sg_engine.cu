@@ -88,6 +88,10 @@ struct sg_system {
   int64_t since_rebuild = 0, last_gap = 8;  // batch length follows the steps between rebuilds
   int* rebuild_h = nullptr;  // pinned
   double *epart = nullptr, *fire_part = nullptr, *alpha_mix = nullptr, *Rn = nullptr;
+  // FIRE sums in the reference's particle order (sg_set_fire_order): the
+  // per-particle terms by replica offset + id, 3 arrays of `slots` doubles
+  int fire_ordered = 0;
+  double* fire_terms = nullptr;
   double dt_global = 0.0;
   bool e1_applied = false;
   bool forces_fresh = false;  // forces equal those the next start-of-step pass would compute
@@ -125,7 +129,11 @@ struct sg_system {
   struct Rescale { double rescale = 1.0, scale = 1.0; int steps = 1000, freq = 10; };
   std::vector<Rescale> cons_rescale;
   int64_t rescaled_at = -1;  // global step whose rescale sg_begin_step already applied
-  int build_mode = 0;        // list build: 0 automatic, 1 one thread per particle, 2 teams of TEAM lanes
+  int build_mode = 0;        // list build: 0 automatic, 1 one thread per particle, 2 teams of TEAM lanes, 3 cell tiles
+  // cell-tile build: the tiles of the flagged replicas (rebuilt when the flagged set changes)
+  TileRef* tiles = nullptr;
+  int tiles_cap = 0, ntiles = 0;
+  std::vector<int> tiles_for;
   bool tile_valid = false;
   // ordered variants: per-block lane order by neighbour count (k_lane_order)
   uint8_t* lane_order = nullptr;
@@ -572,6 +580,45 @@ static const int* blist_of(const sg_system* s) { return s->nblist == s->nblocks 
 // cost more than its shorter chains save (4,194,304 disks: 2.8 vs 1.3 ms).
 static constexpr int64_t kTeamBelow = 1 << 16;
 
+// The cell-tile build (k_rb_build_tile) applies when every flagged replica is
+// quasi-2-D on the cell path (tile_eligible) and, in automatic mode, when at
+// least kTeamBelow particles are rebuilt.
+static bool use_tiles(const sg_system* s, int64_t nflag) {
+  if (!(s->build_mode == 3 || (s->build_mode == 0 && nflag >= kTeamBelow))) return false;
+  for (int r = 0; r < s->nrep; r++) {
+    if (!s->rebuild_h[r]) continue;
+    const Replica& R = s->reps_h[r];
+    if (!tile_eligible(R.use_cell, R.cnx, R.cny, R.cnz)) return false;
+  }
+  return true;
+}
+
+// Tile list of the flagged replicas: per replica, per a, runs of TILE_B
+// columns along b.  Reused while the flagged set is unchanged.
+static int prepare_tiles(sg_system* s) {
+  std::vector<int> flagged;
+  for (int r = 0; r < s->nrep; r++)
+    if (s->rebuild_h[r]) flagged.push_back(r);
+  if (flagged == s->tiles_for && s->tiles) return SG_OK;
+  std::vector<TileRef> t;
+  for (int r : flagged) {
+    const Replica& R = s->reps_h[r];
+    for (int a = 0; a < R.cnx; a++)
+      for (int b0 = 0; b0 < R.cny; b0 += TILE_B) t.push_back(TileRef{r, a, b0, std::min(TILE_B, R.cny - b0)});
+  }
+  if ((int)t.size() > s->tiles_cap) {
+    s->mem.release(s->tiles);
+    s->tiles = s->mem.alloc<TileRef>(t.size());
+    if (!s->tiles) { s->mem.err = cudaSuccess; s->tiles_cap = 0; return fail(s, SG_ERR_NOMEM, "tile list"); }
+    s->tiles_cap = (int)t.size();
+  }
+  CU(s, cudaMemcpyAsync(s->tiles, t.data(), sizeof(TileRef) * t.size(), cudaMemcpyHostToDevice, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));  // t is freed on return
+  s->ntiles = (int)t.size();
+  s->tiles_for = flagged;
+  return SG_OK;
+}
+
 static int rebuild_flagged(sg_system* s, bool* sorted, bool blist_ready = false) {
   s->forces_fresh = false;
   bool any_sort = false;
@@ -633,8 +680,14 @@ static int rebuild_flagged(sg_system* s, bool* sorted, bool blist_ready = false)
       LAUNCH_CHECK(s);
     }
     // a rebuild of few particles is latency bound: split each particle's
-    // stencil over a team of lanes; a large one is issue bound: one thread each
-    if (s->build_mode == 2 || (s->build_mode == 0 && nflag < kTeamBelow))
+    // stencil over a team of lanes; a large quasi-2-D one stages cell tiles in
+    // shared memory; any other large one: one thread per particle
+    if (use_tiles(s, nflag)) {
+      int trc = prepare_tiles(s);
+      if (trc) return trc;
+      k_rb_build_tile<<<s->ntiles, BLOCK, 0, s->stream>>>(s->reps, s->tiles, s->rebuild, s->cur, s->st, s->nl,
+                                                          s->perm, s->cell_start, s->cell_cnt, s->bstatus, s->maxnb);
+    } else if (s->build_mode == 2 || (s->build_mode == 0 && nflag < kTeamBelow))
       k_rb_build_team<<<ng * TEAM_SUB, TEAM * TEAM_PARTS, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur,
                                                                           s->st, s->nl, s->perm, s->cell_start,
                                                                           s->cell_cnt, s->bstatus, s->maxnb, bl);
@@ -1309,9 +1362,13 @@ static int step_unfused(sg_system* s, bool energy, bool driver) {
       LAUNCH_CHECK(s);
       if ((rc = launch_force(s, 0.0, true, true, true, true, na, al))) return rc;
       s->forces_fresh = true;
+      if (s->fire_ordered && !s->fire_terms) {
+        s->fire_terms = s->mem.alloc<double>((size_t)3 * s->slots);
+        if (!s->fire_terms) { s->mem.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "FIRE term arrays"); }
+      }
       k_fire_b<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->st, s->fire_part, nb,
                                             s->rep_blk0, s->rep_nblk, s->epart, c, driver ? 1 : 0, s->alpha_mix,
-                                            s->fire_cnt, al);
+                                            s->fire_cnt, al, s->fire_ordered ? s->fire_terms : nullptr, s->slots);
       LAUNCH_CHECK(s);
       k_fire_d<<<na, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alpha_mix, s->nl,
                                             s->has_nlist ? 1 : 0, s->rebuild, s->status, al);
@@ -1845,7 +1902,13 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
   if (!s || steps < 0) return SG_ERR_ARG;
   if (s->prog.ninteg == 0) return fail(s, SG_ERR_STATE, "Integrator has not been defined");
   if (s->prog.ncons == 0) return fail(s, SG_ERR_STATE, "Constraint has not been defined");
-  if (!(s->dt_global > 0.0)) return fail(s, SG_ERR_STATE, "timestep has not been set");
+  // Every integrator has its own step (checked when it is added); the global
+  // one defaults to 0 as in System (system.cpp:71) and is read only by the
+  // phase-in factor, age / dt (pair_soft_potential.cpp:60-76): refuse that
+  // division by a zero step, which the reference leaves undefined.
+  for (int c = 0; c < s->prog.npair; c++)
+    if (s->prog.pair[c].phase_in && !(s->dt_global > 0.0))
+      return fail(s, SG_ERR_STATE, "timestep has not been set (phase_in divides the age by it)");
   const bool needs_nl = (s->prog.npair + s->prog.nalign) > 0;
   if (needs_nl && !s->has_nlist) return fail(s, SG_ERR_STATE, "pair terms need a neighbour list");
   if (!s->nl.nb) { int rc = nlist_alloc(s, 1); if (rc) return rc; }
@@ -2087,8 +2150,14 @@ int sg_set_variant(sg_system* s, int variant) {
 
 int sg_get_variant(const sg_system* s) { return s ? (s->tuned ? s->abp_variant : -1) : SG_ERR_ARG; }
 
+int sg_set_fire_order(sg_system* s, int ordered) {
+  if (!s || ordered < 0 || ordered > 1) return SG_ERR_ARG;
+  s->fire_ordered = ordered;
+  return SG_OK;
+}
+
 int sg_set_build(sg_system* s, int mode) {
-  if (!s || mode < 0 || mode > 2) return SG_ERR_ARG;
+  if (!s || mode < 0 || mode > 3) return SG_ERR_ARG;
   s->build_mode = mode;
   return SG_OK;
 }

@@ -766,10 +766,35 @@ __device__ void fire_control(const Replica& R, Clock& C, int r, int c, const dou
 // convergence test and the dt / alpha control (96-147) of fire_control: the
 // blocks of a replica count themselves done on fire_cnt[r] after their
 // partials are visible, so the last one sees them all.
+// Reference-order sums (the parity mode): P, |F|^2 and |v|^2 accumulated one
+// particle at a time in particle-id order, as the reference's loop over the
+// group does (integrator_fire.cpp:79-94), from the per-particle terms in
+// `terms` (three arrays of `stride` doubles, indexed by replica offset + id).
+// One warp: 32 terms loaded at a time, then added in order through shuffles,
+// so every lane holds the same sequential sums.
+__device__ void fire_ordered_sums(const double* __restrict__ terms, int stride, int off, int n, double out[3]) {
+  const int lane = threadIdx.x & 31;
+  double sP = 0.0, sF = 0.0, sV = 0.0;
+  for (int base = 0; base < n; base += 32) {
+    const int i = base + lane;
+    const double a = i < n ? __ldcg(terms + off + i) : 0.0;
+    const double b = i < n ? __ldcg(terms + (size_t)stride + off + i) : 0.0;
+    const double v = i < n ? __ldcg(terms + (size_t)2 * stride + off + i) : 0.0;
+    const int m = n - base < 32 ? n - base : 32;
+    for (int u = 0; u < m; u++) {
+      sP += __shfl_sync(0xffffffffu, a, u);
+      sF += __shfl_sync(0xffffffffu, b, u);
+      sV += __shfl_sync(0xffffffffu, v, u);
+    }
+  }
+  out[0] = sP; out[1] = sF; out[2] = sV;
+}
+
 __global__ void k_fire_b(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                          Clock* __restrict__ clk, Dyn d, Stat st, double* part, int nblocks, const int* rep_blk0,
                          const int* rep_nblk, const double* epart, int c, int driver, double* alpha_mix,
-                         int* __restrict__ fire_cnt, const int* __restrict__ blist = nullptr) {
+                         int* __restrict__ fire_cnt, const int* __restrict__ blist = nullptr,
+                         double* __restrict__ terms = nullptr, int terms_stride = 0) {
   const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
   const int r = blk_rep[bid_];
   const Replica& R = reps[r];
@@ -789,6 +814,10 @@ __global__ void k_fire_b(Program P, const Replica* __restrict__ reps, const int*
     v[1] = f2;
     fmax2 = f2;
     v[2] = p.vx * p.vx + p.vy * p.vy + p.vz * p.vz;
+    if (terms) {  // parity mode: the per-particle terms, by particle id
+      const size_t q = (size_t)R.off + (size_t)p.id;
+      terms[q] = v[0]; terms[(size_t)terms_stride + q] = v[1]; terms[(size_t)2 * terms_stride + q] = v[2];
+    }
     enforce_all(P, R, p);
     p.omega += dt_2 * project_torque(P, R, p);
     store_dyn_moved<true, false>(d, k, p);
@@ -814,6 +843,11 @@ __global__ void k_fire_b(Program P, const Replica* __restrict__ reps, const int*
     __threadfence();
     double sums[5];
     fire_sums(P, part, epart, nblocks, rep_blk0[r], rep_nblk[r], sums);
+    if (terms && threadIdx.x < 32) {  // parity mode: P, |F|^2, |v|^2 in the reference's order
+      double o[3];
+      fire_ordered_sums(terms, terms_stride, R.off, R.n, o);
+      if (threadIdx.x == 0) { sums[0] = o[0]; sums[1] = o[1]; sums[2] = o[2]; }
+    }
     if (threadIdx.x == 0) {
       fire_control(R, clk[r], r, c, sums, driver, alpha_mix);
       fire_cnt[r] = 0;
@@ -1297,6 +1331,160 @@ k_rb_build_team(const Replica* __restrict__ reps, const int* __restrict__ blk_re
   }
   for (int i = 0; i < nup; i++) nl.nb[(size_t)(tot_lo + pup + i) * nl.stride + k] = up[i];
   if (t == 0) { nl.cnt[k] = total; nl.lo[k] = tot_lo; }
+}
+
+// ---------------------------------------------------------------------------
+// Cell-tile list build for large quasi-2-D replicas (cell path, cnx, cny >= 3,
+// cnz == 3, so the 27-cell stencil holds no cell twice).  A block takes a
+// tile: TILE_B consecutive (a, b) cell columns along b at one a, every z
+// layer.  It stages the particles of the tile and its halo (columns a-1..a+1,
+// b0-1..b0+TILE_B, with periodic wrap) in shared memory once -- position, id
+// and slot, in each cell's own order -- and every particle of the tile then
+// sweeps its stencil there.  The candidates, their order and the arithmetic
+// are build_particle's, so the lists are identical; only the global loads
+// (one dependent chain per candidate in the one-thread build) are replaced by
+// one staging pass whose loads are all independent.  A tile whose halo holds
+// more than TILE_CAP particles builds its own particles with build_particle.
+// ---------------------------------------------------------------------------
+constexpr int TILE_B = 64;
+constexpr int TILE_HB = TILE_B + 2;
+constexpr int TILE_CZ = 3;
+constexpr int TILE_HCELLS = 3 * TILE_HB * TILE_CZ;
+constexpr int TILE_CAP = 640;
+
+struct TileRef { int rep, a, b0, nb; };  // nb: own columns (TILE_B, fewer at the end of a row)
+
+__host__ __device__ constexpr bool tile_eligible(int use_cell, int cnx, int cny, int cnz) {
+  return use_cell && cnx >= 3 && cny >= 3 && cnz == TILE_CZ;
+}
+
+__global__ void __launch_bounds__(BLOCK)
+k_rb_build_tile(const Replica* __restrict__ reps, const TileRef* __restrict__ tiles, const int* __restrict__ rebuild,
+                Dyn d, Stat st, NbList nl, const int* __restrict__ cslot, const int* __restrict__ cstart,
+                const int* __restrict__ ccnt, int* __restrict__ status, int* __restrict__ maxnb) {
+  __shared__ int hstart[TILE_HCELLS + 1];  // local first particle of each halo cell; [TILE_HCELLS]: total
+  __shared__ double sx[TILE_CAP], sy[TILE_CAP], sz[TILE_CAP];
+  __shared__ int sid[TILE_CAP], sslot[TILE_CAP];
+  __shared__ short scell[TILE_CAP];
+  __shared__ int shw[32];
+  const TileRef T = tiles[blockIdx.x];
+  const int mode = rebuild[T.rep];
+  if (!mode) return;
+  const Replica& R = reps[T.rep];
+  const int base0 = cstart[R.cell_off];
+  const int nh = 3 * (T.nb + 2) * TILE_CZ;  // halo cells of this tile, ordered (ha, hb, c)
+  // global cell of halo cell h
+  auto hcell = [&](int h) {
+    const int c = h % TILE_CZ, hb = (h / TILE_CZ) % (T.nb + 2), ha = h / (TILE_CZ * (T.nb + 2));
+    int ia = T.a + ha - 1, ib = T.b0 + hb - 1;
+    if (ia < 0) ia += R.cnx; else if (ia >= R.cnx) ia -= R.cnx;
+    if (ib < 0) ib += R.cny; else if (ib >= R.cny) ib -= R.cny;
+    return R.cell_off + R.cny * R.cnz * ia + R.cnz * ib + c;
+  };
+  // counts -> local starts (each thread a run of consecutive halo cells)
+  constexpr int CPT = (TILE_HCELLS + BLOCK - 1) / BLOCK;
+  int cntv[CPT];
+  int run = 0;
+#pragma unroll
+  for (int u = 0; u < CPT; u++) {
+    const int h = threadIdx.x * CPT + u;
+    cntv[u] = h < nh ? ccnt[hcell(h)] : 0;
+    run += cntv[u];
+  }
+  int total;
+  int ex = block_excl_scan(run, shw, total);
+#pragma unroll
+  for (int u = 0; u < CPT; u++) {
+    const int h = threadIdx.x * CPT + u;
+    if (h < nh) hstart[h] = ex;
+    ex += cntv[u];
+  }
+  if (threadIdx.x == 0) hstart[nh] = total;
+  __syncthreads();
+  // own cells: ha = 1, hb = 1..nb, every c -- contiguous in halo order
+  const int own0 = (1 * (T.nb + 2) + 1) * TILE_CZ, own1 = (1 * (T.nb + 2) + T.nb + 1) * TILE_CZ;
+  if (total > TILE_CAP) {  // too dense to stage: the one-thread build for this tile's own particles
+    for (int h = own0; h < own1; h++) {
+      const int cg = hcell(h);
+      const int s0 = R.off + cstart[cg] - base0, n = ccnt[cg];
+      for (int q = threadIdx.x; q < n; q += BLOCK)
+        build_particle(R, mode, mode == 2 ? s0 + q : cslot[s0 + q], d, st, nl, cslot, cstart, ccnt, status, maxnb);
+    }
+    return;
+  }
+  // stage every halo particle: one halo cell per thread at a time
+  for (int h = threadIdx.x; h < nh; h += BLOCK) {
+    const int cg = hcell(h);
+    const int s0 = R.off + cstart[cg] - base0, n = hstart[h + 1] - hstart[h];
+    for (int q = 0; q < n; q++) {
+      const int j = mode == 2 ? s0 + q : cslot[s0 + q];
+      const int li = hstart[h] + q;
+      sx[li] = d.x[j]; sy[li] = d.y[j]; sz[li] = d.z[j];
+      sid[li] = st.id[j]; sslot[li] = j; scell[li] = (short)h;
+    }
+  }
+  __syncthreads();
+  // every own particle sweeps its stencil in the staged cells
+  const int p0 = hstart[own0], p1 = hstart[own1];
+  for (int li = p0 + threadIdx.x; li < p1; li += BLOCK) {
+    const double x = sx[li], y = sy[li], z = sz[li];
+    const int myid = sid[li], k = sslot[li];
+    const int h = scell[li];
+    const int c = h % TILE_CZ, hb = (h / TILE_CZ) % (T.nb + 2);
+    unsigned long long lo[NB_LOCAL];  // (id << 32) | slot
+    int nlo = 0, nup = 0;
+    // pass 1: lower-id keys and the count of higher-id neighbours (the
+    // stencil visiting order of build_stencil: x offset outermost, z innermost)
+    for (int m = 0; m < 27; m++) {
+      const int ha2 = m / 9, hb2 = hb + (m / 3) % 3 - 1, c2 = (c + m % 3 - 1 + TILE_CZ) % TILE_CZ;
+      const int hh = (ha2 * (T.nb + 2) + hb2) * TILE_CZ + c2;
+      for (int q = hstart[hh]; q < hstart[hh + 1]; q++) {
+        const int jid = sid[q];
+        if (jid == myid) continue;
+        double dx, dy, dz;
+        if (myid < jid) { dx = x - sx[q]; dy = y - sy[q]; dz = z - sz[q]; }
+        else { dx = sx[q] - x; dy = sy[q] - y; dz = sz[q] - z; }
+        apply_periodic(R, dx, dy, dz);
+        if (dx * dx + dy * dy + dz * dz < R.cut2) {
+          if (jid < myid) {
+            if (nlo < NB_LOCAL) lo[nlo] = ((unsigned long long)(unsigned)jid << 32) | (unsigned)sslot[q];
+            nlo++;
+          } else {
+            nup++;
+          }
+        }
+      }
+    }
+    const int tot = nlo + nup;
+    atomicMax(maxnb, tot);
+    nl.ox[k] = x; nl.oy[k] = y; nl.oz[k] = z;
+    if (nlo > NB_LOCAL || tot > nl.cap) {  // build_particle's overflow rule
+      atomicOr(status, ST_OVERFLOW);
+      nl.cnt[k] = 0; nl.lo[k] = 0;
+      continue;
+    }
+    for (int i = 1; i < nlo; i++) {  // insertion sort by id
+      const unsigned long long v = lo[i];
+      int m = i - 1;
+      while (m >= 0 && (lo[m] >> 32) > (v >> 32)) { lo[m + 1] = lo[m]; m--; }
+      lo[m + 1] = v;
+    }
+    for (int q = 0; q < nlo; q++) nl.nb[(size_t)q * nl.stride + k] = (int)(unsigned)(lo[q] & 0xffffffffull);
+    // pass 2: the higher-id neighbours, written in visiting order
+    int w = nlo;
+    for (int m = 0; m < 27; m++) {
+      const int ha2 = m / 9, hb2 = hb + (m / 3) % 3 - 1, c2 = (c + m % 3 - 1 + TILE_CZ) % TILE_CZ;
+      const int hh = (ha2 * (T.nb + 2) + hb2) * TILE_CZ + c2;
+      for (int q = hstart[hh]; q < hstart[hh + 1]; q++) {
+        const int jid = sid[q];
+        if (jid <= myid) continue;
+        double dx = x - sx[q], dy = y - sy[q], dz = z - sz[q];
+        apply_periodic(R, dx, dy, dz);
+        if (dx * dx + dy * dy + dz * dz < R.cut2) nl.nb[(size_t)(w++) * nl.stride + k] = sslot[q];
+      }
+    }
+    nl.cnt[k] = tot; nl.lo[k] = nlo;
+  }
 }
 
 }  // namespace sg

@@ -111,6 +111,7 @@ def load() -> C.CDLL:
         "sg_host_free": (I, [P]),
         "sg_set_variant": (I, [P, I]),
         "sg_set_build": (I, [P, I]),
+        "sg_set_fire_order": (I, [P, I]),
         "sg_get_variant": (I, [P]),
         "sg_compute_static": (I, [I, D, D, D, I, D, D] + [P] * 7 + [D, D, I, I, D, D] + [P] * 6 + [P]),
         "sg_compute_static_scratch_bytes": (I64, []),
@@ -372,8 +373,13 @@ class Engine:
         """Pin a step-kernel variant (0..27) or re-enable autotuning (-1)."""
         self._check(self.lib.sg_set_variant(self.h, int(v)))
 
+    def set_fire_order(self, ordered: bool) -> None:
+        """FIRE's sums in the reference's particle order (True) or a fixed tree (False)."""
+        self._check(self.lib.sg_set_fire_order(self.h, int(bool(ordered))))
+
     def set_build(self, mode: int) -> None:
-        """Neighbour-list build kernel: 0 automatic, 1 one thread per particle, 2 teams."""
+        """Neighbour-list build kernel: 0 automatic, 1 one thread per particle, 2 teams,
+        3 cell tiles staged in shared memory (quasi-2-D replicas on the cell path)."""
         self._check(self.lib.sg_set_build(self.h, int(mode)))
 
     def variant(self) -> int:

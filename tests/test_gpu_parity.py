@@ -120,7 +120,7 @@ def test_team_and_thread_list_builds_identical(case):
         box = (L, L, lz)
     n = len(parts["x"])
     lists, pairs = [], []
-    for mode in (1, 2):
+    for mode in (1, 2, 3):  # one thread per particle, teams, cell tiles (where eligible)
         e = Engine(n)
         e.set_build(mode)
         drive(e, parts, box, periodic=periodic, nlist=(2.4, 0.3), constraint=cons)
@@ -128,13 +128,35 @@ def test_team_and_thread_list_builds_identical(case):
         pairs.append(e.pairs())
     o = OracleSystem(n)
     drive(o, parts, box, periodic=periodic, nlist=(2.4, 0.3), constraint=cons)
-    assert lists[0] == lists[1]
+    assert lists[0] == lists[1] == lists[2]
     oi, oj = o.pairs()
     for ei, ej in pairs:
         np.testing.assert_array_equal(ei, oi)
         np.testing.assert_array_equal(ej, oj)
     if case == "plane_clumps":  # some disks have more finds on one side than a lane stages (16)
         assert max(max(sum(j < i for j in v), sum(j > i for j in v)) for i, v in lists[0].items()) > 16
+
+
+def test_tile_build_through_list_only_rebuilds_and_resorts():
+    # the cell-tile build (mode 3) against the one-thread build (mode 1) over
+    # a run with many rebuilds: list-only rebuilds through the cell-ordered
+    # slot index and every 8th one a full re-sort; every field bit for bit
+    n = 20000
+    parts, L = plane_disks(n, 0.7, seed=71, bidisperse=(1.0, 1.4))
+    out = []
+    for mode in (1, 3):
+        e = Engine(n)
+        e.set_build(mode)
+        sim = drive(e, parts, (L, L, 10.0), nlist=(2.8, 0.1), pairs=[("soft", {"k": "10", "use_particle_radii": ""})],
+                    aligns=[("nematic", {"J": "0.5"})], dt=1e-3,
+                    integrators=[("brownian", {"v0": "2.0", "nu": "0.1", "seed": "9"})])
+        st = sim.run(299)
+        out.append((e, st.nlist_builds))
+    (a, ba), (b, bb) = out
+    assert ba == bb >= 10
+    for f in ("x", "y", "nx", "ny", "vx", "vy", "fx", "fy", "tau_z", "ix", "iy"):
+        np.testing.assert_array_equal(a.download(f), b.download(f), err_msg=f)
+    assert full_lists(a) == full_lists(b)
 
 
 def compute_both(parts, box, pairs=(), aligns=(), externals=(), nlist=(2.4, 0.3), periodic=True,
@@ -322,6 +344,28 @@ def test_fire_matches_oracle():
         assert f.max() < 1e-10
     assert abs(se - so) <= max(5, so // 20)
     assert_traj(e, o, ("x", "y"), tol=1e-7)
+
+
+@pytest.mark.parametrize("n,phi,seed", [(600, 0.86, 11), (1500, 0.88, 12)])
+def test_fire_parity_mode_takes_the_reference_iterations(n, phi, seed):
+    # FIRE with its sums P, |F|^2, |v|^2 taken in particle-id order, as the
+    # reference loops (integrator_fire.cpp:79-94): the dt / alpha branches
+    # and the velocity mixing then see the reference's values, so the
+    # quench takes the oracle's iterations exactly and lands on its bits
+    parts, L = plane_disks(n, phi, seed=seed, bidisperse=(1.0, 1.4))
+    out = []
+    for b in (Engine(n), OracleSystem(n)):
+        if isinstance(b, Engine):
+            b.set_fire_order(True)
+        sim = drive(b, parts, (L, L, 10.0), nlist=(2.8, 0.3), pairs=[("soft", {"k": "1", "use_particle_radii": ""})],
+                    dt=0.01, integrators=[("fire", {"dt_max": "0.1", "fmax_tolerance": "1e-10"})])
+        sim.commit()
+        steps, _ = b.minimize(200000)
+        out.append((b, int(steps[0])))
+    (e, se), (o, so) = out
+    assert se == so > 0
+    for f in ("x", "y", "vx", "vy", "fx", "fy"):
+        np.testing.assert_array_equal(e.download(f), o.download(f), err_msg=f)
 
 
 @pytest.mark.parametrize("shape", ["plane", "sphere"])
