@@ -520,6 +520,8 @@ def main():
     ap.add_argument("--no-ml", action="store_true", help="skip the learned FIRE warm-start leg")
     ap.add_argument("--variant", type=int, default=-1,
                     help="pin the step-kernel variant instead of autotuning (profiling runs: ncu distorts the tuner's timings)")
+    ap.add_argument("--build", type=int, default=0,
+                    help="neighbour-list build kernel (0 automatic, 1 one thread per particle, 2 teams, 3 cell tiles)")
     ap.add_argument("--particles", type=int, default=N_PART,
                     help="system size (profiling runs use a smaller system of the same density)")
     ap.add_argument("--ensemble-only", action="store_true",
@@ -556,6 +558,7 @@ def main():
     n_part = args.particles
     parts, L = make_particles(n_part, seed=1 + rank)
     eng = Engine(n_part, device=local)
+    eng.set_build(args.build)
     sim = Simulation(eng)
     configure(sim, parts, L)
 

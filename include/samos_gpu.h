@@ -270,6 +270,14 @@ int  sg_set_build(sg_system* s, int mode);
  * bit for bit (the energy in the reference's own convergence test stays a
  * tree sum).  Costs a sequential pass over each replica per iteration.      */
 int  sg_set_fire_order(sg_system* s, int ordered);
+/* Generic fused step kernel (programs outside the specialised plane /
+ * sphere Brownian kernels: vicsek, curved and implicit constraints, groups,
+ * phase-in): the blocks per SM its registers are bounded for, 6 or 8; 0
+ * (default) times both on the run's first steps and keeps the faster.
+ * Same bits either way.  sg_get_generic_occupancy reports the choice (0 =
+ * not yet tuned).  No reference counterpart.                                */
+int  sg_set_generic_occupancy(sg_system* s, int blocks_per_sm);
+int  sg_get_generic_occupancy(const sg_system* s);
 
 /* ---- device view (for kernels that work on the engine's state) -----------
  * No reference counterpart.  Device pointers into the handle's current

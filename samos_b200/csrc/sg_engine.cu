@@ -139,6 +139,12 @@ struct sg_system {
   uint8_t* lane_order = nullptr;
   bool order_valid = false;
   int abp_variant = 1;
+  // generic fused kernel: blocks per SM of its launch bounds (8 or 6), timed
+  // on the run's first steps unless pinned (sg_set_generic_occupancy)
+  int gen_minb = 8, gen_pin = 0, gen_trial = 0;
+  bool gen_tuned = false;
+  double gen_ms[2] = {0.0, 0.0};
+  int gen_n[2] = {0, 0};
   // autotuner: every variant yields the same bits, so candidates are timed on
   // the run's own first steps (CUDA events around the step kernel)
   bool tuned = false;
@@ -1385,20 +1391,56 @@ static int step_unfused(sg_system* s, bool energy, bool driver) {
   return SG_OK;
 }
 
-static int step_fused(sg_system* s, bool apply_e1, bool energy) {
+static constexpr int kGenMinb[2] = {8, 6};
+static constexpr int kGenTuneReps = 3;  // timed steps per candidate (after one untimed)
+
+extern "C++" {
+template <bool ENERGY>
+static void launch_generic(sg_system* s, int minb, bool apply_e1) {
   const int nb = s->nblocks;
-  if (s->profile) CU(s, cudaEventRecord(s->ev_k0, s->stream));
-  if (energy)
-    k_step_brownian<true><<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alt, s->st, s->nl,
-                                                       s->rebuild, s->status, s->dt_global, apply_e1 ? 1 : 0,
-                                                       s->epart, nb, s->gmask, s->grank, s->slots);
+  if (minb == 6)
+    k_step_brownian<ENERGY, 6><<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alt,
+                                                            s->st, s->nl, s->rebuild, s->status, s->dt_global,
+                                                            apply_e1 ? 1 : 0, s->epart, nb, s->gmask, s->grank,
+                                                            s->slots);
   else
-    k_step_brownian<false><<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alt, s->st, s->nl,
-                                                        s->rebuild, s->status, s->dt_global, apply_e1 ? 1 : 0,
-                                                        s->epart, nb, s->gmask, s->grank, s->slots);
+    k_step_brownian<ENERGY, 8><<<nb, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->clk, s->cur, s->alt,
+                                                            s->st, s->nl, s->rebuild, s->status, s->dt_global,
+                                                            apply_e1 ? 1 : 0, s->epart, nb, s->gmask, s->grank,
+                                                            s->slots);
+}
+}  // extern "C++"
+
+// One generic fused step.  `may_tune`: a step launched on its own (not in a
+// batch, whose halted kernels would time as empty), which may serve as one
+// of the occupancy tuner's timed trials.
+static int step_fused(sg_system* s, bool apply_e1, bool energy, bool may_tune = false) {
+  const bool tuning = may_tune && !energy && !s->gen_pin && !s->gen_tuned;
+  int cand = 0;
+  if (tuning) {
+    cand = (s->gen_trial / (kGenTuneReps + 1)) % 2;
+    s->gen_minb = kGenMinb[cand];
+    CU(s, cudaEventRecord(s->ev_t0, s->stream));
+  }
+  const int minb = s->gen_pin ? s->gen_pin : s->gen_minb;
+  if (s->profile) CU(s, cudaEventRecord(s->ev_k0, s->stream));
+  if (energy) launch_generic<true>(s, minb, apply_e1);
+  else launch_generic<false>(s, minb, apply_e1);
   LAUNCH_CHECK(s);
   if (s->profile) CU(s, cudaEventRecord(s->ev_k1, s->stream));
   std::swap(s->cur, s->alt);
+  if (tuning) {
+    CU(s, cudaEventRecord(s->ev_t1, s->stream));
+    CU(s, cudaEventSynchronize(s->ev_t1));
+    float ms = 0.f;
+    CU(s, cudaEventElapsedTime(&ms, s->ev_t0, s->ev_t1));
+    if (s->gen_trial % (kGenTuneReps + 1) != 0) { s->gen_ms[cand] += ms; s->gen_n[cand]++; }
+    s->gen_trial++;
+    if (s->gen_trial >= 2 * (kGenTuneReps + 1)) {
+      s->gen_minb = s->gen_ms[1] / s->gen_n[1] < s->gen_ms[0] / s->gen_n[0] ? kGenMinb[1] : kGenMinb[0];
+      s->gen_tuned = true;
+    }
+  }
   return SG_OK;
 }
 
@@ -1983,7 +2025,7 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
       t += ex - 1;
       continue;
     }
-    if (shape == HOT_NONE && fused && !resc && t > 0 && !last && K > 1 && !s->profile) {
+    if (shape == HOT_NONE && fused && !resc && t > 0 && !last && K > 1 && !s->profile && (s->gen_tuned || s->gen_pin)) {
       int64_t ex = 0;
       if ((rc = run_batch_generic(s, K, needs_nl, &ex, &rebuild_ms))) return rc;
       done += ex;
@@ -2005,7 +2047,7 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
         k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, nullptr);
         LAUNCH_CHECK(s);
       }
-      rc = step_fused(s, !last && !resc, last);
+      rc = step_fused(s, !last && !resc, last, true);
       s->e1_applied = !last && !resc;
     } else {
       rc = step_unfused(s, last, driver);
@@ -2149,6 +2191,22 @@ int sg_set_variant(sg_system* s, int variant) {
 }
 
 int sg_get_variant(const sg_system* s) { return s ? (s->tuned ? s->abp_variant : -1) : SG_ERR_ARG; }
+
+int sg_set_generic_occupancy(sg_system* s, int blocks_per_sm) {
+  if (!s || !(blocks_per_sm == 0 || blocks_per_sm == 6 || blocks_per_sm == 8)) return SG_ERR_ARG;
+  s->gen_pin = blocks_per_sm;
+  if (blocks_per_sm == 0) {  // re-tune on the next run
+    s->gen_tuned = false; s->gen_trial = 0;
+    s->gen_ms[0] = s->gen_ms[1] = 0.0; s->gen_n[0] = s->gen_n[1] = 0;
+  }
+  return SG_OK;
+}
+
+int sg_get_generic_occupancy(const sg_system* s) {
+  if (!s) return SG_ERR_ARG;
+  if (s->gen_pin) return s->gen_pin;
+  return s->gen_tuned ? s->gen_minb : 0;
+}
 
 int sg_set_fire_order(sg_system* s, int ordered) {
   if (!s || ordered < 0 || ordered > 1) return SG_ERR_ARG;

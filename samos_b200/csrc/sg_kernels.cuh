@@ -339,8 +339,11 @@ __global__ void k_force(Program P, const Replica* __restrict__ reps, const int* 
 // Fused Brownian-family step: F, tau from the current buffer, integrators in
 // map order, skin test, then (apply_e1) the next step's start-of-step
 // Constrainer::enforce; result into the next buffer.
-template <bool ENERGY>
-__global__ void __launch_bounds__(BLOCK, 8)
+// MINB: blocks per SM the register allocation is bounded for (8: 64
+// registers with some spills, 6: 80); the engine times both on a run's first
+// steps and keeps the faster, since which one wins depends on the program.
+template <bool ENERGY, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB)
 k_step_brownian(Program P, const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                 const Clock* __restrict__ clk, Dyn cur, Dyn nxt, Stat st, NbList nl,
                 int* __restrict__ rebuild, int* __restrict__ status, double dt_global, int apply_e1,
@@ -1426,6 +1429,7 @@ k_rb_build_tile(const Replica* __restrict__ reps, const TileRef* __restrict__ ti
   __syncthreads();
   // every own particle sweeps its stencil in the staged cells
   const int p0 = hstart[own0], p1 = hstart[own1];
+  int mymax = 0;  // longest list of this thread: one atomicMax per block below
   for (int li = p0 + threadIdx.x; li < p1; li += BLOCK) {
     const double x = sx[li], y = sy[li], z = sz[li];
     const int myid = sid[li], k = sslot[li];
@@ -1456,7 +1460,7 @@ k_rb_build_tile(const Replica* __restrict__ reps, const TileRef* __restrict__ ti
       }
     }
     const int tot = nlo + nup;
-    atomicMax(maxnb, tot);
+    mymax = tot > mymax ? tot : mymax;
     nl.ox[k] = x; nl.oy[k] = y; nl.oz[k] = z;
     if (nlo > NB_LOCAL || tot > nl.cap) {  // build_particle's overflow rule
       atomicOr(status, ST_OVERFLOW);
@@ -1484,6 +1488,16 @@ k_rb_build_tile(const Replica* __restrict__ reps, const TileRef* __restrict__ ti
       }
     }
     nl.cnt[k] = tot; nl.lo[k] = nlo;
+  }
+  // block maximum of the list lengths, then one atomic
+  mymax = __reduce_max_sync(0xffffffffu, mymax);
+  __shared__ int wmax[BLOCK / 32];
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = mymax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int m = 0;
+    for (int w = 0; w < BLOCK / 32; w++) m = wmax[w] > m ? wmax[w] : m;
+    atomicMax(maxnb, m);
   }
 }
 

@@ -112,6 +112,7 @@ def load() -> C.CDLL:
         "sg_set_variant": (I, [P, I]),
         "sg_set_build": (I, [P, I]),
         "sg_set_fire_order": (I, [P, I]),
+        "sg_set_generic_occupancy": (I, [P, I]), "sg_get_generic_occupancy": (I, [P]),
         "sg_get_variant": (I, [P]),
         "sg_compute_static": (I, [I, D, D, D, I, D, D] + [P] * 7 + [D, D, I, I, D, D] + [P] * 6 + [P]),
         "sg_compute_static_scratch_bytes": (I64, []),
@@ -372,6 +373,13 @@ class Engine:
     def set_variant(self, v: int) -> None:
         """Pin a step-kernel variant (0..27) or re-enable autotuning (-1)."""
         self._check(self.lib.sg_set_variant(self.h, int(v)))
+
+    def set_generic_occupancy(self, blocks_per_sm: int) -> None:
+        """Generic fused kernel: 6 or 8 blocks per SM, or 0 to time both and keep the faster."""
+        self._check(self.lib.sg_set_generic_occupancy(self.h, int(blocks_per_sm)))
+
+    def generic_occupancy(self) -> int:
+        return int(self.lib.sg_get_generic_occupancy(self.h))
 
     def set_fire_order(self, ordered: bool) -> None:
         """FIRE's sums in the reference's particle order (True) or a fixed tree (False)."""
