@@ -352,9 +352,11 @@ ROWS = (
 
 
 def row_system(backend, row, n, seed):
+    """The row's program on a backend (engine or C oracle), or, given a
+    RefSimulation, on the reference's own classes."""
     from samos_b200.plugins import Simulation
     name, geom, pair, align, integ, dt, _ = row
-    sim = Simulation(backend)
+    sim = backend if hasattr(backend, "input_file") else Simulation(backend)
     if geom == "sphere":
         parts, R = sphere_parts(n, seed)
         zero = np.zeros(n)
@@ -410,18 +412,32 @@ def rows_leg(n=1_048_576, warm=50, steps=200, cpu_n=16_384, cpu_warm=5, cpu_step
             extra += 20
         st = eng.run(steps - 1)
         ms = st.device_ms / st.steps_done
+        occ = eng.generic_occupancy()
         eng.close()
-        o = OracleSystem(cpu_n)
-        row_system(o, row, cpu_n, 100 + i).run(cpu_warm - 1)
-        t0 = time.perf_counter()
-        o.run(cpu_steps - 1)
-        cpu = cpu_n * cpu_steps / (time.perf_counter() - t0)
+        cpu, cpu_kind = None, "reference"
+        try:  # the reference's own sources (Release flags), else the C oracle
+            from oracle.refsrc import RefSimulation, available
+            if not available(fast=True):
+                raise FileNotFoundError
+            with _Quiet():
+                ref = row_system(RefSimulation(fast=True), row, cpu_n, 100 + i)
+                ref.run(cpu_warm - 1)
+                t0 = time.perf_counter()
+                ref.run(cpu_steps - 1)
+                cpu = cpu_n * cpu_steps / (time.perf_counter() - t0)
+        except Exception:
+            cpu_kind = "port"
+            o = OracleSystem(cpu_n)
+            row_system(o, row, cpu_n, 100 + i).run(cpu_warm - 1)
+            t0 = time.perf_counter()
+            o.run(cpu_steps - 1)
+            cpu = cpu_n * cpu_steps / (time.perf_counter() - t0)
         gbs = n * row[6] / (ms * 1e-3) / 1e9
         out.append(dict(row=row[0], particles=n, steps=int(st.steps_done), ms_per_step=ms,
                         particle_steps_per_s=n / (ms * 1e-3), nlist_builds=int(st.nlist_builds),
                         state_bytes_per_particle_step=row[6], state_gbs=gbs, frac_of_hbm=gbs / peak,
-                        cpu_particles=cpu_n, cpu_particle_steps_per_s=cpu,
-                        gpu_over_cpu=n / (ms * 1e-3) / cpu))
+                        cpu_particles=cpu_n, cpu_particle_steps_per_s=cpu, cpu_kind=cpu_kind,
+                        gpu_over_cpu=n / (ms * 1e-3) / cpu, generic_blocks_per_sm=occ or None))
     return out
 
 
@@ -615,10 +631,15 @@ def main():
     t0 = time.perf_counter()
     for f in fields_in:
         eng.upload(f, host_in[f])
+    t_up = time.perf_counter()
     eng.build_nlist()
     est = eng.run(e2e_steps - 1)
+    t_run = time.perf_counter()
     outs = {f: eng.download(f, out=host_out[f]) for f in fields_out}
-    e2e_s = max_over_ranks(time.perf_counter() - t0, ws)
+    t_end = time.perf_counter()
+    e2e_s = max_over_ranks(t_end - t0, ws)
+    e2e_split = dict(upload_ms=(t_up - t0) * 1e3, build_and_run_ms=(t_run - t_up) * 1e3,
+                     download_ms=(t_end - t_run) * 1e3)
     h2d = len(fields_in) * 8 * n_part / e2e_steps
     d2h = len(fields_out) * 8 * n_part / e2e_steps
     e2e_value = ws * n_part * e2e_steps / e2e_s
@@ -650,7 +671,7 @@ def main():
                           list_build_ms=rebuild_ms, list_builds_profiled=int(pst.nlist_builds),
                           peak_source="MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"),
             e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
-                     steps=e2e_steps, finite=bool(finite)),
+                     steps=e2e_steps, finite=bool(finite), **e2e_split),
             gpu_launches=int(launches),
             clocks=clocks.summary(),
             cpu_baseline=cpu,

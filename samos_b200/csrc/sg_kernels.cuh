@@ -1365,34 +1365,42 @@ __global__ void __launch_bounds__(BLOCK)
 k_rb_build_tile(const Replica* __restrict__ reps, const TileRef* __restrict__ tiles, const int* __restrict__ rebuild,
                 Dyn d, Stat st, NbList nl, const int* __restrict__ cslot, const int* __restrict__ cstart,
                 const int* __restrict__ ccnt, int* __restrict__ status, int* __restrict__ maxnb) {
-  __shared__ int hstart[TILE_HCELLS + 1];  // local first particle of each halo cell; [TILE_HCELLS]: total
+  __shared__ int hstart[TILE_HCELLS + 1];  // local first particle of each halo cell; [nh]: total
+  __shared__ int hgs[TILE_HCELLS];         // slot-index position of each halo cell's first particle
   __shared__ double sx[TILE_CAP], sy[TILE_CAP], sz[TILE_CAP];
   __shared__ int sid[TILE_CAP], sslot[TILE_CAP];
   __shared__ short scell[TILE_CAP];
   __shared__ int shw[32];
+  __shared__ int wmax[BLOCK / 32];
   const TileRef T = tiles[blockIdx.x];
   const int mode = rebuild[T.rep];
   if (!mode) return;
   const Replica& R = reps[T.rep];
   const int base0 = cstart[R.cell_off];
-  const int nh = 3 * (T.nb + 2) * TILE_CZ;  // halo cells of this tile, ordered (ha, hb, c)
-  // global cell of halo cell h
-  auto hcell = [&](int h) {
-    const int c = h % TILE_CZ, hb = (h / TILE_CZ) % (T.nb + 2), ha = h / (TILE_CZ * (T.nb + 2));
-    int ia = T.a + ha - 1, ib = T.b0 + hb - 1;
-    if (ia < 0) ia += R.cnx; else if (ia >= R.cnx) ia -= R.cnx;
-    if (ib < 0) ib += R.cny; else if (ib >= R.cny) ib -= R.cny;
-    return R.cell_off + R.cny * R.cnz * ia + R.cnz * ib + c;
-  };
-  // counts -> local starts (each thread a run of consecutive halo cells)
+  const int HB = T.nb + 2;
+  const int nh = 3 * HB * TILE_CZ;  // halo cells of this tile, ordered (ha, hb, c), c innermost
+  // counts and starts of the halo cells (each thread a run of consecutive cells)
   constexpr int CPT = (TILE_HCELLS + BLOCK - 1) / BLOCK;
   int cntv[CPT];
   int run = 0;
+  {
+    const int h0 = threadIdx.x * CPT;
+    int hb = (h0 / TILE_CZ) % HB, ha = h0 / (TILE_CZ * HB), c = h0 % TILE_CZ;
 #pragma unroll
-  for (int u = 0; u < CPT; u++) {
-    const int h = threadIdx.x * CPT + u;
-    cntv[u] = h < nh ? ccnt[hcell(h)] : 0;
-    run += cntv[u];
+    for (int u = 0; u < CPT; u++) {
+      const int h = h0 + u;
+      cntv[u] = 0;
+      if (h < nh) {
+        int ia = T.a + ha - 1, ib = T.b0 + hb - 1;
+        if (ia < 0) ia += R.cnx; else if (ia >= R.cnx) ia -= R.cnx;
+        if (ib < 0) ib += R.cny; else if (ib >= R.cny) ib -= R.cny;
+        const int cg = R.cell_off + R.cny * R.cnz * ia + R.cnz * ib + c;
+        cntv[u] = ccnt[cg];
+        hgs[h] = R.off + cstart[cg] - base0;
+      }
+      run += cntv[u];
+      if (++c == TILE_CZ) { c = 0; if (++hb == HB) { hb = 0; ha++; } }
+    }
   }
   int total;
   int ex = block_excl_scan(run, shw, total);
@@ -1405,60 +1413,74 @@ k_rb_build_tile(const Replica* __restrict__ reps, const TileRef* __restrict__ ti
   if (threadIdx.x == 0) hstart[nh] = total;
   __syncthreads();
   // own cells: ha = 1, hb = 1..nb, every c -- contiguous in halo order
-  const int own0 = (1 * (T.nb + 2) + 1) * TILE_CZ, own1 = (1 * (T.nb + 2) + T.nb + 1) * TILE_CZ;
+  const int own0 = (HB + 1) * TILE_CZ, own1 = (HB + T.nb + 1) * TILE_CZ;
   if (total > TILE_CAP) {  // too dense to stage: the one-thread build for this tile's own particles
     for (int h = own0; h < own1; h++) {
-      const int cg = hcell(h);
-      const int s0 = R.off + cstart[cg] - base0, n = ccnt[cg];
+      const int s0 = hgs[h], n = hstart[h + 1] - hstart[h];
       for (int q = threadIdx.x; q < n; q += BLOCK)
         build_particle(R, mode, mode == 2 ? s0 + q : cslot[s0 + q], d, st, nl, cslot, cstart, ccnt, status, maxnb);
     }
     return;
   }
-  // stage every halo particle: one halo cell per thread at a time
-  for (int h = threadIdx.x; h < nh; h += BLOCK) {
-    const int cg = hcell(h);
-    const int s0 = R.off + cstart[cg] - base0, n = hstart[h + 1] - hstart[h];
-    for (int q = 0; q < n; q++) {
-      const int j = mode == 2 ? s0 + q : cslot[s0 + q];
-      const int li = hstart[h] + q;
-      sx[li] = d.x[j]; sy[li] = d.y[j]; sz[li] = d.z[j];
-      sid[li] = st.id[j]; sslot[li] = j; scell[li] = (short)h;
+  // stage every halo particle, one per thread at a time: its cell by binary
+  // search over the starts, then one slot-index load and the record
+  for (int li = threadIdx.x; li < total; li += BLOCK) {
+    int lo = 0, hi = nh - 1;  // last cell h with hstart[h] <= li (empty cells share their start)
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (hstart[mid] <= li) lo = mid; else hi = mid - 1;
     }
+    const int s = hgs[lo] + (li - hstart[lo]);
+    const int j = mode == 2 ? s : cslot[s];
+    sx[li] = d.x[j]; sy[li] = d.y[j]; sz[li] = d.z[j];
+    sid[li] = st.id[j]; sslot[li] = j; scell[li] = (short)lo;
   }
   __syncthreads();
-  // every own particle sweeps its stencil in the staged cells
+  // every own particle sweeps its stencil in the staged cells, in the
+  // visiting order of build_stencil: x offset outermost, then y, then z.  A
+  // particle in the middle layer (c = 1) visits the layers 0, 1, 2 of each
+  // column: one contiguous run of staged particles per column.
   const int p0 = hstart[own0], p1 = hstart[own1];
   int mymax = 0;  // longest list of this thread: one atomicMax per block below
   for (int li = p0 + threadIdx.x; li < p1; li += BLOCK) {
     const double x = sx[li], y = sy[li], z = sz[li];
     const int myid = sid[li], k = sslot[li];
     const int h = scell[li];
-    const int c = h % TILE_CZ, hb = (h / TILE_CZ) % (T.nb + 2);
+    const int c = h % TILE_CZ, hb = (h / TILE_CZ) % HB;
     unsigned long long lo[NB_LOCAL];  // (id << 32) | slot
     int nlo = 0, nup = 0;
-    // pass 1: lower-id keys and the count of higher-id neighbours (the
-    // stencil visiting order of build_stencil: x offset outermost, z innermost)
-    for (int m = 0; m < 27; m++) {
-      const int ha2 = m / 9, hb2 = hb + (m / 3) % 3 - 1, c2 = (c + m % 3 - 1 + TILE_CZ) % TILE_CZ;
-      const int hh = (ha2 * (T.nb + 2) + hb2) * TILE_CZ + c2;
-      for (int q = hstart[hh]; q < hstart[hh + 1]; q++) {
-        const int jid = sid[q];
-        if (jid == myid) continue;
-        double dx, dy, dz;
-        if (myid < jid) { dx = x - sx[q]; dy = y - sy[q]; dz = z - sz[q]; }
-        else { dx = sx[q] - x; dy = sy[q] - y; dz = sz[q] - z; }
-        apply_periodic(R, dx, dy, dz);
-        if (dx * dx + dy * dy + dz * dz < R.cut2) {
-          if (jid < myid) {
-            if (nlo < NB_LOCAL) lo[nlo] = ((unsigned long long)(unsigned)jid << 32) | (unsigned)sslot[q];
-            nlo++;
+    // pass 1: lower-id keys and the count of higher-id neighbours
+    for (int ox = 0; ox < 3; ox++)
+      for (int oy = -1; oy <= 1; oy++) {
+        const int col = (ox * HB + hb + oy) * TILE_CZ;
+        for (int oz = -1; oz <= 1; oz++) {
+          int qa, qb;
+          if (c == 1) {  // the whole column at once
+            qa = hstart[col]; qb = hstart[col + TILE_CZ]; oz = 1;
           } else {
-            nup++;
+            int c2 = c + oz;
+            c2 += c2 < 0 ? TILE_CZ : 0;
+            c2 -= c2 >= TILE_CZ ? TILE_CZ : 0;
+            qa = hstart[col + c2]; qb = hstart[col + c2 + 1];
+          }
+          for (int q = qa; q < qb; q++) {
+            const int jid = sid[q];
+            if (jid == myid) continue;
+            double dx, dy, dz;
+            if (myid < jid) { dx = x - sx[q]; dy = y - sy[q]; dz = z - sz[q]; }
+            else { dx = sx[q] - x; dy = sy[q] - y; dz = sz[q] - z; }
+            apply_periodic(R, dx, dy, dz);
+            if (dx * dx + dy * dy + dz * dz < R.cut2) {
+              if (jid < myid) {
+                if (nlo < NB_LOCAL) lo[nlo] = ((unsigned long long)(unsigned)jid << 32) | (unsigned)sslot[q];
+                nlo++;
+              } else {
+                nup++;
+              }
+            }
           }
         }
       }
-    }
     const int tot = nlo + nup;
     mymax = tot > mymax ? tot : mymax;
     nl.ox[k] = x; nl.oy[k] = y; nl.oz[k] = z;
@@ -1476,22 +1498,32 @@ k_rb_build_tile(const Replica* __restrict__ reps, const TileRef* __restrict__ ti
     for (int q = 0; q < nlo; q++) nl.nb[(size_t)q * nl.stride + k] = (int)(unsigned)(lo[q] & 0xffffffffull);
     // pass 2: the higher-id neighbours, written in visiting order
     int w = nlo;
-    for (int m = 0; m < 27; m++) {
-      const int ha2 = m / 9, hb2 = hb + (m / 3) % 3 - 1, c2 = (c + m % 3 - 1 + TILE_CZ) % TILE_CZ;
-      const int hh = (ha2 * (T.nb + 2) + hb2) * TILE_CZ + c2;
-      for (int q = hstart[hh]; q < hstart[hh + 1]; q++) {
-        const int jid = sid[q];
-        if (jid <= myid) continue;
-        double dx = x - sx[q], dy = y - sy[q], dz = z - sz[q];
-        apply_periodic(R, dx, dy, dz);
-        if (dx * dx + dy * dy + dz * dz < R.cut2) nl.nb[(size_t)(w++) * nl.stride + k] = sslot[q];
+    for (int ox = 0; ox < 3; ox++)
+      for (int oy = -1; oy <= 1; oy++) {
+        const int col = (ox * HB + hb + oy) * TILE_CZ;
+        for (int oz = -1; oz <= 1; oz++) {
+          int qa, qb;
+          if (c == 1) {
+            qa = hstart[col]; qb = hstart[col + TILE_CZ]; oz = 1;
+          } else {
+            int c2 = c + oz;
+            c2 += c2 < 0 ? TILE_CZ : 0;
+            c2 -= c2 >= TILE_CZ ? TILE_CZ : 0;
+            qa = hstart[col + c2]; qb = hstart[col + c2 + 1];
+          }
+          for (int q = qa; q < qb; q++) {
+            const int jid = sid[q];
+            if (jid <= myid) continue;
+            double dx = x - sx[q], dy = y - sy[q], dz = z - sz[q];
+            apply_periodic(R, dx, dy, dz);
+            if (dx * dx + dy * dy + dz * dz < R.cut2) nl.nb[(size_t)(w++) * nl.stride + k] = sslot[q];
+          }
+        }
       }
-    }
     nl.cnt[k] = tot; nl.lo[k] = nlo;
   }
   // block maximum of the list lengths, then one atomic
   mymax = __reduce_max_sync(0xffffffffu, mymax);
-  __shared__ int wmax[BLOCK / 32];
   if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = mymax;
   __syncthreads();
   if (threadIdx.x == 0) {

@@ -633,6 +633,26 @@ def test_trajectory_rescaled_cylinder_and_tetrahedron(kind, shape, conf, box, pe
         assert np.max(np.abs(tetra_value(np.stack([x, y, z], 1), 10.0 * f ** 20, 0.3))) < 2e-6
 
 
+def test_generic_kernel_occupancy_choices_give_the_same_bits():
+    # the generic fused kernel bounded for 6 or 8 blocks per SM, pinned or
+    # picked by timing the run's first steps: same bits
+    n = 1500
+    parts = surface_disks("torus", n, seed=17, c=20.0, a=8.0)
+    kw = dict(periodic=False, nlist=(2.4, 0.3), constraint=("torus", {"c": "20.0", "a": "8.0"}),
+              pairs=[("soft", {"k": "10"})], aligns=[("polar", {"J": "0.2"})], dt=1e-3,
+              integrators=[("brownian", {"v0": "1.0", "nu": "0.1", "seed": "4"})])
+    outs = []
+    for occ in (6, 8, 0):
+        e = Engine(n)
+        e.set_generic_occupancy(occ)
+        drive(e, parts, (70.0, 70.0, 30.0), **kw).run(199)
+        assert e.generic_occupancy() in ((6, 8) if occ == 0 else (occ,))
+        outs.append(e)
+    for f in ("x", "y", "z", "nx", "ny", "nz", "vx", "vy", "vz"):
+        np.testing.assert_array_equal(outs[0].download(f), outs[1].download(f), err_msg=f)
+        np.testing.assert_array_equal(outs[0].download(f), outs[2].download(f), err_msg=f)
+
+
 @pytest.mark.parametrize("kind", ["torus", "vicsek"])
 def test_generic_batched_stepping_gives_the_stepwise_bits(kind):
     # the generic fused kernel enqueues up to 32 steps per host round trip,
