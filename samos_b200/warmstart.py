@@ -1,8 +1,12 @@
 """Learned FIRE warm start.
 
 A two-layer message-passing network (hidden width 64, neighbours within
-rc = 2.8; kernels in csrc/sg_ml.cu) predicts, from a quenched configuration,
-each particle's displacement to its FIRE minimum.  Training data are
+rc = 2.8; kernels in csrc/sg_ml.cu) predicts, from a configuration, each
+particle's displacement to its FIRE minimum.  Two places to apply it: at the
+quench itself, or at the hand-off -- plain FIRE runs until max |F_i| first
+drops below a hand-off tolerance, the network moves the particles from
+there, and a fresh FIRE finishes to the final tolerance.  Up to the hand-off
+both arms share every bit, so they start the last stretch in the same basin.  Training data are
 quench-then-FIRE relaxations run by the engine's own GPU FIRE; training runs
 the project's forward/backward kernels (BF16 tensor-core GEMMs, FP32
 accumulation) with Adam.  At use, the predicted displacement is applied only
@@ -179,13 +183,17 @@ class WarmStartNet:
         torch.cuda.synchronize()
         eng.positions_changed()
 
-    def save(self, path: str) -> None:
-        np.savez(path, params=self.get_params(), rc=self.rc)
+    def save(self, path: str, handoff: float | None = None) -> None:
+        np.savez(path, params=self.get_params(), rc=self.rc, handoff=np.nan if handoff is None else handoff)
 
-    def load(self, path: str) -> None:
+    def load(self, path: str) -> float | None:
+        """Loads the parameters; returns the hand-off tolerance they were
+        trained for (None: trained on quenches)."""
         d = np.load(path)
         self.rc = float(d["rc"])
         self.set_params(d["params"])
+        h = float(d["handoff"]) if "handoff" in d.files else float("nan")
+        return None if np.isnan(h) else h
 
 
 def min_image(d: np.ndarray, L: float) -> np.ndarray:
@@ -194,29 +202,53 @@ def min_image(d: np.ndarray, L: float) -> np.ndarray:
 
 # -- data: quench-then-FIRE relaxations on the GPU ---------------------------------------
 class Batch:
-    """One engine holding `R` quenched systems, with their relaxation targets
-    (displacement quench -> FIRE minimum, slot order) kept on the device."""
+    """One engine holding `R` systems, with their relaxation targets
+    (displacement from the network's input state to the FIRE minimum, slot
+    order) kept on the device.  The input state is the quench, or with
+    `handoff` the state where FIRE from the quench first has max |F_i| below
+    `handoff` (the minimum then comes from FIRE continued from there)."""
 
     def __init__(self, net: WarmStartNet, insts, k: float = 1.0, dt: float = 0.01, dt_max: float = 0.2,
-                 fmax: float = 1e-10, max_steps: int = 400000):
+                 fmax: float = 1e-10, max_steps: int = 400000, handoff: float | None = None):
         from .ensemble import plane_fire_ensemble
         self.insts = insts
-        self.eng = plane_fire_ensemble(insts, k=k, dt=dt, dt_max=dt_max, fmax=fmax)
+        self.handoff = handoff
+        self.eng = plane_fire_ensemble(insts, k=k, dt=dt, dt_max=dt_max, fmax=handoff or fmax)
         self.eng.build_nlist()
         t0 = time.perf_counter()
+        start = insts
+        if handoff is not None:
+            self.conv_handoff, st_h = self.eng.minimize(max_steps)
+            start = snapshot(self.eng, insts)
+            for r in range(len(insts)):
+                self.eng.set_replica_param(r, 4, 0, 11, fmax)  # FIRE's max |F_i| tolerance
         self.conv, st = self.eng.minimize(max_steps)
         self.fire_s = time.perf_counter() - t0
-        self.fire_device_ms = st.device_ms
+        self.fire_device_ms = st.device_ms + (st_h.device_ms if handoff is not None else 0.0)
         self.energy = np.array([self.eng.energy(0, 0, r) for r in range(len(insts))])
         targets = []
-        for r, (parts, L) in enumerate(insts):
+        for r, (parts, L) in enumerate(start):
             fx, fy = self.eng.download("x", r), self.eng.download("y", r)
             targets.append(np.stack([min_image(fx - parts["x"], L), min_image(fy - parts["y"], L)], 1))
         self.targets = targets
-        restore_quench(self.eng, insts)
+        restore_quench(self.eng, start)
+        self.start = start
         self.box = net.box_array(self.eng)
         self.target = net.slot_targets(self.eng, targets)
         self.n_valid = int(sum(len(p["x"]) for p, _ in insts))
+
+
+def snapshot(eng: E.Engine, insts):
+    """The engine's current positions as new instances (same radii and box,
+    zero velocities): [(parts, L), ...]."""
+    out = []
+    for r, (parts, L) in enumerate(insts):
+        p = dict(parts)
+        p["x"], p["y"] = eng.download("x", r), eng.download("y", r)
+        z = np.zeros(len(p["x"]))
+        p["vx"], p["vy"] = z, z.copy()
+        out.append((p, L))
+    return out
 
 
 def restore_quench(eng: E.Engine, insts, replicas=None) -> None:
@@ -301,8 +333,9 @@ def relax(insts, net: WarmStartNet | None, k: float = 1.0, dt: float = 0.01, dt_
     warm_ms = start.elapsed_time(mid)
     conv, st = eng.minimize(max_steps)
     energy = np.array([eng.energy(0, 0, r) for r in range(R)])
-    out = dict(steps=conv, energy=energy, fire_ms=st.device_ms, warm_ms=warm_ms, fallback=fallback,
-               total_ms=warm_ms + st.device_ms)
+    steps = np.where((conv >= 0) & (head_steps >= 0), conv + head_steps, -1)
+    out = dict(steps=steps, energy=energy, fire_ms=st.device_ms + head_ms, warm_ms=warm_ms, fallback=fallback,
+               total_ms=warm_ms + st.device_ms + head_ms, head_ms=head_ms, head_steps=head_steps)
     eng.close()
     return out
 
@@ -322,6 +355,10 @@ def summarize(plain: dict, warm: dict, insts) -> dict:
         plain_steps_mean=float(plain["steps"][ok].mean()), warm_steps_mean=float(warm["steps"][ok].mean()),
         plain_steps_max=int(plain["steps"].max()), warm_steps_max=int(warm["steps"].max()),
         steps_ratio_median=float(np.median(plain["steps"][ok] / warm["steps"][ok])),
+        steps_ratio_p10=float(np.percentile(plain["steps"][ok] / warm["steps"][ok], 10)),
+        steps_ratio_p90=float(np.percentile(plain["steps"][ok] / warm["steps"][ok], 90)),
+        handoff_steps_mean=float(np.mean(warm.get("head_steps", np.zeros(1)))),
+        handoff_s=warm.get("head_ms", 0.0) / 1e3,
         unconverged_plain=int((plain["steps"] < 0).sum()), unconverged_warm=int((warm["steps"] < 0).sum()),
         fallback=int(warm["fallback"].sum()),
         energy_rel_diff_median=float(np.median(rel[ok])), energy_rel_diff_max=float(rel[ok].max()),
@@ -341,26 +378,51 @@ def main(argv=None) -> int:
     t.add_argument("--per-engine", type=int, default=500)
     t.add_argument("--steps", type=int, default=2000)
     t.add_argument("--seed", type=int, default=1)
+    t.add_argument("--handoff", type=float, default=None,
+                   help="train on hand-off states (max |F_i| first below this) instead of quenches")
     t.add_argument("--out", required=True)
     e = sub.add_parser("eval")
     e.add_argument("--params", required=True)
     e.add_argument("--count", type=int, default=512)
     e.add_argument("--seed", type=int, default=99)
+    e.add_argument("--handoff", type=float, default=None, help="default: the value stored with the parameters")
     e.add_argument("--out")
+    pr = sub.add_parser("profile", help="a few training steps and one inference on one batch (for profilers)")
+    pr.add_argument("--count", type=int, default=64)
+    pr.add_argument("--n", type=int, default=4096)
+    pr.add_argument("--steps", type=int, default=3)
+    pr.add_argument("--fmax", type=float, default=1e-3, help="FIRE tolerance of the targets (loose: fast)")
     a = ap.parse_args(argv)
+    if a.cmd == "profile":
+        net = WarmStartNet(seed=1)
+        b = Batch(net, quench_set(a.count, a.n, a.n, 0.84, 0.90, seed=5), fmax=a.fmax)
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record()
+        for _ in range(a.steps):
+            net.loss_and_grad(b.eng, b.box, b.target, b.n_valid)
+            net.adam_step(1e-3)
+        ev[1].record()
+        net.forward(b.eng, b.box)
+        ev[2].record()
+        torch.cuda.synchronize()
+        print(json.dumps(dict(slots=b.eng.view().slots, particles=b.n_valid,
+                              train_step_ms=ev[0].elapsed_time(ev[1]) / a.steps,
+                              inference_ms=ev[1].elapsed_time(ev[2]))), flush=True)
+        return 0
     if a.cmd == "train":
         net = WarmStartNet(seed=a.seed)
         data = quench_set(a.count + 64, a.n, a.n, 0.84, 0.90, seed=a.seed)
         t0 = time.perf_counter()
-        batches = [Batch(net, data[i:i + a.per_engine]) for i in range(0, a.count, a.per_engine)]
-        held = Batch(net, data[a.count:])
+        batches = [Batch(net, data[i:i + a.per_engine], handoff=a.handoff) for i in range(0, a.count, a.per_engine)]
+        held = Batch(net, data[a.count:], handoff=a.handoff)
         gen_s = time.perf_counter() - t0
         t0 = time.perf_counter()
         hist = train(net, batches, a.steps, log_every=max(1, a.steps // 10))
         torch.cuda.synchronize()
         train_s = time.perf_counter() - t0
-        net.save(a.out)
-        rep = dict(relaxations=a.count, n=a.n, generation_s=gen_s, fire_device_s=sum(b.fire_device_ms for b in batches) / 1e3,
+        net.save(a.out, handoff=a.handoff)
+        rep = dict(relaxations=a.count, handoff=a.handoff, n=a.n, generation_s=gen_s, fire_device_s=sum(b.fire_device_ms for b in batches) / 1e3,
                    fire_steps_max=[int(b.conv.max()) for b in batches],
                    unconverged=int(sum((b.conv < 0).sum() for b in batches)), adam_steps=a.steps, train_s=train_s,
                    loss_first=hist[0], loss_last=float(np.mean(hist[-len(batches):])),
@@ -368,11 +430,13 @@ def main(argv=None) -> int:
         print(json.dumps(rep), flush=True)
         return 0
     net = WarmStartNet()
-    net.load(a.params)
+    stored = net.load(a.params)
+    handoff = a.handoff if a.handoff is not None else stored
     insts = quench_set(a.count, 1024, 16384, 0.84, 0.90, seed=a.seed)
     plain = relax(insts, None)
-    warm = relax(insts, net)
+    warm = relax(insts, net, handoff=handoff)
     rep = summarize(plain, warm, insts)
+    rep["handoff"] = handoff
     print(json.dumps(rep), flush=True)
     if a.out:
         np.savez(a.out, plain_steps=plain["steps"], warm_steps=warm["steps"], plain_energy=plain["energy"],
