@@ -42,13 +42,18 @@ struct AbpParams {
 // 21-27 twins of 18 / 17 / 19 / 11 / 3 / 12 / 13 that read the parameters of
 // a one-replica system from the kernel's own parameter space (constant-bank
 // operands of the FP64 instructions) instead of a shared-memory copy, whose
-// per-neighbour loads otherwise sit on the sweep's dependency chains.
-constexpr int ABP_NVARIANT = 28;
-__host__ __device__ constexpr bool abp_byval(int v) { return v >= 21; }
+// per-neighbour loads otherwise sit on the sweep's dependency chains; 30-31
+// pipelined with two neighbours per iteration (both records requested one
+// iteration ahead, the two pair terms independent chains the scheduler can
+// interleave, added in list order) at 6 and 5 blocks per SM, and 28-29 their
+// by-value twins.
+constexpr int ABP_NVARIANT = 32;
+__host__ __device__ constexpr bool abp_byval(int v) { return v >= 21 && v <= 29; }
 // the shared-memory twin of a by-value variant (taken when several replicas
 // share the launch); every other property of a by-value variant is its twin's
 __host__ __device__ constexpr int abp_twin(int v) {
-  return v == 21 ? 18 : v == 22 ? 17 : v == 23 ? 19 : v == 24 ? 11 : v == 25 ? 3 : v == 26 ? 12 : v == 27 ? 13 : v;
+  return v == 21 ? 18 : v == 22 ? 17 : v == 23 ? 19 : v == 24 ? 11 : v == 25 ? 3 : v == 26 ? 12 : v == 27 ? 13
+       : v == 28 ? 30 : v == 29 ? 31 : v;
 }
 __host__ __device__ constexpr int abp_chunk(int v0) {
   const int v = abp_twin(v0);
@@ -58,15 +63,17 @@ __host__ __device__ constexpr int abp_minb(int v0) {
   const int v = abp_twin(v0);
   return v == 0 ? 5 : v == 1 ? 4 : v == 2 ? 6 : v == 3 ? 4 : v == 9 ? 6 : v == 10 ? 5 : v == 11 ? 6 : v == 12 ? 7
        : v == 13 ? 8 : v == 14 ? 10 : v == 15 ? 7 : v == 16 ? 6 : v == 17 ? 8 : v == 18 ? 9 : v == 19 ? 10 : v == 20 ? 12
-       : 3;
+       : v == 30 ? 6 : v == 31 ? 5 : 3;
 }
 __host__ __device__ constexpr bool abp_ordered(int v) { return abp_twin(v) >= 9; }
 __host__ __device__ constexpr bool abp_prenoise(int v) { return abp_twin(v) >= 11; }
 __host__ __device__ constexpr bool abp_pipelined(int v) { return abp_twin(v) >= 15; }
+__host__ __device__ constexpr bool abp_pair2(int v) { return abp_twin(v) >= 30; }
 
 // The variants the autotuner times (every one can still be pinned): those
 // that never won on the plane, sphere or replica workloads are left out.
-constexpr int ABP_TUNED[] = {0, 1, 2, 3, 8, 9, 10, 11, 12, 13, 15, 16, 17, 18, 21, 22, 23, 24, 25, 26, 27};
+constexpr int ABP_TUNED[] = {0, 1, 2, 3, 8, 9, 10, 11, 12, 13, 15, 16, 17, 18, 21, 22, 23, 24, 25, 26, 27, 28, 29,
+                             30, 31};
 constexpr int ABP_NTUNED = (int)(sizeof(ABP_TUNED) / sizeof(ABP_TUNED[0]));
 
 // Lane order of a block for the ordered variants: its particles sorted by
@@ -337,7 +344,37 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
     // list entries of the first chunk; each iteration then fetches the next
     // chunk's entries while its own records are in flight (index -> record
     // would otherwise be two dependent memory latencies per chunk)
-    if constexpr (abp_pipelined(VAR)) {
+    if constexpr (abp_pair2(VAR)) {
+      // two neighbours per iteration, both records requested during the
+      // previous iteration and the list entries two iterations ahead.  Past
+      // the end of the list a lane reads its own record: that term is an
+      // exact zero (d = 0, n x n = 0), so adding it changes no bit, and both
+      // terms stay unconditional, free to interleave.
+      int jn0 = 2 < cnt ? __ldg(nl.nb + (size_t)2 * nl.stride + k) : k;
+      int jn1 = 3 < cnt ? __ldg(nl.nb + (size_t)3 * nl.stride + k) : k;
+      const int j0 = 0 < cnt ? __ldg(nl.nb + k) : k;
+      const int j1 = 1 < cnt ? __ldg(nl.nb + (size_t)1 * nl.stride + k) : k;
+      D4 ga = ldg4(Gin + j0), gb = ldg4(Gin + j1), ha{0.0, 0.0, 0.0, 0.0}, hb{0.0, 0.0, 0.0, 0.0};
+      double ra = PLANE ? (S.use_radii ? __ldg(st.r + j0) : 1.0) : 0.0;
+      double rb = PLANE ? (S.use_radii ? __ldg(st.r + j1) : 1.0) : 0.0;
+      if (!PLANE && ALIGN != ABP_ALIGN_NONE) { ha = ldg4(Hin + j0); hb = ldg4(Hin + j1); }
+      for (int q = 0; q < cnt; q += 2) {
+        const D4 g0 = ga, g1 = gb, h0 = ha, h1 = hb;
+        const double r0 = PLANE ? ra : g0.w, r1 = PLANE ? rb : g1.w;
+        if (q + 2 < cnt) {
+          ga = ldg4(Gin + jn0);
+          gb = ldg4(Gin + jn1);
+          if (PLANE) { ra = S.use_radii ? __ldg(st.r + jn0) : 1.0; rb = S.use_radii ? __ldg(st.r + jn1) : 1.0; }
+          if (!PLANE && ALIGN != ABP_ALIGN_NONE) { ha = ldg4(Hin + jn0); hb = ldg4(Hin + jn1); }
+          jn0 = q + 4 < cnt ? __ldg(nl.nb + (size_t)(q + 4) * nl.stride + k) : k;
+          jn1 = q + 5 < cnt ? __ldg(nl.nb + (size_t)(q + 5) * nl.stride + k) : k;
+        }
+        abp_pair_term<SHAPE, ALIGN, ENERGY>(S, x, y, z, nx, ny, nz, ri, g0, h0, r0, q >= lo, fx, fy, fz, tx, ty, tz,
+                                            epair, ealign);
+        abp_pair_term<SHAPE, ALIGN, ENERGY>(S, x, y, z, nx, ny, nz, ri, g1, h1, r1, q + 1 >= lo, fx, fy, fz, tx, ty,
+                                            tz, epair, ealign);
+      }
+    } else if constexpr (abp_pipelined(VAR)) {
       // one neighbour per iteration: its record was requested during the
       // previous iteration, the entry after it two iterations ahead
       int jnext = 1 < cnt ? __ldg(nl.nb + (size_t)1 * nl.stride + k) : k;

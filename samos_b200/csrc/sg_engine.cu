@@ -1669,6 +1669,10 @@ static void launch_abp3(sg_system* s, bool apply_e1, bool last, bool energy) {
     case 25: launch_abp_v<SHAPE, ALIGN, SP, false, 25>(s, apply_e1, last); break;
     case 26: launch_abp_v<SHAPE, ALIGN, SP, false, 26>(s, apply_e1, last); break;
     case 27: launch_abp_v<SHAPE, ALIGN, SP, false, 27>(s, apply_e1, last); break;
+    case 28: launch_abp_v<SHAPE, ALIGN, SP, false, 28>(s, apply_e1, last); break;
+    case 29: launch_abp_v<SHAPE, ALIGN, SP, false, 29>(s, apply_e1, last); break;
+    case 30: launch_abp_v<SHAPE, ALIGN, SP, false, 30>(s, apply_e1, last); break;
+    case 31: launch_abp_v<SHAPE, ALIGN, SP, false, 31>(s, apply_e1, last); break;
     case 0: launch_abp_v<SHAPE, ALIGN, SP, false, 0>(s, apply_e1, last); break;
     case 1: launch_abp_v<SHAPE, ALIGN, SP, false, 1>(s, apply_e1, last); break;
     case 2: launch_abp_v<SHAPE, ALIGN, SP, false, 2>(s, apply_e1, last); break;

@@ -405,7 +405,7 @@ VARIANT_CASES = {
 
 
 @pytest.mark.parametrize("case", sorted(VARIANT_CASES))
-@pytest.mark.parametrize("variant", list(range(28)))
+@pytest.mark.parametrize("variant", list(range(32)))
 def test_every_tuning_variant_gives_identical_bits(variant, case):
     c = VARIANT_CASES[case]
     n = c["n"]
