@@ -629,13 +629,12 @@ def main():
     for a in host_out.values():
         a[:] = 0.0
     t0 = time.perf_counter()
-    for f in fields_in:
-        eng.upload(f, host_in[f])
+    eng.upload_fields(host_in)  # all fields' copies back to back, one wait
     t_up = time.perf_counter()
     eng.build_nlist()
     est = eng.run(e2e_steps - 1)
     t_run = time.perf_counter()
-    outs = {f: eng.download(f, out=host_out[f]) for f in fields_out}
+    outs = eng.download_fields(fields_out, out=host_out)
     t_end = time.perf_counter()
     e2e_s = max_over_ranks(t_end - t0, ws)
     e2e_split = dict(upload_ms=(t_up - t0) * 1e3, build_and_run_ms=(t_run - t_up) * 1e3,

@@ -86,6 +86,16 @@ int  sg_set_timestep(sg_system* s, double dt);
  * "ix","iy","iz".  Arrays are in particle-id order (length n_particles[r]). */
 int  sg_upload(sg_system* s, int replica, const char* field, const void* host);
 int  sg_download(sg_system* s, int replica, const char* field, void* host);
+/* Several fields of one replica in one call (System's reader / a dump's
+ * loop over Particle fields, src/system/system.cpp:76-450,
+ * src/dump/dump.cpp:504-708): the same as one sg_upload / sg_download per
+ * field, but every copy is enqueued back to back and the call waits once.
+ * From page-locked host arrays (sg_host_alloc) the copies run at the link's
+ * bandwidth.                                                                */
+int  sg_upload_fields(sg_system* s, int replica, int nfields, const char* const* fields,
+                      const void* const* hosts);
+int  sg_download_fields(sg_system* s, int replica, int nfields, const char* const* fields,
+                        void* const* hosts);
 /* Page-locked host memory for the arrays given to sg_upload / sg_download:
  * copies from and to it run at the link's speed, where pageable arrays go
  * through the driver's staging buffers (and a fresh pageable destination is

@@ -92,6 +92,9 @@ struct sg_system {
   // per-particle terms by replica offset + id, 3 arrays of `slots` doubles
   int fire_ordered = 0;
   double* fire_terms = nullptr;
+  // multi-field transfers: staging for several fields of one replica at once
+  double* xfer_multi = nullptr;
+  size_t xfer_multi_cap = 0;  // doubles
   double dt_global = 0.0;
   bool e1_applied = false;
   bool forces_fresh = false;  // forces equal those the next start-of-step pass would compute
@@ -458,6 +461,105 @@ static int field_ptr(sg_system* s, const char* field, void** p, bool* is_int, in
     *p = nullptr; *is_int = false; return SG_OK;
   }
   return fail(s, SG_ERR_ARG, std::string("unknown particle field '") + field + "'");
+}
+
+// Staging for `nf` fields of a replica (grown on demand, kept).
+static int xfer_multi_ready(sg_system* s, int nf) {
+  int rc = xfer_ready(s);
+  if (rc) return rc;
+  int maxn = 0;
+  for (int v : s->n) maxn = std::max(maxn, v);
+  const size_t need = (size_t)nf * (size_t)std::max(1, maxn);
+  if (need <= s->xfer_multi_cap) return SG_OK;
+  s->mem.release(s->xfer_multi);
+  s->xfer_multi = s->mem.alloc<double>(need);
+  if (!s->xfer_multi) { s->mem.err = cudaSuccess; s->xfer_multi_cap = 0; return fail(s, SG_ERR_NOMEM, "transfer staging"); }
+  s->xfer_multi_cap = need;
+  return SG_OK;
+}
+
+// Several fields in one go: every copy is enqueued back to back on the
+// engine stream (the DMA engine streams them without gaps), then the id-order
+// gathers or scatters, and one synchronisation at the end instead of one per
+// field.  Surface normals (kept on the host) go through the one-field path.
+static int xfer_fields(sg_system* s, int replica, int nf, const char* const* fields, void* const* hosts,
+                       bool to_device) {
+  if (!s || replica < 0 || replica >= s->nrep || nf < 1 || !fields || !hosts)
+    return fail(s, SG_ERR_ARG, "multi-field transfer: bad argument");
+  std::vector<void*> dps(nf);
+  std::vector<char> ints(nf), staged(nf);
+  for (int i = 0; i < nf; i++) {
+    if (!fields[i] || !hosts[i]) return fail(s, SG_ERR_ARG, "multi-field transfer: null field or buffer");
+    bool is_int; int nfld;
+    int rc = field_ptr(s, fields[i], &dps[i], &is_int, &nfld);
+    if (rc) return rc;
+    ints[i] = is_int;
+    staged[i] = dps[i] != nullptr;
+    if (to_device && !std::strcmp(fields[i], "type")) {
+      const int* h = (const int*)hosts[i];
+      for (int k = 0; k < s->n[replica]; k++)
+        if (h[k] < 1 || h[k] > s->ntypes) return fail(s, SG_ERR_ARG, "particle type outside 1..ntypes");
+    }
+  }
+  int rc = xfer_multi_ready(s, nf);
+  if (rc) return rc;
+  const int n = s->n[replica], off = s->off[replica];
+  if (n == 0) return SG_OK;
+  const int g = (n + 255) / 256;
+  const size_t slice = (size_t)std::max(1, n);
+  CU(s, cudaMemsetAsync(s->xerr, 0, sizeof(int), s->stream));
+  if (to_device) {
+    for (int i = 0; i < nf; i++)
+      if (staged[i])
+        CU(s, cudaMemcpyAsync(s->xfer_multi + i * slice, hosts[i], (ints[i] ? sizeof(int) : sizeof(double)) * n,
+                              cudaMemcpyHostToDevice, s->stream));
+    for (int i = 0; i < nf; i++) {
+      if (!staged[i]) continue;
+      if (ints[i])
+        k_gather_ids<int><<<g, 256, 0, s->stream>>>((int*)dps[i] + off, (const int*)(s->xfer_multi + i * slice),
+                                                   s->st.id + off, n, s->xerr);
+      else
+        k_gather_ids<double><<<g, 256, 0, s->stream>>>((double*)dps[i] + off, s->xfer_multi + i * slice,
+                                                      s->st.id + off, n, s->xerr);
+    }
+  } else {
+    for (int i = 0; i < nf; i++) {
+      if (!staged[i]) continue;
+      if (ints[i])
+        k_scatter_ids<int><<<g, 256, 0, s->stream>>>((int*)(s->xfer_multi + i * slice), (const int*)dps[i] + off,
+                                                    s->st.id + off, n, s->xerr);
+      else
+        k_scatter_ids<double><<<g, 256, 0, s->stream>>>(s->xfer_multi + i * slice, (const double*)dps[i] + off,
+                                                       s->st.id + off, n, s->xerr);
+    }
+    for (int i = 0; i < nf; i++)
+      if (staged[i])
+        CU(s, cudaMemcpyAsync(hosts[i], s->xfer_multi + i * slice, (ints[i] ? sizeof(int) : sizeof(double)) * n,
+                              cudaMemcpyDeviceToHost, s->stream));
+  }
+  CU(s, cudaGetLastError());
+  int bad = 0;
+  CU(s, cudaMemcpyAsync(&bad, s->xerr, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  CU(s, cudaStreamSynchronize(s->stream));
+  if (bad) return fail(s, SG_ERR_STATE, "corrupt id map");
+  for (int i = 0; i < nf; i++)  // surface normals: the one-field path
+    if (!staged[i]) {
+      rc = to_device ? sg_upload(s, replica, fields[i], hosts[i]) : sg_download(s, replica, fields[i], hosts[i]);
+      if (rc) return rc;
+    }
+  if (to_device) {
+    s->e1_applied = false;
+    s->forces_fresh = false;
+  }
+  return SG_OK;
+}
+
+int sg_upload_fields(sg_system* s, int replica, int nfields, const char* const* fields, const void* const* hosts) {
+  return xfer_fields(s, replica, nfields, fields, const_cast<void* const*>(hosts), true);
+}
+
+int sg_download_fields(sg_system* s, int replica, int nfields, const char* const* fields, void* const* hosts) {
+  return xfer_fields(s, replica, nfields, fields, hosts, false);
 }
 
 int sg_upload(sg_system* s, int replica, const char* field, const void* host) {

@@ -112,6 +112,8 @@ def load() -> C.CDLL:
         "sg_set_variant": (I, [P, I]),
         "sg_set_build": (I, [P, I]),
         "sg_set_fire_order": (I, [P, I]),
+        "sg_upload_fields": (I, [P, I, I, C.POINTER(C.c_char_p), C.POINTER(C.c_void_p)]),
+        "sg_download_fields": (I, [P, I, I, C.POINTER(C.c_char_p), C.POINTER(C.c_void_p)]),
         "sg_set_generic_occupancy": (I, [P, I]), "sg_get_generic_occupancy": (I, [P]),
         "sg_get_variant": (I, [P]),
         "sg_compute_static": (I, [I, D, D, D, I, D, D] + [P] * 7 + [D, D, I, I, D, D] + [P] * 6 + [P]),
@@ -210,6 +212,35 @@ class Engine:
         if a.shape != (self.n[replica],):
             raise ValueError(f"{field}: expected {self.n[replica]} values, got {a.shape}")
         self._check(self.lib.sg_upload(self.h, replica, field.encode(), a.ctypes.data_as(C.c_void_p)))
+
+    def upload_fields(self, arrays: dict, replica: int = 0) -> None:
+        """Several fields at once ({name: values}): copies enqueued back to back, one wait."""
+        names, bufs = [], []
+        for field, values in arrays.items():
+            dtype = np.int32 if field in INT_FIELDS else np.float64
+            a = values if (isinstance(values, np.ndarray) and values.dtype == dtype and values.flags.c_contiguous) \
+                else np.ascontiguousarray(values, dtype=dtype)
+            if a.shape != (self.n[replica],):
+                raise ValueError(f"{field}: expected {self.n[replica]} values, got {a.shape}")
+            names.append(field.encode())
+            bufs.append(a)
+        cn = (C.c_char_p * len(names))(*names)
+        cp = (C.c_void_p * len(bufs))(*[b.ctypes.data for b in bufs])
+        self._check(self.lib.sg_upload_fields(self.h, replica, len(names), cn, cp))
+
+    def download_fields(self, fields, replica: int = 0, out: dict | None = None) -> dict:
+        """Several fields at once; written into `out[field]` arrays when given."""
+        res = {}
+        for f in fields:
+            dtype = np.int32 if f in INT_FIELDS else np.float64
+            a = out[f] if out is not None and f in out else np.empty(self.n[replica], dtype=dtype)
+            if a.dtype != dtype or a.shape != (self.n[replica],) or not a.flags.c_contiguous or not a.flags.writeable:
+                raise ValueError(f"{f}: out must be a writeable contiguous {dtype} array of {self.n[replica]}")
+            res[f] = a
+        cn = (C.c_char_p * len(res))(*[f.encode() for f in res])
+        cp = (C.c_void_p * len(res))(*[a.ctypes.data for a in res.values()])
+        self._check(self.lib.sg_download_fields(self.h, replica, len(res), cn, cp))
+        return res
 
     def download(self, field: str, replica: int = 0, out: np.ndarray | None = None) -> np.ndarray:
         """The field in particle-id order; written into `out` when given
