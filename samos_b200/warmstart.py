@@ -303,12 +303,23 @@ def eval_loss(net: WarmStartNet, batch: Batch) -> float:
 
 # -- use: warm-started FIRE with plain FIRE as the fallback ----------------------------
 def relax(insts, net: WarmStartNet | None, k: float = 1.0, dt: float = 0.01, dt_max: float = 0.2,
-          fmax: float = 1e-10, max_steps: int = 400000) -> dict:
+          fmax: float = 1e-10, max_steps: int = 400000, handoff: float | None = None) -> dict:
     """Relax every instance to Fmax < fmax in one engine.  With a network,
     the predicted displacement is applied first, and every replica whose
-    energy it raises goes back to its quench (plain FIRE).  Returns per-replica
-    steps, final energies and the device time of inference + minimisation."""
+    energy it raises goes back to its start (plain FIRE is the fallback).
+    With `handoff`, plain FIRE first runs every instance to max |F_i| <
+    handoff, and the network then acts on that state before a fresh FIRE
+    finishes.  Returns per-replica steps (both stretches summed), final
+    energies and the device time of minimisation + inference."""
     from .ensemble import plane_fire_ensemble
+    head_ms, head_steps = 0.0, np.zeros(len(insts), np.int64)
+    if handoff is not None and net is not None:
+        eng0 = plane_fire_ensemble(insts, k=k, dt=dt, dt_max=dt_max, fmax=handoff)
+        eng0.build_nlist()
+        head_steps, st0 = eng0.minimize(max_steps)
+        head_ms = st0.device_ms
+        insts = snapshot(eng0, insts)
+        eng0.close()
     eng = plane_fire_ensemble(insts, k=k, dt=dt, dt_max=dt_max, fmax=fmax)
     eng.build_nlist()
     R = len(insts)
