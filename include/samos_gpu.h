@@ -262,13 +262,12 @@ int  sg_set_path(sg_system* s, int path);
 int  sg_set_variant(sg_system* s, int variant);
 int  sg_get_variant(const sg_system* s);
 /* Neighbour-list build kernel: 0 = automatic (lanes of a team share one
- * particle's 27-cell stencil when fewer than 2^16 particles are rebuilt;
- * from 2^16 on, cell tiles staged in shared memory when every rebuilt
- * replica is quasi-2-D -- cell path, at least 3 cells along x and y, exactly
- * 3 along z -- else one thread per particle), 1 = always one thread per
- * particle, 2 = always teams, 3 = cell tiles wherever eligible (one thread
- * per particle elsewhere).  All build the same lists.  No reference
- * counterpart.                                                              */
+ * particle's 27-cell stencil when fewer than 2^16 particles are rebuilt,
+ * one thread per particle otherwise), 1 = always one thread per particle,
+ * 2 = always teams, 3 = cell tiles staged in shared memory for quasi-2-D
+ * replicas (cell path, at least 3 cells along x and y, exactly 3 along z;
+ * one thread per particle elsewhere; slower than 1 on the plane workloads
+ * measured).  All build the same lists.  No reference counterpart.         */
 int  sg_set_build(sg_system* s, int mode);
 /* Order of FIRE's sums P = sum v.F, |F|^2 and |v|^2 (integrator_fire.cpp:
  * 79-94), whose values steer dt, alpha and the velocity mixing:

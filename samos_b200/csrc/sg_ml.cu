@@ -12,10 +12,14 @@
 //   disp_i = sum_j w_ij d_ij / r_ij                         edge kernel, FP32
 // The 64-wide products are node-level (the first edge layer is summed before
 // W1b, the second is split into P_i + Q_j), so the tensor-core GEMMs are
-// [slots x 64] x [64 x 64|128] with FP32 accumulation (mma.sync m16n8k16 BF16).
+// [slots x 64] x [64 x 64|128] with FP32 accumulation (mma.sync m16n8k16 BF16),
+// and the weight gradients, reductions over every slot ([64 x slots] x
+// [slots x 64|128]), run on the 5th-generation tensor cores: TMA tiles,
+// tcgen05.mma with the accumulator in tensor memory (k_ml_wgrad_tc).
 // Activations s, h and the GEMM operands of the backward pass are BF16.
 #include "samos_gpu.h"
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -140,79 +144,224 @@ __global__ void __launch_bounds__(128) k_ml_gemm(const __nv_bfloat16* __restrict
   }
 }
 
-// ---- weight gradient: W[k][n] = sum_m X[m][k] G[m][n] ---------------------------
-// Fixed grid; every block reduces a contiguous row range into its own
-// [K x N] partial (deterministic), k_ml_reduce sums the partials in order.
-// Warp w of 4 owns the n-slice [32 * (w % (N/32)), +32) and, when N == 64,
-// every other 16-row chunk.
-template <int K, int N>
-__global__ void __launch_bounds__(128) k_ml_wgrad(const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ G,
-                                                  int M, float* __restrict__ partial) {
-  constexpr int SLICES = N / 32, REPL = 4 / SLICES;  // warps per slice
-  __shared__ __align__(16) __nv_bfloat16 sX[4][16 * K];
-  __shared__ __align__(16) __nv_bfloat16 sG[4][16 * N];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int slice = warp % SLICES, rep = warp / SLICES;
-  const int rows_per_block = (M + gridDim.x - 1) / gridDim.x;
-  const int m_begin = blockIdx.x * rows_per_block, m_end = min(M, m_begin + rows_per_block);
-  float acc[K / 16][4][4];
+// ---- weight gradient on tcgen05: W[k][n] = sum_m X[m][k] G[m][n] ----------------
+// The reduction runs over all slots, so it is the MMA's K dimension: per
+// 64-row chunk, D[128 x 64] += G_chunk^T (A: M = G's features, zero rows
+// above NF) x X_chunk (B: N = X's 64 features), four K = 16 steps.  Both
+// operands are the tiles exactly as TMA lands them with the 128-byte swizzle
+// (rows of 64 BF16 features = 128 B; "MN-major" in the MMA's terms, 8-row
+// groups 1024 B apart).  One CTA per SM owns a contiguous run of chunks and a
+// private [64 x NF] FP32 partial (deterministic: chunks in order, partials
+// summed in block order by k_ml_reduce).  Thread 0 issues the TMA loads (four
+// stages) and the MMAs; tcgen05.commit releases a stage; the accumulator is
+// read back with tcgen05.ld by the four warps, one 32-lane quarter each.
+// Every mbarrier wait is bounded: on a timeout the kernel records it in
+// *err, drains what it issued, frees its tensor memory and returns.
+constexpr int WG_STAGES = 4;
+constexpr int WG_ROWS = 64;                     // slots per chunk (4 MMA K steps)
+constexpr int WG_A_BYTES = 2 * WG_ROWS * 128;   // G^T: two 128-B feature groups
+constexpr int WG_B_BYTES = WG_ROWS * 128;       // X: one 128-B feature group
+constexpr int WG_STAGE_BYTES = WG_A_BYTES + WG_B_BYTES;
+constexpr int WG_SMEM = 1024 + WG_STAGES * WG_STAGE_BYTES + 128;
+constexpr uint32_t WG_TMEM_COLS = 64;
+__device__ int g_wgrad_err;  // set by a k_ml_wgrad_tc whose bounded wait ran out
+constexpr long long WG_SPIN_LIMIT = 1ll << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+  for (long long it = 0; it < WG_SPIN_LIMIT; it++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok) : "r"(bar), "r"(phase) : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+// shared-memory matrix descriptor of a 128-B-swizzled tile (layout type 2,
+// descriptor version 1): start address, leading byte offset (between 64-wide
+// feature groups), stride byte offset (between 8-row groups), all >> 4
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// instruction descriptor: D FP32, A and B BF16, both MN-major, N = 64, M = 128
+constexpr uint32_t WG_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((64u >> 3) << 17) |
+                              ((128u >> 4) << 24);
+
+template <int NF>
+__global__ void __launch_bounds__(128, 1)
+k_ml_wgrad_tc(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmG, int M,
+              int chunks_per_block, float* __restrict__ partial, int* __restrict__ err) {
+  static_assert(NF == 64 || NF == 128, "G has 64 or 128 features");
+  extern __shared__ uint8_t wg_smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(wg_smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + WG_STAGES * WG_STAGE_BYTES);  // full[S], empty[S], done
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * WG_STAGES + 1);
+  __shared__ int abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nchunks = (M + WG_ROWS - 1) / WG_ROWS;
+  const int c0 = blockIdx.x * chunks_per_block;
+  const int n = max(0, min(nchunks, c0 + chunks_per_block) - c0);
+
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+    for (int i = 0; i < 2 * WG_STAGES + 1; i++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bars + i)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (NF == 64) {  // the A tiles' second feature group stays zero (rows 64..127 of D)
+    for (int s = 0; s < WG_STAGES; s++)
+      for (int i = threadIdx.x; i < WG_ROWS * 128 / 16; i += blockDim.x)
+        reinterpret_cast<uint4*>(smem + s * WG_STAGE_BYTES + WG_ROWS * 128)[i] = make_uint4(0u, 0u, 0u, 0u);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                 ::"r"(smem_u32(tmem_slot)), "r"(WG_TMEM_COLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + WG_STAGES), done = smem_u32(bars + 2 * WG_STAGES);
+
+  if (threadIdx.x == 0 && n > 0) {
+    const uint64_t mapX = reinterpret_cast<uint64_t>(&tmX), mapG = reinterpret_cast<uint64_t>(&tmG);
+    constexpr uint32_t tx_bytes = (NF == 128 ? WG_A_BYTES : WG_ROWS * 128) + WG_B_BYTES;
+    auto issue = [&](int i) {  // TMA loads of chunk i into stage i % S
+      const int s = i % WG_STAGES;
+      const uint32_t a = smem_u32(smem + s * WG_STAGE_BYTES), b = a + WG_A_BYTES, bar = full0 + 8 * s;
+      const int row = (c0 + i) * WG_ROWS;
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
+      asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+                   ::"r"(a), "l"(mapG), "r"(0), "r"(row), "r"(bar) : "memory");
+      if (NF == 128)
+        asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+                     ::"r"(a + WG_ROWS * 128), "l"(mapG), "r"(64), "r"(row), "r"(bar) : "memory");
+      asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+                   ::"r"(b), "l"(mapX), "r"(0), "r"(row), "r"(bar) : "memory");
+    };
+    const int pre = min(WG_STAGES, n);
+    for (int i = 0; i < pre; i++) issue(i);
+    int issued = pre, consumed = 0;
+    bool ok = true;
+    for (int i = 0; i < n && ok; i++) {
+      const int s = i % WG_STAGES;
+      const uint32_t phase = (uint32_t)((i / WG_STAGES) & 1);
+      if (!mbar_wait(full0 + 8 * s, phase)) { ok = false; break; }
+      consumed = i + 1;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t a = smem_u32(smem + s * WG_STAGE_BYTES), b = a + WG_A_BYTES;
 #pragma unroll
-  for (int a = 0; a < K / 16; a++)
-#pragma unroll
-    for (int b = 0; b < 4; b++) acc[a][b][0] = acc[a][b][1] = acc[a][b][2] = acc[a][b][3] = 0.f;
-  for (int c0 = m_begin + 16 * rep; c0 < m_end; c0 += 16 * REPL) {
-    // stage this warp's 16-row chunk of X and G
-    for (int idx = lane; idx < 16 * K; idx += 32) {
-      const int rr = idx / K, kk = idx % K, m = c0 + rr;
-      sX[warp][idx] = m < m_end ? X[(size_t)m * K + kk] : __float2bfloat16_rn(0.f);
-    }
-    for (int idx = lane; idx < 16 * N; idx += 32) {
-      const int rr = idx / N, nn = idx % N, m = c0 + rr;
-      sG[warp][idx] = m < m_end ? G[(size_t)m * N + nn] : __float2bfloat16_rn(0.f);
-    }
-    __syncwarp();
-    // A = X^T chunk: A[kf][row]; B = G chunk: B[row][n]
-#pragma unroll
-    for (int mt = 0; mt < K / 16; mt++) {
-      const int kf = mt * 16 + g;
-      __nv_bfloat162 p0, p1, p2, p3;
-      p0.x = sX[warp][(2 * t) * K + kf];         p0.y = sX[warp][(2 * t + 1) * K + kf];
-      p1.x = sX[warp][(2 * t) * K + kf + 8];     p1.y = sX[warp][(2 * t + 1) * K + kf + 8];
-      p2.x = sX[warp][(2 * t + 8) * K + kf];     p2.y = sX[warp][(2 * t + 9) * K + kf];
-      p3.x = sX[warp][(2 * t + 8) * K + kf + 8]; p3.y = sX[warp][(2 * t + 9) * K + kf + 8];
-      const uint32_t a0 = *reinterpret_cast<uint32_t*>(&p0), a1 = *reinterpret_cast<uint32_t*>(&p1);
-      const uint32_t a2 = *reinterpret_cast<uint32_t*>(&p2), a3 = *reinterpret_cast<uint32_t*>(&p3);
-#pragma unroll
-      for (int nt = 0; nt < 4; nt++) {
-        const int n = slice * 32 + nt * 8 + g;
-        __nv_bfloat162 q0, q1;
-        q0.x = sG[warp][(2 * t) * N + n];     q0.y = sG[warp][(2 * t + 1) * N + n];
-        q1.x = sG[warp][(2 * t + 8) * N + n]; q1.y = sG[warp][(2 * t + 9) * N + n];
-        mma16816(acc[mt][nt], a0, a1, a2, a3, *reinterpret_cast<uint32_t*>(&q0), *reinterpret_cast<uint32_t*>(&q1));
+      for (int k = 0; k < WG_ROWS / 16; k++) {  // 16 slots per MMA: two 8-row groups, 2048 B
+        const uint64_t da = umma_desc_sw128(a + k * 2048, WG_ROWS * 128, 1024);
+        const uint64_t db = umma_desc_sw128(b + k * 2048, WG_ROWS * 128, 1024);
+        const uint32_t acc = (i > 0 || k > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+            ::"r"(tmem), "l"(da), "l"(db), "r"(WG_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                   ::"r"(empty0 + 8 * s) : "memory");
+      if (i + WG_STAGES < n) {  // refill this stage once its MMAs have read it
+        if (!mbar_wait(empty0 + 8 * s, phase)) { ok = false; break; }
+        issue(i + WG_STAGES);
+        issued++;
       }
     }
-    __syncwarp();
-  }
-  // each slice is owned by REPL warps: the first writes, the others add in order
-  float* out = partial + (size_t)blockIdx.x * K * N;
-  for (int r = 0; r < REPL; r++) {
-    if (rep == r) {
-#pragma unroll
-      for (int mt = 0; mt < K / 16; mt++)
-#pragma unroll
-        for (int nt = 0; nt < 4; nt++) {
-          const int kf = mt * 16 + g, n = slice * 32 + nt * 8 + 2 * t;
-          float* o0 = out + kf * N + n;
-          float* o1 = out + (kf + 8) * N + n;
-          if (r == 0) {
-            o0[0] = acc[mt][nt][0]; o0[1] = acc[mt][nt][1]; o1[0] = acc[mt][nt][2]; o1[1] = acc[mt][nt][3];
-          } else {
-            o0[0] += acc[mt][nt][0]; o0[1] += acc[mt][nt][1]; o1[0] += acc[mt][nt][2]; o1[1] += acc[mt][nt][3];
-          }
-        }
+    if (!ok) {  // timed out: drain the loads still in flight before leaving
+      atomicExch(err, 1);
+      abort_flag = 1;
+      for (int i = consumed; i < issued; i++) mbar_wait(full0 + 8 * (i % WG_STAGES), (uint32_t)((i / WG_STAGES) & 1));
     }
-    __syncthreads();
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(done)
+                 : "memory");
   }
+  __syncthreads();
+  bool have = n > 0 && !abort_flag;
+  if (n > 0 && !mbar_wait(done, 0)) {  // every MMA of this CTA has completed
+    if (lane == 0) atomicExch(err, 1);
+    have = false;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  // D row m (G feature) is TMEM lane m, column j (X feature) is column j
+  float* out = partial + (size_t)blockIdx.x * F * NF;
+  const int m = warp * 32 + lane;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    uint32_t r[16];
+    if (n > 0) {
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(q * 16);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+    }
+    if (m < NF)
+#pragma unroll
+      for (int j = 0; j < 16; j++) out[(size_t)(q * 16 + j) * NF + m] = have ? __uint_as_float(r[j]) : 0.f;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(WG_TMEM_COLS) : "memory");
+}
+
+// 2-D row-major BF16 tensor map [rows x cols] with 64 x 64 boxes and the
+// 128-byte swizzle (cuTensorMapEncodeTiled, fetched through the runtime so
+// the library does not link the driver library)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+bool make_bf16_map(CUtensorMap* map, const void* base, int rows, int cols) {
+  static EncodeTiledFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(f);
+  }();
+  if (!fn || (reinterpret_cast<uintptr_t>(base) & 15) || rows < 1) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+  const cuuint32_t box[2] = {64, WG_ROWS};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// partial[b] = X^T G over block b's chunks, for X [M x 64], G [M x NF] (BF16)
+template <int NF>
+int launch_wgrad_tc(const void* X, const void* G, int M, int blocks, float* partial, int* err, cudaStream_t st) {
+  CUtensorMap mx, mg;
+  if (!make_bf16_map(&mx, X, M, F) || !make_bf16_map(&mg, G, M, NF)) return SG_ERR_CUDA;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_ml_wgrad_tc<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, WG_SMEM) != cudaSuccess)
+      return SG_ERR_CUDA;
+    attr = true;
+  }
+  const int nchunks = (M + WG_ROWS - 1) / WG_ROWS;
+  const int per = (nchunks + blocks - 1) / blocks;
+  k_ml_wgrad_tc<NF><<<blocks, 128, WG_SMEM, st>>>(mx, mg, M, per, partial, err);
+  return cudaGetLastError() == cudaSuccess ? SG_OK : SG_ERR_CUDA;
 }
 
 // out[i] += sum_b partial[b][i]   (fixed order)
@@ -494,9 +643,13 @@ int sg_mlp_backward(const sg_view* V, const double* box, double rc, const float*
     const size_t len = (size_t)M * 2 * F;
     k_ml_to_bf16<<<(unsigned)((len + 255) / 256), 256, 0, st>>>(gPQ, (__nv_bfloat16*)gPQ16, len);
   }
-  // gWpq = h^T gPQ
+  // gWpq = h^T gPQ (tensor cores, one CTA per SM)
   constexpr int WG_BLOCKS = 148;
-  k_ml_wgrad<F, 2 * F><<<WG_BLOCKS, 128, 0, st>>>((const __nv_bfloat16*)h16, (const __nv_bfloat16*)gPQ16, M, part);
+  int* werr = nullptr;
+  if (cudaGetSymbolAddress((void**)&werr, g_wgrad_err) != cudaSuccess) return SG_ERR_CUDA;
+  cudaMemsetAsync(werr, 0, sizeof(int), st);
+  int wrc = launch_wgrad_tc<2 * F>(h16, gPQ16, M, WG_BLOCKS, part, werr, st);
+  if (wrc) return wrc;
   k_ml_reduce<<<(F * 2 * F + 255) / 256, 256, 0, st>>>(part, WG_BLOCKS, F * 2 * F, grad + NP_WPQ);
   // gh = gPQ Wpq^T
   const int gb = (M + 63) / 64;
@@ -505,7 +658,8 @@ int sg_mlp_backward(const sg_view* V, const double* box, double rc, const float*
   // through relu(s W1b + b1b)
   k_ml_relu_bwd<<<WG_BLOCKS, 256, 0, st>>>(M, gh, (const __nv_bfloat16*)h16, (__nv_bfloat16*)gpre16, part);
   k_ml_reduce<<<1, 64, 0, st>>>(part, WG_BLOCKS, F, grad + NP_B1B);
-  k_ml_wgrad<F, F><<<WG_BLOCKS, 128, 0, st>>>((const __nv_bfloat16*)s16, (const __nv_bfloat16*)gpre16, M, part);
+  wrc = launch_wgrad_tc<F>(s16, gpre16, M, WG_BLOCKS, part, werr, st);
+  if (wrc) return wrc;
   k_ml_reduce<<<(F * F + 255) / 256, 256, 0, st>>>(part, WG_BLOCKS, F * F, grad + NP_W1B);
   // gs = gpre W1b^T
   k_ml_gemm<F, F><<<gb, 128, 0, st>>>((const __nv_bfloat16*)gpre16, (const __nv_bfloat16*)W1b16, M, nullptr, 0, box, gs,
@@ -516,7 +670,12 @@ int sg_mlp_backward(const sg_view* V, const double* box, double rc, const float*
   k_ml_reduce<<<(L1_GRAD + 255) / 256, 256, 0, st>>>(part, EDGE_BLOCKS, L1_GRAD, red);
   k_ml_place<<<1, 256, 0, st>>>(red, 256, grad, NP_W1A);
   k_ml_place<<<1, 64, 0, st>>>(red + 256, 64, grad, NP_B1A);
-  return cudaGetLastError() == cudaSuccess ? SG_OK : SG_ERR_CUDA;
+  if (cudaGetLastError() != cudaSuccess) return SG_ERR_CUDA;
+  int timed_out = 0;
+  if (cudaMemcpyAsync(&timed_out, werr, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return SG_ERR_CUDA;
+  return timed_out ? SG_ERR_TIMEOUT : SG_OK;
 }
 
 // x += dx, y += dy for the slots with box > 0 (scale 1), wrapped back into
