@@ -398,12 +398,31 @@ def main(argv=None) -> int:
     e.add_argument("--seed", type=int, default=99)
     e.add_argument("--handoff", type=float, default=None, help="default: the value stored with the parameters")
     e.add_argument("--out")
+    sw = sub.add_parser("sweep", help="hand-off sweep: per tolerance, train on hand-off states and evaluate")
+    sw.add_argument("--handoffs", default="1e-2,1e-3,1e-4")
+    sw.add_argument("--count", type=int, default=500)
+    sw.add_argument("--steps", type=int, default=1000)
+    sw.add_argument("--eval", type=int, default=128)
     pr = sub.add_parser("profile", help="a few training steps and one inference on one batch (for profilers)")
     pr.add_argument("--count", type=int, default=64)
     pr.add_argument("--n", type=int, default=4096)
     pr.add_argument("--steps", type=int, default=3)
     pr.add_argument("--fmax", type=float, default=1e-3, help="FIRE tolerance of the targets (loose: fast)")
     a = ap.parse_args(argv)
+    if a.cmd == "sweep":
+        data = quench_set(a.count + 64, 4096, 4096, 0.84, 0.90, seed=1)
+        insts = quench_set(a.eval, 1024, 16384, 0.84, 0.90, seed=99)
+        plain = relax(insts, None)
+        for tau in (float(t) for t in a.handoffs.split(",")):
+            net = WarmStartNet(seed=1)
+            batches = [Batch(net, data[i:i + 500], handoff=tau) for i in range(0, a.count, 500)]
+            held = Batch(net, data[a.count:], handoff=tau)
+            hist = train(net, batches, a.steps)
+            rep = dict(handoff=tau, loss_first=hist[0], loss_last=float(np.mean(hist[-5:])),
+                       held_out_start_loss=mean_target_sq(held), held_out_loss=eval_loss(net, held))
+            rep.update(summarize(plain, relax(insts, net, handoff=tau), insts))
+            print(json.dumps(rep), flush=True)
+        return 0
     if a.cmd == "profile":
         net = WarmStartNet(seed=1)
         b = Batch(net, quench_set(a.count, a.n, a.n, 0.84, 0.90, seed=5), fmax=a.fmax)
