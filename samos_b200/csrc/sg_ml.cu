@@ -12,10 +12,11 @@
 //   disp_i = sum_j w_ij d_ij / r_ij                         edge kernel, FP32
 // The 64-wide products are node-level (the first edge layer is summed before
 // W1b, the second is split into P_i + Q_j), so the tensor-core GEMMs are
-// [slots x 64] x [64 x 64|128] with FP32 accumulation (mma.sync m16n8k16 BF16),
-// and the weight gradients, reductions over every slot ([64 x slots] x
-// [slots x 64|128]), run on the 5th-generation tensor cores: TMA tiles,
-// tcgen05.mma with the accumulator in tensor memory (k_ml_wgrad_tc).
+// [slots x 64] x [64 x 64|128] with FP32 accumulation (k_ml_gemm_tc), and the
+// weight gradients are reductions over every slot ([64 x slots] x [slots x
+// 64|128], k_ml_wgrad_tc); both run on the 5th-generation tensor cores: TMA
+// tiles in the 128-byte swizzle, tcgen05.mma with the accumulator in tensor
+// memory, tcgen05.ld epilogues.
 // Activations s, h and the GEMM operands of the backward pass are BF16.
 #include "samos_gpu.h"
 
@@ -80,70 +81,6 @@ __global__ void k_ml_l1(sg_view V, const double* __restrict__ box, double rc, co
   }
 }
 
-// ---- BF16 tensor-core GEMM: C[m][n] = sum_k A[m][k] Bt[n][k] (+bias, relu) ------
-// One warp: 16 rows x N; Bt staged in shared memory.  Rows with box == 0
-// (padding slots) are written as zero.
-__device__ __forceinline__ uint32_t pack2(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
-
-__device__ __forceinline__ void mma16816(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
-                                         uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
-template <int K, int N>
-__global__ void __launch_bounds__(128) k_ml_gemm(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ Bt,
-                                                 int M, const float* __restrict__ bias, int relu,
-                                                 const double* __restrict__ box, float* __restrict__ C32,
-                                                 __nv_bfloat16* __restrict__ C16) {
-  __shared__ __align__(16) __nv_bfloat16 sB[N * K];
-  for (int t = threadIdx.x; t < N * K / 2; t += blockDim.x)
-    reinterpret_cast<uint32_t*>(sB)[t] = reinterpret_cast<const uint32_t*>(Bt)[t];
-  __syncthreads();
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int row0 = (blockIdx.x * 4 + (threadIdx.x >> 5)) * 16;
-  if (row0 >= M) return;
-  float acc[N / 8][4];
-#pragma unroll
-  for (int nt = 0; nt < N / 8; nt++) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-  const int ra = min(row0 + g, M - 1), rb = min(row0 + g + 8, M - 1);
-#pragma unroll
-  for (int kt = 0; kt < K / 16; kt++) {
-    const int k0 = kt * 16 + 2 * t;
-    const uint32_t a0 = pack2(A + (size_t)ra * K + k0);
-    const uint32_t a1 = pack2(A + (size_t)rb * K + k0);
-    const uint32_t a2 = pack2(A + (size_t)ra * K + k0 + 8);
-    const uint32_t a3 = pack2(A + (size_t)rb * K + k0 + 8);
-#pragma unroll
-    for (int nt = 0; nt < N / 8; nt++) {
-      const int n = nt * 8 + g;
-      const uint32_t b0 = pack2(sB + n * K + k0);
-      const uint32_t b1 = pack2(sB + n * K + k0 + 8);
-      mma16816(acc[nt], a0, a1, a2, a3, b0, b1);
-    }
-  }
-#pragma unroll
-  for (int nt = 0; nt < N / 8; nt++) {
-    const int n = nt * 8 + 2 * t;
-    for (int half = 0; half < 2; half++) {
-      const int row = row0 + g + 8 * half;
-      if (row >= M) continue;
-      const bool valid = box[2 * row] > 0.0;
-      for (int c = 0; c < 2; c++) {
-        float v = acc[nt][2 * half + c];
-        if (bias) v += bias[n + c];
-        if (relu) v = fmaxf(v, 0.f);
-        if (!valid) v = 0.f;
-        if (C32) C32[(size_t)row * N + n + c] = v;
-        if (C16) C16[(size_t)row * N + n + c] = __float2bfloat16_rn(v);
-      }
-    }
-  }
-}
-
 // ---- weight gradient on tcgen05: W[k][n] = sum_m X[m][k] G[m][n] ----------------
 // The reduction runs over all slots, so it is the MMA's K dimension: per
 // 64-row chunk, D[128 x 64] += G_chunk^T (A: M = G's features, zero rows
@@ -164,7 +101,7 @@ constexpr int WG_B_BYTES = WG_ROWS * 128;       // X: one 128-B feature group
 constexpr int WG_STAGE_BYTES = WG_A_BYTES + WG_B_BYTES;
 constexpr int WG_SMEM = 1024 + WG_STAGES * WG_STAGE_BYTES + 128;
 constexpr uint32_t WG_TMEM_COLS = 64;
-__device__ int g_wgrad_err;  // set by a k_ml_wgrad_tc whose bounded wait ran out
+__device__ int g_ml_tc_err;  // set by a tcgen05 kernel of this file whose bounded wait ran out
 constexpr long long WG_SPIN_LIMIT = 1ll << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -321,14 +258,14 @@ k_ml_wgrad_tc(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ C
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(WG_TMEM_COLS) : "memory");
 }
 
-// 2-D row-major BF16 tensor map [rows x cols] with 64 x 64 boxes and the
-// 128-byte swizzle (cuTensorMapEncodeTiled, fetched through the runtime so
+// 2-D row-major BF16 tensor map [rows x cols] with boxes of 64 columns x
+// box_rows rows and the 128-byte swizzle (cuTensorMapEncodeTiled, fetched through the runtime so
 // the library does not link the driver library)
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-bool make_bf16_map(CUtensorMap* map, const void* base, int rows, int cols) {
+bool make_bf16_map(CUtensorMap* map, const void* base, int rows, int cols, int box_rows = WG_ROWS) {
   static EncodeTiledFn fn = [] {
     void* f = nullptr;
     cudaDriverEntryPointQueryResult q;
@@ -340,7 +277,7 @@ bool make_bf16_map(CUtensorMap* map, const void* base, int rows, int cols) {
   if (!fn || (reinterpret_cast<uintptr_t>(base) & 15) || rows < 1) return false;
   const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-  const cuuint32_t box[2] = {64, WG_ROWS};
+  const cuuint32_t box[2] = {64, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1, 1};
   return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -361,6 +298,150 @@ int launch_wgrad_tc(const void* X, const void* G, int M, int blocks, float* part
   const int nchunks = (M + WG_ROWS - 1) / WG_ROWS;
   const int per = (nchunks + blocks - 1) / blocks;
   k_ml_wgrad_tc<NF><<<blocks, 128, WG_SMEM, st>>>(mx, mg, M, per, partial, err);
+  return cudaGetLastError() == cudaSuccess ? SG_OK : SG_ERR_CUDA;
+}
+
+// ---- activation GEMM on tcgen05: C[m][n] = act(sum_k A[m][k] Bt[n][k] + bias[n]) ------
+// One CTA per 128-row tile of A: the tile (K/64 groups of 128 rows x 128 B)
+// and all of Bt (K/64 groups of N rows x 128 B) arrive by TMA in the 128-byte
+// swizzle, K-major for both operands; one thread issues K/16 tcgen05.mma
+// (M = 128, N) into tensor memory; the four warps read their 32 rows back
+// with tcgen05.ld and apply bias, relu and the slot mask (box <= 0: padding,
+// written as 0) in the epilogue, storing FP32 and / or BF16.  Waits bounded
+// as in k_ml_wgrad_tc.
+template <int K, int N>
+__global__ void __launch_bounds__(128)
+k_ml_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M,
+             const float* __restrict__ bias, int relu, const double* __restrict__ box, float* __restrict__ C32,
+             __nv_bfloat16* __restrict__ C16, int* __restrict__ err) {
+  static_assert((K == 64 || K == 128) && (N == 64 || N == 128), "K, N in {64, 128}");
+  constexpr int KG = K / 64;                      // 128-B K groups
+  constexpr int A_GROUP = 128 * 128, B_GROUP = N * 128;
+  constexpr uint32_t TX = KG * (A_GROUP + B_GROUP);
+  constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((128u >> 4) << 24);
+  extern __shared__ uint8_t gm_smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(gm_smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + KG * A_GROUP;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + KG * B_GROUP);  // full, done
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
+  __shared__ int ok_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row0 = blockIdx.x * 128;
+  if (threadIdx.x == 0) {
+    ok_flag = 1;
+    for (int i = 0; i < 2; i++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bars + i)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                 ::"r"(smem_u32(tmem_slot)), "r"((uint32_t)N) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t full = smem_u32(bars), done = smem_u32(bars + 1);
+  if (threadIdx.x == 0) {
+    const uint64_t mapA = reinterpret_cast<uint64_t>(&tmA), mapB = reinterpret_cast<uint64_t>(&tmB);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(full), "r"(TX) : "memory");
+#pragma unroll
+    for (int g = 0; g < KG; g++) {
+      asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+                   ::"r"(smem_u32(sA + g * A_GROUP)), "l"(mapA), "r"(g * 64), "r"(row0), "r"(full) : "memory");
+      asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+                   ::"r"(smem_u32(sB + g * B_GROUP)), "l"(mapB), "r"(g * 64), "r"(0), "r"(full) : "memory");
+    }
+    if (mbar_wait(full, 0)) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+#pragma unroll
+      for (int ks = 0; ks < K / 16; ks++) {  // K-major: 16 elements = 32 B along each 128-B row
+        const int g = ks / 4, off = (ks % 4) * 32;
+        const uint64_t da = umma_desc_sw128(smem_u32(sA + g * A_GROUP) + off, 16, 1024);
+        const uint64_t db = umma_desc_sw128(smem_u32(sB + g * B_GROUP) + off, 16, 1024);
+        const uint32_t acc = ks > 0 ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+            ::"r"(tmem), "l"(da), "l"(db), "r"(IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u) : "memory");
+      }
+    } else {
+      atomicExch(err, 1);
+      ok_flag = 0;
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(done)
+                 : "memory");
+  }
+  __syncthreads();
+  bool have = ok_flag != 0;
+  if (!mbar_wait(done, 0)) {
+    if (lane == 0) atomicExch(err, 1);
+    have = false;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const int row = row0 + warp * 32 + lane;
+  const bool inside = row < M;
+  const bool valid = inside && box[2 * (size_t)row] > 0.0;
+#pragma unroll
+  for (int q = 0; q < N / 16; q++) {
+    uint32_t r[16];
+    const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(q * 16);
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+    if (!inside) continue;
+    float v[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      float t = have ? __uint_as_float(r[j]) : 0.f;
+      if (bias) t += bias[q * 16 + j];
+      if (relu) t = fmaxf(t, 0.f);
+      v[j] = valid ? t : 0.f;
+    }
+    if (C32) {
+      float4* o = reinterpret_cast<float4*>(C32 + (size_t)row * N + q * 16);
+#pragma unroll
+      for (int j = 0; j < 4; j++) o[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+    }
+    if (C16) {
+      __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+      for (int j = 0; j < 16; j++) h[j] = __float2bfloat16_rn(v[j]);
+      uint4* o = reinterpret_cast<uint4*>(C16 + (size_t)row * N + q * 16);
+      o[0] = reinterpret_cast<const uint4*>(h)[0];
+      o[1] = reinterpret_cast<const uint4*>(h)[1];
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"((uint32_t)N) : "memory");
+}
+
+template <int K, int N>
+int launch_gemm_tc(const void* A, const void* Bt, int M, const float* bias, int relu, const double* box, float* C32,
+                   void* C16, int* err, cudaStream_t st) {
+  // at most 512 / N CTAs may share an SM's 512 tensor-memory columns: the
+  // shared-memory request is padded so that no more fit (an allocation
+  // beyond them would wait for another CTA's release)
+  constexpr int NEED = 1024 + (K / 64) * (128 * 128 + N * 128) + 64;
+  constexpr int CAP = (N == 128 ? 48 : 26) * 1024;
+  constexpr int SMEM = NEED > CAP ? NEED : CAP;
+  CUtensorMap ma, mb;
+  if (!make_bf16_map(&ma, A, M, K, 128) || !make_bf16_map(&mb, Bt, N, K, N)) return SG_ERR_CUDA;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_ml_gemm_tc<K, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
+      return SG_ERR_CUDA;
+    attr = true;
+  }
+  k_ml_gemm_tc<K, N><<<(M + 127) / 128, 128, SMEM, st>>>(ma, mb, M, bias, relu, box, C32, (__nv_bfloat16*)C16, err);
   return cudaGetLastError() == cudaSuccess ? SG_OK : SG_ERR_CUDA;
 }
 
@@ -607,13 +688,20 @@ int sg_mlp_forward(const sg_view* V, const double* box, double rc, const float* 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int M = V->slots;
   k_ml_l1<<<EDGE_BLOCKS, 32 * EDGE_WARPS, 0, st>>>(*V, box, rc, params, (__nv_bfloat16*)s16);
-  const int gb = (M + 63) / 64;
-  k_ml_gemm<F, F><<<gb, 128, 0, st>>>((const __nv_bfloat16*)s16, (const __nv_bfloat16*)W1bT16, M,
-                                       params + NP_B1B, 1, box, nullptr, (__nv_bfloat16*)h16);
-  k_ml_gemm<F, 2 * F><<<gb, 128, 0, st>>>((const __nv_bfloat16*)h16, (const __nv_bfloat16*)WpqT16, M, nullptr, 0,
-                                           box, PQ, nullptr);
+  int* gerr = nullptr;
+  if (cudaGetSymbolAddress((void**)&gerr, g_ml_tc_err) != cudaSuccess) return SG_ERR_CUDA;
+  cudaMemsetAsync(gerr, 0, sizeof(int), st);
+  int grc = launch_gemm_tc<F, F>(s16, W1bT16, M, params + NP_B1B, 1, box, nullptr, h16, gerr, st);
+  if (grc) return grc;
+  grc = launch_gemm_tc<F, 2 * F>(h16, WpqT16, M, nullptr, 0, box, PQ, nullptr, gerr, st);
+  if (grc) return grc;
   k_ml_l2<<<EDGE_BLOCKS, 32 * EDGE_WARPS, 0, st>>>(*V, box, rc, params, PQ, disp);
-  return cudaGetLastError() == cudaSuccess ? SG_OK : SG_ERR_CUDA;
+  if (cudaGetLastError() != cudaSuccess) return SG_ERR_CUDA;
+  int timed_out = 0;
+  if (cudaMemcpyAsync(&timed_out, gerr, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return SG_ERR_CUDA;
+  return timed_out ? SG_ERR_TIMEOUT : SG_OK;
 }
 
 // Gradients are ADDED to grad[NP_TOTAL] (zero it first).  work: gPQ [M x 128]
@@ -646,15 +734,14 @@ int sg_mlp_backward(const sg_view* V, const double* box, double rc, const float*
   // gWpq = h^T gPQ (tensor cores, one CTA per SM)
   constexpr int WG_BLOCKS = 148;
   int* werr = nullptr;
-  if (cudaGetSymbolAddress((void**)&werr, g_wgrad_err) != cudaSuccess) return SG_ERR_CUDA;
+  if (cudaGetSymbolAddress((void**)&werr, g_ml_tc_err) != cudaSuccess) return SG_ERR_CUDA;
   cudaMemsetAsync(werr, 0, sizeof(int), st);
   int wrc = launch_wgrad_tc<2 * F>(h16, gPQ16, M, WG_BLOCKS, part, werr, st);
   if (wrc) return wrc;
   k_ml_reduce<<<(F * 2 * F + 255) / 256, 256, 0, st>>>(part, WG_BLOCKS, F * 2 * F, grad + NP_WPQ);
   // gh = gPQ Wpq^T
-  const int gb = (M + 63) / 64;
-  k_ml_gemm<2 * F, F><<<gb, 128, 0, st>>>((const __nv_bfloat16*)gPQ16, (const __nv_bfloat16*)Wpq16, M, nullptr, 0, box,
-                                           gh, nullptr);
+  wrc = launch_gemm_tc<2 * F, F>(gPQ16, Wpq16, M, nullptr, 0, box, gh, nullptr, werr, st);
+  if (wrc) return wrc;
   // through relu(s W1b + b1b)
   k_ml_relu_bwd<<<WG_BLOCKS, 256, 0, st>>>(M, gh, (const __nv_bfloat16*)h16, (__nv_bfloat16*)gpre16, part);
   k_ml_reduce<<<1, 64, 0, st>>>(part, WG_BLOCKS, F, grad + NP_B1B);
@@ -662,8 +749,8 @@ int sg_mlp_backward(const sg_view* V, const double* box, double rc, const float*
   if (wrc) return wrc;
   k_ml_reduce<<<(F * F + 255) / 256, 256, 0, st>>>(part, WG_BLOCKS, F * F, grad + NP_W1B);
   // gs = gpre W1b^T
-  k_ml_gemm<F, F><<<gb, 128, 0, st>>>((const __nv_bfloat16*)gpre16, (const __nv_bfloat16*)W1b16, M, nullptr, 0, box, gs,
-                                       nullptr);
+  wrc = launch_gemm_tc<F, F>(gpre16, W1b16, M, nullptr, 0, box, gs, nullptr, werr, st);
+  if (wrc) return wrc;
   // layer 1 edges
   k_ml_l1_bwd<<<EDGE_BLOCKS, 32 * EDGE_WARPS, 0, st>>>(*V, box, rc, params, gs, part);
   cudaMemsetAsync(red, 0, sizeof(float) * L1_GRAD, st);
