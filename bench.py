@@ -286,12 +286,15 @@ def ml_leg(count=48, seed=4242, device=0):
     warm = relax(insts, net)
     rep = summarize(plain, warm, insts)
     rep["timing"] = "CUDA events on the engine stream: inference + apply + fallback + minimisation (warm), minimisation (plain)"
+    rep["sample"] = (f"{count} fresh quenches, a subsample of the configuration's 512 evaluation instances "
+                     "(the full 512 and the hand-off sweep: python -m samos_b200.warmstart eval / sweep)")
     return rep
 
 
 # ---------------------------------------------------------------------------
 # per-component rows: every potential, aligner, integrator and constraint
-# family of the hot path timed on the GPU beside the oracle on one core
+# family of the hot path timed on the GPU beside the reference's own code
+# (the C oracle when that build is absent) on one core
 # ---------------------------------------------------------------------------
 def plane_mono(n, phi, seed):
     """n radius-1 disks on a square lattice of spacing sqrt(pi/phi) (> 2 below
