@@ -305,7 +305,6 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
   __syncthreads();
   // by-value variants: the one replica's parameters, read from parameter space
   const AbpParams& S = abp_params<abp_byval(VAR)>(pv, S_sh);
-  static_assert(!(abp_ordered(VAR) && ENERGY), "the ordered variants change the block's energy summation order");
   static_assert(!abp_pipelined(VAR) || abp_prenoise(VAR), "the pipelined sweep takes the draws first");
   const int k = blockIdx.x * BLOCK +
                 (abp_ordered(VAR) ? (int)lane_order[(size_t)blockIdx.x * BLOCK + threadIdx.x] : (int)threadIdx.x);
@@ -441,6 +440,16 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
                           s_base, ox, oy, oz, age0, Gout, Hout, d, rebuild, status, apply_e1, last);
   }
   if (ENERGY) {
+    if constexpr (abp_ordered(VAR)) {
+      // lanes in neighbour-count order: the block's sums are taken in slot
+      // order all the same, so every variant stores the same partial sums
+      __shared__ double s_ep[BLOCK], s_ea[BLOCK];
+      s_ep[k - blockIdx.x * BLOCK] = epair;
+      s_ea[k - blockIdx.x * BLOCK] = ealign;
+      __syncthreads();
+      epair = s_ep[threadIdx.x];
+      ealign = s_ea[threadIdx.x];
+    }
     double ev[MAX_PAIR + MAX_ALIGN];
 #pragma unroll
     for (int i = 0; i < MAX_PAIR + MAX_ALIGN; i++) ev[i] = 0.0;

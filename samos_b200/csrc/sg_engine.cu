@@ -1596,6 +1596,21 @@ static int hot_pack(sg_system* s, int shape, bool flagged = false) {
   return SG_OK;
 }
 
+// whole grid: the run's first start-of-step enforce and the packing in one pass
+static int hot_pack_enforce(sg_system* s, int shape) {
+  if (s->nblocks == 0) return SG_OK;
+  if (shape == HOT_PLANE)
+    k_hot_pack_enforce<HOT_PLANE><<<s->nblocks, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->st,
+                                                                      s->G[s->hot_buf], nullptr,
+                                                                      s->prog.cons[0].unlimited);
+  else
+    k_hot_pack_enforce<HOT_SPHERE><<<s->nblocks, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->cur, s->st,
+                                                                       s->G[s->hot_buf], s->H[s->hot_buf],
+                                                                       s->prog.cons[0].unlimited);
+  LAUNCH_CHECK(s);
+  return SG_OK;
+}
+
 static int hot_unpack(sg_system* s, int shape, bool flagged = false) {
   const int ng = flagged ? s->nblist : s->nblocks;
   const int* bl = flagged ? blist_of(s) : nullptr;
@@ -1748,7 +1763,12 @@ static void launch_abp_tile(sg_system* s, bool apply_e1, bool last) {
 
 template <int SHAPE, int ALIGN, bool SP>
 static void launch_abp3(sg_system* s, bool apply_e1, bool last, bool energy) {
-  if (energy) { launch_abp_v<SHAPE, ALIGN, SP, true, 1>(s, apply_e1, last); return; }
+  // energy-reporting steps: the pipelined kernel (by value for one replica)
+  if (energy) {
+    if (s->nrep > 1) launch_abp_v<SHAPE, ALIGN, SP, true, 17>(s, apply_e1, last);
+    else launch_abp_v<SHAPE, ALIGN, SP, true, 22>(s, apply_e1, last);
+    return;
+  }
   // by-value variants carry one replica's parameters: several replicas take the twin
   switch (s->nrep > 1 ? abp_twin(s->abp_variant) : s->abp_variant) {
     case 5: launch_abp_flat<SHAPE, ALIGN, SP, false>(s, apply_e1, last); break;
@@ -1813,7 +1833,7 @@ static int step_hot(sg_system* s, int shape, bool apply_e1, bool last, bool ener
     int rc = tile_prep(s);
     if (rc) return rc;
   }
-  if (s->abp_on && !energy && abp_ordered(s->abp_variant) && !s->order_valid) {
+  if (s->abp_on && (energy || abp_ordered(s->abp_variant)) && !s->order_valid) {  // energy steps run ordered
     if (!s->lane_order) {
       s->lane_order = s->mem.alloc<uint8_t>((size_t)s->nblocks * BLOCK);
       if (!s->lane_order) { s->mem.err = cudaSuccess; return fail(s, SG_ERR_NOMEM, "lane order"); }
@@ -2143,11 +2163,9 @@ static int run_impl(sg_system* s, int64_t steps, sg_run_stats* stats, bool drive
     }
     if (shape != HOT_NONE) {
       if (t == 0) {
-        if (!s->e1_applied) {
-          k_enforce<<<s->nblocks, BLOCK, 0, s->stream>>>(s->prog, s->reps, s->blk_rep, s->cur, s->st, nullptr);
-          LAUNCH_CHECK(s);
-        }
-        if ((rc = hot_pack(s, shape))) return rc;
+        if (!s->e1_applied) rc = hot_pack_enforce(s, shape);
+        else rc = hot_pack(s, shape);
+        if (rc) return rc;
       }
       rc = step_hot(s, shape, !last, last, last);
       s->e1_applied = !last;

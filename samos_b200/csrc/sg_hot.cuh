@@ -69,6 +69,43 @@ __global__ void k_hot_unpack(const Replica* __restrict__ reps, const int* __rest
   }
 }
 
+// The start-of-step Constrainer::enforce of a run's first step (samos.cpp:
+// 887-888) fused with the packing: the plane or sphere enforce on the fields
+// it reads and writes only (the generic enforce pass moves every field of
+// the particle), then the packed records.  Plane: z = zpos, vz = fz = nz = 0,
+// periodic wrap with image flags, director normalised; sphere: projection of
+// position, velocity and director.
+template <int SHAPE>
+__global__ void k_hot_pack_enforce(const Replica* __restrict__ reps, const int* __restrict__ blk_rep, Dyn d,
+                                   Stat st, D4* __restrict__ G, D4* __restrict__ H, int unlimited) {
+  const Replica& R = reps[blk_rep[blockIdx.x]];
+  const int k = blockIdx.x * BLOCK + threadIdx.x;
+  if (k - R.off >= R.n) return;
+  Part p;
+  if (SHAPE == HOT_PLANE) {
+    p.x = d.x[k]; p.y = d.y[k]; p.z = 0.0; p.vz = 0.0; p.fz = 0.0;
+    p.nx = d.nx[k]; p.ny = d.ny[k]; p.nz = 0.0;
+    p.ix = d.ix[k]; p.iy = d.iy[k]; p.iz = 0;
+    const int ix0 = p.ix, iy0 = p.iy;
+    plane_enforce(R, R.cons_p[0], unlimited, p);  // zpos inside the box: z never wraps
+    if (p.ix != ix0) { d.x[k] = p.x; d.ix[k] = p.ix; }
+    if (p.iy != iy0) { d.y[k] = p.y; d.iy[k] = p.iy; }
+    d.z[k] = p.z; d.vz[k] = 0.0; d.fz[k] = 0.0; d.nz[k] = 0.0;
+    d.nx[k] = p.nx; d.ny[k] = p.ny;
+    stg4(G + k, D4{p.x, p.y, p.nx, p.ny});
+  } else {
+    p.x = d.x[k]; p.y = d.y[k]; p.z = d.z[k];
+    p.vx = d.vx[k]; p.vy = d.vy[k]; p.vz = d.vz[k];
+    p.nx = d.nx[k]; p.ny = d.ny[k]; p.nz = d.nz[k];
+    sphere_enforce(R.cons_p[0], p);
+    d.x[k] = p.x; d.y[k] = p.y; d.z[k] = p.z;
+    d.vx[k] = p.vx; d.vy[k] = p.vy; d.vz[k] = p.vz;
+    d.nx[k] = p.nx; d.ny[k] = p.ny; d.nz[k] = p.nz;
+    stg4(G + k, D4{p.x, p.y, p.z, st.r[k]});
+    stg4(H + k, D4{p.nx, p.ny, p.nz, 0.0});
+  }
+}
+
 // ---------------------------------------------------------------------------
 // per-particle pieces specialised to the shapes
 // ---------------------------------------------------------------------------
