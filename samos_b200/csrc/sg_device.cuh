@@ -118,6 +118,21 @@ struct Dyn {
 struct Stat { double *r, *mass; int *type, *id; };
 struct NbList { int *nb, *cnt, *lo; int cap; int stride; double *ox, *oy, *oz; };
 
+// 32-byte record (packed particle data of the step kernels, candidate
+// records of the list build), moved with one 256-bit access
+struct __align__(32) D4 { double x, y, z, w; };
+
+__device__ __forceinline__ D4 ldg4(const D4* p) {
+  D4 v;
+  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+               : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ void stg4(D4* p, const D4& v) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v.x), "d"(v.y), "d"(v.z), "d"(v.w)
+               : "memory");
+}
+
 struct Part {
   double x, y, z, vx, vy, vz, nx, ny, nz, fx, fy, fz, tx, ty, tz, omega, age, r, mass;
   int ix, iy, iz, type, id;

@@ -64,6 +64,7 @@ struct sg_system {
   int ncell_total = 0;
   int *pcell = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
   int *tmp = nullptr, *perm = nullptr, *scan_bsum = nullptr;
+  D4* cand = nullptr;                 // cell-ordered candidate records of the list build (k_rb_rank)
   CellSeg* segs = nullptr;            // cell ranges of the replicas being rebuilt
   int* blist = nullptr;               // blocks of the replicas being rebuilt (null: every block)
   // pinned staging of the small per-rebuild uploads (block list, cell
@@ -285,6 +286,7 @@ int sg_create(int n_replicas, const int32_t* n_particles, int ntypes, sg_system*
   s->pcell = m.alloc<int>(s->slots);
   s->tmp = m.alloc<int>(s->slots);
   s->perm = m.alloc<int>(s->slots);
+  s->cand = m.alloc<D4>(s->slots);
   if (!ok || m.err != cudaSuccess) { m.free_all(); cudaStreamDestroy(s->stream); delete s; return SG_ERR_NOMEM; }
   cudaMallocHost((void**)&s->rebuild_h, sizeof(int) * n_replicas);
   cudaMallocHost((void**)&s->pin_blist, sizeof(int) * std::max(1, s->nblocks));
@@ -781,7 +783,7 @@ static int rebuild_flagged(sg_system* s, bool* sorted, bool blist_ready = false)
                                             bl);
     LAUNCH_CHECK(s);
     k_rb_rank<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->pcell, s->cell_start, s->cell_cnt,
-                                          s->tmp, s->st.id, s->perm, bl);
+                                          s->tmp, s->st.id, s->perm, bl, s->cur, s->cand);
     LAUNCH_CHECK(s);
     if (any_sort) {
       k_rb_gather<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->perm, s->cur, s->alt, s->st,
@@ -803,7 +805,7 @@ static int rebuild_flagged(sg_system* s, bool* sorted, bool blist_ready = false)
                                                                           s->st, s->nl, s->perm, s->cell_start,
                                                                           s->cell_cnt, s->bstatus, s->maxnb, bl);
     else
-      k_rb_build<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->st, s->nl, s->perm,
+      k_rb_build<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->cur, s->st, s->nl, s->cand,
                                              s->cell_start, s->cell_cnt, s->bstatus, s->maxnb, bl);
     LAUNCH_CHECK(s);
     CU(s, cudaMemcpyAsync(s->pin_res, s->bstatus, sizeof(int), cudaMemcpyDeviceToHost, s->stream));

@@ -17,19 +17,6 @@
 
 namespace sg {
 
-struct __align__(32) D4 { double x, y, z, w; };
-
-__device__ __forceinline__ D4 ldg4(const D4* p) {
-  D4 v;
-  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
-               : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w) : "l"(p));
-  return v;
-}
-__device__ __forceinline__ void stg4(D4* p, const D4& v) {
-  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v.x), "d"(v.y), "d"(v.z), "d"(v.w)
-               : "memory");
-}
-
 // hot-shape eligibility (host side)
 enum { HOT_NONE = 0, HOT_PLANE = 1, HOT_SPHERE = 2 };
 

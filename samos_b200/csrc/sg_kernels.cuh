@@ -1054,11 +1054,18 @@ __global__ void k_rb_scatter(const Replica* __restrict__ reps, const int* __rest
   tmp[R.off + pos] = k;
 }
 
-// rank inside the cell by particle id -> deterministic ascending-id order
+// rank inside the cell by particle id -> deterministic ascending-id order;
+// with `cand`, also the particle's candidate record at its cell-ordered
+// position: position, and id and slot packed in the fourth word (the slot it
+// will occupy once a re-sort, rebuild[r] == 2, has moved it there)
+__device__ __forceinline__ double pack_id_slot(int id, int slot) {
+  return __longlong_as_double((long long)(((unsigned long long)(unsigned)id << 32) | (unsigned)slot));
+}
 __global__ void k_rb_rank(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                           const int* __restrict__ rebuild, const int* __restrict__ pcell,
                           const int* __restrict__ cstart, const int* __restrict__ ccnt,
-                          const int* __restrict__ tmp, const int* __restrict__ id, int* __restrict__ perm, const int* __restrict__ blist = nullptr) {
+                          const int* __restrict__ tmp, const int* __restrict__ id, int* __restrict__ perm,
+                          const int* __restrict__ blist = nullptr, Dyn d = Dyn{}, D4* __restrict__ cand = nullptr) {
   const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
   const int r = blk_rep[bid_];
   if (!rebuild[r]) return;
@@ -1072,6 +1079,8 @@ __global__ void k_rb_rank(const Replica* __restrict__ reps, const int* __restric
   int rank = 0;
   for (int q = 0; q < n; q++) rank += id[tmp[s0 + q]] < myid ? 1 : 0;
   perm[s0 + rank] = k;
+  if (cand)
+    stg4(cand + s0 + rank, D4{d.x[k], d.y[k], d.z[k], pack_id_slot(myid, rebuild[r] == 2 ? s0 + rank : k)});
 }
 
 // gather all particle arrays into the permuted order (dst = src[perm])
@@ -1219,9 +1228,118 @@ __device__ __forceinline__ void build_particle(const Replica& R, int mode, int k
   nl.ox[k] = x; nl.oy[k] = y; nl.oz[k] = z;
 }
 
+// build_particle over the candidate records k_rb_rank wrote in cell order:
+// each candidate is one 32-byte record read straight from its cell's range
+// (position, id, slot) instead of a slot index followed by four loads from
+// the particle arrays.  Same candidates, order and arithmetic: same lists.
+__device__ __forceinline__ void build_particle_packed(const Replica& R, int k, Dyn d, Stat st, NbList nl,
+                                                     const D4* __restrict__ cand, const int* __restrict__ cstart,
+                                                     const int* __restrict__ ccnt, int* __restrict__ status,
+                                                     int* __restrict__ maxnb) {
+  const double x = d.x[k], y = d.y[k], z = d.z[k];
+  const int myid = st.id[k];
+  int a, b, c;
+  cell_of(R, x, y, z, a, b, c);
+  const int base0 = cstart[R.cell_off];
+  // the stencil's cells in visiting order as runs of consecutive candidate
+  // records: cells adjacent in the cell arrays merge, empty ones drop out.
+  // Away from the y and z faces the nine cells of one x offset are
+  // consecutive (a-major numbering, z innermost), so the sweep is three runs.
+  int rs[27], rn[27], nr = 0;
+  if (R.use_cell && R.cnx >= 3 && b >= 1 && b + 1 < R.cny && c >= 1 && c + 1 < R.cnz) {
+    for (int ox = -1; ox <= 1; ox++) {
+      int ia = a + ox;
+      if (ia < 0) ia = R.cnx - 1; else if (ia == R.cnx) ia = 0;
+      const int f = R.cell_off + R.cny * R.cnz * ia + R.cnz * (b - 1) + (c - 1);
+      const int l = f + 2 * R.cnz + 2;
+      const int s0 = cstart[f], e = cstart[l] + ccnt[l];
+      if (e > s0) { rs[nr] = R.off + s0 - base0; rn[nr] = e - s0; nr++; }
+    }
+  } else {
+    int cells[27];
+    const int ncells = build_stencil(R, a, b, c, cells);
+    for (int m = 0; m < ncells; m++) {
+      const int cg = R.cell_off + cells[m];
+      const int s0 = R.off + cstart[cg] - base0, n = ccnt[cg];
+      if (n == 0) continue;
+      if (nr > 0 && rs[nr - 1] + rn[nr - 1] == s0) rn[nr - 1] += n;
+      else { rs[nr] = s0; rn[nr] = n; nr++; }
+    }
+  }
+  unsigned long long lo[NB_LOCAL], up[NB_LOCAL];  // (id << 32) | slot
+  int nlo = 0, nup = 0;
+  bool overflow = false;
+  int total = 0;
+  for (int i = 0; i < nr; i++) total += rn[i];
+  // one flat sweep over the runs' records (lanes of a warp stay together
+  // across cell boundaries)
+  int ri = 0, pos = nr > 0 ? rs[0] : 0, end = nr > 0 ? rs[0] + rn[0] : 0;
+  for (int t = 0; t < total; t++) {
+    if (pos == end) { ri++; pos = rs[ri]; end = pos + rn[ri]; }
+    {
+      const D4 cr = ldg4(cand + pos);
+      pos++;
+      const unsigned long long key = (unsigned long long)__double_as_longlong(cr.w);
+      const int jid = (int)(unsigned)(key >> 32);
+      if (jid == myid) continue;
+      double dx, dy, dz;
+      if (myid < jid) { dx = x - cr.x; dy = y - cr.y; dz = z - cr.z; }
+      else { dx = cr.x - x; dy = cr.y - y; dz = cr.z - z; }
+      apply_periodic(R, dx, dy, dz);
+      if (dx * dx + dy * dy + dz * dz < R.cut2) {
+        if (jid < myid) { if (nlo < NB_LOCAL) lo[nlo] = key; nlo++; }
+        else { if (nup < NB_LOCAL) up[nup] = key; nup++; }
+      }
+    }
+  }
+  if (nlo > NB_LOCAL || (!R.use_cell && nup > NB_LOCAL)) overflow = true;
+  const int found = nlo + nup;
+  atomicMax(maxnb, found);
+  if (found > nl.cap || overflow) {
+    atomicOr(status, ST_OVERFLOW);
+    nl.cnt[k] = 0; nl.lo[k] = 0;
+  } else {
+    for (int i = 1; i < nlo; i++) {  // insertion sort by id (stable: equal ids keep their order)
+      const unsigned long long v = lo[i];
+      int m = i - 1;
+      while (m >= 0 && (lo[m] >> 32) > (v >> 32)) { lo[m + 1] = lo[m]; m--; }
+      lo[m + 1] = v;
+    }
+    for (int q = 0; q < nlo; q++) nl.nb[(size_t)q * nl.stride + k] = (int)(unsigned)(lo[q] & 0xffffffffull);
+    if (!R.use_cell) {
+      for (int i = 1; i < nup; i++) {
+        const unsigned long long v = up[i];
+        int m = i - 1;
+        while (m >= 0 && (up[m] >> 32) > (v >> 32)) { up[m + 1] = up[m]; m--; }
+        up[m + 1] = v;
+      }
+      for (int q = 0; q < nup; q++)
+        nl.nb[(size_t)(nlo + q) * nl.stride + k] = (int)(unsigned)(up[q] & 0xffffffffull);
+    } else if (nup <= NB_LOCAL) {
+      for (int q = 0; q < nup; q++)
+        nl.nb[(size_t)(nlo + q) * nl.stride + k] = (int)(unsigned)(up[q] & 0xffffffffull);
+    } else {
+      // more higher-id neighbours than the local array holds: a second sweep
+      // over the same runs writes them in visiting order straight into the list
+      int w = nlo;
+      for (int i = 0; i < nr; i++)
+        for (int q = rs[i]; q < rs[i] + rn[i]; q++) {
+          const D4 cr = ldg4(cand + q);
+          const unsigned long long key = (unsigned long long)__double_as_longlong(cr.w);
+          if ((int)(unsigned)(key >> 32) <= myid) continue;
+          double dx = x - cr.x, dy = y - cr.y, dz = z - cr.z;
+          apply_periodic(R, dx, dy, dz);
+          if (dx * dx + dy * dy + dz * dz < R.cut2) nl.nb[(size_t)(w++) * nl.stride + k] = (int)(unsigned)key;
+        }
+    }
+    nl.cnt[k] = found; nl.lo[k] = nlo;
+  }
+  nl.ox[k] = x; nl.oy[k] = y; nl.oz[k] = z;
+}
+
 __global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restrict__ blk_rep,
                            const int* __restrict__ rebuild, Dyn d, Stat st, NbList nl,
-                           const int* __restrict__ cslot, const int* __restrict__ cstart,
+                           const D4* __restrict__ cand, const int* __restrict__ cstart,
                            const int* __restrict__ ccnt, int* __restrict__ status, int* __restrict__ maxnb, const int* __restrict__ blist = nullptr) {
   const int bid_ = blist ? blist[blockIdx.x] : (int)blockIdx.x;  // block of the packed layout
   const int r = blk_rep[bid_];
@@ -1230,7 +1348,7 @@ __global__ void k_rb_build(const Replica* __restrict__ reps, const int* __restri
   const Replica& R = reps[r];
   const int k = bid_ * BLOCK + threadIdx.x;
   if (k - R.off >= R.n) return;
-  build_particle(R, mode, k, d, st, nl, cslot, cstart, ccnt, status, maxnb);
+  build_particle_packed(R, k, d, st, nl, cand, cstart, ccnt, status, maxnb);
 }
 
 // Cell m (0..26) of the 27-cell stencil of (a, b, c), in the visiting order
