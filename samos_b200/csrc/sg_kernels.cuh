@@ -1272,13 +1272,16 @@ __device__ __forceinline__ void build_particle_packed(const Replica& R, int k, D
   int total = 0;
   for (int i = 0; i < nr; i++) total += rn[i];
   // one flat sweep over the runs' records (lanes of a warp stay together
-  // across cell boundaries)
+  // across cell boundaries); each record requested one candidate ahead
   int ri = 0, pos = nr > 0 ? rs[0] : 0, end = nr > 0 ? rs[0] + rn[0] : 0;
+  D4 nxt = total > 0 ? ldg4(cand + pos) : D4{0.0, 0.0, 0.0, 0.0};
   for (int t = 0; t < total; t++) {
-    if (pos == end) { ri++; pos = rs[ri]; end = pos + rn[ri]; }
+    const D4 cr = nxt;
+    if (t + 1 < total) {
+      if (++pos == end) { ri++; pos = rs[ri]; end = pos + rn[ri]; }
+      nxt = ldg4(cand + pos);
+    }
     {
-      const D4 cr = ldg4(cand + pos);
-      pos++;
       const unsigned long long key = (unsigned long long)__double_as_longlong(cr.w);
       const int jid = (int)(unsigned)(key >> 32);
       if (jid == myid) continue;
