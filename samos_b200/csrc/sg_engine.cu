@@ -315,6 +315,11 @@ int sg_create(int n_replicas, const int32_t* n_particles, int ntypes, sg_system*
   cudaMemcpy(s->st.mass, ones.data(), sizeof(double) * s->slots, cudaMemcpyHostToDevice);
   cudaMemcpy(s->st.id, ids.data(), sizeof(int) * s->slots, cudaMemcpyHostToDevice);
   cudaMemcpy(s->st.type, types.data(), sizeof(int) * s->slots, cudaMemcpyHostToDevice);
+  // the alternate store becomes the store after a full re-sort: same padding
+  cudaMemcpy(s->st_alt.r, ones.data(), sizeof(double) * s->slots, cudaMemcpyHostToDevice);
+  cudaMemcpy(s->st_alt.mass, ones.data(), sizeof(double) * s->slots, cudaMemcpyHostToDevice);
+  cudaMemcpy(s->st_alt.id, ids.data(), sizeof(int) * s->slots, cudaMemcpyHostToDevice);
+  cudaMemcpy(s->st_alt.type, types.data(), sizeof(int) * s->slots, cudaMemcpyHostToDevice);
   s->reps_h.assign(n_replicas, Replica{});
   s->rep_builds.assign(n_replicas, 0);
   s->clk_h.assign(n_replicas, Clock{});
@@ -789,8 +794,19 @@ static int rebuild_flagged(sg_system* s, bool* sorted, bool blist_ready = false)
       k_rb_gather<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->perm, s->cur, s->alt, s->st,
                                                s->st_alt, bl);
       LAUNCH_CHECK(s);
-      k_rb_copyback<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->alt, s->cur, s->st_alt, s->st, bl);
-      LAUNCH_CHECK(s);
+      // every replica re-sorted: the gathered arrays become the store (the
+      // others are scratch between steps); otherwise copy the re-sorted
+      // replicas back
+      bool all = true;
+      for (int r = 0; r < s->nrep; r++) all = all && (s->n[r] == 0 || s->rebuild_h[r] == 2);
+      if (all) {
+        std::swap(s->cur, s->alt);
+        std::swap(s->st, s->st_alt);
+      } else {
+        k_rb_copyback<<<ng, BLOCK, 0, s->stream>>>(s->reps, s->blk_rep, s->rebuild, s->alt, s->cur, s->st_alt, s->st,
+                                                   bl);
+        LAUNCH_CHECK(s);
+      }
     }
     // a rebuild of few particles is latency bound: split each particle's
     // stencil over a team of lanes; a large quasi-2-D one stages cell tiles in
