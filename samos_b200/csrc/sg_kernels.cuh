@@ -1242,18 +1242,24 @@ __device__ __forceinline__ void build_particle_packed(const Replica& R, int k, D
   cell_of(R, x, y, z, a, b, c);
   const int base0 = cstart[R.cell_off];
   // the stencil's cells in visiting order as runs of consecutive candidate
-  // records: cells adjacent in the cell arrays merge, empty ones drop out.
-  // Away from the y and z faces the nine cells of one x offset are
-  // consecutive (a-major numbering, z innermost), so the sweep is three runs.
+  // records: runs that meet in the record array merge, empty ones drop out.
+  // Away from the z faces the three z-cells of one (x, y) column are
+  // consecutive (a-major numbering, z innermost): nine runs, and with three
+  // z-cells (a quasi-2-D box) the three columns of one x offset meet as well.
   int rs[27], rn[27], nr = 0;
-  if (R.use_cell && R.cnx >= 3 && b >= 1 && b + 1 < R.cny && c >= 1 && c + 1 < R.cnz) {
+  if (R.use_cell && c >= 1 && c + 1 < R.cnz) {
     for (int ox = -1; ox <= 1; ox++) {
       int ia = a + ox;
       if (ia < 0) ia = R.cnx - 1; else if (ia == R.cnx) ia = 0;
-      const int f = R.cell_off + R.cny * R.cnz * ia + R.cnz * (b - 1) + (c - 1);
-      const int l = f + 2 * R.cnz + 2;
-      const int s0 = cstart[f], e = cstart[l] + ccnt[l];
-      if (e > s0) { rs[nr] = R.off + s0 - base0; rn[nr] = e - s0; nr++; }
+      for (int oy = -1; oy <= 1; oy++) {
+        int ib = b + oy;
+        if (ib < 0) ib = R.cny - 1; else if (ib == R.cny) ib = 0;
+        const int f = R.cell_off + R.cny * R.cnz * ia + R.cnz * ib + (c - 1);
+        const int s0 = R.off + cstart[f] - base0, n = cstart[f + 2] + ccnt[f + 2] - cstart[f];
+        if (n == 0) continue;
+        if (nr > 0 && rs[nr - 1] + rn[nr - 1] == s0) rn[nr - 1] += n;
+        else { rs[nr] = s0; rn[nr] = n; nr++; }
+      }
     }
   } else {
     int cells[27];
