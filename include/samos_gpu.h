@@ -249,13 +249,13 @@ int  sg_set_profiling(sg_system* s, int on);
  * without the specialisation.  All give the same results; the switch exists
  * so tests can compare them.  No reference counterpart.                     */
 int  sg_set_path(sg_system* s, int path);
-/* Kernel variant of the specialised active-Brownian step (0..27: per-particle
+/* Kernel variant of the specialised active-Brownian step (0..31: per-particle
  * neighbour sweeps that differ in how far ahead neighbour records are
- * fetched, resident blocks per SM, lane order, where the Gaussian draws are
- * taken and, for a one-replica system, whether the parameters are read from
- * kernel parameter space or a shared-memory copy; a flattened warp-wide
- * sweep; shared-memory staged and tiled sweeps); all variants compute the
- * same bits.  By default the engine's autotuner times every variant on the
+ * fetched, one or two neighbours per iteration, resident blocks per SM, lane
+ * order, where the Gaussian draws are taken and, for a one-replica system,
+ * whether the parameters are read from kernel parameter space or a
+ * shared-memory copy; a flattened warp-wide sweep; shared-memory staged and
+ * tiled sweeps); all variants compute the same bits.  By default the engine's autotuner times every variant on the
  * first steps of a run and keeps the fastest; sg_set_variant pins one
  * (-1 re-enables tuning), sg_get_variant reports the choice (-1 = not yet
  * tuned).  No reference counterpart.                                        */

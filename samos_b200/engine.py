@@ -402,7 +402,7 @@ class Engine:
         self._check(self.lib.sg_positions_changed(self.h))
 
     def set_variant(self, v: int) -> None:
-        """Pin a step-kernel variant (0..27) or re-enable autotuning (-1)."""
+        """Pin a step-kernel variant (0..31) or re-enable autotuning (-1)."""
         self._check(self.lib.sg_set_variant(self.h, int(v)))
 
     def set_generic_occupancy(self, blocks_per_sm: int) -> None:
