@@ -631,6 +631,13 @@ def main():
     host_out = {f: pinned_empty(n_part) for f in fields_out}
     for a in host_out.values():
         a[:] = 0.0
+    # one untimed pass of the same sequence first (the transfer path's first
+    # use maps the page-locked buffers; a caller's staging buffers are reused)
+    eng.upload_fields(host_in)
+    eng.build_nlist()
+    eng.run(e2e_steps - 1)
+    eng.download_fields(fields_out, out=host_out)
+    barrier(ws)
     t0 = time.perf_counter()
     eng.upload_fields(host_in)  # all fields' copies back to back, one wait
     t_up = time.perf_counter()
@@ -641,7 +648,7 @@ def main():
     t_end = time.perf_counter()
     e2e_s = max_over_ranks(t_end - t0, ws)
     e2e_split = dict(upload_ms=(t_up - t0) * 1e3, build_and_run_ms=(t_run - t_up) * 1e3,
-                     download_ms=(t_end - t_run) * 1e3)
+                     download_ms=(t_end - t_run) * 1e3, untimed_passes_before=1)
     h2d = len(fields_in) * 8 * n_part / e2e_steps
     d2h = len(fields_out) * 8 * n_part / e2e_steps
     e2e_value = ws * n_part * e2e_steps / e2e_s
