@@ -291,7 +291,9 @@ k_abp_step(const AbpParams* __restrict__ prm, const int* __restrict__ blk_rep, c
   __shared__ AbpParams S_sh;
   __shared__ uint64_t s_base;
   __shared__ int s_step;
-  const int r = blk_rep[blockIdx.x];
+  // by-value variants serve a one-replica system: its replica is 0, and a
+  // halted launch's blocks return after one load instead of two dependent ones
+  const int r = abp_byval(VAR) ? 0 : blk_rep[blockIdx.x];
   if (clk[r].halt) return;  // batched stepping: a rebuild is pending (same value for the whole block)
   {
     constexpr int NW = (int)(sizeof(AbpParams) / 8);
