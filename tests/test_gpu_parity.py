@@ -707,3 +707,27 @@ def test_unfused_batched_stepping_gives_the_stepwise_bits(integ):
     assert out[0][1].nlist_builds >= 1
     for f in ("x", "y", "vx", "vy", "nx", "ny", "omega", "fx", "fy", "age", "ix", "iy"):
         np.testing.assert_array_equal(out[0][0].download(f), out[1][0].download(f), err_msg=f)
+
+
+@pytest.mark.parametrize("align", ["polar", "nematic"])
+def test_run_energies_on_every_path(align):
+    # the energies a run reports come from its last step's force evaluation:
+    # on the specialised path that step runs the pipelined kernel, whose lanes
+    # are in neighbour-count order and whose block sums are taken in slot order,
+    # so they are the generic and packed paths' sums bit for bit; against the
+    # oracle (a sequential sum) within the per-step bar
+    parts, L = plane_disks(3000, 0.8, seed=51, bidisperse=(1.0, 1.4))
+    res = []
+    for backend, path in ((Engine, 0), (Engine, 1), (Engine, 2), (OracleSystem, None)):
+        b = backend(3000)
+        if path is not None:
+            b.set_path(path)
+        sim = drive(b, parts, (L, L, 10.0), nlist=(2.8, 0.3), pairs=[("soft", {"k": "10", "use_particle_radii": ""})],
+                    aligns=[(align, {"J": "0.5"})], dt=5e-4,
+                    integrators=[("brownian", {"v0": "0.3", "nu": "0.1", "seed": "4"})])
+        sim.run(40)
+        res.append((b.energy(0, 0), b.energy(1, 0)))
+    specialised, generic, packed, oracle = res
+    assert specialised == generic == packed
+    assert specialised[0] == pytest.approx(oracle[0], rel=REL)
+    assert specialised[1] == pytest.approx(oracle[1], rel=REL)
